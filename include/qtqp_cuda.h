@@ -1,0 +1,162 @@
+/* C-ABI of libqtqp_cuda.so: the B200 (sm_100a) interior-point hot path of QTQP.
+ *
+ * Conventions
+ *   - Every entry point returns 0 (QTQP_OK) or a negative QTQP_ERR_* code; the
+ *     message of the last failure on the calling thread is qtqp_last_error().
+ *   - Pointers named d_* are device pointers (allocated by the caller, e.g. by
+ *     PyTorch); h_* are host pointers.  No entry point allocates device memory
+ *     unless its comment says so: scratch comes from the caller's workspace.
+ *   - All kernels run on the caller's stream; entry points return without
+ *     synchronising unless documented otherwise.
+ *   - Arithmetic is FP64 except where an options field selects FP32 for the
+ *     KKT factorisation (FP64 iterative refinement recovers the accuracy).
+ *
+ * Reference: google-deepmind/qtqp v0.0.5 (pure Python).  Each function names
+ * the reference interface it replaces.
+ */
+#ifndef QTQP_CUDA_H_
+#define QTQP_CUDA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QTQP_OK 0
+#define QTQP_ERR_BAD_ARG (-1)
+#define QTQP_ERR_CUDA (-2)
+#define QTQP_ERR_NOT_SPD (-3)
+#define QTQP_ERR_TIMEOUT (-4)
+#define QTQP_ERR_NAN (-5)
+
+/* SolutionStatus codes (src/qtqp/__init__.py:129-137). */
+#define QTQP_STATUS_SOLVED 0
+#define QTQP_STATUS_INFEASIBLE 1
+#define QTQP_STATUS_UNBOUNDED 2
+#define QTQP_STATUS_HIT_MAX_ITER 3
+#define QTQP_STATUS_FAILED 4
+#define QTQP_STATUS_UNFINISHED 5
+
+/* Precision of the KKT factorisation. */
+#define QTQP_PREC_FP64 0  /* plain FP64 factor, FP64 refinement            */
+#define QTQP_PREC_MIXED 1 /* FP32 factor + FP64 refinement; an instance whose
+                             refinement stalls is refactorised in FP64 and
+                             stays FP64 from then on                          */
+
+/* Keyword arguments of QTQP.solve (src/qtqp/__init__.py:309-326). */
+typedef struct {
+  double atol, rtol, atol_infeas, rtol_infeas;
+  double step_size_scale;
+  double min_static_regularization;
+  double linear_solver_atol, linear_solver_rtol;
+  int32_t max_iter;
+  int32_t max_iterative_refinement_steps;
+  int32_t equilibrate;   /* 0 / 1 */
+  int32_t precision;     /* QTQP_PREC_* */
+  int32_t collect_stats; /* 1: write one qtqp_iter_stats record per iteration */
+  int32_t tau_mode;      /* 0: quadratic with linearised fallback; 1: always
+                            linearised (__init__.py:736-752)                 */
+} qtqp_options;
+
+/* One QP of a batch.  Offsets are element offsets into the caller's pools. */
+typedef struct {
+  int32_t n, m, z;  /* variables, constraints (after presolve), equalities */
+  int32_t has_p;    /* nnz(P) > 0 (the reference's p.nnz > 0 tests)       */
+  int64_t a_off;    /* A: m x n row-major FP64 in a_pool                   */
+  int64_t p_off;    /* P: n x n row-major FP64 (symmetric) in p_pool       */
+  int64_t n_off;    /* c in c_pool, x in x_pool: n doubles each            */
+  int64_t m_off;    /* b in b_pool, y / s in y_pool / s_pool: m doubles    */
+  int64_t ws_off;   /* byte offset of this instance's global workspace     */
+  int64_t st_off;   /* record offset in the stats pool (collect_stats)     */
+} qtqp_dense_instance;
+
+/* Per-instance outcome. */
+typedef struct {
+  int32_t status;           /* QTQP_STATUS_*                                  */
+  int32_t iterations;       /* IPM steps taken (len(Solution.stats))           */
+  int32_t error;            /* 0, QTQP_ERR_NOT_SPD or QTQP_ERR_NAN             */
+  int32_t fp32_factorizations;
+  int32_t fp64_factorizations;
+  int32_t ir_solves;        /* backend solves summed over all KKT solves       */
+  double tau;               /* final tau                                       */
+  double pcost, dcost, pres, dres, gap;
+} qtqp_result;
+
+/* Per-iteration record (the stats dict of __init__.py:967-1007 plus the three
+ * lin_sys_stats dicts of direct.py:300-307).  Field order is fixed; the host
+ * turns each record into the reference's dictionary. */
+#define QTQP_STATS_DOUBLES 64
+typedef struct {
+  double v[QTQP_STATS_DOUBLES];
+} qtqp_iter_stats;
+
+/* ---- library ------------------------------------------------------------ */
+const char* qtqp_last_error(void);
+int qtqp_version(void);
+/* Number of SMs of the current device (0 when no device is visible). */
+int qtqp_device_sm_count(void);
+
+/* ---- batched dense device-resident IPM ---------------------------------- *
+ * Replaces QTQP._solve_impl (src/qtqp/__init__.py:351-614) with its KKT layer
+ * (src/qtqp/direct.py:112-311) and the dense Gram/Cholesky backend
+ * (src/qtqp/solvers_dense.py:25-145), for a batch of independent QPs: one
+ * thread block runs one QP's whole solve (Ruiz, normalise, KKT factor, IR,
+ * predictor/corrector, ratio test, termination, unscaling).
+ *
+ * qtqp_dense_batch_plan: host-only.  Given the instances' (n, m) it fills
+ * inst[i].ws_off and returns the workspace size in bytes; `order` receives the
+ * processing order (descending cost).  block_threads / smem_bytes (0 = auto)
+ * select the launch shape; the chosen values are written back. */
+int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
+                          const qtqp_options* opt, int32_t* h_order,
+                          int32_t* block_threads, int32_t* smem_bytes,
+                          size_t* workspace_bytes);
+
+/* Device-resident solve of the whole batch in one persistent launch.
+ * d_inst / d_order: the planned descriptors and order, copied to the device by
+ * the caller.  b/c pools are inputs; x/y/s pools and d_results are outputs
+ * (x, y, s after the reference's status-dependent scaling,
+ * __init__.py:580-614; presolve row restoration is the host's job).
+ * d_stats: qtqp_iter_stats[max_iter] per instance, or NULL. */
+int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst,
+                           const int32_t* d_order, int32_t count,
+                           const double* d_a_pool, const double* d_p_pool,
+                           const double* d_b_pool, const double* d_c_pool,
+                           double* d_x_pool, double* d_y_pool,
+                           double* d_s_pool, qtqp_result* d_results,
+                           qtqp_iter_stats* d_stats, void* d_workspace,
+                           size_t workspace_bytes, const qtqp_options* opt,
+                           int32_t block_threads, int32_t smem_bytes,
+                           void* stream);
+
+/* ---- dense KKT backend (the direct.LinearSolver plugin) ------------------ *
+ * Replaces one backend of the plugin interface src/qtqp/direct.py:49-109
+ * (set_dims / set_kkt / update_diag / factorize / solve / __matmul__) with the
+ * Gram/Schur algorithm of src/qtqp/solvers_dense.py:99-142, on the device.
+ * Workspace layout is private; size it with qtqp_kkt_dense_workspace_bytes.
+ * All vectors are device FP64. */
+size_t qtqp_kkt_dense_workspace_bytes(int32_t n, int32_t m);
+/* set_kkt (solvers_dense.py:85-93): A is m x n row-major, P_off is n x n
+ * row-major with a zero diagonal.  Copied into the workspace. */
+int qtqp_kkt_dense_set(int32_t n, int32_t m, const double* d_a,
+                       const double* d_p_off, void* d_ws, void* stream);
+/* update_diag + factorize (solvers_dense.py:95-116): diag is the regularised
+ * KKT diagonal of length n+m with the dual block negative.  d_info (device
+ * int32) receives 0 or the 1-based failing pivot (LAPACK dpotrf convention). */
+int qtqp_kkt_dense_factorize(int32_t n, int32_t m, const double* d_diag,
+                             int32_t precision, void* d_ws, int32_t* d_info,
+                             void* stream);
+/* solve (solvers_dense.py:130-142): out = K_reg^{-1} rhs. */
+int qtqp_kkt_dense_solve(int32_t n, int32_t m, const double* d_rhs,
+                         double* d_out, void* d_ws, void* stream);
+/* __matmul__ (solvers_dense.py:118-128): out = K_reg x. */
+int qtqp_kkt_dense_matvec(int32_t n, int32_t m, const double* d_x,
+                          double* d_out, void* d_ws, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QTQP_CUDA_H_ */

@@ -1,0 +1,312 @@
+"""qtqp_b200: the QTQP interior-point hot path, native to NVIDIA B200 (sm_100a).
+
+Drop-in for the reference solver's public API (google-deepmind/qtqp v0.0.5,
+src/qtqp/__init__.py):
+
+    sol = qtqp_b200.QTQP(a=a, b=b, c=c, z=z, p=p).solve(
+        linear_solver=qtqp_b200.LinearSolver.CUDA)
+
+``LinearSolver.CUDA`` runs the whole interior-point method on the GPU (one
+thread block per QP, hand-written CUDA kernels behind a C-ABI); only
+validation, presolve/postsolve and result formatting stay on the host.
+``solve_batch`` solves many independent QPs in one persistent launch.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import enum
+import sys
+import timeit
+from typing import Any, Dict, List, Sequence
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from . import batch as _batch
+from . import direct
+
+__version__ = "0.0.5+b200"
+
+_HEADER = ("| iter |      pcost |      dcost |     pres |     dres |      gap |"
+           "   infeas |       mu |  q, p, c |     time |")
+_SEPARA = ("|------|------------|------------|----------|----------|----------|"
+           "----------|----------|----------|----------|")
+
+
+class LinearSolver(enum.Enum):
+  """KKT backends (src/qtqp/__init__.py:54-68).
+
+  AUTO resolves to CUDA.  CUDA runs the device-resident loop whose KKT layer is
+  the CudaDenseSolver algorithm; the class is also usable on its own as a
+  plugin for the reference's DirectKktSolver.
+  """
+
+  AUTO = "auto"
+  CUDA = direct.CudaDenseSolver
+
+
+class SolutionStatus(enum.Enum):
+  """Possible statuses of the QP solution (src/qtqp/__init__.py:129-137)."""
+
+  SOLVED = "solved"
+  INFEASIBLE = "infeasible"
+  UNBOUNDED = "unbounded"
+  HIT_MAX_ITER = "hit_max_iter"
+  FAILED = "failed"
+  UNFINISHED = "unfinished"
+
+
+_STATUS_FROM_CODE = {
+    0: SolutionStatus.SOLVED,
+    1: SolutionStatus.INFEASIBLE,
+    2: SolutionStatus.UNBOUNDED,
+    3: SolutionStatus.HIT_MAX_ITER,
+    4: SolutionStatus.FAILED,
+    5: SolutionStatus.UNFINISHED,
+}
+_LIN_STATUS = {0: "non-converged", 1: "converged", 2: "stalled"}
+_TAU_METHOD = {0: "quadratic", 1: "linearized"}
+_FOOTER = {
+    SolutionStatus.SOLVED: "Solved",
+    SolutionStatus.INFEASIBLE: "Primal infeasible / dual unbounded",
+    SolutionStatus.UNBOUNDED: "Dual infeasible / primal unbounded",
+    SolutionStatus.HIT_MAX_ITER: "Hit maximum iterations",
+    SolutionStatus.FAILED: "Failed to converge",
+}
+
+
+@dataclasses.dataclass(frozen=True)
+class Solution:
+  """Solution of a QP (src/qtqp/__init__.py:140-156).
+
+  x, y, s: primal/dual/slack solution or infeasibility certificate; stats:
+  per-iteration dicts (collect_stats=True); status: SolutionStatus.
+  """
+
+  x: np.ndarray
+  y: np.ndarray
+  s: np.ndarray
+  stats: List[Dict[str, Any]]
+  status: SolutionStatus
+
+
+@dataclasses.dataclass(frozen=True)
+class _PresolveState:
+  keep: np.ndarray
+  a_dropped: sp.csc_matrix
+  b_dropped: np.ndarray
+
+
+class QTQP:
+  """Primal-dual interior point method for QPs (src/qtqp/__init__.py:168-307).
+
+    min (1/2) x'Px + c'x  s.t.  Ax + s = b,  s[:z] == 0,  s[z:] >= 0.
+  """
+
+  def __init__(self, *, a: sp.csc_matrix, b: np.ndarray, c: np.ndarray, z: int,
+               p: sp.csc_matrix | None = None):
+    self.m, self.n = a.shape
+    self.z = z
+    if not sp.isspmatrix_csc(a):
+      raise TypeError("Constraint matrix 'a' must be in CSC format.")
+    self.a = a
+    self.b = np.array(b, dtype=np.float64)
+    if self.b.shape != (self.m,):
+      raise ValueError(f"b must have shape ({self.m},), got {self.b.shape}")
+    self.c = np.array(c, dtype=np.float64)
+    if self.c.shape != (self.n,):
+      raise ValueError(f"c must have shape ({self.n},), got {self.c.shape}")
+    if self.z < 0 or self.z > self.m:
+      raise ValueError(f"Number of equality constraints z={self.z} must satisfy "
+                       f"0 <= z <= m={self.m}")
+    self._presolve()
+    if self.z == self.m:
+      raise ValueError("effective z == m after presolve; some rows may have been dropped")
+    if p is None:
+      self.p = sp.csc_matrix((self.n, self.n))
+    else:
+      if not sp.isspmatrix_csc(p):
+        raise TypeError("QP matrix 'p' must be in CSC format.")
+      if p.shape != (self.n, self.n):
+        raise ValueError(f"p must have shape ({self.n}, {self.n}), got {p.shape}")
+      if not np.all(np.isfinite(p.data)):
+        raise ValueError("QP matrix 'p' must contain only finite values.")
+      asym = p - p.T
+      if asym.nnz and np.max(np.abs(asym.data), initial=0.0) > 1e-12:
+        raise ValueError("QP matrix 'p' must be symmetric.")
+      self.p = p
+
+  def _presolve(self, inf_bound: float = 1e20):
+    """Drops inequality rows with b >= inf_bound (__init__.py:248-270)."""
+    self._presolve_state = None
+    if not np.all(np.isfinite(self.b[:self.z])):
+      raise ValueError("Equality RHS entries in 'b' must be finite.")
+    ineq_b = self.b[self.z:]
+    if np.any(np.isnan(ineq_b) | np.isneginf(ineq_b)):
+      raise ValueError("Inequality RHS entries in 'b' must be finite, +inf, or >= inf_bound.")
+    drop = np.zeros(self.m, dtype=bool)
+    drop[self.z:] = ineq_b >= inf_bound
+    if not np.any(drop):
+      return
+    keep = ~drop
+    self._presolve_state = _PresolveState(keep=keep, a_dropped=self.a[drop],
+                                          b_dropped=self.b[drop])
+    self.a = self.a[keep]
+    self.b = self.b[keep]
+    self.m = int(keep.sum())
+
+  def _postsolve(self, y, s, y_dropped=0.0, s_dropped=np.nan):
+    """Restores the dropped rows (__init__.py:272-290)."""
+    if self._presolve_state is None:
+      return y, s
+    ps = self._presolve_state
+    m_full = ps.keep.shape[0]
+    y_full = np.empty(m_full)
+    s_full = np.empty(m_full)
+    y_full[ps.keep], y_full[~ps.keep] = y, y_dropped
+    s_full[ps.keep], s_full[~ps.keep] = s, s_dropped
+    return y_full, s_full
+
+  def _dropped_slack(self, x):
+    ps = self._presolve_state
+    return 0.0 if ps is None else ps.b_dropped - ps.a_dropped @ x
+
+  def dense_problem(self) -> _batch.DenseProblem:
+    """The presolved QP in the dense form the device solver consumes."""
+    p = self.p.toarray() if self.p.nnz else None
+    return _batch.DenseProblem(a=self.a.toarray(), b=self.b, c=self.c, z=self.z, p=p)
+
+  def solve(self, *, atol: float = 1e-7, rtol: float = 1e-8, atol_infeas: float = 1e-8,
+            rtol_infeas: float = 1e-9, max_iter: int = 100, step_size_scale: float = 0.99,
+            min_static_regularization: float = 1e-8,
+            max_iterative_refinement_steps: int = 20, linear_solver_atol: float = 1e-12,
+            linear_solver_rtol: float = 1e-12,
+            linear_solver: LinearSolver = LinearSolver.AUTO, verbose: bool = True,
+            equilibrate: bool = True, collect_stats: bool = False,
+            precision: str = "fp64") -> Solution:
+    """Solves the QP on the GPU (same keyword arguments as the reference,
+    __init__.py:309-326, plus ``precision``: 'fp64' or 'mixed')."""
+    opts = _batch.SolveOptions(
+        atol=atol, rtol=rtol, atol_infeas=atol_infeas, rtol_infeas=rtol_infeas,
+        max_iter=max_iter, step_size_scale=step_size_scale,
+        min_static_regularization=min_static_regularization,
+        max_iterative_refinement_steps=max_iterative_refinement_steps,
+        linear_solver_atol=linear_solver_atol, linear_solver_rtol=linear_solver_rtol,
+        equilibrate=equilibrate, collect_stats=collect_stats, precision=precision)
+    opts.validate()
+    if linear_solver not in (LinearSolver.AUTO, LinearSolver.CUDA):
+      raise ValueError(f"unsupported linear_solver {linear_solver}")
+    _lib.require_device()
+    start = timeit.default_timer()
+    if verbose:
+      print(f"| QTQP v{__version__}: m={self.m}, n={self.n}, z={self.z}, "
+            f"nnz(A)={self.a.nnz}, nnz(P)={self.p.nnz}, linear_solver=CUDA")
+    out = solve_batch([self], _opts=opts, _verbose=verbose, _start=start)[0]
+    return out
+
+
+def _record_to_dict(rec: np.ndarray, collect: bool, t_offset: float) -> Dict[str, Any]:
+  """One device stats record -> the reference's per-iteration dict
+  (__init__.py:967-1007, direct.py:300-307)."""
+  keys = ["iter", "ctx", "bty", "pcost", "dcost", "pres", "dres", "gap", "pinfeas",
+          "dinfeas", "dinfeas_a", "dinfeas_p", "mu", "sigma", "alpha", "tau", "norm_x",
+          "norm_y", "status", "time", "prelrhs", "drelrhs"]
+  d: Dict[str, Any] = {}
+  for name, blk in (("q_lin_sys_stats", 0), ("predictor_lin_sys_stats", 1),
+                    ("corrector_lin_sys_stats", 2)):
+    base = 31 + blk * 7
+    lin = {"solves": int(rec[base]), "final_residual_norm": float(rec[base + 1]),
+           "rhs_norm": float(rec[base + 2]), "tolerance": float(rec[base + 3]),
+           "converged": int(rec[base + 4]) == 1, "status": _LIN_STATUS[int(rec[base + 4])],
+           "factor_bits": int(rec[base + 6])}
+    if int(rec[base + 5]) >= 0:
+      lin["tau_method"] = _TAU_METHOD[int(rec[base + 5])]
+    d[name] = lin
+  for i, k in enumerate(keys):
+    d[k] = float(rec[i])
+  d["iter"] = int(rec[0])
+  d["status"] = _STATUS_FROM_CODE[int(rec[18])]
+  d["time"] = float(rec[19]) + t_offset
+  if collect:
+    for i, k in enumerate(["complementarity", "norm_s", "max_sy", "min_sy", "std_sy",
+                           "max_s_over_y", "min_s_over_y", "mean_s_over_y",
+                           "std_s_over_y"]):
+      d[k] = float(rec[22 + i])
+  return d
+
+
+def _log_iteration(st: Dict[str, Any]) -> None:
+  """The reference's iteration line (__init__.py:1014-1035)."""
+  infeas = min(st["pinfeas"], st["dinfeas"])
+
+  def ls(d):
+    return " *" if d.get("status") == "stalled" else f"{d.get('solves', 0):2}"
+
+  solves = (f"{ls(st['q_lin_sys_stats'])},{ls(st['predictor_lin_sys_stats'])},"
+            f"{ls(st['corrector_lin_sys_stats'])}")
+  print(f"| {st['iter']:>4} | {st['pcost']:>10.3e} | {st['dcost']:>10.3e} |"
+        f" {st['pres']:>8.2e} | {st['dres']:>8.2e} | {st['gap']:>8.2e} |"
+        f" {infeas:>8.2e} | {st['mu']:>8.2e} | {solves:>8} | {st['time']:>8.2e} |")
+
+
+def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", _opts=None,
+                _verbose: bool = False, _start: float | None = None,
+                **solve_kwargs) -> List[Solution]:
+  """Solves independent QPs in one persistent GPU launch.
+
+  Accepts the keyword arguments of QTQP.solve (verbose defaults to False).
+  Returns one Solution per problem, in order.
+  """
+  start = timeit.default_timer() if _start is None else _start
+  if _opts is None:
+    verbose = solve_kwargs.pop("verbose", False)
+    solve_kwargs.pop("linear_solver", None)
+    opts = _batch.SolveOptions(precision=precision, **solve_kwargs)
+    opts.validate()
+  else:
+    opts, verbose = _opts, _verbose
+  _lib.require_device()
+  hb = _batch.HostBatch([q.dense_problem() for q in problems], opts)
+  db = _batch.DeviceBatch(hb, records=bool(verbose or opts.collect_stats))
+  db.upload()
+  t_launch = timeit.default_timer() - start
+  db.launch()
+  res, x_pool, y_pool, s_pool, stats = db.fetch()
+  out = []
+  for i, q in enumerate(problems):
+    r = res[i]
+    d = hb.inst[i]
+    if int(r["error"]) == _lib.QTQP_ERR_NOT_SPD:
+      raise np.linalg.LinAlgError("Cholesky failed: the KKT Gram matrix is not positive definite")
+    if int(r["error"]) == _lib.QTQP_ERR_NAN:
+      raise ValueError("Linear solver returned NaNs.")
+    n0, m0 = int(d["n_off"]), int(d["m_off"])
+    x = x_pool[n0:n0 + q.n].copy()
+    y = y_pool[m0:m0 + q.m].copy()
+    s = s_pool[m0:m0 + q.m].copy()
+    status = _STATUS_FROM_CODE[int(r["status"])]
+    if status == SolutionStatus.INFEASIBLE:
+      y, s = q._postsolve(y, s)
+    elif status == SolutionStatus.UNBOUNDED:
+      y, s = q._postsolve(y, s, y_dropped=np.nan)
+    else:
+      y, s = q._postsolve(y, s, s_dropped=q._dropped_slack(x))
+    st_list: List[Dict[str, Any]] = []
+    iters = int(r["iterations"])
+    if stats is not None or verbose:
+      recs = stats[i] if stats is not None else None
+      if recs is not None:
+        st_list = [_record_to_dict(recs[k], opts.collect_stats, t_launch) for k in range(iters)]
+    if verbose:
+      print(f"{_SEPARA}\n{_HEADER}\n{_SEPARA}")
+      for st in st_list:
+        _log_iteration(st)
+      print(f"{_SEPARA}\n| {_FOOTER.get(status, 'Failed to converge')}")
+    out.append(Solution(x, y, s, st_list if opts.collect_stats else [], status))
+  return out
+
+
+__all__ = ["QTQP", "Solution", "SolutionStatus", "LinearSolver", "solve_batch", "direct",
+           "__version__"]

@@ -1,0 +1,166 @@
+"""ctypes binding of libqtqp_cuda.so (declarations in include/qtqp_cuda.h).
+
+Loading fails loudly: a missing library raises OSError and a machine without a
+CUDA device raises ImportError when a backend is instantiated.  There is no
+CPU fallback anywhere in this package.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqtqp_cuda.so")
+
+QTQP_OK = 0
+QTQP_ERR_BAD_ARG = -1
+QTQP_ERR_CUDA = -2
+QTQP_ERR_NOT_SPD = -3
+QTQP_ERR_TIMEOUT = -4
+QTQP_ERR_NAN = -5
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+STATS_DOUBLES = 64
+
+# Exported symbols; tests check that the library provides every one of them.
+EXPORTS = (
+    "qtqp_last_error",
+    "qtqp_version",
+    "qtqp_device_sm_count",
+    "qtqp_dense_batch_plan",
+    "qtqp_dense_batch_solve",
+    "qtqp_kkt_dense_workspace_bytes",
+    "qtqp_kkt_dense_set",
+    "qtqp_kkt_dense_factorize",
+    "qtqp_kkt_dense_solve",
+    "qtqp_kkt_dense_matvec",
+)
+
+
+class Options(ctypes.Structure):
+  _fields_ = [
+      ("atol", ctypes.c_double),
+      ("rtol", ctypes.c_double),
+      ("atol_infeas", ctypes.c_double),
+      ("rtol_infeas", ctypes.c_double),
+      ("step_size_scale", ctypes.c_double),
+      ("min_static_regularization", ctypes.c_double),
+      ("linear_solver_atol", ctypes.c_double),
+      ("linear_solver_rtol", ctypes.c_double),
+      ("max_iter", ctypes.c_int32),
+      ("max_iterative_refinement_steps", ctypes.c_int32),
+      ("equilibrate", ctypes.c_int32),
+      ("precision", ctypes.c_int32),
+      ("collect_stats", ctypes.c_int32),
+      ("tau_mode", ctypes.c_int32),
+  ]
+
+
+class DenseInstance(ctypes.Structure):
+  _fields_ = [
+      ("n", ctypes.c_int32),
+      ("m", ctypes.c_int32),
+      ("z", ctypes.c_int32),
+      ("has_p", ctypes.c_int32),
+      ("a_off", ctypes.c_int64),
+      ("p_off", ctypes.c_int64),
+      ("n_off", ctypes.c_int64),
+      ("m_off", ctypes.c_int64),
+      ("ws_off", ctypes.c_int64),
+      ("st_off", ctypes.c_int64),
+  ]
+
+
+class Result(ctypes.Structure):
+  _fields_ = [
+      ("status", ctypes.c_int32),
+      ("iterations", ctypes.c_int32),
+      ("error", ctypes.c_int32),
+      ("fp32_factorizations", ctypes.c_int32),
+      ("fp64_factorizations", ctypes.c_int32),
+      ("ir_solves", ctypes.c_int32),
+      ("tau", ctypes.c_double),
+      ("pcost", ctypes.c_double),
+      ("dcost", ctypes.c_double),
+      ("pres", ctypes.c_double),
+      ("dres", ctypes.c_double),
+      ("gap", ctypes.c_double),
+  ]
+
+
+# numpy views of the same layouts (for bulk packing / unpacking).
+INSTANCE_DTYPE = np.dtype([(name, np.int32 if ct is ctypes.c_int32 else np.int64)
+                           for name, ct in DenseInstance._fields_])
+RESULT_DTYPE = np.dtype([(name, np.int32 if ct is ctypes.c_int32 else np.float64)
+                         for name, ct in Result._fields_])
+assert INSTANCE_DTYPE.itemsize == ctypes.sizeof(DenseInstance)
+assert RESULT_DTYPE.itemsize == ctypes.sizeof(Result)
+
+_lock = threading.Lock()
+_lib = None
+
+
+class QtqpCudaError(RuntimeError):
+  """A C-ABI call returned an error code."""
+
+  def __init__(self, code: int, msg: str):
+    super().__init__(f"libqtqp_cuda error {code}: {msg}")
+    self.code = code
+
+
+def load() -> ctypes.CDLL:
+  """Loads the library (building nothing); raises OSError when it is absent."""
+  global _lib
+  with _lock:
+    if _lib is not None:
+      return _lib
+    if not os.path.exists(LIB_PATH):
+      raise OSError(
+          f"{LIB_PATH} is missing: build it with `python -m qtqp_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_size_t
+    lib.qtqp_last_error.restype = ctypes.c_char_p
+    lib.qtqp_version.restype = ctypes.c_int
+    lib.qtqp_device_sm_count.restype = ctypes.c_int
+    lib.qtqp_dense_batch_plan.argtypes = [vp, i32, ctypes.POINTER(Options), vp,
+                                          ctypes.POINTER(i32), ctypes.POINTER(i32),
+                                          ctypes.POINTER(sz)]
+    lib.qtqp_dense_batch_solve.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp,
+                                           vp, vp, sz, ctypes.POINTER(Options), i32, i32,
+                                           vp]
+    lib.qtqp_kkt_dense_workspace_bytes.restype = sz
+    lib.qtqp_kkt_dense_workspace_bytes.argtypes = [i32, i32]
+    lib.qtqp_kkt_dense_set.argtypes = [i32, i32, vp, vp, vp, vp]
+    lib.qtqp_kkt_dense_factorize.argtypes = [i32, i32, vp, i32, vp, vp, vp]
+    lib.qtqp_kkt_dense_solve.argtypes = [i32, i32, vp, vp, vp, vp]
+    lib.qtqp_kkt_dense_matvec.argtypes = [i32, i32, vp, vp, vp, vp]
+    for name in EXPORTS:  # every declared entry point must resolve
+      getattr(lib, name)
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+  if rc != QTQP_OK:
+    msg = load().qtqp_last_error()
+    raise QtqpCudaError(rc, msg.decode() if msg else "")
+
+
+def require_device():
+  """Returns torch with a visible CUDA device, else raises ImportError."""
+  import torch  # pylint: disable=g-import-not-at-top
+  if not torch.cuda.is_available():
+    raise ImportError("qtqp_b200: no CUDA device is visible (the CUDA backend "
+                      "has no CPU fallback)")
+  load()
+  return torch
+
+
+def stream_handle(torch_stream) -> int:
+  return int(torch_stream.cuda_stream)

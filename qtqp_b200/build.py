@@ -1,0 +1,72 @@
+"""Builds libqtqp_cuda.so in-tree with nvcc for sm_100a (B200).
+
+Usage: python -m qtqp_b200.build [--debug]
+
+The library is a plain C-ABI shared object (include/qtqp_cuda.h); it does not
+link against PyTorch.  The build is incremental on source mtimes.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ROOT = os.path.dirname(_HERE)
+_CSRC = os.path.join(_HERE, "csrc")
+_INC = os.path.join(_ROOT, "include")
+LIB_PATH = os.path.join(_HERE, "libqtqp_cuda.so")
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+  cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+  if not os.path.exists(cand):
+    raise RuntimeError("nvcc not found; the CUDA toolkit is required to build")
+  return cand
+
+
+def sources() -> list[str]:
+  return sorted(os.path.join(_CSRC, f) for f in os.listdir(_CSRC) if f.endswith(".cu"))
+
+
+def _deps() -> list[str]:
+  files = sources()
+  files += [os.path.join(_CSRC, f) for f in os.listdir(_CSRC) if f.endswith((".cuh", ".h"))]
+  files += [os.path.join(_INC, f) for f in os.listdir(_INC) if f.endswith(".h")]
+  return files
+
+
+def up_to_date() -> bool:
+  if not os.path.exists(LIB_PATH):
+    return False
+  t = os.path.getmtime(LIB_PATH)
+  return all(os.path.getmtime(f) <= t for f in _deps())
+
+
+def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
+  """Compiles every .cu under csrc/ into libqtqp_cuda.so; returns its path."""
+  if not force and not debug and up_to_date():
+    return LIB_PATH
+  cmd = [_nvcc(), *ARCH_FLAGS, "-lineinfo", "-std=c++17", "-shared",
+         "-Xcompiler", "-fPIC", "-I", _INC, "-I", _CSRC,
+         "--expt-relaxed-constexpr", "-o", LIB_PATH + ".tmp"]
+  cmd += ["-O0", "-G"] if debug else ["-O3"]
+  if verbose:
+    cmd += ["-Xptxas", "-v"]
+  cmd += sources()
+  proc = subprocess.run(cmd, capture_output=True, text=True)
+  if proc.returncode != 0:
+    raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stderr}\n{proc.stdout}")
+  if verbose:
+    sys.stderr.write(proc.stderr)
+  os.replace(LIB_PATH + ".tmp", LIB_PATH)
+  return LIB_PATH
+
+
+if __name__ == "__main__":
+  build(force=True, debug="--debug" in sys.argv, verbose="-v" in sys.argv)
+  print(LIB_PATH)

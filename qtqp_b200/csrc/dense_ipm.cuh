@@ -1,0 +1,1142 @@
+// Device-resident interior-point solve of one dense QP by one thread block.
+//
+// Algorithm: the homogeneous-embedding Mehrotra predictor-corrector of
+// google-deepmind/qtqp v0.0.5, src/qtqp/__init__.py:351-614, with the KKT layer
+// of src/qtqp/direct.py:112-311 and the Gram/Cholesky backend of
+// src/qtqp/solvers_dense.py:25-145.  Every scalar decision (IR convergence and
+// stall, tau root selection and fallback, ratio test, termination precedence)
+// follows the reference; only the summation order of reductions differs.
+//
+// Work distribution inside the block ("ownership"): every per-element vector
+// lives in the N-space [0, n+m) with the x-part at [0, n) and the y/s-part at
+// [n, n+m); element k is always handled by thread k % NT.  Elementwise phases
+// therefore need no barrier between them; a barrier is only needed before a
+// phase that reads other threads' elements (matrix-vector products, the
+// triangular solves) and is folded into the block reductions where possible.
+#pragma once
+
+#include <math.h>
+
+#include "common.cuh"
+
+namespace qtqp {
+
+// ----------------------------------------------------------------------------
+// Per-instance memory layout (shared by host planning and device code).
+// ----------------------------------------------------------------------------
+enum VecId : int {
+  kQ = 0,    // q = [c_eq; b_eq]
+  kXY,       // iterate [x; y]
+  kKQ,       // K^{-1} q (warm-started across iterations)
+  kKQ0,      // warm start of K^{-1} q kept for an FP64 redo (mixed precision)
+  kXYP,      // predictor K^{-1} r, then [x_p; y_p]
+  kXYC,      // corrector K^{-1} r, then [x_c; y_c]
+  kRHS,      // KKT right-hand side with the dual block negated
+  kRES,      // IR residual
+  kTMP,      // solve scratch (FP64 Gram right-hand side / solution)
+  kREG,      // regularised KKT diagonal (dual block negative)
+  kCORR,     // reg - true diagonal
+  kDE,       // [e; d] accumulated Ruiz scalings
+  kPI,       // [diag(P_eq); 1/Ry]
+  kPW,       // [P_eq K^{-1}q_x; 1/sqrt(Ry)]
+  kRS,       // [P_eq K^{-1}r_x; s]
+  kXD,       // [P_eq x; d_s]
+  kCT,       // [FP32 scratch (n floats); Mehrotra correction]
+  kNumVec
+};
+
+__host__ __device__ inline int odd_ld(int n) { return (n & 1) ? n : n + 1; }
+__host__ __device__ inline size_t round16(size_t b) { return (b + 15) & ~size_t(15); }
+
+struct InstLayout {
+  int lda, ldp, ldg, np;  // leading dims (doubles) and padded vector length
+  size_t a_bytes, p_bytes, g_bytes, v_bytes;
+  int ap_smem, gv_smem;   // 1 when that region lives in shared memory
+  size_t smem_bytes, global_bytes;
+};
+
+// Places G + vectors (and A + P when they also fit) in `smem_cap` bytes of
+// shared memory; everything else goes to the instance's global workspace.
+__host__ __device__ inline InstLayout plan_layout(int n, int m, size_t smem_cap) {
+  InstLayout L;
+  L.lda = odd_ld(n);
+  L.ldp = odd_ld(n);
+  L.ldg = odd_ld(n);
+  L.np = (n + m + 1) & ~1;
+  L.a_bytes = round16(size_t(m) * L.lda * 8);
+  L.p_bytes = round16(size_t(n) * L.ldp * 8);
+  L.g_bytes = round16(size_t(n) * L.ldg * 8);
+  L.v_bytes = round16(size_t(kNumVec) * L.np * 8);
+  const size_t gv = L.g_bytes + L.v_bytes, ap = L.a_bytes + L.p_bytes;
+  L.gv_smem = gv <= smem_cap;
+  L.ap_smem = L.gv_smem && (gv + ap <= smem_cap);
+  L.smem_bytes = (L.gv_smem ? gv : 0) + (L.ap_smem ? ap : 0);
+  L.global_bytes = (L.gv_smem ? 0 : gv) + (L.ap_smem ? 0 : ap);
+  return L;
+}
+
+// Fields of one qtqp_iter_stats record.
+enum StatField : int {
+  kStIter = 0, kStCtx, kStBty, kStPcost, kStDcost, kStPres, kStDres, kStGap,
+  kStPinfeas, kStDinfeas, kStDinfeasA, kStDinfeasP, kStMu, kStSigma,
+  kStAlpha, kStTau, kStNormX, kStNormY, kStStatus, kStTime, kStPrel, kStDrel,
+  kStCompl, kStNormS, kStMaxSy, kStMinSy, kStStdSy, kStMaxSoy, kStMinSoy,
+  kStMeanSoy, kStStdSoy,
+  kStLin0 = 31,  // three blocks of kLinFields: q, predictor, corrector
+};
+enum LinField : int {
+  kLinSolves = 0, kLinFinalRes, kLinRhsNorm, kLinTol, kLinStatus, kLinTau,
+  kLinPrec, kLinFields
+};
+// kLinStatus: 0 non-converged, 1 converged, 2 stalled.  kLinTau: -1 none,
+// 0 quadratic, 1 linearised.  kLinPrec: 32 or 64 (factor precision used).
+
+struct IrOutcome {
+  int solves;
+  int status;  // 0 non-converged, 1 converged, 2 stalled
+  double final_res, rhs_norm, tol;
+  bool nan;
+};
+
+// ----------------------------------------------------------------------------
+// The solver state of one instance, replicated in every thread of the block.
+// ----------------------------------------------------------------------------
+template <int NT>
+struct DenseIpm {
+  int tid;
+  int n, m, z, N;
+  bool has_p;
+  // Original (presolved, unequilibrated) data in global memory.
+  const double* A0;
+  const double* P0;
+  const double* b0;
+  const double* c0;
+  // Working data.
+  double* A;  // m x lda equilibrated A
+  double* P;  // n x ldp equilibrated P with a zero diagonal (P_off)
+  double* G;  // n x ldg Gram matrix / Cholesky factor (FP64, or FP32 alias)
+  double* V;  // kNumVec vectors of np doubles
+  int lda, ldp, ldg, np;
+  double* red;
+  int phase;
+  // Options.
+  const qtqp_options* o;
+
+  __device__ __forceinline__ double* vec(int id) const { return V + size_t(id) * np; }
+  // First index >= lo owned by this thread (k % NT == tid).
+  __device__ __forceinline__ int own(int lo) const { return lo + ((tid - lo) & (NT - 1)); }
+  __device__ __forceinline__ float* g32() const { return reinterpret_cast<float*>(G); }
+  __device__ __forceinline__ float* t32() const { return reinterpret_cast<float*>(vec(kCT)); }
+
+  // --------------------------------------------------------------------------
+  // Binding of memory regions.
+  // --------------------------------------------------------------------------
+  __device__ void bind(int n_, int m_, char* smem, char* gmem, size_t smem_cap) {
+    tid = threadIdx.x;
+    n = n_;
+    m = m_;
+    N = n + m;
+    const InstLayout L = plan_layout(n, m, smem_cap);
+    lda = L.lda;
+    ldp = L.ldp;
+    ldg = L.ldg;
+    np = L.np;
+    char* gv = L.gv_smem ? smem : gmem;
+    G = reinterpret_cast<double*>(gv);
+    V = reinterpret_cast<double*>(gv + L.g_bytes);
+    char* ap = L.ap_smem ? smem + L.g_bytes + L.v_bytes
+                         : gmem + (L.gv_smem ? 0 : L.g_bytes + L.v_bytes);
+    A = reinterpret_cast<double*>(ap);
+    P = reinterpret_cast<double*>(ap + L.a_bytes);
+  }
+
+  // --------------------------------------------------------------------------
+  // Ruiz equilibration (src/qtqp/__init__.py:616-663), done in place on the
+  // working copies, bit-compatible with the reference: the nonzero a_ij is
+  // multiplied by (d_i * e_j), the clip bounds are [1e-3, 1e3].
+  // --------------------------------------------------------------------------
+  __device__ void load_and_equilibrate(bool equilibrate, double& nb, double& nc) {
+    double* de = vec(kDE);
+    double* sc = vec(kTMP);  // per-sweep [e_i; d_i]
+    for (int idx = tid; idx < m * n; idx += NT) {
+      const int i = idx / n, j = idx - i * n;
+      A[i * lda + j] = A0[idx];
+    }
+    for (int idx = tid; idx < n * n; idx += NT) {
+      const int i = idx / n, j = idx - i * n;
+      P[i * ldp + j] = has_p ? P0[idx] : 0.0;
+    }
+    for (int k = tid; k < N; k += NT) de[k] = 1.0;
+    group_sync<NT>();
+    if (equilibrate) {
+      for (int sweep = 0; sweep < 10; ++sweep) {
+        for (int k = tid; k < N; k += NT) {
+          double mx = 0.0;
+          if (k < n) {  // column k: max over A's column and P's column
+            for (int i = 0; i < m; ++i) mx = fmax(mx, fabs(A[i * lda + k]));
+            if (has_p)
+              for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(P[i * ldp + k]));
+          } else {  // row k - n of A
+            const double* row = A + (k - n) * lda;
+            for (int j = 0; j < n; ++j) mx = fmax(mx, fabs(row[j]));
+          }
+          if (mx == 0.0) mx = 1.0;
+          sc[k] = fmin(fmax(1.0 / sqrt(mx), 1e-3), 1e3);
+        }
+        group_sync<NT>();
+        for (int idx = tid; idx < m * n; idx += NT) {
+          const int i = idx / n, j = idx - i * n;
+          A[i * lda + j] *= sc[n + i] * sc[j];
+        }
+        if (has_p) {
+          for (int idx = tid; idx < n * n; idx += NT) {
+            const int i = idx / n, j = idx - i * n;
+            P[i * ldp + j] *= sc[i] * sc[j];
+          }
+        }
+        for (int k = tid; k < N; k += NT) de[k] *= sc[k];
+        group_sync<NT>();
+      }
+    }
+    double* q = vec(kQ);
+    double* pi = vec(kPI);
+    double mx[2] = {0.0, 0.0};
+    double dummy[1] = {0.0};
+    for (int k = tid; k < N; k += NT) {
+      if (k < n) {
+        q[k] = c0[k] * de[k];
+        pi[k] = P[k * ldp + k];  // diag(P_eq); P keeps only its off-diagonal
+        P[k * ldp + k] = 0.0;
+        mx[1] = nanmax(mx[1], fabs(c0[k]));
+      } else {
+        q[k] = b0[k - n] * de[k];
+        mx[0] = nanmax(mx[0], fabs(b0[k - n]));
+      }
+    }
+    block_reduce<NT, 0, 2>(dummy, mx, red, phase);
+    nb = mx[0];
+    nc = mx[1];
+    group_sync<NT>();
+  }
+
+  // --------------------------------------------------------------------------
+  // DirectKktSolver.update (direct.py:183-216): true and regularised diagonal,
+  // the backend's update_diag (solvers_dense.py:95-97) and the derived
+  // 1/Ry and 1/sqrt(Ry) used by factorize/solve (solvers_dense.py:103, 132).
+  // Owner-wise; the caller synchronises before factorising.
+  // --------------------------------------------------------------------------
+  __device__ void kkt_diag(double mu, double min_reg) {
+    const double* xy = vec(kXY);
+    const double* s = vec(kRS);
+    const double* pi = vec(kPI);
+    double* reg = vec(kREG);
+    double* corr = vec(kCORR);
+    double* piw = vec(kPI);
+    double* pw = vec(kPW);
+    for (int k = tid; k < N; k += NT) {
+      double t;
+      if (k < n) {
+        t = pi[k];
+        t += mu;
+      } else if (k < n + z) {
+        t = mu;
+      } else {
+        t = s[k] / xy[k] + mu;
+      }
+      double r = fmax(t, min_reg);
+      if (k >= n) {
+        t = -t;
+        r = -r;
+        const double ry = -r;
+        piw[k] = 1.0 / ry;
+        pw[k] = 1.0 / sqrt(ry);
+      }
+      reg[k] = r;
+      corr[k] = r - t;
+    }
+  }
+
+  // Same for an externally supplied diagonal (the plugin's update_diag).
+  __device__ void kkt_diag_given(const double* diag) {
+    double* reg = vec(kREG);
+    double* piw = vec(kPI);
+    double* pw = vec(kPW);
+    for (int k = tid; k < N; k += NT) {
+      const double r = diag[k];
+      reg[k] = r;
+      if (k >= n) {
+        const double ry = -r;
+        piw[k] = 1.0 / ry;
+        pw[k] = 1.0 / sqrt(ry);
+      }
+    }
+  }
+
+  // --------------------------------------------------------------------------
+  // factorize (solvers_dense.py:99-116): G = P_off + diag(Rx) + A_s^T A_s with
+  // A_s = diag(1/sqrt(Ry)) A, a relative diagonal jitter, then Cholesky.
+  // Returns 0 or the 1-based index of the first non-positive pivot.
+  // --------------------------------------------------------------------------
+  template <typename T>
+  __device__ int factorize() {
+    T* g = reinterpret_cast<T*>(G);
+    const double* reg = vec(kREG);
+    const double* wsc = vec(kPW);
+    const int nb = (n + 3) >> 2;
+    const int tiles = nb * (nb + 1) / 2;
+    double dmax[1] = {0.0};
+    double dummy[1] = {0.0};
+    for (int t = tid; t < tiles; t += NT) {
+      int bi = int((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+      while (bi * (bi + 1) / 2 > t) --bi;
+      while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+      const int bj = t - bi * (bi + 1) / 2;
+      const int i0 = bi * 4, j0 = bj * 4;
+      T acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+      for (int r = 0; r < m; ++r) {
+        const double w = wsc[n + r];
+        const double* row = A + r * lda;
+        T ai[4], aj[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          ai[a] = (i0 + a < n) ? T(row[i0 + a] * w) : T(0);
+          aj[a] = (j0 + a < n) ? T(row[j0 + a] * w) : T(0);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(ai[a], aj[b], acc[a][b]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = i0 + a;
+        if (i >= n) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int j = j0 + b;
+          if (j > i) continue;
+          double base = P[i * ldp + j];
+          if (i == j) base += reg[i];
+          const T v = T(base) + acc[a][b];
+          g[i * ldg + j] = v;
+          if (i == j) dmax[0] = nanmax(dmax[0], double(v));
+        }
+      }
+    }
+    block_reduce<NT, 0, 1>(dummy, dmax, red, phase);
+    // FP64: the reference's 1e-14 relative jitter (solvers_dense.py:112).
+    // FP32: the same idea at FP32 resolution (2^-22 relative).
+    const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
+    for (int k = tid; k < n; k += NT) g[k * ldg + k] = T(double(g[k * ldg + k]) + jit);
+    group_sync<NT>();
+    return cholesky<T>(g);
+  }
+
+  // Right-looking Cholesky of the lower triangle, two barriers per column.
+  template <typename T>
+  __device__ int cholesky(T* g) {
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NW = NT / 32;
+    for (int k = 0; k < n; ++k) {
+      const T d = g[k * ldg + k];
+      if (!(d > T(0))) {
+        group_sync<NT>();
+        return k + 1;
+      }
+      const T lkk = sqrt(d);
+      for (int i = k + 1 + tid; i < n; i += NT) g[i * ldg + k] /= lkk;
+      group_sync<NT>();
+      if (tid == 0) g[k * ldg + k] = lkk;
+      for (int j = k + 1 + warp; j < n; j += NW) {
+        const T ljk = g[j * ldg + k];
+        for (int i = j + lane; i < n; i += 32) g[i * ldg + j] -= g[i * ldg + k] * ljk;
+      }
+      group_sync<NT>();
+    }
+    return 0;
+  }
+
+  // Solves L L^T v = v in place (v of length n, shared or global memory):
+  // blocks of 32 columns, the diagonal block by warp 0 with shuffles, the
+  // off-diagonal update by the whole block.
+  template <typename T>
+  __device__ void chol_solve(const T* g, T* v) {
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int kb = 0; kb < n; kb += 32) {
+      const int bs = min(32, n - kb);
+      if (warp == 0) {
+        T zl = lane < bs ? v[kb + lane] : T(0);
+        for (int k = 0; k < bs; ++k) {
+          if (lane == k) zl = zl / g[(kb + k) * ldg + kb + k];
+          const T zk = __shfl_sync(0xffffffffu, zl, k);
+          if (lane > k && lane < bs) zl -= g[(kb + lane) * ldg + kb + k] * zk;
+        }
+        if (lane < bs) v[kb + lane] = zl;
+      }
+      group_sync<NT>();
+      if (kb + bs < n) {
+        for (int i = kb + bs + tid; i < n; i += NT) {
+          T acc = v[i];
+          const T* li = g + i * ldg + kb;
+          for (int k = 0; k < bs; ++k) acc -= li[k] * v[kb + k];
+          v[i] = acc;
+        }
+        group_sync<NT>();
+      }
+    }
+    for (int kb = ((n - 1) / 32) * 32; kb >= 0; kb -= 32) {
+      const int bs = min(32, n - kb);
+      if (warp == 0) {
+        T xl = lane < bs ? v[kb + lane] : T(0);
+        for (int k = bs - 1; k >= 0; --k) {
+          if (lane == k) xl = xl / g[(kb + k) * ldg + kb + k];
+          const T xk = __shfl_sync(0xffffffffu, xl, k);
+          if (lane < k) xl -= g[(kb + k) * ldg + kb + lane] * xk;
+        }
+        if (lane < bs) v[kb + lane] = xl;
+      }
+      group_sync<NT>();
+      if (kb > 0) {
+        for (int i = tid; i < kb; i += NT) {
+          T acc = v[i];
+          for (int k = 0; k < bs; ++k) acc -= g[(kb + k) * ldg + i] * v[kb + k];
+          v[i] = acc;
+        }
+        group_sync<NT>();
+      }
+    }
+  }
+
+  // --------------------------------------------------------------------------
+  // Backend solve (solvers_dense.py:130-142): out (+)= K_reg^{-1} r.
+  // Entry: r complete (barrier passed).  Exit: out written owner-wise.
+  // --------------------------------------------------------------------------
+  __device__ void kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
+    const double* iry = vec(kPI);
+    double* tmp = vec(kTMP);
+    float* t32 = this->t32();
+    for (int k = tid; k < n; k += NT) {
+      double acc = 0.0;
+      for (int i = 0; i < m; ++i) acc = fma(A[i * lda + k], iry[n + i] * r[n + i], acc);
+      const double g = r[k] + acc;
+      if (fp64) {
+        tmp[k] = g;
+      } else {
+        t32[k] = float(g);
+      }
+    }
+    group_sync<NT>();
+    if (fp64) {
+      chol_solve<double>(G, tmp);
+    } else {
+      chol_solve<float>(g32(), t32);
+    }
+    for (int k = tid; k < N; k += NT) {
+      double val;
+      if (k < n) {
+        val = fp64 ? tmp[k] : double(t32[k]);
+      } else {
+        const double* row = A + (k - n) * lda;
+        double ax = 0.0;
+        if (fp64) {
+          for (int j = 0; j < n; ++j) ax = fma(row[j], tmp[j], ax);
+        } else {
+          for (int j = 0; j < n; ++j) ax = fma(row[j], double(t32[j]), ax);
+        }
+        val = iry[k] * (ax - r[k]);
+      }
+      out[k] = accumulate ? out[k] + val : val;
+    }
+  }
+
+  // K_reg v for owner k (solvers_dense.py:118-128).  Reads all of v.
+  __device__ __forceinline__ double kkt_row(const double* v, int k) const {
+    const double* reg = vec(kREG);
+    if (k < n) {
+      double t = 0.0;
+      if (has_p)
+        for (int j = 0; j < n; ++j) t = fma(P[j * ldp + k], v[j], t);
+      t += reg[k] * v[k];
+      double u = 0.0;
+      for (int i = 0; i < m; ++i) u = fma(A[i * lda + k], v[n + i], u);
+      return t + u;
+    }
+    const double* row = A + (k - n) * lda;
+    double t = 0.0;
+    for (int j = 0; j < n; ++j) t = fma(row[j], v[j], t);
+    return t - (-reg[k]) * v[k];
+  }
+
+  // --------------------------------------------------------------------------
+  // DirectKktSolver.solve (direct.py:218-307).  `rhs_k(k)` produces the
+  // un-negated right-hand side element k; `sol` holds the warm start and
+  // receives the solution.  Entry: sol complete (barrier passed).
+  // --------------------------------------------------------------------------
+  template <typename RhsF>
+  __device__ IrOutcome ir_solve(RhsF rhs_k, double* sol, bool fp64) {
+    const qtqp_options& op = *o;
+    double* krhs = vec(kRHS);
+    double* res = vec(kRES);
+    const double* corr = vec(kCORR);
+    double dummy[1] = {0.0};
+    IrOutcome out;
+    {
+      double mx[3] = {0.0, 0.0, 0.0};  // |rhs|, |res|, nan(sol)
+      for (int k = tid; k < N; k += NT) {
+        double r = rhs_k(k);
+        if (k >= n) r = -r;
+        krhs[k] = r;
+        const double rk = r - kkt_row(sol, k) + corr[k] * sol[k];
+        res[k] = rk;
+        mx[0] = nanmax(mx[0], fabs(r));
+        mx[1] = nanmax(mx[1], fabs(rk));
+      }
+      block_reduce<NT, 0, 3>(dummy, mx, red, phase);
+      group_sync<NT>();
+      out.rhs_norm = mx[0];
+      out.final_res = mx[1];
+    }
+    out.tol = op.linear_solver_atol + op.linear_solver_rtol * out.rhs_norm;
+    out.status = 0;
+    out.solves = 0;
+    out.nan = false;
+    double rn = out.final_res;
+    for (int it = 1; it <= op.max_iterative_refinement_steps; ++it) {
+      out.solves = it;
+      const double prev = rn;
+      kkt_solve(res, sol, true, fp64);
+      group_sync<NT>();
+      double mx[2] = {0.0, 0.0};
+      for (int k = tid; k < N; k += NT) {
+        const double rk = krhs[k] - kkt_row(sol, k) + corr[k] * sol[k];
+        res[k] = rk;
+        mx[0] = nanmax(mx[0], fabs(rk));
+        mx[1] = fmax(mx[1], (sol[k] != sol[k]) ? 1.0 : 0.0);
+      }
+      block_reduce<NT, 0, 2>(dummy, mx, red, phase);
+      group_sync<NT>();
+      rn = mx[0];
+      out.nan = mx[1] > 0.0;
+      if (rn < out.tol) {
+        out.status = 1;
+        break;
+      }
+      if (rn >= prev) {
+        out.status = 2;
+        break;
+      }
+    }
+    out.final_res = rn;
+    return out;
+  }
+
+  // IR with the mixed-precision policy: an FP32 factor whose refinement does
+  // not converge is replaced by an FP64 factor (kept for the rest of the
+  // solve) and the refinement is redone from the same warm start, so the
+  // outcome is the one the plain FP64 path would produce.
+  template <typename RhsF, typename WarmF>
+  __device__ IrOutcome ir_solve_policy(RhsF rhs_k, WarmF warm_k, double* sol, bool& fp64,
+                                       int& n32, int& n64, int& err) {
+    for (int k = tid; k < N; k += NT) sol[k] = warm_k(k);
+    group_sync<NT>();
+    IrOutcome r = ir_solve(rhs_k, sol, fp64);
+    if (!fp64 && r.status != 1) {
+      fp64 = true;
+      ++n64;
+      const int info = factorize<double>();
+      if (info != 0) {
+        err = QTQP_ERR_NOT_SPD;
+        return r;
+      }
+      for (int k = tid; k < N; k += NT) sol[k] = warm_k(k);
+      group_sync<NT>();
+      r = ir_solve(rhs_k, sol, fp64);
+    }
+    return r;
+  }
+
+  // --------------------------------------------------------------------------
+  // tau+ of the homogeneous embedding: the quadratic root
+  // (__init__.py:759-817) or, when the KKT solve was not accurate or the
+  // quadratic fails, the linearised update (__init__.py:819-857).
+  // `kr` is K^{-1} r (complete).  Per-iteration constants come in `it`.
+  // --------------------------------------------------------------------------
+  struct IterConsts {
+    double kqq;    // K^{-1}q . q
+    double kqpkq;  // (K^{-1}q)_x . P (K^{-1}q)_x
+    double qz;     // q_x . x + q_y . y
+    double xpx;    // x . P x
+    double pxkq;   // P x . (K^{-1}q)_x
+  };
+
+  __device__ double tau_step(const double* kr, const IrOutcome& irr, double mu, double mu_t,
+                             double r_tau, double tau, double tau_anchor, const IterConsts& ic,
+                             int& method) {
+    const double* q = vec(kQ);
+    const double* kq = vec(kKQ);
+    const double* pkq = vec(kPW);
+    const double* px = vec(kXD);
+    const double* pi = vec(kPI);
+    double* pkr = vec(kRS);
+    double sm[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // kr.q, kr.Pkq, kq.Pkr, kr.Pkr, Px.kr
+    double dummy[1] = {0.0};
+    for (int k = tid; k < N; k += NT) {
+      sm[0] = fma(kr[k], q[k], sm[0]);
+      if (k < n && has_p) {
+        double t = 0.0;
+        for (int j = 0; j < n; ++j) t = fma(P[j * ldp + k], kr[j], t);
+        t = fma(pi[k], kr[k], t);
+        pkr[k] = t;
+        sm[1] = fma(kr[k], pkq[k], sm[1]);
+        sm[2] = fma(kq[k], t, sm[2]);
+        sm[3] = fma(kr[k], t, sm[3]);
+        sm[4] = fma(px[k], kr[k], sm[4]);
+      }
+    }
+    block_reduce<NT, 5, 0>(sm, dummy, red, phase);
+    const bool accurate = irr.status == 1 || irr.final_res < 1e-7;
+    if (o->tau_mode == 0 && accurate) {
+      double ta = mu + ic.kqq;
+      double tb = -r_tau - sm[0];
+      double tc = -mu_t;
+      if (has_p) {
+        ta -= ic.kqpkq;
+        tb += sm[1] + sm[2];
+        tc -= sm[3];
+      }
+      double root = 0.0;
+      bool ok = true;
+      if (fabs(ta) < kEps) {
+        if (fabs(tb) < kEps) {
+          ok = false;
+        } else {
+          root = -tc / tb;
+          ok = isfinite(root) && !(root < -1e-10);
+        }
+      } else {
+        double disc = tb * tb - 4.0 * ta * tc;
+        if (disc < -1e-9) {
+          ok = false;
+        } else {
+          disc = fmax(0.0, disc);
+          if (tb > 0.0) {
+            root = tc / (-0.5 * (tb + sqrt(disc)));
+          } else {
+            root = (-0.5 * (tb - sqrt(disc))) / ta;
+          }
+          ok = isfinite(root) && !(root < -1e-10);
+        }
+      }
+      if (ok) {
+        method = 0;
+        return fmax(0.0, root);
+      }
+    }
+    method = 1;
+    const double q_rz = sm[0] - tau * ic.kqq - ic.qz;
+    const double px_rz = (has_p ? sm[4] : 0.0) - tau * ic.pxkq - ic.xpx;
+    const double g = mu * tau * tau + (mu_t - mu) * tau_anchor * tau - tau * ic.qz - mu_t - ic.xpx;
+    const double num = g - tau * q_rz - 2.0 * px_rz;
+    const double den =
+        2.0 * mu * tau + (mu_t - mu) * tau_anchor - ic.qz + tau * ic.kqq + 2.0 * ic.pxkq;
+    const double root = tau + (fabs(den) < 1e-16 ? 0.0 : -num / den);
+    if (!isfinite(root)) return tau;
+    return fmin(fmax(root, 0.1 * tau), 10.0 * tau);
+  }
+
+  // Ratio test (__init__.py:671-680, 882-886) over the inequality block for
+  // the step (dy, ds) given owner-wise by `dir(k, dy, ds)`.
+  template <typename DirF>
+  __device__ double step_to_boundary(DirF dir) {
+    const double* xy = vec(kXY);
+    const double* s = vec(kRS);
+    double mx[1] = {-1.0};  // max of -alpha candidates == -(min alpha)
+    double dummy[1] = {0.0};
+    for (int k = own(n + z); k < N; k += NT) {
+      double dy, ds;
+      dir(k, dy, ds);
+      if (ds < -kEps) mx[0] = fmax(mx[0], -(-s[k] / ds));
+      if (dy < -kEps) mx[0] = fmax(mx[0], -(-xy[k] / dy));
+    }
+    block_reduce<NT, 0, 1>(dummy, mx, red, phase);
+    return fmin(1.0, -mx[0]);
+  }
+
+  // --------------------------------------------------------------------------
+  // _check_termination (__init__.py:888-1008) on the unequilibrated iterate,
+  // computed from the equilibrated products: A_o x_o = (A_eq x)/d,
+  // A_o^T y_o = (A_eq^T y)/e, P_o x_o = (P_eq x)/e.
+  // --------------------------------------------------------------------------
+  __device__ int termination(double tau, double nb, double nc, double* st, bool collect) {
+    const qtqp_options& op = *o;
+    const double* xy = vec(kXY);
+    const double* s = vec(kRS);
+    const double* de = vec(kDE);
+    const double* pi = vec(kPI);
+    const double inv_tau = 1.0 / fmax(tau, kEps);
+    // sums: ctx, bty, xpx ; maxes: pres, dres, |aty|, |px|, |ax+s|, |ax|, |s|, |x|, |y|
+    double sm[3] = {0.0, 0.0, 0.0};
+    double mx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = tid; k < N; k += NT) {
+      if (k < n) {
+        double aty = 0.0;
+        for (int i = 0; i < m; ++i) aty = fma(A[i * lda + k], xy[n + i], aty);
+        aty /= de[k];
+        double px = 0.0;
+        if (has_p) {
+          for (int j = 0; j < n; ++j) px = fma(P[j * ldp + k], xy[j], px);
+          px = fma(pi[k], xy[k], px);
+          px /= de[k];
+        }
+        const double xo = de[k] * xy[k];
+        sm[0] = fma(c0[k], xo, sm[0]);
+        sm[2] = fma(xo, px, sm[2]);
+        mx[1] = nanmax(mx[1], fabs((px + aty) * inv_tau + c0[k]));
+        mx[2] = nanmax(mx[2], fabs(aty));
+        mx[3] = nanmax(mx[3], fabs(px));
+        mx[7] = nanmax(mx[7], fabs(xo));
+      } else {
+        const double* row = A + (k - n) * lda;
+        double ax = 0.0;
+        for (int j = 0; j < n; ++j) ax = fma(row[j], xy[j], ax);
+        ax /= de[k];
+        const double yo = de[k] * xy[k];
+        const double so = s[k] / de[k];
+        const double bo = b0[k - n];
+        sm[1] = fma(bo, yo, sm[1]);
+        mx[0] = nanmax(mx[0], fabs((ax + so) * inv_tau - bo));
+        mx[4] = nanmax(mx[4], fabs(ax + so));
+        mx[5] = nanmax(mx[5], fabs(ax));
+        mx[6] = nanmax(mx[6], fabs(so));
+        mx[8] = nanmax(mx[8], fabs(yo));
+      }
+    }
+    block_reduce<NT, 3, 9>(sm, mx, red, phase);
+    const double ctx = sm[0], bty = sm[1], xpx = has_p ? sm[2] : 0.0;
+    const double pcost = (ctx + 0.5 * xpx * inv_tau) * inv_tau;
+    const double dcost = (-bty - 0.5 * xpx * inv_tau) * inv_tau;
+    const double pres = mx[0], dres = mx[1];
+    const double gap = fabs((ctx + bty + xpx * inv_tau) * inv_tau);
+    const double norm_aty = mx[2], norm_px = mx[3];
+    const double dinf_a = mx[4] / (fabs(ctx) + kEps);
+    const double dinf_p = norm_px / (fabs(ctx) + kEps);
+    const double dinf = fmax(dinf_a, dinf_p);
+    const double pinf = norm_aty / (fabs(bty) + kEps);
+    const double prel = fmax(fmax(mx[5] * inv_tau, mx[6] * inv_tau), nb);
+    const double drel = fmax(fmax(norm_px * inv_tau, norm_aty * inv_tau), nc);
+    const double nx = mx[7], ny = mx[8];
+    int status;
+    if (gap < op.atol + op.rtol * fmin(fabs(pcost), fabs(dcost)) &&
+        pres < op.atol + op.rtol * prel && dres < op.atol + op.rtol * drel) {
+      status = QTQP_STATUS_SOLVED;
+    } else if (ctx < -kEps && dinf < op.atol_infeas + op.rtol_infeas * nx / fabs(ctx)) {
+      status = QTQP_STATUS_UNBOUNDED;
+    } else if (bty < -kEps && pinf < op.atol_infeas + op.rtol_infeas * ny / fabs(bty)) {
+      status = QTQP_STATUS_INFEASIBLE;
+    } else {
+      status = QTQP_STATUS_UNFINISHED;
+    }
+    if (st != nullptr && tid == 0) {
+      st[kStCtx] = ctx;
+      st[kStBty] = bty;
+      st[kStPcost] = pcost;
+      st[kStDcost] = dcost;
+      st[kStPres] = pres;
+      st[kStDres] = dres;
+      st[kStGap] = gap;
+      st[kStPinfeas] = pinf;
+      st[kStDinfeas] = dinf;
+      st[kStDinfeasA] = dinf_a;
+      st[kStDinfeasP] = dinf_p;
+      st[kStNormX] = nx;
+      st[kStNormY] = ny;
+      st[kStStatus] = status;
+      st[kStPrel] = prel;
+      st[kStDrel] = drel;
+    }
+    if (collect && st != nullptr) {
+      // collect_stats extras (__init__.py:992-1007): complementarity, norm_s
+      // and the per-inequality statistics of s*y and s/y.
+      double a[5] = {0, 0, 0, 0, 0};  // y.s, sum sy, sum s/y
+      double b[5] = {0, 0, -INFINITY, 0, 0};  // max sy, max -sy, max soy, max -soy
+      b[0] = -INFINITY;
+      b[1] = -INFINITY;
+      b[3] = -INFINITY;
+      for (int k = own(n); k < N; k += NT) {
+        const double yo = de[k] * xy[k], so = s[k] / de[k];
+        a[0] = fma(yo, so, a[0]);
+        if (k >= n + z) {
+          const double sy = so * yo, soy = so / fmax(kEps, yo);
+          a[1] += sy;
+          a[2] += soy;
+          b[0] = fmax(b[0], sy);
+          b[1] = fmax(b[1], -sy);
+          b[2] = fmax(b[2], soy);
+          b[3] = fmax(b[3], -soy);
+        }
+      }
+      block_reduce<NT, 5, 5>(a, b, red, phase);
+      const int cnt = m - z;
+      const double mean_sy = a[1] / cnt, mean_soy = a[2] / cnt;
+      double v[2] = {0, 0};
+      double dummy[1] = {0};
+      for (int k = own(n + z); k < N; k += NT) {
+        const double yo = de[k] * xy[k], so = s[k] / de[k];
+        const double sy = so * yo, soy = so / fmax(kEps, yo);
+        v[0] += (sy - mean_sy) * (sy - mean_sy);
+        v[1] += (soy - mean_soy) * (soy - mean_soy);
+      }
+      block_reduce<NT, 2, 0>(v, dummy, red, phase);
+      if (tid == 0) {
+        st[kStCompl] = fabs(a[0] * inv_tau * inv_tau);
+        st[kStNormS] = mx[6];
+        st[kStMaxSy] = b[0];
+        st[kStMinSy] = -b[1];
+        st[kStStdSy] = sqrt(v[0] / cnt);
+        st[kStMaxSoy] = b[2];
+        st[kStMinSoy] = -b[3];
+        st[kStMeanSoy] = mean_soy;
+        st[kStStdSoy] = sqrt(v[1] / cnt);
+      }
+    }
+    last_pcost = pcost;
+    last_dcost = dcost;
+    last_pres = pres;
+    last_dres = dres;
+    last_gap = gap;
+    return status;
+  }
+  double last_pcost = 0, last_dcost = 0, last_pres = 0, last_dres = 0, last_gap = 0;
+
+  __device__ void write_lin_stats(double* st, int block, const IrOutcome& r, int tau_method,
+                                  bool fp64) const {
+    if (st == nullptr || tid != 0) return;
+    double* b = st + kStLin0 + block * kLinFields;
+    b[kLinSolves] = r.solves;
+    b[kLinFinalRes] = r.final_res;
+    b[kLinRhsNorm] = r.rhs_norm;
+    b[kLinTol] = r.tol;
+    b[kLinStatus] = r.status;
+    b[kLinTau] = tau_method;
+    b[kLinPrec] = fp64 ? 64 : 32;
+  }
+
+  // --------------------------------------------------------------------------
+  // The whole solve (QTQP._solve_impl, __init__.py:429-614).
+  // --------------------------------------------------------------------------
+  __device__ void solve(qtqp_result* result, double* stats, double* x_out, double* y_out,
+                        double* s_out) {
+    const qtqp_options& op = *o;
+    const uint64_t t_start = globaltimer_ns();
+    double nb, nc;
+    load_and_equilibrate(op.equilibrate != 0, nb, nc);
+    double* xy = vec(kXY);
+    double* s = vec(kRS);
+    double* kq = vec(kKQ);
+    double* kq0 = vec(kKQ0);
+    double* xyp = vec(kXYP);
+    double* xyc = vec(kXYC);
+    double* ds = vec(kXD);  // d_s at [n, N)
+    double* ct = vec(kCT);  // Mehrotra correction at [n, N)
+    const double* q = vec(kQ);
+    const double* de = vec(kDE);
+    // _init_variables (__init__.py:299-307): x = 0, y[z:] = s[z:] = 1, then
+    // equilibrated (x/e, y/d, s*d); K^{-1} q starts at zero.
+    for (int k = tid; k < N; k += NT) {
+      kq[k] = 0.0;
+      if (k < n) {
+        xy[k] = 0.0 / de[k];
+      } else if (k < n + z) {
+        xy[k] = 0.0;
+        s[k] = 0.0;
+      } else {
+        xy[k] = 1.0 / de[k];
+        s[k] = 1.0 * de[k];
+      }
+      ds[k] = 0.0;
+      ct[k] = 0.0;
+    }
+    group_sync<NT>();
+    double tau = 1.0, alpha = 0.0, sigma = 0.0, mu = 0.0;
+    bool fp64 = op.precision == QTQP_PREC_FP64;
+    int n32 = 0, n64 = 0, nsolves = 0, err = 0;
+    int status = QTQP_STATUS_UNFINISHED;
+    int it = 0, taken = 0;
+    const double cnt = double(m - z);
+    double dummy[1] = {0.0};
+    for (it = 0; it < op.max_iter; ++it) {
+      double* st = (stats != nullptr) ? stats + size_t(it) * QTQP_STATS_DOUBLES : nullptr;
+      // _normalize (__init__.py:859-880) and mu (:477).
+      {
+        double sm[2] = {0.0, 0.0};
+        for (int k = tid; k < N; k += NT) {
+          sm[0] = fma(xy[k], xy[k], sm[0]);
+          if (k >= n) sm[1] = fma(xy[k], s[k], sm[1]);
+        }
+        block_reduce<NT, 2, 0>(sm, dummy, red, phase);
+        const double scale = sqrt(double(m - z + 1)) / fmax(kEps, sqrt(sm[0] + tau * tau));
+        for (int k = tid; k < N; k += NT) {
+          xy[k] *= scale;
+          if (k >= n) s[k] *= scale;
+        }
+        tau *= scale;
+        mu = (sm[1] * scale * scale) / cnt;
+      }
+      // DirectKktSolver.update (direct.py:183-216).
+      kkt_diag(mu, op.min_static_regularization);
+      group_sync<NT>();
+      {
+        int info;
+        if (fp64) {
+          ++n64;
+          info = factorize<double>();
+        } else {
+          ++n32;
+          info = factorize<float>();
+          if (info != 0) {  // FP32 pivot failure: refactor in FP64 for good
+            fp64 = true;
+            ++n64;
+            info = factorize<double>();
+          }
+        }
+        if (info != 0) {
+          err = QTQP_ERR_NOT_SPD;
+          break;
+        }
+      }
+      // kinv_q = K^{-1} q, warm-started (__init__.py:484).
+      for (int k = tid; k < N; k += NT) kq0[k] = kq[k];
+      IrOutcome rq = ir_solve_policy([&](int k) { return q[k]; }, [&](int k) { return kq0[k]; },
+                                     kq, fp64, n32, n64, err);
+      nsolves += rq.solves;
+      if (err) break;
+      if (rq.nan) {
+        err = QTQP_ERR_NAN;
+        break;
+      }
+      write_lin_stats(st, 0, rq, -1, fp64);
+      // Per-iteration constants of the tau equations: P K^{-1}q, P x and dots.
+      IterConsts ic;
+      {
+        double* pkq = vec(kPW);
+        double* px = vec(kXD);
+        const double* pi = vec(kPI);
+        double sm[5] = {0, 0, 0, 0, 0};
+        for (int k = tid; k < N; k += NT) {
+          sm[0] = fma(kq[k], q[k], sm[0]);
+          sm[2] = fma(q[k], xy[k], sm[2]);
+          if (k < n) {
+            double a = 0.0, b = 0.0;
+            if (has_p) {
+              for (int j = 0; j < n; ++j) {
+                const double pjk = P[j * ldp + k];
+                a = fma(pjk, kq[j], a);
+                b = fma(pjk, xy[j], b);
+              }
+              a = fma(pi[k], kq[k], a);
+              b = fma(pi[k], xy[k], b);
+            }
+            pkq[k] = a;
+            px[k] = b;
+            sm[1] = fma(kq[k], a, sm[1]);
+            sm[3] = fma(xy[k], b, sm[3]);
+            sm[4] = fma(b, kq[k], sm[4]);
+          }
+        }
+        block_reduce<NT, 5, 0>(sm, dummy, red, phase);
+        ic.kqq = sm[0];
+        ic.kqpkq = sm[1];
+        ic.qz = sm[2];
+        ic.xpx = has_p ? sm[3] : 0.0;
+        ic.pxkq = has_p ? sm[4] : 0.0;
+      }
+      // ---- Predictor (__init__.py:489-516) -------------------------------
+      const double mu_c = mu;
+      auto rhs_pred = [&](int k) {
+        double r = (mu_c - 0.0) * xy[k];
+        if (k >= n + z) r += s[k];
+        return r;
+      };
+      IrOutcome rp = ir_solve_policy(rhs_pred, [&](int k) { return xy[k]; }, xyp, fp64, n32,
+                                     n64, err);
+      nsolves += rp.solves;
+      if (err) break;
+      if (rp.nan) {
+        err = QTQP_ERR_NAN;
+        break;
+      }
+      int tm_p = 0;
+      const double tau_p = tau_step(xyp, rp, mu, 0.0, mu * tau, tau, tau, ic, tm_p);
+      write_lin_stats(st, 1, rp, tm_p, fp64);
+      for (int k = tid; k < N; k += NT) {
+        xyp[k] -= kq[k] * tau_p;  // [x_p; y_p]
+        if (k >= n + z) ds[k] = -xyp[k] * s[k] / xy[k];
+      }
+      const double alpha_p = step_to_boundary([&](int k, double& dy, double& dsk) {
+        dy = xyp[k] - xy[k];
+        dsk = ds[k];
+      });
+      // _compute_sigma (__init__.py:682-706).
+      {
+        double sm[3] = {0, 0, 0};
+        const double dtp = tau_p - tau;
+        for (int k = tid; k < N; k += NT) {
+          const double va = xy[k] + alpha_p * (xyp[k] - xy[k]);
+          if (k < n) {
+            sm[0] = fma(va, va, sm[0]);
+          } else {
+            sm[1] = fma(va, va, sm[1]);
+            const double sa = s[k] + alpha_p * ds[k];
+            sm[2] = fma(va, sa, sm[2]);
+          }
+        }
+        block_reduce<NT, 3, 0>(sm, dummy, red, phase);
+        const double ta = tau + alpha_p * dtp;
+        const double nrm2 = sm[0] + sm[1] + ta * ta;
+        const double scale_sq = double(m - z + 1) / fmax(kEps * kEps, nrm2);
+        const double mu_aff = scale_sq * sm[2] / cnt;
+        const double sb = mu_aff / fmax(kEps, mu);
+        sigma = fmin(fmax(sb * sb * sb, 0.0), 1.0);
+      }
+      // Mehrotra correction (__init__.py:528).
+      for (int k = own(n + z); k < N; k += NT) {
+        const double dyp = xyp[k] - xy[k];
+        ct[k] = -ds[k] * dyp / xy[k];
+      }
+      // ---- Corrector (__init__.py:529-543) -------------------------------
+      const double mu_t = sigma * mu;
+      auto rhs_corr = [&](int k) {
+        double r = (mu_c - mu_t) * xyp[k];
+        if (k >= n + z) {
+          if (mu_t != 0.0) r += mu_t / xy[k];
+          r += s[k];
+          r += ct[k];
+        }
+        return r;
+      };
+      group_sync<NT>();  // x_p, y_p complete before the corrector reads them
+      IrOutcome rc = ir_solve_policy(rhs_corr, [&](int k) { return xyp[k]; }, xyc, fp64, n32,
+                                     n64, err);
+      nsolves += rc.solves;
+      if (err) break;
+      if (rc.nan) {
+        err = QTQP_ERR_NAN;
+        break;
+      }
+      int tm_c = 0;
+      const double tau_c =
+          tau_step(xyc, rc, mu, mu_t, (mu - mu_t) * tau_p, tau, tau_p, ic, tm_c);
+      write_lin_stats(st, 2, rc, tm_c, fp64);
+      for (int k = tid; k < N; k += NT) {
+        xyc[k] -= kq[k] * tau_c;  // [x_c; y_c]
+        if (k >= n + z) ds[k] = mu_t / xy[k] + ct[k] - xyc[k] * s[k] / xy[k];
+      }
+      alpha = step_to_boundary([&](int k, double& dy, double& dsk) {
+        dy = xyc[k] - xy[k];
+        dsk = ds[k];
+      });
+      // ---- Update (__init__.py:556-565) --------------------------------
+      {
+        const double stp = op.step_size_scale * alpha;
+        for (int k = tid; k < N; k += NT) {
+          xy[k] += stp * (xyc[k] - xy[k]);
+          if (k >= n) s[k] += stp * ds[k];
+          if (k >= n + z) {
+            xy[k] = fmax(xy[k], 1e-30);
+            s[k] = fmax(s[k], 1e-30);
+          }
+        }
+        tau += stp * (tau_c - tau);
+        tau = fmax(tau, 1e-30);
+      }
+      group_sync<NT>();
+      status = termination(tau, nb, nc, st, op.collect_stats != 0);
+      taken = it + 1;
+      if (st != nullptr && tid == 0) {
+        st[kStIter] = it;
+        st[kStMu] = mu;
+        st[kStSigma] = sigma;
+        st[kStAlpha] = alpha;
+        st[kStTau] = tau;
+        st[kStTime] = double(globaltimer_ns() - t_start) * 1e-9;
+      }
+      if (status != QTQP_STATUS_UNFINISHED) break;
+    }
+    if (err == 0 && status == QTQP_STATUS_UNFINISHED && taken == op.max_iter) {
+      status = QTQP_STATUS_HIT_MAX_ITER;
+      if (stats != nullptr && tid == 0)
+        stats[size_t(taken - 1) * QTQP_STATS_DOUBLES + kStStatus] = status;
+    }
+    group_sync<NT>();
+    finish(status, tau, x_out, y_out, s_out);
+    if (tid == 0) {
+      result->status = err ? QTQP_STATUS_FAILED : status;
+      result->iterations = taken;
+      result->error = err;
+      result->fp32_factorizations = n32;
+      result->fp64_factorizations = n64;
+      result->ir_solves = nsolves;
+      result->tau = tau;
+      result->pcost = last_pcost;
+      result->dcost = last_dcost;
+      result->pres = last_pres;
+      result->dres = last_dres;
+      result->gap = last_gap;
+    }
+  }
+
+  // Unequilibrate and scale by status (__init__.py:580-614).
+  __device__ void finish(int status, double tau, double* x_out, double* y_out, double* s_out) {
+    const double* xy = vec(kXY);
+    const double* s = vec(kRS);
+    const double* de = vec(kDE);
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    double sm[2] = {0.0, 0.0};  // b_o . y_o, c_o . x_o
+    double dummy[1] = {0.0};
+    if (status == QTQP_STATUS_INFEASIBLE || status == QTQP_STATUS_UNBOUNDED) {
+      for (int k = tid; k < N; k += NT) {
+        if (k < n) {
+          sm[1] = fma(c0[k], de[k] * xy[k], sm[1]);
+        } else {
+          sm[0] = fma(b0[k - n], de[k] * xy[k], sm[0]);
+        }
+      }
+      block_reduce<NT, 2, 0>(sm, dummy, red, phase);
+    }
+    for (int k = tid; k < N; k += NT) {
+      if (k < n) {
+        const double xo = de[k] * xy[k];
+        double v;
+        if (status == QTQP_STATUS_INFEASIBLE) {
+          v = nan;
+        } else if (status == QTQP_STATUS_UNBOUNDED) {
+          v = xo / fabs(sm[1]);
+        } else {
+          v = xo / tau;
+        }
+        x_out[k] = v;
+      } else {
+        const double yo = de[k] * xy[k], so = s[k] / de[k];
+        double vy, vs;
+        if (status == QTQP_STATUS_INFEASIBLE) {
+          vy = yo / fabs(sm[0]);
+          vs = nan;
+        } else if (status == QTQP_STATUS_UNBOUNDED) {
+          vy = nan;
+          vs = so / fabs(sm[1]);
+        } else {
+          vy = yo / tau;
+          vs = so / tau;
+        }
+        y_out[k - n] = vy;
+        s_out[k - n] = vs;
+      }
+    }
+  }
+};
+
+}  // namespace qtqp

@@ -1,0 +1,214 @@
+"""Seeded synthetic QP generators.
+
+Workloads: the five benchmark configurations (a single sparse QP, a batch of
+uneven small dense QPs, a large dense QP, a long-horizon MPC QP and its
+parametric family) and the three certificate families used by the tests
+(feasible, primal infeasible, dual infeasible).  Every generator takes a seed
+and returns (a: csc, b, c, z, p: csc).
+
+Seeds: configuration k uses ``default_rng(1000 + k)``; instance i of a batch
+uses ``default_rng([1000 + k, i])``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+
+def _feasible_pair(rng, a, p, z):
+  """b, c from a primal-dual optimal pair (x0, y0, s0).
+
+  x0 ~ N(0,1); y0[:z] ~ N(0,1); y0[z:] = |N(0,1)| on a random half, else 0;
+  s0[:z] = 0; s0[z:] ~ U(0,1) where y0 == 0, else 0 (complementary).
+  """
+  m, n = a.shape
+  x0 = rng.normal(size=n)
+  y0 = np.zeros(m)
+  y0[:z] = rng.normal(size=z)
+  active = rng.random(m - z) < 0.5
+  y0[z:] = np.where(active, np.abs(rng.normal(size=m - z)), 0.0)
+  s0 = np.zeros(m)
+  s0[z:] = np.where(active, 0.0, rng.random(m - z))
+  b = a @ x0 + s0
+  c = -(p @ x0 + a.T @ y0)
+  return np.asarray(b).ravel(), np.asarray(c).ravel()
+
+
+# ---------------------------------------------------------------------------
+# Benchmark configurations.
+# ---------------------------------------------------------------------------
+CFG0_M_DENSITY = 0.10  # density of M in P = M M^T + 1e-2 I (not fixed upstream)
+
+
+def config0(seed: int = 1000):
+  """Single sparse QP: n=200, m=300, z=50; A = 5% Bernoulli mask x N(0,1);
+  P = M M^T + 1e-2 I with M 200x20 sparse N(0,1) (10% dense)."""
+  rng = np.random.default_rng(seed)
+  n, m, z = 200, 300, 50
+  mask = rng.random((m, n)) < 0.05
+  a = sp.csc_matrix(np.where(mask, rng.normal(size=(m, n)), 0.0))
+  mm = sp.random(n, 20, density=CFG0_M_DENSITY, format="csc", rng=rng,
+                 data_rvs=lambda k: rng.normal(size=k))
+  p = sp.csc_matrix(mm @ mm.T + 1e-2 * sp.eye(n))
+  b, c = _feasible_pair(rng, a, p, z)
+  return a, b, c, z, p
+
+
+def config1_instance(i: int, base: int = 1001):
+  """One of the uneven small dense QPs: n ~ U{8..64}, m = 2n, z = n // 4,
+  A ~ N(0,1) dense, P = L L^T + 1e-3 I with L n x n//2 ~ N(0,1)."""
+  rng = np.random.default_rng([base, i])
+  n = int(rng.integers(8, 65))
+  m, z = 2 * n, n // 4
+  a_d = rng.normal(size=(m, n))
+  l = rng.normal(size=(n, n // 2))
+  p_d = l @ l.T + 1e-3 * np.eye(n)
+  p_d = 0.5 * (p_d + p_d.T)
+  b, c = _feasible_pair(rng, a_d, p_d, z)
+  return sp.csc_matrix(a_d), b, c, z, sp.csc_matrix(p_d)
+
+
+def config1(count: int = 4096):
+  return [config1_instance(i) for i in range(count)]
+
+
+def config2(seed: int = 1002, n: int = 4096, m: int = 8192, z: int = 1024, rank: int = 256):
+  """Large dense QP: A ~ N(0, 1/n); P = U diag(d) U^T + 1e-4 I with U n x rank
+  ~ N(0,1), d ~ U(0.1, 10).  Returns dense arrays (a, b, c, z, p)."""
+  rng = np.random.default_rng(seed)
+  a = rng.normal(scale=1.0 / np.sqrt(n), size=(m, n))
+  u = rng.normal(size=(n, rank))
+  d = rng.uniform(0.1, 10.0, size=rank)
+  p = (u * d) @ u.T + 1e-4 * np.eye(n)
+  p = 0.5 * (p + p.T)
+  b, c = _feasible_pair(rng, a, p, z)
+  return a, b, c, z, p
+
+
+def mpc_structure(horizon: int, nx: int = 40, nu: int = 20, seed: int = 1003):
+  """Stage-interleaved MPC QP structure [x_0, u_0, ..., x_{T-1}, u_{T-1}]:
+  equalities x_0 = b_0, x_{t+1} - A_d x_t - B_d u_t = b_t; box rows [I; -I]
+  with bounds 5 (x) and 1 (u); P = blockdiag(diag(Q), 0.1 I).
+  Returns (a csc, z, p csc, ub)."""
+  rng = np.random.default_rng(seed)
+  st = nx + nu
+  n = horizon * st
+  ad = np.eye(nx) + 0.01 * rng.normal(size=(nx, nx))
+  bd = rng.normal(scale=1.0 / np.sqrt(nx), size=(nx, nu))
+  rows, cols, vals = [], [], []
+  for k in range(nx):  # x_0 = b_0
+    rows.append(k)
+    cols.append(k)
+    vals.append(1.0)
+  r0 = nx
+  for t in range(horizon - 1):
+    xt, ut, xn = t * st, t * st + nx, (t + 1) * st
+    for i in range(nx):
+      rows.append(r0 + i)
+      cols.append(xn + i)
+      vals.append(1.0)
+      for j in range(nx):
+        rows.append(r0 + i)
+        cols.append(xt + j)
+        vals.append(-ad[i, j])
+      for j in range(nu):
+        rows.append(r0 + i)
+        cols.append(ut + j)
+        vals.append(-bd[i, j])
+    r0 += nx
+  z = r0
+  a_eq = sp.csc_matrix((vals, (rows, cols)), shape=(z, n))
+  eye = sp.eye(n, format="csc")
+  a = sp.vstack([a_eq, eye, -eye], format="csc")
+  q = rng.uniform(0.1, 1.0, size=nx)
+  pdiag = np.tile(np.concatenate([q, np.full(nu, 0.1)]), horizon)
+  p = sp.diags(pdiag, format="csc")
+  ub = np.tile(np.concatenate([np.full(nx, 5.0), np.full(nu, 1.0)]), horizon)
+  return a, z, p, ub
+
+
+def mpc_feasible(horizon: int, seed: int = 1003, active_frac: float = 0.1):
+  """MPC QP with b, c from a feasible pair: x_bar strictly inside the boxes
+  except a fraction `active_frac` at +-bound (with positive duals there)."""
+  a, z, p, ub = mpc_structure(horizon, seed=seed)
+  rng = np.random.default_rng([seed, 1])
+  n = p.shape[0]
+  xbar = rng.uniform(-0.5, 0.5, size=n) * ub
+  act = rng.random(n) < active_frac
+  sgn = np.where(rng.random(n) < 0.5, 1.0, -1.0)
+  xbar = np.where(act, sgn * ub, xbar)
+  ybar = np.zeros(a.shape[0])
+  ybar[:z] = rng.normal(size=z)
+  lam = np.abs(rng.normal(size=n))
+  ybar[z:z + n] = np.where(act & (sgn > 0), lam, 0.0)       # x <= ub active
+  ybar[z + n:] = np.where(act & (sgn < 0), lam, 0.0)        # -x <= ub active
+  b = np.concatenate([a[:z] @ xbar, ub, ub])
+  c = -(p @ xbar + a.T @ ybar)
+  return a, b, c, z, p
+
+
+def config3():
+  return mpc_feasible(500)
+
+
+def config4_family(count: int = 20000, horizon: int = 50, dim: int = 32, seed: int = 1004):
+  """Parametric family: fixed (A, P) of the T=50 MPC QP; (b, c) = (b_bar,
+  c_bar) + W theta, theta ~ N(0, I_dim), W ~ N(0, 0.1^2) fixed.
+  Returns (a, z, p, b_bar, c_bar, W, thetas)."""
+  a, b_bar, c_bar, z, p = mpc_feasible(horizon, seed=seed)
+  rng = np.random.default_rng(seed)
+  mtot, n = a.shape
+  w = rng.normal(scale=0.1, size=(mtot + n, dim))
+  thetas = np.random.default_rng([seed, 2]).normal(size=(count, dim))
+  return a, z, p, b_bar, c_bar, w, thetas
+
+
+# ---------------------------------------------------------------------------
+# Certificate families for tests.
+# ---------------------------------------------------------------------------
+def feasible(m: int, n: int, z: int, seed, density: float = 0.1):
+  """Sparse feasible QP with a known optimal primal-dual pair."""
+  rng = np.random.default_rng(seed)
+  a = sp.random(m, n, density=density, format="csc", rng=rng,
+                data_rvs=lambda k: rng.normal(size=k))
+  g = sp.random(n, n, density=0.05, format="csc", rng=rng,
+                data_rvs=lambda k: rng.normal(size=k))
+  p = sp.csc_matrix(0.01 * (g.T @ g))
+  b, c = _feasible_pair(rng, a, p, z)
+  return a, b, c, z, p
+
+
+def infeasible(m: int, n: int, z: int, seed):
+  """Primal infeasible QP: a Farkas ray y (y[z:] >= 0, A^T y = 0, b^T y = -1)."""
+  rng = np.random.default_rng(seed)
+  y = rng.random(m) + 0.1
+  a = rng.normal(size=(m, n))
+  a -= np.outer(y, y @ a) / (y @ y)
+  b = rng.normal(size=m)
+  b = -b / (b @ y)
+  g = rng.normal(size=(n, n))
+  p = 0.01 * g.T @ g
+  c = rng.normal(size=n)
+  return sp.csc_matrix(a), b, c, z, sp.csc_matrix(p)
+
+
+def unbounded(m: int, n: int, z: int, seed):
+  """Dual infeasible QP: a ray x with P x = 0, A x + s = 0 (s[z:] >= 0,
+  s[:z] = 0) and c^T x = -1."""
+  rng = np.random.default_rng(seed)
+  g = rng.normal(size=(n, n))
+  p = 0.01 * g.T @ g
+  w, v = np.linalg.eigh(p)
+  w[0] = 0.0
+  p = (v * w) @ v.T
+  p = 0.5 * (p + p.T)
+  x = v[:, 0]
+  s = np.zeros(m)
+  s[z:] = rng.random(m - z)
+  a = rng.normal(size=(m, n))
+  a -= np.outer(a @ x + s, x) / (x @ x)
+  c = rng.normal(size=n)
+  c = -c / (c @ x)
+  b = rng.normal(size=m)
+  return sp.csc_matrix(a), b, c, z, sp.csc_matrix(p)

@@ -1,0 +1,77 @@
+"""C-ABI checks that need no GPU: the library builds, loads, exports every
+entry point declared in include/*.h, and its host-only planner works."""
+
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from qtqp_b200 import _lib, batch, problems
+from qtqp_b200 import build as qbuild
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+  names = set()
+  for hdr in glob.glob(os.path.join(ROOT, "include", "*.h")):
+    text = open(hdr).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names |= set(re.findall(r"\b(qtqp_\w+)\s*\(", text))
+  return sorted(names)
+
+
+@pytest.fixture(scope="module")
+def lib():
+  qbuild.build()
+  return _lib.load()
+
+
+def test_library_exports_every_declared_symbol(lib):
+  declared = _declared()
+  assert declared, "no entry points found in include/"
+  for name in declared:
+    assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+  assert set(_lib.EXPORTS) <= set(declared)
+
+
+def test_version_and_last_error(lib):
+  assert lib.qtqp_version() >= 1
+  assert isinstance(lib.qtqp_last_error(), bytes)
+
+
+def test_plan_orders_by_cost_and_sizes_workspace(lib):
+  probs = [batch.DenseProblem(*_dense(problems.config1_instance(i))) for i in range(50)]
+  hb = batch.HostBatch(probs, batch.SolveOptions())
+  ns = hb.inst["n"][hb.order[:hb.count]]
+  costs = hb.inst["m"][hb.order] * ns.astype(float) ** 2 + ns.astype(float) ** 3 / 3
+  assert np.all(np.diff(costs) <= 0)
+  assert sorted(hb.order.tolist()) == list(range(50))
+  assert hb.block_threads in (32, 64, 128, 256)
+  assert hb.workspace_bytes >= 256
+  assert np.all(np.diff(hb.inst["ws_off"]) >= 0)
+
+
+def test_plan_rejects_bad_instances(lib):
+  inst = np.zeros(1, dtype=_lib.INSTANCE_DTYPE)
+  inst["n"], inst["m"], inst["z"] = 3, 2, 2  # z == m: no inequality
+  order = np.zeros(1, dtype=np.int32)
+  nt, sm, ws = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_size_t(0)
+  opts = batch.SolveOptions().to_c()
+  rc = lib.qtqp_dense_batch_plan(inst.ctypes.data, 1, ctypes.byref(opts), order.ctypes.data,
+                                 ctypes.byref(nt), ctypes.byref(sm), ctypes.byref(ws))
+  assert rc == _lib.QTQP_ERR_BAD_ARG
+  assert b"0 <= z < m" in lib.qtqp_last_error()
+
+
+def test_kkt_workspace_size(lib):
+  assert lib.qtqp_kkt_dense_workspace_bytes(0, 3) == 0
+  assert lib.qtqp_kkt_dense_workspace_bytes(10, 20) > 8 * (10 * 20 + 10 * 10)
+
+
+def _dense(prob):
+  a, b, c, z, p = prob
+  return a.toarray(), b, c, z, p.toarray()
