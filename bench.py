@@ -328,8 +328,8 @@ def run_ours(args) -> None:
         "data": "synthetic (seeded generator of the workload's distribution)",
         "config": {"workload": WORKLOAD, "instances_per_gpu": args.count,
                    "precision": args.precision, "l2": "flushed between steps (256 MiB write);"
-                   " inputs also exceed L2", "block_threads": hb.block_threads,
-                   "smem_bytes": hb.smem_bytes},
+                   " inputs also exceed L2",
+                   "launch_groups": [list(g) for g in hb.groups]},
         "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
         "statuses_identical_to_fp64": same_status,
         "solved_per_step": solved_total, "instances_per_step": args.count * world,

@@ -92,6 +92,23 @@ typedef struct {
   double v[QTQP_STATS_DOUBLES];
 } qtqp_iter_stats;
 
+/* A batch is solved by up to QTQP_MAX_GROUPS concurrent persistent launches,
+ * one per size class of the instances (the shared-memory footprint of a QP
+ * fixes how many thread blocks fit on an SM). */
+#define QTQP_MAX_GROUPS 8
+typedef struct {
+  int32_t begin, count;  /* slice of the processing order                  */
+  int32_t block_threads; /* threads per block                             */
+  int32_t smem_bytes;    /* dynamic shared memory per block               */
+} qtqp_launch_group;
+
+typedef struct {
+  int32_t num_groups;
+  int32_t reserved;
+  qtqp_launch_group groups[QTQP_MAX_GROUPS];
+  uint64_t workspace_bytes; /* global scratch the solve needs               */
+} qtqp_batch_plan;
+
 /* ---- library ------------------------------------------------------------ */
 const char* qtqp_last_error(void);
 int qtqp_version(void);
@@ -105,30 +122,30 @@ int qtqp_device_sm_count(void);
  * thread block runs one QP's whole solve (Ruiz, normalise, KKT factor, IR,
  * predictor/corrector, ratio test, termination, unscaling).
  *
- * qtqp_dense_batch_plan: host-only.  Given the instances' (n, m) it fills
- * inst[i].ws_off and returns the workspace size in bytes; `order` receives the
- * processing order (descending cost).  block_threads / smem_bytes (0 = auto)
- * select the launch shape; the chosen values are written back. */
+ * qtqp_dense_batch_plan: host-only.  Given the instances' (n, m, z) it fills
+ * inst[i].ws_off, writes the processing order (descending cost) to h_order
+ * and the launch groups and workspace size to *plan.  block_threads and
+ * smem_bytes force one launch shape for every group when non-zero. */
 int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
                           const qtqp_options* opt, int32_t* h_order,
-                          int32_t* block_threads, int32_t* smem_bytes,
-                          size_t* workspace_bytes);
+                          int32_t block_threads, int32_t smem_bytes,
+                          qtqp_batch_plan* plan);
 
-/* Device-resident solve of the whole batch in one persistent launch.
+/* Device-resident solve of the whole batch.
  * d_inst / d_order: the planned descriptors and order, copied to the device by
- * the caller.  b/c pools are inputs; x/y/s pools and d_results are outputs
- * (x, y, s after the reference's status-dependent scaling,
- * __init__.py:580-614; presolve row restoration is the host's job).
- * d_stats: qtqp_iter_stats[max_iter] per instance, or NULL. */
+ * the caller; plan: the host plan that produced them.  b/c pools are inputs;
+ * x/y/s pools and d_results are outputs (x, y, s after the reference's
+ * status-dependent scaling, __init__.py:580-614; presolve row restoration is
+ * the host's job).  d_stats: qtqp_iter_stats[max_iter] per instance, or NULL.
+ * The groups run on side streams forked from and joined back to `stream`. */
 int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst,
-                           const int32_t* d_order, int32_t count,
+                           const int32_t* d_order, const qtqp_batch_plan* plan,
                            const double* d_a_pool, const double* d_p_pool,
                            const double* d_b_pool, const double* d_c_pool,
                            double* d_x_pool, double* d_y_pool,
                            double* d_s_pool, qtqp_result* d_results,
                            qtqp_iter_stats* d_stats, void* d_workspace,
                            size_t workspace_bytes, const qtqp_options* opt,
-                           int32_t block_threads, int32_t smem_bytes,
                            void* stream);
 
 /* ---- dense KKT backend (the direct.LinearSolver plugin) ------------------ *

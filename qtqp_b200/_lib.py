@@ -94,6 +94,19 @@ class Result(ctypes.Structure):
   ]
 
 
+MAX_GROUPS = 8
+
+
+class LaunchGroup(ctypes.Structure):
+  _fields_ = [("begin", ctypes.c_int32), ("count", ctypes.c_int32),
+              ("block_threads", ctypes.c_int32), ("smem_bytes", ctypes.c_int32)]
+
+
+class BatchPlan(ctypes.Structure):
+  _fields_ = [("num_groups", ctypes.c_int32), ("reserved", ctypes.c_int32),
+              ("groups", LaunchGroup * MAX_GROUPS), ("workspace_bytes", ctypes.c_uint64)]
+
+
 # numpy views of the same layouts (for bulk packing / unpacking).
 INSTANCE_DTYPE = np.dtype([(name, np.int32 if ct is ctypes.c_int32 else np.int64)
                            for name, ct in DenseInstance._fields_])
@@ -128,12 +141,11 @@ def load() -> ctypes.CDLL:
     lib.qtqp_last_error.restype = ctypes.c_char_p
     lib.qtqp_version.restype = ctypes.c_int
     lib.qtqp_device_sm_count.restype = ctypes.c_int
-    lib.qtqp_dense_batch_plan.argtypes = [vp, i32, ctypes.POINTER(Options), vp,
-                                          ctypes.POINTER(i32), ctypes.POINTER(i32),
-                                          ctypes.POINTER(sz)]
-    lib.qtqp_dense_batch_solve.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp,
-                                           vp, vp, sz, ctypes.POINTER(Options), i32, i32,
-                                           vp]
+    lib.qtqp_dense_batch_plan.argtypes = [vp, i32, ctypes.POINTER(Options), vp, i32, i32,
+                                          ctypes.POINTER(BatchPlan)]
+    lib.qtqp_dense_batch_solve.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp, vp,
+                                           vp, vp, vp, vp, vp, vp, sz,
+                                           ctypes.POINTER(Options), vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz
     lib.qtqp_kkt_dense_workspace_bytes.argtypes = [i32, i32]
     lib.qtqp_kkt_dense_set.argtypes = [i32, i32, vp, vp, vp, vp]

@@ -111,17 +111,20 @@ class HostBatch:
       self.c_pool[d["n_off"]:d["n_off"] + n] = pr.c
     self.n_total, self.m_total = n_off, m_off
     order = np.zeros(max(count, 1), dtype=np.int32)
-    nt = ctypes.c_int32(block_threads)
-    sm = ctypes.c_int32(smem_bytes)
-    ws = ctypes.c_size_t(0)
+    plan = _lib.BatchPlan()
     copts = opts.to_c()
     _lib.check(lib.qtqp_dense_batch_plan(inst.ctypes.data, count, ctypes.byref(copts),
-                                         order.ctypes.data, ctypes.byref(nt),
-                                         ctypes.byref(sm), ctypes.byref(ws)))
-    self.inst, self.order = inst, order
-    self.block_threads, self.smem_bytes = nt.value, sm.value
-    self.workspace_bytes = ws.value
+                                         order.ctypes.data, block_threads, smem_bytes,
+                                         ctypes.byref(plan)))
+    self.inst, self.order, self.plan = inst, order, plan
+    self.workspace_bytes = int(plan.workspace_bytes)
     self.opts = opts
+
+  @property
+  def groups(self):
+    """(begin, count, block_threads, smem_bytes) of each launch group."""
+    return [(g.begin, g.count, g.block_threads, g.smem_bytes)
+            for g in self.plan.groups[:self.plan.num_groups]]
 
   @property
   def input_bytes(self) -> int:
@@ -171,12 +174,12 @@ class DeviceBatch:
     st = stream or torch.cuda.current_stream(self.device)
     hb = self.hb
     _lib.check(lib.qtqp_dense_batch_solve(
-        self.inst.data_ptr(), self.order.data_ptr(), hb.count, self.a.data_ptr(),
-        self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(), self.x.data_ptr(),
-        self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
+        self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan),
+        self.a.data_ptr(), self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
+        self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
         self.stats.data_ptr() if self.stats is not None else None,
         self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts),
-        hb.block_threads, hb.smem_bytes, _lib.stream_handle(st)))
+        _lib.stream_handle(st)))
 
   def fetch(self):
     """Synchronises and returns (results, x, y, s, stats) as numpy arrays."""

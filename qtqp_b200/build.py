@@ -48,21 +48,33 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
-  """Compiles every .cu under csrc/ into libqtqp_cuda.so; returns its path."""
+  """Compiles every .cu under csrc/ (in parallel) into libqtqp_cuda.so."""
   if not force and not debug and up_to_date():
     return LIB_PATH
-  cmd = [_nvcc(), *ARCH_FLAGS, "-lineinfo", "-std=c++17", "-shared",
-         "-Xcompiler", "-fPIC", "-I", _INC, "-I", _CSRC,
-         "--expt-relaxed-constexpr", "-o", LIB_PATH + ".tmp"]
-  cmd += ["-O0", "-G"] if debug else ["-O3"]
+  import concurrent.futures
+  import tempfile
+  common = [_nvcc(), *ARCH_FLAGS, "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+            "-I", _INC, "-I", _CSRC, "--expt-relaxed-constexpr"]
+  common += ["-O0", "-G"] if debug else ["-O3"]
   if verbose:
-    cmd += ["-Xptxas", "-v"]
-  cmd += sources()
-  proc = subprocess.run(cmd, capture_output=True, text=True)
-  if proc.returncode != 0:
-    raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stderr}\n{proc.stdout}")
-  if verbose:
-    sys.stderr.write(proc.stderr)
+    common += ["-Xptxas", "-v"]
+  with tempfile.TemporaryDirectory(prefix="qtqp_build_") as tmp:
+    def compile_one(src):
+      obj = os.path.join(tmp, os.path.basename(src) + ".o")
+      proc = subprocess.run([*common, "-c", src, "-o", obj], capture_output=True, text=True)
+      return src, obj, proc
+    objs = []
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+      for src, obj, proc in ex.map(compile_one, sources()):
+        if proc.returncode != 0:
+          raise RuntimeError(f"nvcc failed on {src}:\n{proc.stderr}\n{proc.stdout}")
+        if verbose:
+          sys.stderr.write(proc.stderr)
+        objs.append(obj)
+    link = [_nvcc(), *ARCH_FLAGS, "-shared", "-o", LIB_PATH + ".tmp", *objs]
+    proc = subprocess.run(link, capture_output=True, text=True)
+    if proc.returncode != 0:
+      raise RuntimeError(f"nvcc link failed:\n{proc.stderr}\n{proc.stdout}")
   os.replace(LIB_PATH + ".tmp", LIB_PATH)
   return LIB_PATH
 

@@ -41,7 +41,8 @@ enum VecId : int {
   kPW,       // [P_eq K^{-1}q_x; 1/sqrt(Ry)]
   kRS,       // [P_eq K^{-1}r_x; s]
   kXD,       // [P_eq x; d_s]
-  kCT,       // [FP32 scratch (n floats); Mehrotra correction]
+  kCT,       // [FP32 scratch (2n floats); Mehrotra correction]
+  kW,        // triangular-solve scratch (FP64)
   kNumVec
 };
 
@@ -336,7 +337,9 @@ struct DenseIpm {
     return cholesky<T>(g);
   }
 
-  // Right-looking Cholesky of the lower triangle, two barriers per column.
+  // Right-looking Cholesky of the lower triangle, two barriers per column;
+  // afterwards every 32x32 diagonal block of L is replaced by its inverse so
+  // that the triangular solves are block-parallel (see chol_solve).
   template <typename T>
   __device__ int cholesky(T* g) {
     const int warp = tid >> 5, lane = tid & 31;
@@ -357,54 +360,75 @@ struct DenseIpm {
       }
       group_sync<NT>();
     }
+    invert_diag_blocks<T>(g);
     return 0;
   }
 
-  // Solves L L^T v = v in place (v of length n, shared or global memory):
-  // blocks of 32 columns, the diagonal block by warp 0 with shuffles, the
-  // off-diagonal update by the whole block.
+  // In-place inverse of each 32x32 lower-triangular diagonal block of L, one
+  // warp per block, column by column from the last: for i > j,
+  // X_ij = -(sum_{j<k<=i} X_ik L_kj) / L_jj, X_jj = 1 / L_jj.
   template <typename T>
-  __device__ void chol_solve(const T* g, T* v) {
+  __device__ void invert_diag_blocks(T* g) {
     const int warp = tid >> 5, lane = tid & 31;
-    for (int kb = 0; kb < n; kb += 32) {
-      const int bs = min(32, n - kb);
-      if (warp == 0) {
-        T zl = lane < bs ? v[kb + lane] : T(0);
-        for (int k = 0; k < bs; ++k) {
-          if (lane == k) zl = zl / g[(kb + k) * ldg + kb + k];
-          const T zk = __shfl_sync(0xffffffffu, zl, k);
-          if (lane > k && lane < bs) zl -= g[(kb + lane) * ldg + kb + k] * zk;
+    constexpr int NW = NT / 32;
+    const int nblk = (n + 31) >> 5;
+    for (int blk = warp; blk < nblk; blk += NW) {
+      const int kb = blk * 32, bs = min(32, n - kb);
+      T* L = g + kb * ldg + kb;
+      for (int j = bs - 1; j >= 0; --j) {
+        const T inv_jj = T(1) / L[j * ldg + j];
+        T w = T(0);
+        if (lane > j && lane < bs) {
+          const T* row = L + lane * ldg;
+          for (int k = j + 1; k <= lane; ++k) w = fma(row[k], L[k * ldg + j], w);
         }
-        if (lane < bs) v[kb + lane] = zl;
+        __syncwarp();
+        if (lane > j && lane < bs) L[lane * ldg + j] = -w * inv_jj;
+        if (lane == j) L[j * ldg + j] = inv_jj;
+        __syncwarp();
+      }
+    }
+    group_sync<NT>();
+  }
+
+  // Solves L L^T v = v in place with the block-inverted factor: forward
+  // z_b = X_bb (v_b - sum_{c<b} L_bc z_c), backward x_b = X_bb^T (z_b -
+  // sum_{c>b} L_cb^T x_c), two barriers per 32-block; w is n scratch entries.
+  template <typename T>
+  __device__ void chol_solve(const T* g, T* v, T* w) {
+    const int nblk = (n + 31) >> 5;
+    for (int blk = 0; blk < nblk; ++blk) {
+      const int kb = blk * 32, bs = min(32, n - kb);
+      for (int r = tid; r < bs; r += NT) {
+        const T* row = g + (kb + r) * ldg + kb;
+        T acc = T(0);
+        for (int k = 0; k <= r; ++k) acc = fma(row[k], v[kb + k], acc);
+        w[kb + r] = acc;
       }
       group_sync<NT>();
       if (kb + bs < n) {
         for (int i = kb + bs + tid; i < n; i += NT) {
-          T acc = v[i];
           const T* li = g + i * ldg + kb;
-          for (int k = 0; k < bs; ++k) acc -= li[k] * v[kb + k];
+          T acc = v[i];
+          for (int k = 0; k < bs; ++k) acc = fma(-li[k], w[kb + k], acc);
           v[i] = acc;
         }
         group_sync<NT>();
       }
     }
-    for (int kb = ((n - 1) / 32) * 32; kb >= 0; kb -= 32) {
-      const int bs = min(32, n - kb);
-      if (warp == 0) {
-        T xl = lane < bs ? v[kb + lane] : T(0);
-        for (int k = bs - 1; k >= 0; --k) {
-          if (lane == k) xl = xl / g[(kb + k) * ldg + kb + k];
-          const T xk = __shfl_sync(0xffffffffu, xl, k);
-          if (lane < k) xl -= g[(kb + k) * ldg + kb + lane] * xk;
-        }
-        if (lane < bs) v[kb + lane] = xl;
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+      const int kb = blk * 32, bs = min(32, n - kb);
+      for (int r = tid; r < bs; r += NT) {
+        T acc = T(0);
+        for (int k = r; k < bs; ++k) acc = fma(g[(kb + k) * ldg + kb + r], w[kb + k], acc);
+        v[kb + r] = acc;
       }
       group_sync<NT>();
       if (kb > 0) {
         for (int i = tid; i < kb; i += NT) {
-          T acc = v[i];
-          for (int k = 0; k < bs; ++k) acc -= g[(kb + k) * ldg + i] * v[kb + k];
-          v[i] = acc;
+          T acc = w[i];
+          for (int k = 0; k < bs; ++k) acc = fma(-g[(kb + k) * ldg + i], v[kb + k], acc);
+          w[i] = acc;
         }
         group_sync<NT>();
       }
@@ -431,9 +455,9 @@ struct DenseIpm {
     }
     group_sync<NT>();
     if (fp64) {
-      chol_solve<double>(G, tmp);
+      chol_solve<double>(G, tmp, vec(kW));
     } else {
-      chol_solve<float>(g32(), t32);
+      chol_solve<float>(g32(), t32, t32 + n);
     }
     for (int k = tid; k < N; k += NT) {
       double val;

@@ -167,14 +167,14 @@ def config4_family(count: int = 20000, horizon: int = 50, dim: int = 32, seed: i
 # ---------------------------------------------------------------------------
 # Certificate families for tests.
 # ---------------------------------------------------------------------------
-def feasible(m: int, n: int, z: int, seed, density: float = 0.1):
-  """Sparse feasible QP with a known optimal primal-dual pair."""
+def feasible(m: int, n: int, z: int, seed, density: float = 0.1, lp: bool = False):
+  """Sparse feasible QP with a known optimal primal-dual pair (P = 0 if lp)."""
   rng = np.random.default_rng(seed)
   a = sp.random(m, n, density=density, format="csc", rng=rng,
                 data_rvs=lambda k: rng.normal(size=k))
   g = sp.random(n, n, density=0.05, format="csc", rng=rng,
                 data_rvs=lambda k: rng.normal(size=k))
-  p = sp.csc_matrix(0.01 * (g.T @ g))
+  p = sp.csc_matrix((n, n)) if lp else sp.csc_matrix(0.01 * (g.T @ g))
   b, c = _feasible_pair(rng, a, p, z)
   return a, b, c, z, p
 

@@ -50,21 +50,36 @@ def test_plan_orders_by_cost_and_sizes_workspace(lib):
   costs = hb.inst["m"][hb.order] * ns.astype(float) ** 2 + ns.astype(float) ** 3 / 3
   assert np.all(np.diff(costs) <= 0)
   assert sorted(hb.order.tolist()) == list(range(50))
-  assert hb.block_threads in (32, 64, 128, 256)
+  groups = hb.groups
+  assert 1 <= len(groups) <= _lib.MAX_GROUPS
+  assert sum(g[1] for g in groups) == 50 and groups[0][0] == 0
+  for (b0, c0, _, _), (b1, _, _, _) in zip(groups, groups[1:]):
+    assert b0 + c0 == b1  # groups tile the processing order
+  for _, _, nt, smem in groups:
+    assert nt in (32, 64, 128, 256) and 0 < smem <= 227 * 1024
   assert hb.workspace_bytes >= 256
-  assert np.all(np.diff(hb.inst["ws_off"]) >= 0)
+
+
+def test_plan_large_instance_spills_to_global(lib):
+  a = np.ones((400, 300))
+  hb = batch.HostBatch([batch.DenseProblem(a, np.ones(400), np.ones(300), 10)],
+                       batch.SolveOptions())
+  assert hb.workspace_bytes > 8 * 400 * 300  # A (and the rest) in the global workspace
 
 
 def test_plan_rejects_bad_instances(lib):
   inst = np.zeros(1, dtype=_lib.INSTANCE_DTYPE)
   inst["n"], inst["m"], inst["z"] = 3, 2, 2  # z == m: no inequality
   order = np.zeros(1, dtype=np.int32)
-  nt, sm, ws = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_size_t(0)
+  plan = _lib.BatchPlan()
   opts = batch.SolveOptions().to_c()
   rc = lib.qtqp_dense_batch_plan(inst.ctypes.data, 1, ctypes.byref(opts), order.ctypes.data,
-                                 ctypes.byref(nt), ctypes.byref(sm), ctypes.byref(ws))
+                                 0, 0, ctypes.byref(plan))
   assert rc == _lib.QTQP_ERR_BAD_ARG
   assert b"0 <= z < m" in lib.qtqp_last_error()
+  rc = lib.qtqp_dense_batch_plan(inst.ctypes.data, 1, ctypes.byref(opts), order.ctypes.data,
+                                 96, 0, ctypes.byref(plan))
+  assert rc == _lib.QTQP_ERR_BAD_ARG
 
 
 def test_kkt_workspace_size(lib):

@@ -125,8 +125,8 @@ def test_known_answers_and_edge_shapes():
   sol = _solve(sp.csc_matrix([[-1.0], [1.0]]), np.array([0.0, 2.0]), np.array([-1.0]), 0,
                sp.csc_matrix([[1.0]]))
   np.testing.assert_allclose(sol.x, [1.0], atol=1e-5)
-  # LP (p=None) equals explicit zero P.
-  a, b, c, z, _ = problems.feasible(30, 20, 3, 42)
+  # LP (p=None) equals explicit zero P (c built for P = 0 so the LP is bounded).
+  a, b, c, z, _ = problems.feasible(30, 20, 3, 42, lp=True)
   s1 = qb.QTQP(a=a, b=b, c=c, z=z).solve(verbose=False)
   s2 = qb.QTQP(a=a, b=b, c=c, z=z, p=sp.csc_matrix((20, 20))).solve(verbose=False)
   assert s1.status == s2.status == qb.SolutionStatus.SOLVED

@@ -1,0 +1,156 @@
+"""Host-side logic that runs without a GPU: input validation and presolve
+(src/qtqp/__init__.py:183-297), the enum surface, the DirectKktSolver driver
+(direct.py:112-311) with a CPU test double standing in for the GPU backend,
+and the conversion of device stats records into the reference's dicts."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import qtqp_b200 as qb
+from oracle import qtqp_oracle as orc
+from qtqp_b200 import batch, direct, problems
+
+
+def test_enum_surface():
+  assert qb.LinearSolver.AUTO.value == "auto"
+  assert qb.LinearSolver.CUDA.value is direct.CudaDenseSolver
+  assert {s.value for s in qb.SolutionStatus} == {
+      "solved", "infeasible", "unbounded", "hit_max_iter", "failed", "unfinished"}
+
+
+def test_validation_errors():
+  a, b, c, z, p = problems.feasible(6, 5, 3, 742)
+  with pytest.raises(ValueError):
+    qb.QTQP(a=a, b=np.zeros(7), c=c, z=z, p=p)
+  with pytest.raises(ValueError):
+    qb.QTQP(a=a, b=b, c=np.zeros(7), z=z, p=p)
+  with pytest.raises(ValueError):
+    qb.QTQP(a=a, b=b, c=c, z=z, p=sp.csc_matrix(np.ones((6, 5))))
+  with pytest.raises(ValueError):
+    qb.QTQP(a=a, b=b, c=c, z=-1, p=p)
+  with pytest.raises(ValueError):
+    qb.QTQP(a=a, b=b, c=c, z=7, p=p)
+  with pytest.raises(TypeError):
+    qb.QTQP(a=a.tocsr(), b=b, c=c, z=z, p=p)
+  with pytest.raises(TypeError):
+    qb.QTQP(a=a, b=b, c=c, z=z, p=p.tocsr())
+  with pytest.raises(ValueError, match="symmetric"):
+    qb.QTQP(a=sp.eye(2, format="csc"), b=np.ones(2), c=np.zeros(2), z=0,
+            p=sp.csc_matrix([[1.0, 2.0], [0.0, 1.0]]))
+  with pytest.raises(ValueError, match="finite"):
+    qb.QTQP(a=sp.eye(2, format="csc"), b=np.ones(2), c=np.zeros(2), z=0,
+            p=sp.csc_matrix([[1.0, np.nan], [np.nan, 1.0]]))
+  with pytest.raises(ValueError, match="Equality RHS entries"):
+    qb.QTQP(a=sp.eye(3, format="csc"), b=np.array([1.0, np.inf, 3.0]), c=np.zeros(3), z=3)
+  with pytest.raises(ValueError, match="effective z == m"):
+    qb.QTQP(a=sp.eye(3, format="csc"), b=np.ones(3), c=np.zeros(3), z=3)
+
+
+def test_presolve_drops_and_restores_rows():
+  a, b, c, z, p = problems.feasible(20, 10, 3, 7)
+  extra = sp.csc_matrix(np.ones((3, 10)))
+  a2 = sp.vstack([a, extra], format="csc")
+  b2 = np.concatenate([b, [1e21, np.inf, 1e20]])
+  q = qb.QTQP(a=a2, b=b2, c=c, z=z, p=p)
+  assert q.m == 20 and q.a.shape == (20, 10)
+  y, s = q._postsolve(np.arange(20.0), np.arange(20.0), s_dropped=np.array([7.0, 8.0, 9.0]))
+  assert y.shape == (23,) and np.all(y[20:] == 0.0) and np.all(s[20:] == [7, 8, 9])
+  with pytest.raises(ValueError, match="effective z == m"):
+    qb.QTQP(a=a2, b=np.concatenate([b[:3], np.full(20, 1e21)]), c=c, z=3, p=p)
+  with pytest.raises(ValueError, match="Inequality RHS"):
+    qb.QTQP(a=a, b=np.concatenate([b[:19], [-np.inf]]), c=c, z=z, p=p)
+
+
+def test_dense_problem_packing():
+  a, b, c, z, p = problems.config1_instance(3)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  dp = q.dense_problem()
+  np.testing.assert_array_equal(dp.a, a.toarray())
+  np.testing.assert_array_equal(dp.p, p.toarray())
+  assert qb.QTQP(a=a, b=b, c=c, z=z).dense_problem().p is None
+
+
+def test_options_validation():
+  with pytest.raises(AssertionError):
+    batch.SolveOptions(step_size_scale=1.0).validate()
+  with pytest.raises(AssertionError):
+    batch.SolveOptions(max_iterative_refinement_steps=0).validate()
+  with pytest.raises(ValueError):
+    batch.SolveOptions(precision="fp16").validate()
+
+
+def test_diag_data_indices_matches_loop():
+  rng = np.random.default_rng(0)
+  for fmt in ("csc", "csr"):
+    m = sp.random(40, 40, density=0.2, format=fmt, rng=rng) + sp.eye(40, format=fmt)
+    m = m.asformat(fmt)
+    idx = direct.diag_data_indices(m)
+    np.testing.assert_array_equal(m.data[idx], m.diagonal())
+
+
+class _CpuGram(direct.LinearSolver):
+  """CPU test double with the plugin contract (wraps the oracle's backend)."""
+
+  def set_kkt(self, kkt):
+    super().set_kkt(kkt)
+
+  def set_dims(self, n, m, z):
+    self.n, self.m = n, m
+
+  def factorize(self):
+    n = self.n
+    up = self._kkt.tocsr()
+    a = up[:n, n:].T
+    p_up = up[:n, :n]
+    p = p_up + p_up.T - sp.diags(p_up.diagonal())
+    self.be = orc.DenseGramKkt(a, p)
+    self.be.update_diag(self._kkt_diag)
+    self.be.factorize()
+
+  def solve(self, rhs):
+    return self.be.solve(rhs)
+
+  def format(self):
+    return "csr"
+
+
+def test_direct_kkt_solver_host_driver():
+  """DirectKktSolver + a CPU double: the reference's KKT residual criterion."""
+  rng = np.random.default_rng(842)
+  m, n, z = 150, 100, 10
+  a, b, c, _, p = problems.feasible(m, n, z, rng)
+  mu = rng.uniform()
+  s, y = rng.uniform(size=m), rng.uniform(size=m)
+  s[:z] = 0.0
+  d = np.concatenate([np.zeros(z), s[z:] / y[z:]])
+  kkt = direct.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
+                               max_iterative_refinement_steps=10, atol=1e-12, rtol=1e-12,
+                               solver=_CpuGram())
+  kkt.update(mu=mu, s=s, y=y)
+  sol, st = kkt.solve(rhs=np.concatenate([c, b]), warm_start=np.zeros(n + m))
+  assert st["converged"] and st["solves"] >= 1
+  np.testing.assert_allclose(p @ sol[:n] + mu * sol[:n] + a.T @ sol[n:], c, atol=1e-10,
+                             rtol=1e-10)
+  np.testing.assert_allclose(-a @ sol[:n] + (d + mu) * sol[n:], b, atol=1e-10, rtol=1e-10)
+  assert (kkt._kkt - sp.triu(kkt._kkt)).nnz == 0
+
+
+def test_stats_record_conversion_and_log_line(capsys):
+  rec = np.zeros(64)
+  rec[:22] = np.arange(22, dtype=float)
+  rec[18] = 0  # SOLVED
+  for blk in range(3):
+    base = 31 + 7 * blk
+    rec[base:base + 7] = [2, 1e-13, 1.0, 1e-12, 1 if blk else 2, -1 if blk == 0 else 0, 64]
+  d = qb._record_to_dict(rec, True, 0.5)
+  assert d["iter"] == 0 and d["status"] == qb.SolutionStatus.SOLVED
+  assert d["time"] == 19.5
+  assert d["q_lin_sys_stats"]["status"] == "stalled"
+  assert "tau_method" not in d["q_lin_sys_stats"]
+  assert d["predictor_lin_sys_stats"]["tau_method"] == "quadratic"
+  assert d["corrector_lin_sys_stats"]["converged"]
+  assert {"complementarity", "std_s_over_y"} <= d.keys()
+  qb._log_iteration(d)
+  line = capsys.readouterr().out
+  assert line.startswith("|    0 |") and " *, 2, 2 |" in line
