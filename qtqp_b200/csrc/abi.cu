@@ -22,6 +22,23 @@ int cuda_check(cudaError_t err, const char* what) {
 
 }  // namespace qtqp
 
+#ifdef QTQP_PHASE_TIMERS
+namespace qtqp {
+__device__ unsigned long long g_phase_cycles[kNumPhases];
+}
+// Profiling builds only: copies (and clears) the per-phase cycle counters.
+extern "C" int qtqp_phase_cycles(unsigned long long* h_out, int count) {
+  if (count > qtqp::kNumPhases) count = qtqp::kNumPhases;
+  int rc = qtqp::cuda_check(cudaMemcpyFromSymbol(h_out, qtqp::g_phase_cycles,
+                                                 sizeof(unsigned long long) * count),
+                            "cudaMemcpyFromSymbol");
+  if (rc) return rc;
+  unsigned long long zero[qtqp::kNumPhases] = {};
+  return qtqp::cuda_check(cudaMemcpyToSymbol(qtqp::g_phase_cycles, zero, sizeof(zero)),
+                          "cudaMemcpyToSymbol");
+}
+#endif
+
 extern "C" const char* qtqp_last_error(void) { return qtqp::g_last_error.c_str(); }
 
 extern "C" int qtqp_version(void) { return 1; }

@@ -23,6 +23,11 @@ __device__ __forceinline__ double nanmax(double a, double b) {
   return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(a, b);
 }
 
+// The IPM's heavy phases are compiled as separate device functions: each then
+// gets its own register allocation, which keeps the long solve loop's live
+// state from spilling into the phases' inner loops.
+#define QTQP_PHASE __device__ __noinline__
+
 // Largest number of values one fused reduction may carry.
 constexpr int kRedMax = 16;
 
@@ -91,5 +96,33 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+
+// Optional per-phase cycle counters for profiling builds (-DQTQP_PHASE_TIMERS):
+// thread 0 of each block adds the SM cycles spent in a phase to
+// g_phase_cycles[phase].  Default builds compile these to nothing.
+enum Phase : int {
+  kPhLoad = 0, kPhNormalize, kPhGram, kPhChol, kPhSolve, kPhResidual, kPhTau, kPhStep,
+  kPhTerm, kPhOther, kNumPhases
+};
+#ifdef QTQP_PHASE_TIMERS
+extern __device__ unsigned long long g_phase_cycles[kNumPhases];
+#define QTQP_TIC() long long qtqp_t0_ = clock64()
+#define QTQP_RETIC() qtqp_t0_ = clock64()
+#define QTQP_TOC(ph)                                                                   \
+  do {                                                                                 \
+    if (threadIdx.x == 0)                                                              \
+      atomicAdd(&qtqp::g_phase_cycles[ph], (unsigned long long)(clock64() - qtqp_t0_)); \
+  } while (0)
+#else
+#define QTQP_TIC() \
+  do {             \
+  } while (0)
+#define QTQP_RETIC() \
+  do {               \
+  } while (0)
+#define QTQP_TOC(ph) \
+  do {               \
+  } while (0)
+#endif
 
 }  // namespace qtqp

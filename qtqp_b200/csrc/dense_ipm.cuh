@@ -63,7 +63,7 @@ __host__ __device__ inline InstLayout plan_layout(int n, int m, size_t smem_cap)
   L.lda = odd_ld(n);
   L.ldp = odd_ld(n);
   L.ldg = odd_ld(n);
-  L.np = (n + m + 1) & ~1;
+  L.np = (max(n + m, n + 4) + 1) & ~1;  // >= n + 4: pivot broadcast scalars
   L.a_bytes = round16(size_t(m) * L.lda * 8);
   L.p_bytes = round16(size_t(n) * L.ldp * 8);
   L.g_bytes = round16(size_t(n) * L.ldg * 8);
@@ -99,6 +99,20 @@ struct IrOutcome {
   bool nan;
 };
 
+// Copies of the instance's fields as local constants.  Phase functions are
+// not inlined, so `this` points at a stack object; reading fields through it
+// inside loops would be a local-memory load after every store that might
+// alias it.  Each phase therefore starts with QTQP_LOCALS.
+#define QTQP_LOCALS                                                             \
+  const int tid = this->tid, n = this->n, m = this->m, z = this->z, N = this->N; \
+  const int lda = this->lda, ldp = this->ldp, ldg = this->ldg;                   \
+  double* const A = this->A;                                                     \
+  double* const P = this->P;                                                     \
+  double* const G = this->G;                                                     \
+  const bool has_p = this->has_p;                                                \
+  (void)tid; (void)n; (void)m; (void)z; (void)N; (void)lda; (void)ldp; (void)ldg; \
+  (void)A; (void)P; (void)G; (void)has_p
+
 // ----------------------------------------------------------------------------
 // The solver state of one instance, replicated in every thread of the block.
 // ----------------------------------------------------------------------------
@@ -127,6 +141,45 @@ struct DenseIpm {
   // First index >= lo owned by this thread (k % NT == tid).
   __device__ __forceinline__ int own(int lo) const { return lo + ((tid - lo) & (NT - 1)); }
   __device__ __forceinline__ float* g32() const { return reinterpret_cast<float*>(G); }
+
+  // Lanes cooperating on one dot product when K outputs share the block.
+  __device__ __forceinline__ int lanes_for(int K) const {
+    int s = 1;
+    while (s < 32 && K * s * 2 <= NT) s <<= 1;
+    return s;
+  }
+
+  // out_k = sum_{i < len} body(k, i) for k < K, S = lanes_for(K) lanes per
+  // output.  The S lanes of an output are strided across the warp (lane =
+  // s * (32/S) + g) so that neighbouring lanes work on neighbouring outputs;
+  // their partial sums are combined with xor shuffles, and lane s == 0 calls
+  // epi(k, sum).  NACC independent sums per output.  No barrier inside.
+  template <int NACC, bool MAXOP = false, typename Body, typename Epi>
+  __device__ __forceinline__ void rowdot(int K, int len, Body body, Epi epi) const {
+    const int S = lanes_for(K);
+    const int per_warp = 32 / S;
+    const int tid = this->tid;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int s = lane / per_warp, g = lane - s * per_warp;
+    const int per_pass = (NT / 32) * per_warp;
+    for (int k0 = 0; k0 < K; k0 += per_pass) {
+      const int k = k0 + warp * per_warp + g;
+      double acc[NACC];
+#pragma unroll
+      for (int a = 0; a < NACC; ++a) acc[a] = 0.0;
+      if (k < K) {
+        for (int i = s; i < len; i += S) body(k, i, acc);
+      }
+      for (int off = 16; off >= per_warp; off >>= 1) {
+#pragma unroll
+        for (int a = 0; a < NACC; ++a) {
+          const double o = __shfl_xor_sync(0xffffffffu, acc[a], off);
+          acc[a] = MAXOP ? fmax(acc[a], o) : acc[a] + o;
+        }
+      }
+      if (k < K && s == 0) epi(k, acc);
+    }
+  }
   __device__ __forceinline__ float* t32() const { return reinterpret_cast<float*>(vec(kCT)); }
 
   // --------------------------------------------------------------------------
@@ -156,43 +209,49 @@ struct DenseIpm {
   // working copies, bit-compatible with the reference: the nonzero a_ij is
   // multiplied by (d_i * e_j), the clip bounds are [1e-3, 1e3].
   // --------------------------------------------------------------------------
-  __device__ void load_and_equilibrate(bool equilibrate, double& nb, double& nc) {
+  QTQP_PHASE void load_and_equilibrate(bool equilibrate, double& nb, double& nc) {
+    QTQP_LOCALS;
     double* de = vec(kDE);
     double* sc = vec(kTMP);  // per-sweep [e_i; d_i]
-    for (int idx = tid; idx < m * n; idx += NT) {
-      const int i = idx / n, j = idx - i * n;
-      A[i * lda + j] = A0[idx];
-    }
-    for (int idx = tid; idx < n * n; idx += NT) {
-      const int i = idx / n, j = idx - i * n;
-      P[i * ldp + j] = has_p ? P0[idx] : 0.0;
-    }
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NW = NT / 32;
+    for (int i = warp; i < m; i += NW)
+      for (int j = lane; j < n; j += 32) A[i * lda + j] = A0[size_t(i) * n + j];
+    for (int i = warp; i < n; i += NW)
+      for (int j = lane; j < n; j += 32) P[i * ldp + j] = has_p ? P0[size_t(i) * n + j] : 0.0;
     for (int k = tid; k < N; k += NT) de[k] = 1.0;
     group_sync<NT>();
     if (equilibrate) {
+      const double* Ap = A;
+      const double* Pp = P;
+      const int la = lda, lp = ldp, mm = m, nn = n;
+      const int plen = has_p ? n : 0;
+      auto scale_of = [](double mx) {
+        if (mx == 0.0) mx = 1.0;
+        return fmin(fmax(1.0 / sqrt(mx), 1e-3), 1e3);
+      };
       for (int sweep = 0; sweep < 10; ++sweep) {
-        for (int k = tid; k < N; k += NT) {
-          double mx = 0.0;
-          if (k < n) {  // column k: max over A's column and P's column
-            for (int i = 0; i < m; ++i) mx = fmax(mx, fabs(A[i * lda + k]));
-            if (has_p)
-              for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(P[i * ldp + k]));
-          } else {  // row k - n of A
-            const double* row = A + (k - n) * lda;
-            for (int j = 0; j < n; ++j) mx = fmax(mx, fabs(row[j]));
-          }
-          if (mx == 0.0) mx = 1.0;
-          sc[k] = fmin(fmax(1.0 / sqrt(mx), 1e-3), 1e3);
-        }
+        // Column maxima over A and P, row maxima over A.
+        rowdot<1, true>(n, m + plen,
+                        [&](int k, int i, double* acc) {
+                          const double v = i < mm ? Ap[i * la + k] : Pp[(i - mm) * lp + k];
+                          acc[0] = fmax(acc[0], fabs(v));
+                        },
+                        [&](int k, double* acc) { sc[k] = scale_of(acc[0]); });
+        rowdot<1, true>(m, n,
+                        [&](int k, int j, double* acc) {
+                          acc[0] = fmax(acc[0], fabs(Ap[k * la + j]));
+                        },
+                        [&](int k, double* acc) { sc[nn + k] = scale_of(acc[0]); });
         group_sync<NT>();
-        for (int idx = tid; idx < m * n; idx += NT) {
-          const int i = idx / n, j = idx - i * n;
-          A[i * lda + j] *= sc[n + i] * sc[j];
+        for (int i = warp; i < m; i += NW) {
+          const double di = sc[n + i];
+          for (int j = lane; j < n; j += 32) A[i * lda + j] *= di * sc[j];
         }
         if (has_p) {
-          for (int idx = tid; idx < n * n; idx += NT) {
-            const int i = idx / n, j = idx - i * n;
-            P[i * ldp + j] *= sc[i] * sc[j];
+          for (int i = warp; i < n; i += NW) {
+            const double ei = sc[i];
+            for (int j = lane; j < n; j += 32) P[i * ldp + j] *= ei * sc[j];
           }
         }
         for (int k = tid; k < N; k += NT) de[k] *= sc[k];
@@ -227,6 +286,7 @@ struct DenseIpm {
   // Owner-wise; the caller synchronises before factorising.
   // --------------------------------------------------------------------------
   __device__ void kkt_diag(double mu, double min_reg) {
+    QTQP_LOCALS;
     const double* xy = vec(kXY);
     const double* s = vec(kRS);
     const double* pi = vec(kPI);
@@ -259,6 +319,7 @@ struct DenseIpm {
 
   // Same for an externally supplied diagonal (the plugin's update_diag).
   __device__ void kkt_diag_given(const double* diag) {
+    QTQP_LOCALS;
     double* reg = vec(kREG);
     double* piw = vec(kPI);
     double* pw = vec(kPW);
@@ -277,9 +338,162 @@ struct DenseIpm {
   // factorize (solvers_dense.py:99-116): G = P_off + diag(Rx) + A_s^T A_s with
   // A_s = diag(1/sqrt(Ry)) A, a relative diagonal jitter, then Cholesky.
   // Returns 0 or the 1-based index of the first non-positive pivot.
+  // Small n: the register-tiled path; otherwise Gram into memory + cholesky.
   // --------------------------------------------------------------------------
   template <typename T>
-  __device__ int factorize() {
+  QTQP_PHASE int factorize() {
+    const int nb = (n + 3) >> 2;
+    if (nb * (nb + 1) / 2 <= NT) return factorize_regs<T>();
+    return factorize_mem<T>();
+  }
+
+  // One thread per 4x4 tile of the lower triangle of G: the tile is formed
+  // in registers by the Gram product, and the Cholesky runs on the registers.
+  // Column k (as left by step k-1) is broadcast through a double-buffered
+  // vector in memory together with its pivot d, 1/d and sqrt(d); each step is
+  // one barrier and 16 independent FMAs per thread:
+  //   g_ij -= g_ik g_jk / d   (j > k),   l_ik = g_ik / sqrt(d),  l_kk = sqrt(d).
+  // The finished L is written to G for the solves.
+  template <typename T>
+  __device__ int factorize_regs() {
+    QTQP_LOCALS;
+    QTQP_TIC();
+    T* g = reinterpret_cast<T*>(G);
+    const double* reg = vec(kREG);
+    const double* wsc = vec(kPW);
+    const int nb = (n + 3) >> 2;
+    const int tiles = nb * (nb + 1) / 2;
+    const bool mine = tid < tiles;
+    int bi = 0, bj = 0;
+    if (mine) {
+      bi = int((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
+      while (bi * (bi + 1) / 2 > tid) --bi;
+      while ((bi + 1) * (bi + 2) / 2 <= tid) ++bi;
+      bj = tid - bi * (bi + 1) / 2;
+    }
+    const int i0 = bi * 4, j0 = bj * 4;
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+    if (mine) {
+      for (int r = 0; r < m; ++r) {
+        const double w = wsc[n + r];
+        const double* row = A + r * lda;
+        T ai[4], aj[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          ai[a] = (i0 + a < n) ? T(row[i0 + a] * w) : T(0);
+          aj[a] = (j0 + a < n) ? T(row[j0 + a] * w) : T(0);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(ai[a], aj[b], acc[a][b]);
+      }
+    }
+    double dmax[1] = {0.0};
+    double dummy[1] = {0.0};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int i = i0 + a, j = j0 + b;
+        if (mine && i < n && j <= i) {
+          double base = P[i * ldp + j];
+          if (i == j) base += reg[i];
+          acc[a][b] = T(base) + acc[a][b];
+          if (i == j) dmax[0] = nanmax(dmax[0], double(acc[a][b]));
+        }
+      }
+    }
+    block_reduce<NT, 0, 1>(dummy, dmax, red, phase);
+    const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+      if (mine && bi == bj && i0 + a < n) acc[a][a] = T(double(acc[a][a]) + jit);
+    QTQP_TOC(kPhGram);
+    QTQP_RETIC();
+    // Broadcast buffers: column k (as left by step k-1) at [0, n).
+    T* buf0 = reinterpret_cast<T*>(vec(kW));
+    T* buf1 = reinterpret_cast<T*>(vec(kTMP));
+    auto publish = [&](int k, T* buf) {
+      if (!mine || bj != (k >> 2)) return;
+      const int c = k & 3;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = i0 + a;
+        if (i >= k && i < n) {
+          T v = acc[a][0];  // acc[a][c] without a run-time register index
+#pragma unroll
+          for (int b = 1; b < 4; ++b)
+            if (b == c) v = acc[a][b];
+          buf[i] = v;
+        }
+      }
+    };
+    publish(0, buf0);
+    group_sync<NT>();
+    int info = 0;
+    for (int k = 0; k < n; ++k) {
+      T* buf = (k & 1) ? buf1 : buf0;
+      const T d = buf[k];
+      if (!(d > T(0))) {
+        info = k + 1;
+        break;
+      }
+      // Every thread derives the pivot scalars itself (no divide on the
+      // critical path): 1/sqrt(d), 1/d = (1/sqrt(d))^2.
+      const T il = rsqrt(d);
+      if (mine && j0 + 3 > k) {
+        const T inv_d = il * il;
+        T ci[4], cj[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          ci[a] = (i0 + a < n && i0 + a > k) ? buf[i0 + a] : T(0);
+          cj[a] = (j0 + a < n && j0 + a > k) ? buf[j0 + a] * inv_d : T(0);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(-ci[a], cj[b], acc[a][b]);
+      }
+      if (mine && bj == (k >> 2)) {  // finish column k; the diagonal keeps 1/l_kk
+        const int c = k & 3;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int i = i0 + a;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            if (b != c) continue;
+            if (i == k) acc[a][b] = il;
+            else if (i > k) acc[a][b] *= il;
+          }
+        }
+      }
+      if (k + 1 < n) publish(k + 1, (k & 1) ? buf0 : buf1);
+      group_sync<NT>();
+    }
+    if (info == 0 && mine) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int i = i0 + a, j = j0 + b;
+          if (i < n && j <= i) g[i * ldg + j] = acc[a][b];
+        }
+    }
+    group_sync<NT>();
+    if (info == 0) invert_diag_blocks<T>(g);
+    QTQP_TOC(kPhChol);
+    return info;
+  }
+
+  template <typename T>
+  __device__ int factorize_mem() {
+    QTQP_LOCALS;
+    QTQP_TIC();
     T* g = reinterpret_cast<T*>(G);
     const double* reg = vec(kREG);
     const double* wsc = vec(kPW);
@@ -334,41 +548,60 @@ struct DenseIpm {
     const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
     for (int k = tid; k < n; k += NT) g[k * ldg + k] = T(double(g[k * ldg + k]) + jit);
     group_sync<NT>();
-    return cholesky<T>(g);
+    QTQP_TOC(kPhGram);
+    QTQP_RETIC();
+    const int info = cholesky<T>(g);
+    QTQP_TOC(kPhChol);
+    return info;
   }
 
   // Right-looking Cholesky of the lower triangle, two barriers per column;
   // afterwards every 32x32 diagonal block of L is replaced by its inverse so
   // that the triangular solves are block-parallel (see chol_solve).
+  //
+  // One barrier per column: phase k updates the trailing matrix with the
+  // still-unscaled column k (a_ij -= a_ik a_jk / d_k) and, independently,
+  // finishes column k-1 (l_ik = a_ik / sqrt(d_{k-1}), l_kk = sqrt(d_{k-1})),
+  // which phase k does not read.
   template <typename T>
-  __device__ int cholesky(T* g) {
+  QTQP_PHASE int cholesky(T* g) {
+    QTQP_LOCALS;
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    for (int k = 0; k < n; ++k) {
+    T d_prev = T(1);
+    for (int k = 0; k <= n; ++k) {
+      if (k > 0) {  // finish column k-1
+        const T lkk = sqrt(d_prev);
+        const T inv = T(1) / lkk;
+        for (int i = k + tid; i < n; i += NT) g[i * ldg + k - 1] *= inv;
+        if (tid == NT - 1) g[(k - 1) * ldg + k - 1] = inv;  // diagonal keeps 1/l_kk
+      }
+      if (k == n) break;
       const T d = g[k * ldg + k];
       if (!(d > T(0))) {
         group_sync<NT>();
         return k + 1;
       }
-      const T lkk = sqrt(d);
-      for (int i = k + 1 + tid; i < n; i += NT) g[i * ldg + k] /= lkk;
-      group_sync<NT>();
-      if (tid == 0) g[k * ldg + k] = lkk;
+      const T inv_d = T(1) / d;
       for (int j = k + 1 + warp; j < n; j += NW) {
-        const T ljk = g[j * ldg + k];
-        for (int i = j + lane; i < n; i += 32) g[i * ldg + j] -= g[i * ldg + k] * ljk;
+        const T t = g[j * ldg + k] * inv_d;
+        for (int i = j + lane; i < n; i += 32) g[i * ldg + j] = fma(-g[i * ldg + k], t, g[i * ldg + j]);
       }
+      d_prev = d;
       group_sync<NT>();
     }
+    group_sync<NT>();
     invert_diag_blocks<T>(g);
     return 0;
   }
 
   // In-place inverse of each 32x32 lower-triangular diagonal block of L, one
   // warp per block, column by column from the last: for i > j,
-  // X_ij = -(sum_{j<k<=i} X_ik L_kj) / L_jj, X_jj = 1 / L_jj.
+  // X_ij = -(sum_{j<k<=i} X_ik L_kj) / L_jj, X_jj = 1 / L_jj.  Both Cholesky
+  // variants already store 1 / L_jj on the diagonal.
   template <typename T>
-  __device__ void invert_diag_blocks(T* g) {
+  QTQP_PHASE void invert_diag_blocks(T* g) {
+    QTQP_LOCALS;
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
     const int nblk = (n + 31) >> 5;
@@ -376,15 +609,19 @@ struct DenseIpm {
       const int kb = blk * 32, bs = min(32, n - kb);
       T* L = g + kb * ldg + kb;
       for (int j = bs - 1; j >= 0; --j) {
-        const T inv_jj = T(1) / L[j * ldg + j];
-        T w = T(0);
+        const T inv_jj = L[j * ldg + j];  // the factor's diagonal holds 1 / L_jj
+        T w0 = T(0), w1 = T(0);
         if (lane > j && lane < bs) {
           const T* row = L + lane * ldg;
-          for (int k = j + 1; k <= lane; ++k) w = fma(row[k], L[k * ldg + j], w);
+          int k = j + 1;
+          for (; k + 1 <= lane; k += 2) {
+            w0 = fma(row[k], L[k * ldg + j], w0);
+            w1 = fma(row[k + 1], L[(k + 1) * ldg + j], w1);
+          }
+          if (k <= lane) w0 = fma(row[k], L[k * ldg + j], w0);
         }
         __syncwarp();
-        if (lane > j && lane < bs) L[lane * ldg + j] = -w * inv_jj;
-        if (lane == j) L[j * ldg + j] = inv_jj;
+        if (lane > j && lane < bs) L[lane * ldg + j] = -(w0 + w1) * inv_jj;
         __syncwarp();
       }
     }
@@ -395,7 +632,8 @@ struct DenseIpm {
   // z_b = X_bb (v_b - sum_{c<b} L_bc z_c), backward x_b = X_bb^T (z_b -
   // sum_{c>b} L_cb^T x_c), two barriers per 32-block; w is n scratch entries.
   template <typename T>
-  __device__ void chol_solve(const T* g, T* v, T* w) {
+  QTQP_PHASE void chol_solve(const T* g, T* v, T* w) {
+    QTQP_LOCALS;
     const int nblk = (n + 31) >> 5;
     for (int blk = 0; blk < nblk; ++blk) {
       const int kb = blk * 32, bs = min(32, n - kb);
@@ -437,75 +675,129 @@ struct DenseIpm {
 
   // --------------------------------------------------------------------------
   // Backend solve (solvers_dense.py:130-142): out (+)= K_reg^{-1} r.
-  // Entry: r complete (barrier passed).  Exit: out written owner-wise.
+  // Entry: r complete (barrier passed).  Exit: out written (barrier needed
+  // before other threads read it).
   // --------------------------------------------------------------------------
-  __device__ void kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
+  QTQP_PHASE void kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
+    QTQP_LOCALS;
+    QTQP_TIC();
     const double* iry = vec(kPI);
     double* tmp = vec(kTMP);
     float* t32 = this->t32();
-    for (int k = tid; k < n; k += NT) {
-      double acc = 0.0;
-      for (int i = 0; i < m; ++i) acc = fma(A[i * lda + k], iry[n + i] * r[n + i], acc);
-      const double g = r[k] + acc;
-      if (fp64) {
-        tmp[k] = g;
-      } else {
-        t32[k] = float(g);
-      }
-    }
+    const double* Ap = A;
+    const int ld = lda, nn = n;
+    // g = r_x + A^T (r_y / Ry)
+    rowdot<1>(n, m,
+              [&](int k, int i, double* acc) {
+                acc[0] = fma(Ap[i * ld + k], iry[nn + i] * r[nn + i], acc[0]);
+              },
+              [&](int k, double* acc) {
+                const double g = r[k] + acc[0];
+                if (fp64) {
+                  tmp[k] = g;
+                } else {
+                  t32[k] = float(g);
+                }
+              });
     group_sync<NT>();
     if (fp64) {
       chol_solve<double>(G, tmp, vec(kW));
     } else {
       chol_solve<float>(g32(), t32, t32 + n);
     }
-    for (int k = tid; k < N; k += NT) {
-      double val;
-      if (k < n) {
-        val = fp64 ? tmp[k] : double(t32[k]);
-      } else {
-        const double* row = A + (k - n) * lda;
-        double ax = 0.0;
-        if (fp64) {
-          for (int j = 0; j < n; ++j) ax = fma(row[j], tmp[j], ax);
-        } else {
-          for (int j = 0; j < n; ++j) ax = fma(row[j], double(t32[j]), ax);
-        }
-        val = iry[k] * (ax - r[k]);
-      }
+    for (int k = tid; k < n; k += NT) {
+      const double val = fp64 ? tmp[k] : double(t32[k]);
       out[k] = accumulate ? out[k] + val : val;
     }
+    // y = (A x - r_y) / Ry
+    rowdot<1>(m, n,
+              [&](int k, int j, double* acc) {
+                const double xj = fp64 ? tmp[j] : double(t32[j]);
+                acc[0] = fma(Ap[k * ld + j], xj, acc[0]);
+              },
+              [&](int k, double* acc) {
+                const double val = iry[nn + k] * (acc[0] - r[nn + k]);
+                out[nn + k] = accumulate ? out[nn + k] + val : val;
+              });
+    QTQP_TOC(kPhSolve);
   }
 
-  // K_reg v for owner k (solvers_dense.py:118-128).  Reads all of v.
-  __device__ __forceinline__ double kkt_row(const double* v, int k) const {
+  // res = krhs - K_reg v + corr o v (direct.py:256, 266 with the matvec of
+  // solvers_dense.py:118-128).  Reads all of v; returns this thread's partial
+  // max |res| and NaN flag of v (combined by the caller's reduction).
+  QTQP_PHASE void kkt_residual(const double* v, const double* krhs, double* res, double& mres,
+                               double& vnan) const {
+    QTQP_LOCALS;
     const double* reg = vec(kREG);
-    if (k < n) {
-      double t = 0.0;
-      if (has_p)
-        for (int j = 0; j < n; ++j) t = fma(P[j * ldp + k], v[j], t);
-      t += reg[k] * v[k];
-      double u = 0.0;
-      for (int i = 0; i < m; ++i) u = fma(A[i * lda + k], v[n + i], u);
-      return t + u;
-    }
-    const double* row = A + (k - n) * lda;
-    double t = 0.0;
-    for (int j = 0; j < n; ++j) t = fma(row[j], v[j], t);
-    return t - (-reg[k]) * v[k];
+    const double* corr = vec(kCORR);
+    const double* Ap = A;
+    const double* Pp = P;
+    const int la = lda, lp = ldp, nn = n, mm = m;
+    const int plen = has_p ? n : 0;
+    rowdot<2>(n, m + plen,
+              [&](int k, int i, double* acc) {
+                if (i < mm) {
+                  acc[1] = fma(Ap[i * la + k], v[nn + i], acc[1]);
+                } else {
+                  acc[0] = fma(Pp[(i - mm) * lp + k], v[i - mm], acc[0]);
+                }
+              },
+              [&](int k, double* acc) {
+                double t = acc[0];
+                t += reg[k] * v[k];
+                const double kv = t + acc[1];
+                const double rk = krhs[k] - kv + corr[k] * v[k];
+                res[k] = rk;
+                mres = nanmax(mres, fabs(rk));
+                vnan = fmax(vnan, (v[k] != v[k]) ? 1.0 : 0.0);
+              });
+    rowdot<1>(m, n,
+              [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], v[j], acc[0]); },
+              [&](int k, double* acc) {
+                const int kk = nn + k;
+                const double kv = acc[0] - (-reg[kk]) * v[kk];
+                const double rk = krhs[kk] - kv + corr[kk] * v[kk];
+                res[kk] = rk;
+                mres = nanmax(mres, fabs(rk));
+                vnan = fmax(vnan, (v[kk] != v[kk]) ? 1.0 : 0.0);
+              });
+  }
+
+  // K_reg x (solvers_dense.py:118-128), written to out.
+  __device__ void kkt_matvec(const double* v, double* out) const {
+    QTQP_LOCALS;
+    const double* reg = vec(kREG);
+    const double* Ap = A;
+    const double* Pp = P;
+    const int la = lda, lp = ldp, nn = n, mm = m;
+    rowdot<2>(n, m + n,
+              [&](int k, int i, double* acc) {
+                if (i < mm) {
+                  acc[1] = fma(Ap[i * la + k], v[nn + i], acc[1]);
+                } else {
+                  acc[0] = fma(Pp[(i - mm) * lp + k], v[i - mm], acc[0]);
+                }
+              },
+              [&](int k, double* acc) {
+                double t = acc[0];
+                t += reg[k] * v[k];
+                out[k] = t + acc[1];
+              });
+    rowdot<1>(m, n,
+              [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], v[j], acc[0]); },
+              [&](int k, double* acc) { out[nn + k] = acc[0] - (-reg[nn + k]) * v[nn + k]; });
   }
 
   // --------------------------------------------------------------------------
   // DirectKktSolver.solve (direct.py:218-307).  `rhs_k(k)` produces the
-  // un-negated right-hand side element k; `sol` holds the warm start and
-  // receives the solution.  Entry: sol complete (barrier passed).
+  // un-negated right-hand side element k (owner-wise); `sol` holds the warm
+  // start and receives the solution.  Entry: sol complete (barrier passed).
   // --------------------------------------------------------------------------
   template <typename RhsF>
-  __device__ IrOutcome ir_solve(RhsF rhs_k, double* sol, bool fp64) {
+  QTQP_PHASE IrOutcome ir_solve(RhsF rhs_k, double* sol, bool fp64) {
     const qtqp_options& op = *o;
     double* krhs = vec(kRHS);
     double* res = vec(kRES);
-    const double* corr = vec(kCORR);
     double dummy[1] = {0.0};
     IrOutcome out;
     {
@@ -514,13 +806,14 @@ struct DenseIpm {
         double r = rhs_k(k);
         if (k >= n) r = -r;
         krhs[k] = r;
-        const double rk = r - kkt_row(sol, k) + corr[k] * sol[k];
-        res[k] = rk;
         mx[0] = nanmax(mx[0], fabs(r));
-        mx[1] = nanmax(mx[1], fabs(rk));
       }
+      group_sync<NT>();
+      QTQP_TIC();
+      kkt_residual(sol, krhs, res, mx[1], mx[2]);
       block_reduce<NT, 0, 3>(dummy, mx, red, phase);
       group_sync<NT>();
+      QTQP_TOC(kPhResidual);
       out.rhs_norm = mx[0];
       out.final_res = mx[1];
     }
@@ -534,15 +827,12 @@ struct DenseIpm {
       const double prev = rn;
       kkt_solve(res, sol, true, fp64);
       group_sync<NT>();
+      QTQP_TIC();
       double mx[2] = {0.0, 0.0};
-      for (int k = tid; k < N; k += NT) {
-        const double rk = krhs[k] - kkt_row(sol, k) + corr[k] * sol[k];
-        res[k] = rk;
-        mx[0] = nanmax(mx[0], fabs(rk));
-        mx[1] = fmax(mx[1], (sol[k] != sol[k]) ? 1.0 : 0.0);
-      }
+      kkt_residual(sol, krhs, res, mx[0], mx[1]);
       block_reduce<NT, 0, 2>(dummy, mx, red, phase);
       group_sync<NT>();
+      QTQP_TOC(kPhResidual);
       rn = mx[0];
       out.nan = mx[1] > 0.0;
       if (rn < out.tol) {
@@ -597,9 +887,10 @@ struct DenseIpm {
     double pxkq;   // P x . (K^{-1}q)_x
   };
 
-  __device__ double tau_step(const double* kr, const IrOutcome& irr, double mu, double mu_t,
+  QTQP_PHASE double tau_step(const double* kr, const IrOutcome& irr, double mu, double mu_t,
                              double r_tau, double tau, double tau_anchor, const IterConsts& ic,
                              int& method) {
+    QTQP_LOCALS;
     const double* q = vec(kQ);
     const double* kq = vec(kKQ);
     const double* pkq = vec(kPW);
@@ -608,18 +899,19 @@ struct DenseIpm {
     double* pkr = vec(kRS);
     double sm[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // kr.q, kr.Pkq, kq.Pkr, kr.Pkr, Px.kr
     double dummy[1] = {0.0};
-    for (int k = tid; k < N; k += NT) {
-      sm[0] = fma(kr[k], q[k], sm[0]);
-      if (k < n && has_p) {
-        double t = 0.0;
-        for (int j = 0; j < n; ++j) t = fma(P[j * ldp + k], kr[j], t);
-        t = fma(pi[k], kr[k], t);
-        pkr[k] = t;
-        sm[1] = fma(kr[k], pkq[k], sm[1]);
-        sm[2] = fma(kq[k], t, sm[2]);
-        sm[3] = fma(kr[k], t, sm[3]);
-        sm[4] = fma(px[k], kr[k], sm[4]);
-      }
+    for (int k = tid; k < N; k += NT) sm[0] = fma(kr[k], q[k], sm[0]);
+    if (has_p) {
+      const double* Pp = P;
+      const int lp = ldp;
+      rowdot<1>(n, n, [&](int k, int j, double* acc) { acc[0] = fma(Pp[j * lp + k], kr[j], acc[0]); },
+                [&](int k, double* acc) {
+                  const double t = fma(pi[k], kr[k], acc[0]);
+                  pkr[k] = t;
+                  sm[1] = fma(kr[k], pkq[k], sm[1]);
+                  sm[2] = fma(kq[k], t, sm[2]);
+                  sm[3] = fma(kr[k], t, sm[3]);
+                  sm[4] = fma(px[k], kr[k], sm[4]);
+                });
     }
     block_reduce<NT, 5, 0>(sm, dummy, red, phase);
     const bool accurate = irr.status == 1 || irr.final_res < 1e-7;
@@ -676,6 +968,7 @@ struct DenseIpm {
   // the step (dy, ds) given owner-wise by `dir(k, dy, ds)`.
   template <typename DirF>
   __device__ double step_to_boundary(DirF dir) {
+    QTQP_LOCALS;
     const double* xy = vec(kXY);
     const double* s = vec(kRS);
     double mx[1] = {-1.0};  // max of -alpha candidates == -(min alpha)
@@ -695,7 +988,8 @@ struct DenseIpm {
   // computed from the equilibrated products: A_o x_o = (A_eq x)/d,
   // A_o^T y_o = (A_eq^T y)/e, P_o x_o = (P_eq x)/e.
   // --------------------------------------------------------------------------
-  __device__ int termination(double tau, double nb, double nc, double* st, bool collect) {
+  QTQP_PHASE int termination(double tau, double nb, double nc, double* st, bool collect) {
+    QTQP_LOCALS;
     const qtqp_options& op = *o;
     const double* xy = vec(kXY);
     const double* s = vec(kRS);
@@ -705,40 +999,46 @@ struct DenseIpm {
     // sums: ctx, bty, xpx ; maxes: pres, dres, |aty|, |px|, |ax+s|, |ax|, |s|, |x|, |y|
     double sm[3] = {0.0, 0.0, 0.0};
     double mx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int k = tid; k < N; k += NT) {
-      if (k < n) {
-        double aty = 0.0;
-        for (int i = 0; i < m; ++i) aty = fma(A[i * lda + k], xy[n + i], aty);
-        aty /= de[k];
-        double px = 0.0;
-        if (has_p) {
-          for (int j = 0; j < n; ++j) px = fma(P[j * ldp + k], xy[j], px);
-          px = fma(pi[k], xy[k], px);
-          px /= de[k];
-        }
-        const double xo = de[k] * xy[k];
-        sm[0] = fma(c0[k], xo, sm[0]);
-        sm[2] = fma(xo, px, sm[2]);
-        mx[1] = nanmax(mx[1], fabs((px + aty) * inv_tau + c0[k]));
-        mx[2] = nanmax(mx[2], fabs(aty));
-        mx[3] = nanmax(mx[3], fabs(px));
-        mx[7] = nanmax(mx[7], fabs(xo));
-      } else {
-        const double* row = A + (k - n) * lda;
-        double ax = 0.0;
-        for (int j = 0; j < n; ++j) ax = fma(row[j], xy[j], ax);
-        ax /= de[k];
-        const double yo = de[k] * xy[k];
-        const double so = s[k] / de[k];
-        const double bo = b0[k - n];
-        sm[1] = fma(bo, yo, sm[1]);
-        mx[0] = nanmax(mx[0], fabs((ax + so) * inv_tau - bo));
-        mx[4] = nanmax(mx[4], fabs(ax + so));
-        mx[5] = nanmax(mx[5], fabs(ax));
-        mx[6] = nanmax(mx[6], fabs(so));
-        mx[8] = nanmax(mx[8], fabs(yo));
-      }
-    }
+    const double* Ap = A;
+    const double* Pp = P;
+    const int la = lda, lp = ldp, nn = n, mm = m;
+    const int plen = has_p ? n : 0;
+    const bool hp = has_p;
+    const double* b0p = b0;
+    const double* c0p = c0;
+    rowdot<2>(n, m + plen,
+              [&](int k, int i, double* acc) {
+                if (i < mm) {
+                  acc[0] = fma(Ap[i * la + k], xy[nn + i], acc[0]);
+                } else {
+                  acc[1] = fma(Pp[(i - mm) * lp + k], xy[i - mm], acc[1]);
+                }
+              },
+              [&](int k, double* acc) {
+                const double aty = acc[0] / de[k];
+                const double px = hp ? fma(pi[k], xy[k], acc[1]) / de[k] : 0.0;
+                const double xo = de[k] * xy[k];
+                sm[0] = fma(c0p[k], xo, sm[0]);
+                sm[2] = fma(xo, px, sm[2]);
+                mx[1] = nanmax(mx[1], fabs((px + aty) * inv_tau + c0p[k]));
+                mx[2] = nanmax(mx[2], fabs(aty));
+                mx[3] = nanmax(mx[3], fabs(px));
+                mx[7] = nanmax(mx[7], fabs(xo));
+              });
+    rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], xy[j], acc[0]); },
+              [&](int k, double* acc) {
+                const int kk = nn + k;
+                const double ax = acc[0] / de[kk];
+                const double yo = de[kk] * xy[kk];
+                const double so = s[kk] / de[kk];
+                const double bo = b0p[k];
+                sm[1] = fma(bo, yo, sm[1]);
+                mx[0] = nanmax(mx[0], fabs((ax + so) * inv_tau - bo));
+                mx[4] = nanmax(mx[4], fabs(ax + so));
+                mx[5] = nanmax(mx[5], fabs(ax));
+                mx[6] = nanmax(mx[6], fabs(so));
+                mx[8] = nanmax(mx[8], fabs(yo));
+              });
     block_reduce<NT, 3, 9>(sm, mx, red, phase);
     const double ctx = sm[0], bty = sm[1], xpx = has_p ? sm[2] : 0.0;
     const double pcost = (ctx + 0.5 * xpx * inv_tau) * inv_tau;
@@ -857,7 +1157,11 @@ struct DenseIpm {
     const qtqp_options& op = *o;
     const uint64_t t_start = globaltimer_ns();
     double nb, nc;
-    load_and_equilibrate(op.equilibrate != 0, nb, nc);
+    {
+      QTQP_TIC();
+      load_and_equilibrate(op.equilibrate != 0, nb, nc);
+      QTQP_TOC(kPhLoad);
+    }
     double* xy = vec(kXY);
     double* s = vec(kRS);
     double* kq = vec(kKQ);
@@ -896,6 +1200,7 @@ struct DenseIpm {
       double* st = (stats != nullptr) ? stats + size_t(it) * QTQP_STATS_DOUBLES : nullptr;
       // _normalize (__init__.py:859-880) and mu (:477).
       {
+        QTQP_TIC();
         double sm[2] = {0.0, 0.0};
         for (int k = tid; k < N; k += NT) {
           sm[0] = fma(xy[k], xy[k], sm[0]);
@@ -909,6 +1214,7 @@ struct DenseIpm {
         }
         tau *= scale;
         mu = (sm[1] * scale * scale) / cnt;
+        QTQP_TOC(kPhNormalize);
       }
       // DirectKktSolver.update (direct.py:183-216).
       kkt_diag(mu, op.min_static_regularization);
@@ -953,23 +1259,25 @@ struct DenseIpm {
         for (int k = tid; k < N; k += NT) {
           sm[0] = fma(kq[k], q[k], sm[0]);
           sm[2] = fma(q[k], xy[k], sm[2]);
-          if (k < n) {
-            double a = 0.0, b = 0.0;
-            if (has_p) {
-              for (int j = 0; j < n; ++j) {
-                const double pjk = P[j * ldp + k];
-                a = fma(pjk, kq[j], a);
-                b = fma(pjk, xy[j], b);
-              }
-              a = fma(pi[k], kq[k], a);
-              b = fma(pi[k], xy[k], b);
-            }
-            pkq[k] = a;
-            px[k] = b;
-            sm[1] = fma(kq[k], a, sm[1]);
-            sm[3] = fma(xy[k], b, sm[3]);
-            sm[4] = fma(b, kq[k], sm[4]);
-          }
+        }
+        if (has_p) {
+          const double* Pp = P;
+          const int lp = ldp;
+          rowdot<2>(n, n,
+                    [&](int k, int j, double* acc) {
+                      const double pjk = Pp[j * lp + k];
+                      acc[0] = fma(pjk, kq[j], acc[0]);
+                      acc[1] = fma(pjk, xy[j], acc[1]);
+                    },
+                    [&](int k, double* acc) {
+                      const double a = fma(pi[k], kq[k], acc[0]);
+                      const double b = fma(pi[k], xy[k], acc[1]);
+                      pkq[k] = a;
+                      px[k] = b;
+                      sm[1] = fma(kq[k], a, sm[1]);
+                      sm[3] = fma(xy[k], b, sm[3]);
+                      sm[4] = fma(b, kq[k], sm[4]);
+                    });
         }
         block_reduce<NT, 5, 0>(sm, dummy, red, phase);
         ic.kqq = sm[0];
@@ -994,7 +1302,12 @@ struct DenseIpm {
         break;
       }
       int tm_p = 0;
-      const double tau_p = tau_step(xyp, rp, mu, 0.0, mu * tau, tau, tau, ic, tm_p);
+      double tau_p;
+      {
+        QTQP_TIC();
+        tau_p = tau_step(xyp, rp, mu, 0.0, mu * tau, tau, tau, ic, tm_p);
+        QTQP_TOC(kPhTau);
+      }
       write_lin_stats(st, 1, rp, tm_p, fp64);
       for (int k = tid; k < N; k += NT) {
         xyp[k] -= kq[k] * tau_p;  // [x_p; y_p]
@@ -1078,7 +1391,11 @@ struct DenseIpm {
         tau = fmax(tau, 1e-30);
       }
       group_sync<NT>();
-      status = termination(tau, nb, nc, st, op.collect_stats != 0);
+      {
+        QTQP_TIC();
+        status = termination(tau, nb, nc, st, op.collect_stats != 0);
+        QTQP_TOC(kPhTerm);
+      }
       taken = it + 1;
       if (st != nullptr && tid == 0) {
         st[kStIter] = it;
@@ -1114,7 +1431,8 @@ struct DenseIpm {
   }
 
   // Unequilibrate and scale by status (__init__.py:580-614).
-  __device__ void finish(int status, double tau, double* x_out, double* y_out, double* s_out) {
+  QTQP_PHASE void finish(int status, double tau, double* x_out, double* y_out, double* s_out) {
+    QTQP_LOCALS;
     const double* xy = vec(kXY);
     const double* s = vec(kRS);
     const double* de = vec(kDE);

@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(kPluginThreads)
     plugin_matvec_kernel(int n, int m, const double* x, double* out, char* ws) {
   DenseIpm<kPluginThreads> s;
   plugin_bind(s, n, m, ws, nullptr);
-  for (int k = threadIdx.x; k < n + m; k += kPluginThreads) out[k] = s.kkt_row(x, k);
+  s.kkt_matvec(x, out);
 }
 
 static int plugin_args(int n, int m, const void* ws) {
