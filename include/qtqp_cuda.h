@@ -148,6 +148,32 @@ int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst,
                            size_t workspace_bytes, const qtqp_options* opt,
                            void* stream);
 
+/* Allocation-free variant of qtqp_dense_batch_solve.  It has no counterpart
+ * in the reference (whose solver is pure Python).  It exists for callers that
+ * cannot allocate device memory at solve time -- code inside another
+ * framework's memory pool, or a control loop that must not call the
+ * allocator once running -- so it takes no workspace: its scratch is a fixed
+ * 16 MiB array inside this library (reserved on every GPU that loads the
+ * library until the process exits).  Plans needing more scratch than
+ * qtqp_dense_batch_noalloc_max_workspace() are rejected with
+ * QTQP_ERR_BAD_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call uses the same array, so calls whose work overlaps on
+ * the GPU (e.g. on two streams) race and must not be issued; groups run in
+ * sequence on `stream`.  Arguments and results as qtqp_dense_batch_solve. */
+size_t qtqp_dense_batch_noalloc_max_workspace(void);
+int qtqp_dense_batch_solve_noalloc(const qtqp_dense_instance* d_inst,
+                                   const int32_t* d_order,
+                                   const qtqp_batch_plan* plan,
+                                   const double* d_a_pool,
+                                   const double* d_p_pool,
+                                   const double* d_b_pool,
+                                   const double* d_c_pool, double* d_x_pool,
+                                   double* d_y_pool, double* d_s_pool,
+                                   qtqp_result* d_results,
+                                   qtqp_iter_stats* d_stats,
+                                   const qtqp_options* opt, void* stream);
+
 /* ---- dense KKT backend (the direct.LinearSolver plugin) ------------------ *
  * Replaces one backend of the plugin interface src/qtqp/direct.py:49-109
  * (set_dims / set_kkt / update_diag / factorize / solve / __matmul__) with the

@@ -35,6 +35,8 @@ EXPORTS = (
     "qtqp_device_sm_count",
     "qtqp_dense_batch_plan",
     "qtqp_dense_batch_solve",
+    "qtqp_dense_batch_noalloc_max_workspace",
+    "qtqp_dense_batch_solve_noalloc",
     "qtqp_kkt_dense_workspace_bytes",
     "qtqp_kkt_dense_set",
     "qtqp_kkt_dense_factorize",
@@ -146,6 +148,11 @@ def load() -> ctypes.CDLL:
     lib.qtqp_dense_batch_solve.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp, vp,
                                            vp, vp, vp, vp, vp, vp, sz,
                                            ctypes.POINTER(Options), vp]
+    lib.qtqp_dense_batch_noalloc_max_workspace.restype = sz
+    lib.qtqp_dense_batch_noalloc_max_workspace.argtypes = []
+    lib.qtqp_dense_batch_solve_noalloc.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp,
+                                                   vp, vp, vp, vp, vp, vp, vp,
+                                                   ctypes.POINTER(Options), vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz
     lib.qtqp_kkt_dense_workspace_bytes.argtypes = [i32, i32]
     lib.qtqp_kkt_dense_set.argtypes = [i32, i32, vp, vp, vp, vp]

@@ -181,6 +181,21 @@ class DeviceBatch:
         self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts),
         _lib.stream_handle(st)))
 
+  def launch_noalloc(self, stream=None) -> None:
+    """Enqueues the allocation-free variant: same solve, but its scratch is the
+    library's fixed device array instead of this batch's workspace tensor (for
+    callers that may not allocate device memory at solve time).  Raises
+    QtqpCudaError when the plan needs more scratch than that array holds."""
+    torch = self.torch
+    lib = _lib.load()
+    st = stream or torch.cuda.current_stream(self.device)
+    _lib.check(lib.qtqp_dense_batch_solve_noalloc(
+        self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(self.hb.plan),
+        self.a.data_ptr(), self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
+        self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
+        self.stats.data_ptr() if self.stats is not None else None, ctypes.byref(self._copts),
+        _lib.stream_handle(st)))
+
   def fetch(self):
     """Synchronises and returns (results, x, y, s, stats) as numpy arrays."""
     self.torch.cuda.synchronize(self.device)

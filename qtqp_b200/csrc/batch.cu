@@ -232,3 +232,106 @@ extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const i
   }
   return QTQP_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free batch solve.
+//
+// Some callers cannot allocate device memory when they solve: code running
+// inside another framework's memory pool, a real-time control loop that must
+// not touch the allocator after start-up, or a process whose allocator is
+// locked.  For them the scratch of the batch solve lives in a fixed array
+// that is part of this library's device image; it is reserved on every GPU
+// that loads the library, for the lifetime of the process.
+// ---------------------------------------------------------------------------
+namespace qtqp {
+
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mu;
+static void* g_static_ptr[64];
+
+// Device address of g_static_scratch on the current device.  The symbol's
+// name is only a host-side handle, so the address is looked up once per
+// device (with that device current) and cached.
+static int static_scratch(void** out) {
+  int dev = 0;
+  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= 64) return fail(QTQP_ERR_BAD_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (g_static_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    rc = cuda_check(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress");
+    if (rc) return rc;
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return QTQP_OK;
+}
+
+}  // namespace qtqp
+
+extern "C" size_t qtqp_dense_batch_noalloc_max_workspace(void) { return kStaticScratchBytes; }
+
+extern "C" int qtqp_dense_batch_solve_noalloc(
+    const qtqp_dense_instance* d_inst, const int32_t* d_order, const qtqp_batch_plan* plan,
+    const double* d_a_pool, const double* d_p_pool, const double* d_b_pool,
+    const double* d_c_pool, double* d_x_pool, double* d_y_pool, double* d_s_pool,
+    qtqp_result* d_results, qtqp_iter_stats* d_stats, const qtqp_options* opt, void* stream) {
+  if (plan == nullptr || opt == nullptr)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_noalloc: null plan/options");
+  if (plan->num_groups == 0) return QTQP_OK;
+  if (plan->num_groups < 0 || plan->num_groups > QTQP_MAX_GROUPS)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_noalloc: bad group count");
+  if (plan->workspace_bytes > kStaticScratchBytes)
+    return fail(QTQP_ERR_BAD_ARG,
+                "qtqp_dense_batch_solve_noalloc: the plan needs " +
+                    std::to_string(plan->workspace_bytes) +
+                    " bytes of scratch, more than the library's fixed 16 MiB; use "
+                    "qtqp_dense_batch_solve with a caller-provided workspace");
+  if (d_inst == nullptr || d_order == nullptr || d_a_pool == nullptr || d_b_pool == nullptr ||
+      d_c_pool == nullptr || d_x_pool == nullptr || d_y_pool == nullptr || d_s_pool == nullptr ||
+      d_results == nullptr)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_noalloc: null argument");
+  if (opt->max_iter < 1 || opt->max_iterative_refinement_steps < 1 ||
+      !(opt->step_size_scale > 0.0 && opt->step_size_scale < 1.0))
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_noalloc: invalid options");
+  void* ws = nullptr;
+  int rc = static_scratch(&ws);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The work counters must start at zero; everything else in the scratch is
+  // written by the kernel before it is read.
+  rc = cuda_check(cudaMemsetAsync(ws, 0, kWsHeader, st), "cudaMemsetAsync");
+  if (rc) return rc;
+  BatchParams base;
+  base.inst = d_inst;
+  base.a_pool = d_a_pool;
+  base.p_pool = d_p_pool != nullptr ? d_p_pool : d_a_pool;
+  base.b_pool = d_b_pool;
+  base.c_pool = d_c_pool;
+  base.x_pool = d_x_pool;
+  base.y_pool = d_y_pool;
+  base.s_pool = d_s_pool;
+  base.results = d_results;
+  base.stats = d_stats;
+  base.ws = static_cast<char*>(ws);
+  base.opt = *opt;
+  // Groups run one after another on the caller's stream (no side streams).
+  for (int g = 0; g < plan->num_groups; ++g) {
+    const qtqp_launch_group& G = plan->groups[g];
+    if (G.count <= 0) continue;
+    const size_t red = red_bytes_rt(G.block_threads);
+    if (size_t(G.smem_bytes) < red)
+      return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_noalloc: group smem below scratch");
+    BatchParams p = base;
+    p.order = d_order + G.begin;
+    p.count = G.count;
+    p.counter = static_cast<int*>(ws) + g;
+    p.smem_cap = size_t(G.smem_bytes) - red;
+    rc = launch_nt(G.block_threads, p, G.smem_bytes, st);
+    if (rc) return rc;
+  }
+  return QTQP_OK;
+}
