@@ -100,6 +100,10 @@ typedef struct {
   int32_t begin, count;  /* slice of the processing order                  */
   int32_t block_threads; /* threads per block                             */
   int32_t smem_bytes;    /* dynamic shared memory per block               */
+  int32_t slots;         /* banded batches: workspace slots (max blocks)   */
+  int32_t reserved;
+  uint64_t slot_off;     /* banded batches: byte offset of the first slot  */
+  uint64_t slot_bytes;   /* banded batches: bytes per slot                 */
 } qtqp_launch_group;
 
 typedef struct {
@@ -173,6 +177,42 @@ int qtqp_dense_batch_solve_noalloc(const qtqp_dense_instance* d_inst,
                                    qtqp_result* d_results,
                                    qtqp_iter_stats* d_stats,
                                    const qtqp_options* opt, void* stream);
+
+/* ---- batched banded / sparse device-resident IPM ------------------------ *
+ * Same algorithm and outputs as qtqp_dense_batch_solve for QPs whose A and P
+ * are sparse and whose Gram matrix G = P + A^T diag(1/Ry) A is banded with
+ * half-bandwidth bw (e.g. stage-ordered MPC problems): A is given as CSR and
+ * CSC, P as CSR with both triangles; the factor is a band Cholesky.  Replaces
+ * QTQP._solve_impl (src/qtqp/__init__.py:351-614) with the KKT layer of
+ * src/qtqp/direct.py:112-311 for this storage (the reference's sparse
+ * backends factorise the full KKT; the Gram reduction follows
+ * src/qtqp/solvers_dense.py:25-145 in band storage).
+ * Offsets are element offsets: *_ptr/*_idx into the int32 pool, *_val into
+ * the double pool. */
+typedef struct {
+  int32_t n, m, z, has_p;
+  int32_t bw, nnz_a, nnz_p, reserved;
+  int64_t a_ptr, a_idx, a_val;    /* A CSR: m+1 row pointers, columns, values */
+  int64_t at_ptr, at_idx, at_val; /* A CSC: n+1 column pointers, rows, values */
+  int64_t p_ptr, p_idx, p_val;    /* P CSR (symmetric, both triangles)       */
+  int64_t n_off, m_off;           /* c/x and b/y/s pools                     */
+  int64_t st_off;                 /* stats record offset (collect_stats)     */
+} qtqp_band_instance;
+
+/* Host-only planning.  Every block in flight owns one workspace slot sized
+ * for the largest instance, so the workspace does not grow with the batch;
+ * num_sms (0: 148) bounds the number of resident blocks. */
+int qtqp_band_batch_plan(qtqp_band_instance* h_inst, int32_t count,
+                         const qtqp_options* opt, int32_t num_sms,
+                         int32_t* h_order, qtqp_batch_plan* plan);
+int qtqp_band_batch_solve(const qtqp_band_instance* d_inst,
+                          const int32_t* d_order, const qtqp_batch_plan* plan,
+                          const int32_t* d_ipool, const double* d_vpool,
+                          const double* d_b_pool, const double* d_c_pool,
+                          double* d_x_pool, double* d_y_pool, double* d_s_pool,
+                          qtqp_result* d_results, qtqp_iter_stats* d_stats,
+                          void* d_workspace, size_t workspace_bytes,
+                          const qtqp_options* opt, void* stream);
 
 /* ---- dense KKT backend (the direct.LinearSolver plugin) ------------------ *
  * Replaces one backend of the plugin interface src/qtqp/direct.py:49-109

@@ -178,6 +178,20 @@ class QTQP:
     p = self.p.toarray() if self.p.nnz else None
     return _batch.DenseProblem(a=self.a.toarray(), b=self.b, c=self.c, z=self.z, p=p)
 
+  def band_problem(self):
+    """The presolved QP in the sparse form of the banded device solver."""
+    from . import band as _band  # pylint: disable=g-import-not-at-top
+    return _band.BandProblem(self.a, self.b, self.c, self.z, self.p if self.p.nnz else None)
+
+  def storage_format(self) -> str:
+    """'band' when the Gram matrix P + A^T D A is narrow-banded (its
+    half-bandwidth at most n/4) and n > 96, else 'dense'."""
+    if self.n <= 96:
+      return "dense"
+    from . import band as _band  # pylint: disable=g-import-not-at-top
+    bw = _band.gram_bandwidth(self.a, self.p if self.p.nnz else None)
+    return "band" if 4 * (bw + 1) <= self.n else "dense"
+
   def solve(self, *, atol: float = 1e-7, rtol: float = 1e-8, atol_infeas: float = 1e-8,
             rtol_infeas: float = 1e-9, max_iter: int = 100, step_size_scale: float = 0.99,
             min_static_regularization: float = 1e-8,
@@ -251,13 +265,15 @@ def _log_iteration(st: Dict[str, Any]) -> None:
         f" {infeas:>8.2e} | {st['mu']:>8.2e} | {solves:>8} | {st['time']:>8.2e} |")
 
 
-def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", _opts=None,
+def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: str = "auto",
+                _opts=None,
                 _verbose: bool = False, _start: float | None = None,
                 **solve_kwargs) -> List[Solution]:
   """Solves independent QPs in one persistent GPU launch.
 
   Accepts the keyword arguments of QTQP.solve (verbose defaults to False).
-  Returns one Solution per problem, in order.
+  storage: 'auto' (per problem: banded when the Gram matrix is narrow-banded,
+  else dense), 'dense' or 'band'.  Returns one Solution per problem, in order.
   """
   start = timeit.default_timer() if _start is None else _start
   if _opts is None:
@@ -268,16 +284,33 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", _opts=None
   else:
     opts, verbose = _opts, _verbose
   _lib.require_device()
-  hb = _batch.HostBatch([q.dense_problem() for q in problems], opts)
-  db = _batch.DeviceBatch(hb, records=bool(verbose or opts.collect_stats))
-  db.upload()
-  t_launch = timeit.default_timer() - start
-  db.launch()
-  res, x_pool, y_pool, s_pool, stats = db.fetch()
+  records = bool(verbose or opts.collect_stats)
+  # Dense and banded problems go to their own device batches.
+  kinds = [q.storage_format() if storage == "auto" else storage for q in problems]
+  per = {}  # kind -> (indices, results, x, y, s, stats, inst)
+  t_launch = 0.0
+  for kind in ("dense", "band"):
+    idx = [i for i, k in enumerate(kinds) if k == kind]
+    if not idx:
+      continue
+    if kind == "dense":
+      hb = _batch.HostBatch([problems[i].dense_problem() for i in idx], opts)
+      db = _batch.DeviceBatch(hb, records=records)
+    else:
+      from . import band as _band  # pylint: disable=g-import-not-at-top
+      hb = _band.HostBandBatch([problems[i].band_problem() for i in idx], opts)
+      db = _band.DeviceBandBatch(hb, records=records)
+    db.upload()
+    t_launch = timeit.default_timer() - start
+    db.launch()
+    per[kind] = (idx, *db.fetch(), hb.inst)
+  where = {}
+  for kind, (idx, res, xp, yp, sp_, st, inst) in per.items():
+    for j, i in enumerate(idx):
+      where[i] = (res[j], xp, yp, sp_, None if st is None else st[j], inst[j])
   out = []
   for i, q in enumerate(problems):
-    r = res[i]
-    d = hb.inst[i]
+    r, x_pool, y_pool, s_pool, recs, d = where[i]
     if int(r["error"]) == _lib.QTQP_ERR_NOT_SPD:
       raise np.linalg.LinAlgError("Cholesky failed: the KKT Gram matrix is not positive definite")
     if int(r["error"]) == _lib.QTQP_ERR_NAN:
@@ -295,10 +328,8 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", _opts=None
       y, s = q._postsolve(y, s, s_dropped=q._dropped_slack(x))
     st_list: List[Dict[str, Any]] = []
     iters = int(r["iterations"])
-    if stats is not None or verbose:
-      recs = stats[i] if stats is not None else None
-      if recs is not None:
-        st_list = [_record_to_dict(recs[k], opts.collect_stats, t_launch) for k in range(iters)]
+    if recs is not None:
+      st_list = [_record_to_dict(recs[k], opts.collect_stats, t_launch) for k in range(iters)]
     if verbose:
       print(f"{_SEPARA}\n{_HEADER}\n{_SEPARA}")
       for st in st_list:

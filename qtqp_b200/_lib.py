@@ -37,6 +37,8 @@ EXPORTS = (
     "qtqp_dense_batch_solve",
     "qtqp_dense_batch_noalloc_max_workspace",
     "qtqp_dense_batch_solve_noalloc",
+    "qtqp_band_batch_plan",
+    "qtqp_band_batch_solve",
     "qtqp_kkt_dense_workspace_bytes",
     "qtqp_kkt_dense_set",
     "qtqp_kkt_dense_factorize",
@@ -101,7 +103,9 @@ MAX_GROUPS = 8
 
 class LaunchGroup(ctypes.Structure):
   _fields_ = [("begin", ctypes.c_int32), ("count", ctypes.c_int32),
-              ("block_threads", ctypes.c_int32), ("smem_bytes", ctypes.c_int32)]
+              ("block_threads", ctypes.c_int32), ("smem_bytes", ctypes.c_int32),
+              ("slots", ctypes.c_int32), ("reserved", ctypes.c_int32),
+              ("slot_off", ctypes.c_uint64), ("slot_bytes", ctypes.c_uint64)]
 
 
 class BatchPlan(ctypes.Structure):
@@ -153,6 +157,11 @@ def load() -> ctypes.CDLL:
     lib.qtqp_dense_batch_solve_noalloc.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp,
                                                    vp, vp, vp, vp, vp, vp, vp,
                                                    ctypes.POINTER(Options), vp]
+    lib.qtqp_band_batch_plan.argtypes = [vp, i32, ctypes.POINTER(Options), i32, vp,
+                                         ctypes.POINTER(BatchPlan)]
+    lib.qtqp_band_batch_solve.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp, vp,
+                                          vp, vp, vp, vp, vp, vp, sz,
+                                          ctypes.POINTER(Options), vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz
     lib.qtqp_kkt_dense_workspace_bytes.argtypes = [i32, i32]
     lib.qtqp_kkt_dense_set.argtypes = [i32, i32, vp, vp, vp, vp]
@@ -183,3 +192,19 @@ def require_device():
 
 def stream_handle(torch_stream) -> int:
   return int(torch_stream.cuda_stream)
+
+
+class BandInstance(ctypes.Structure):
+  _fields_ = [("n", ctypes.c_int32), ("m", ctypes.c_int32), ("z", ctypes.c_int32),
+              ("has_p", ctypes.c_int32), ("bw", ctypes.c_int32), ("nnz_a", ctypes.c_int32),
+              ("nnz_p", ctypes.c_int32), ("reserved", ctypes.c_int32),
+              ("a_ptr", ctypes.c_int64), ("a_idx", ctypes.c_int64), ("a_val", ctypes.c_int64),
+              ("at_ptr", ctypes.c_int64), ("at_idx", ctypes.c_int64),
+              ("at_val", ctypes.c_int64), ("p_ptr", ctypes.c_int64),
+              ("p_idx", ctypes.c_int64), ("p_val", ctypes.c_int64),
+              ("n_off", ctypes.c_int64), ("m_off", ctypes.c_int64), ("st_off", ctypes.c_int64)]
+
+
+BAND_DTYPE = np.dtype([(name, np.int32 if ct is ctypes.c_int32 else np.int64)
+                       for name, ct in BandInstance._fields_])
+assert BAND_DTYPE.itemsize == ctypes.sizeof(BandInstance)

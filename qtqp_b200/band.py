@@ -1,0 +1,176 @@
+"""Batched banded/sparse device solve through the C-ABI.
+
+For QPs whose Gram matrix ``P + A^T D A`` has a small half-bandwidth (such as
+stage-ordered MPC problems), A is packed as CSR and CSC and P as CSR, and the
+device IPM factorises the Gram matrix in band storage.  Same algorithm,
+options and outputs as the dense batch (``qtqp_b200.batch``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Sequence
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from .batch import SolveOptions
+
+
+def gram_bandwidth(a: sp.spmatrix, p: sp.spmatrix | None) -> int:
+  """Half-bandwidth of P + A^T D A for any positive diagonal D."""
+  a = sp.csr_matrix(a)
+  bw = 0
+  if a.nnz:
+    rows = np.repeat(np.arange(a.shape[0]), np.diff(a.indptr))
+    lo = np.full(a.shape[0], np.iinfo(np.int64).max)
+    hi = np.full(a.shape[0], -1)
+    np.minimum.at(lo, rows, a.indices)
+    np.maximum.at(hi, rows, a.indices)
+    ok = hi >= 0
+    if np.any(ok):
+      bw = int(np.max(hi[ok] - lo[ok]))
+  if p is not None and p.nnz:
+    pc = sp.coo_matrix(p)
+    bw = max(bw, int(np.max(np.abs(pc.row - pc.col))))
+  return bw
+
+
+class BandProblem:
+  """One presolved sparse QP (A, P as scipy matrices; P may be None)."""
+
+  def __init__(self, a: sp.spmatrix, b, c, z: int, p: sp.spmatrix | None = None):
+    self.a = sp.csr_matrix(a, dtype=np.float64)
+    self.a.sort_indices()
+    self.at = sp.csr_matrix(self.a.T)  # CSC of A = CSR of A^T
+    self.at.sort_indices()
+    self.p = None
+    if p is not None and sp.csr_matrix(p).nnz:
+      self.p = sp.csr_matrix(p, dtype=np.float64)
+      self.p.sort_indices()
+    self.b = np.asarray(b, dtype=np.float64)
+    self.c = np.asarray(c, dtype=np.float64)
+    self.z = int(z)
+    self.bw = gram_bandwidth(self.a, self.p)
+
+
+class HostBandBatch:
+  """Packed int32/double pools, descriptors and plan of a banded batch."""
+
+  def __init__(self, problems: Sequence[BandProblem], opts: SolveOptions, num_sms: int = 0):
+    lib = _lib.load()
+    count = len(problems)
+    self.count = count
+    inst = np.zeros(count, dtype=_lib.BAND_DTYPE)
+    ints, vals = [], []
+    ioff = voff = n_off = m_off = 0
+
+    def put_i(arr):
+      nonlocal ioff
+      ints.append(np.asarray(arr, dtype=np.int32))
+      o = ioff
+      ioff += len(arr)
+      return o
+
+    def put_v(arr):
+      nonlocal voff
+      vals.append(np.asarray(arr, dtype=np.float64))
+      o = voff
+      voff += len(arr)
+      return o
+
+    for i, pr in enumerate(problems):
+      m, n = pr.a.shape
+      d = inst[i]
+      d["n"], d["m"], d["z"] = n, m, pr.z
+      d["has_p"] = int(pr.p is not None)
+      d["bw"] = min(pr.bw, n - 1)
+      d["nnz_a"] = pr.a.nnz
+      d["a_ptr"], d["a_idx"], d["a_val"] = (put_i(pr.a.indptr), put_i(pr.a.indices),
+                                            put_v(pr.a.data))
+      d["at_ptr"], d["at_idx"], d["at_val"] = (put_i(pr.at.indptr), put_i(pr.at.indices),
+                                               put_v(pr.at.data))
+      if pr.p is not None:
+        d["nnz_p"] = pr.p.nnz
+        d["p_ptr"], d["p_idx"], d["p_val"] = (put_i(pr.p.indptr), put_i(pr.p.indices),
+                                              put_v(pr.p.data))
+      else:
+        d["p_ptr"] = put_i(np.zeros(n + 1, dtype=np.int32))
+      d["n_off"], d["m_off"] = n_off, m_off
+      d["st_off"] = i * opts.max_iter
+      n_off += n
+      m_off += m
+    self.ipool = np.concatenate(ints) if ints else np.zeros(1, np.int32)
+    self.vpool = np.concatenate(vals) if vals else np.zeros(1)
+    self.b_pool = np.concatenate([pr.b for pr in problems]) if count else np.zeros(1)
+    self.c_pool = np.concatenate([pr.c for pr in problems]) if count else np.zeros(1)
+    self.n_total, self.m_total = n_off, m_off
+    order = np.zeros(max(count, 1), dtype=np.int32)
+    plan = _lib.BatchPlan()
+    copts = opts.to_c()
+    _lib.check(lib.qtqp_band_batch_plan(inst.ctypes.data, count, ctypes.byref(copts), num_sms,
+                                        order.ctypes.data, ctypes.byref(plan)))
+    self.inst, self.order, self.plan, self.opts = inst, order, plan, opts
+    self.workspace_bytes = int(plan.workspace_bytes)
+
+  @property
+  def input_bytes(self) -> int:
+    return sum(int(x.nbytes) for x in (self.ipool, self.vpool, self.b_pool, self.c_pool))
+
+
+class DeviceBandBatch:
+  """Device copy of a HostBandBatch, outputs and workspace (torch tensors)."""
+
+  def __init__(self, hb: HostBandBatch, device=None, records: bool | None = None):
+    torch = _lib.require_device()
+    self.torch, self.hb = torch, hb
+    dev = torch.device(device or "cuda")
+    self.device = dev
+    f64 = dict(dtype=torch.float64, device=dev)
+    self.inst = torch.from_numpy(hb.inst.view(np.uint8)).to(dev)
+    self.order = torch.from_numpy(hb.order).to(dev)
+    self.h_pools = [torch.from_numpy(x).pin_memory() for x in
+                    (hb.ipool, hb.vpool, hb.b_pool, hb.c_pool)]
+    self.ipool = torch.empty(hb.ipool.size, dtype=torch.int32, device=dev)
+    self.vpool = torch.empty(hb.vpool.size, **f64)
+    self.b = torch.empty(hb.b_pool.size, **f64)
+    self.c = torch.empty(hb.c_pool.size, **f64)
+    self.x = torch.empty(max(hb.n_total, 1), **f64)
+    self.y = torch.empty(max(hb.m_total, 1), **f64)
+    self.s = torch.empty(max(hb.m_total, 1), **f64)
+    self.results = torch.empty(max(hb.count, 1) * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8,
+                               device=dev)
+    self.stats = None
+    if records or (records is None and hb.opts.collect_stats):
+      self.stats = torch.empty(max(hb.count, 1) * hb.opts.max_iter * _lib.STATS_DOUBLES, **f64)
+    self.workspace = torch.empty(hb.workspace_bytes, dtype=torch.uint8, device=dev)
+    self._copts = hb.opts.to_c()
+
+  def upload(self, stream=None) -> None:
+    torch = self.torch
+    with torch.cuda.stream(stream or torch.cuda.current_stream(self.device)):
+      for dst, src in zip((self.ipool, self.vpool, self.b, self.c), self.h_pools):
+        dst.copy_(src, non_blocking=True)
+
+  def launch(self, stream=None) -> None:
+    torch = self.torch
+    lib = _lib.load()
+    st = stream or torch.cuda.current_stream(self.device)
+    hb = self.hb
+    _lib.check(lib.qtqp_band_batch_solve(
+        self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan),
+        self.ipool.data_ptr(), self.vpool.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
+        self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
+        self.stats.data_ptr() if self.stats is not None else None,
+        self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts),
+        _lib.stream_handle(st)))
+
+  def fetch(self):
+    self.torch.cuda.synchronize(self.device)
+    res = self.results.cpu().numpy().view(_lib.RESULT_DTYPE)[: self.hb.count]
+    stats = None
+    if self.stats is not None:
+      stats = self.stats.cpu().numpy().reshape(self.hb.count, self.hb.opts.max_iter,
+                                                _lib.STATS_DOUBLES)
+    return (res, self.x.cpu().numpy(), self.y.cpu().numpy(), self.s.cpu().numpy(), stats)

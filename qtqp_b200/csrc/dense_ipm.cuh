@@ -76,6 +76,23 @@ __host__ __device__ inline InstLayout plan_layout(int n, int m, size_t smem_cap)
   return L;
 }
 
+// Global workspace of one banded instance: vectors, the band factor (n x
+// (bw+1)) and working copies of the A (CSR and CSC) and P value arrays.
+struct BandLayout {
+  int np;
+  size_t v_bytes, l_bytes, val_bytes, total;
+};
+__host__ __device__ inline BandLayout plan_band_layout(int n, int m, int bw, int nnz_a,
+                                                       int nnz_p) {
+  BandLayout L;
+  L.np = (max(n + m, n + 4) + 1) & ~1;
+  L.v_bytes = round16(size_t(kNumVec) * L.np * 8);
+  L.l_bytes = round16(size_t(n) * (bw + 1) * 8);
+  L.val_bytes = round16((2 * size_t(nnz_a) + size_t(nnz_p)) * 8);
+  L.total = L.v_bytes + L.l_bytes + L.val_bytes;
+  return L;
+}
+
 // Fields of one qtqp_iter_stats record.
 enum StatField : int {
   kStIter = 0, kStCtx, kStBty, kStPcost, kStDcost, kStPres, kStDres, kStGap,
@@ -113,11 +130,18 @@ struct IrOutcome {
   (void)tid; (void)n; (void)m; (void)z; (void)N; (void)lda; (void)ldp; (void)ldg; \
   (void)A; (void)P; (void)G; (void)has_p
 
+// Storage formats of A, P and the KKT factor.
+enum MatFormat : int {
+  kFmtDense = 0,  // dense A (m x n), dense P, dense Gram G / Cholesky factor
+  kFmtBand = 1,   // sparse A (CSR + CSC), sparse P (CSR), banded Gram / factor
+};
+
 // ----------------------------------------------------------------------------
 // The solver state of one instance, replicated in every thread of the block.
+// FMT selects the matrix backend; the interior-point logic is shared.
 // ----------------------------------------------------------------------------
-template <int NT>
-struct DenseIpm {
+template <int NT, int FMT = kFmtDense>
+struct Ipm {
   int tid;
   int n, m, z, N;
   bool has_p;
@@ -136,6 +160,24 @@ struct DenseIpm {
   int phase;
   // Options.
   const qtqp_options* o;
+  // Banded backend (FMT == kFmtBand): A as CSR (ip, ix) and CSC (jp, jx),
+  // P as CSR (pp, px) holding both triangles; the working (equilibrated)
+  // values av / at / pv; the factor in lower band storage by columns,
+  // Lb[j * (bw + 1) + (i - j)] = L_ij for j <= i <= j + bw.
+  const int* ip;
+  const int* ix;
+  const int* jp;
+  const int* jx;
+  const int* pp;
+  const int* px;
+  const double* av0;
+  const double* at0;
+  const double* pv0;
+  double* av;
+  double* at;
+  double* pv;
+  double* Lb;
+  int bw, nnz_a, nnz_p;
 
   __device__ __forceinline__ double* vec(int id) const { return V + size_t(id) * np; }
   // First index >= lo owned by this thread (k % NT == tid).
@@ -210,6 +252,10 @@ struct DenseIpm {
   // multiplied by (d_i * e_j), the clip bounds are [1e-3, 1e3].
   // --------------------------------------------------------------------------
   QTQP_PHASE void load_and_equilibrate(bool equilibrate, double& nb, double& nc) {
+    if constexpr (FMT == kFmtBand) {
+      band_load_and_equilibrate(equilibrate, nb, nc);
+      return;
+    }
     QTQP_LOCALS;
     double* de = vec(kDE);
     double* sc = vec(kTMP);  // per-sweep [e_i; d_i]
@@ -342,6 +388,7 @@ struct DenseIpm {
   // --------------------------------------------------------------------------
   template <typename T>
   QTQP_PHASE int factorize() {
+    if constexpr (FMT == kFmtBand) return band_factorize<T>();
     const int nb = (n + 3) >> 2;
     if (nb * (nb + 1) / 2 <= NT) return factorize_regs<T>();
     return factorize_mem<T>();
@@ -679,6 +726,10 @@ struct DenseIpm {
   // before other threads read it).
   // --------------------------------------------------------------------------
   QTQP_PHASE void kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
+    if constexpr (FMT == kFmtBand) {
+      band_kkt_solve(r, out, accumulate, fp64);
+      return;
+    }
     QTQP_LOCALS;
     QTQP_TIC();
     const double* iry = vec(kPI);
@@ -727,6 +778,10 @@ struct DenseIpm {
   // max |res| and NaN flag of v (combined by the caller's reduction).
   QTQP_PHASE void kkt_residual(const double* v, const double* krhs, double* res, double& mres,
                                double& vnan) const {
+    if constexpr (FMT == kFmtBand) {
+      band_kkt_residual(v, krhs, res, mres, vnan);
+      return;
+    }
     QTQP_LOCALS;
     const double* reg = vec(kREG);
     const double* corr = vec(kCORR);
@@ -901,17 +956,23 @@ struct DenseIpm {
     double dummy[1] = {0.0};
     for (int k = tid; k < N; k += NT) sm[0] = fma(kr[k], q[k], sm[0]);
     if (has_p) {
-      const double* Pp = P;
-      const int lp = ldp;
-      rowdot<1>(n, n, [&](int k, int j, double* acc) { acc[0] = fma(Pp[j * lp + k], kr[j], acc[0]); },
-                [&](int k, double* acc) {
-                  const double t = fma(pi[k], kr[k], acc[0]);
-                  pkr[k] = t;
-                  sm[1] = fma(kr[k], pkq[k], sm[1]);
-                  sm[2] = fma(kq[k], t, sm[2]);
-                  sm[3] = fma(kr[k], t, sm[3]);
-                  sm[4] = fma(px[k], kr[k], sm[4]);
-                });
+      auto epi = [&](int k, double poff) {
+        const double t = fma(pi[k], kr[k], poff);
+        pkr[k] = t;
+        sm[1] = fma(kr[k], pkq[k], sm[1]);
+        sm[2] = fma(kq[k], t, sm[2]);
+        sm[3] = fma(kr[k], t, sm[3]);
+        sm[4] = fma(px[k], kr[k], sm[4]);
+      };
+      if constexpr (FMT == kFmtBand) {
+        for (int k = tid; k < n; k += NT) epi(k, band_poff_row(kr, k));
+      } else {
+        const double* Pp = P;
+        const int lp = ldp;
+        rowdot<1>(n, n,
+                  [&](int k, int j, double* acc) { acc[0] = fma(Pp[j * lp + k], kr[j], acc[0]); },
+                  [&](int k, double* acc) { epi(k, acc[0]); });
+      }
     }
     block_reduce<NT, 5, 0>(sm, dummy, red, phase);
     const bool accurate = irr.status == 1 || irr.final_res < 1e-7;
@@ -1006,39 +1067,46 @@ struct DenseIpm {
     const bool hp = has_p;
     const double* b0p = b0;
     const double* c0p = c0;
-    rowdot<2>(n, m + plen,
-              [&](int k, int i, double* acc) {
-                if (i < mm) {
-                  acc[0] = fma(Ap[i * la + k], xy[nn + i], acc[0]);
-                } else {
-                  acc[1] = fma(Pp[(i - mm) * lp + k], xy[i - mm], acc[1]);
-                }
-              },
-              [&](int k, double* acc) {
-                const double aty = acc[0] / de[k];
-                const double px = hp ? fma(pi[k], xy[k], acc[1]) / de[k] : 0.0;
-                const double xo = de[k] * xy[k];
-                sm[0] = fma(c0p[k], xo, sm[0]);
-                sm[2] = fma(xo, px, sm[2]);
-                mx[1] = nanmax(mx[1], fabs((px + aty) * inv_tau + c0p[k]));
-                mx[2] = nanmax(mx[2], fabs(aty));
-                mx[3] = nanmax(mx[3], fabs(px));
-                mx[7] = nanmax(mx[7], fabs(xo));
-              });
-    rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], xy[j], acc[0]); },
-              [&](int k, double* acc) {
-                const int kk = nn + k;
-                const double ax = acc[0] / de[kk];
-                const double yo = de[kk] * xy[kk];
-                const double so = s[kk] / de[kk];
-                const double bo = b0p[k];
-                sm[1] = fma(bo, yo, sm[1]);
-                mx[0] = nanmax(mx[0], fabs((ax + so) * inv_tau - bo));
-                mx[4] = nanmax(mx[4], fabs(ax + so));
-                mx[5] = nanmax(mx[5], fabs(ax));
-                mx[6] = nanmax(mx[6], fabs(so));
-                mx[8] = nanmax(mx[8], fabs(yo));
-              });
+    auto epi_x = [&](int k, double aty_raw, double poff) {
+      const double aty = aty_raw / de[k];
+      const double px = hp ? fma(pi[k], xy[k], poff) / de[k] : 0.0;
+      const double xo = de[k] * xy[k];
+      sm[0] = fma(c0p[k], xo, sm[0]);
+      sm[2] = fma(xo, px, sm[2]);
+      mx[1] = nanmax(mx[1], fabs((px + aty) * inv_tau + c0p[k]));
+      mx[2] = nanmax(mx[2], fabs(aty));
+      mx[3] = nanmax(mx[3], fabs(px));
+      mx[7] = nanmax(mx[7], fabs(xo));
+    };
+    auto epi_y = [&](int k, double ax_raw) {
+      const int kk = nn + k;
+      const double ax = ax_raw / de[kk];
+      const double yo = de[kk] * xy[kk];
+      const double so = s[kk] / de[kk];
+      const double bo = b0p[k];
+      sm[1] = fma(bo, yo, sm[1]);
+      mx[0] = nanmax(mx[0], fabs((ax + so) * inv_tau - bo));
+      mx[4] = nanmax(mx[4], fabs(ax + so));
+      mx[5] = nanmax(mx[5], fabs(ax));
+      mx[6] = nanmax(mx[6], fabs(so));
+      mx[8] = nanmax(mx[8], fabs(yo));
+    };
+    if constexpr (FMT == kFmtBand) {
+      for (int k = tid; k < n; k += NT) epi_x(k, band_at_col(xy, k), band_poff_row(xy, k));
+      for (int k = tid; k < m; k += NT) epi_y(k, band_a_row(xy, k));
+    } else {
+      rowdot<2>(n, m + plen,
+                [&](int k, int i, double* acc) {
+                  if (i < mm) {
+                    acc[0] = fma(Ap[i * la + k], xy[nn + i], acc[0]);
+                  } else {
+                    acc[1] = fma(Pp[(i - mm) * lp + k], xy[i - mm], acc[1]);
+                  }
+                },
+                [&](int k, double* acc) { epi_x(k, acc[0], acc[1]); });
+      rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], xy[j], acc[0]); },
+                [&](int k, double* acc) { epi_y(k, acc[0]); });
+    }
     block_reduce<NT, 3, 9>(sm, mx, red, phase);
     const double ctx = sm[0], bty = sm[1], xpx = has_p ? sm[2] : 0.0;
     const double pcost = (ctx + 0.5 * xpx * inv_tau) * inv_tau;
@@ -1261,23 +1329,28 @@ struct DenseIpm {
           sm[2] = fma(q[k], xy[k], sm[2]);
         }
         if (has_p) {
-          const double* Pp = P;
-          const int lp = ldp;
-          rowdot<2>(n, n,
-                    [&](int k, int j, double* acc) {
-                      const double pjk = Pp[j * lp + k];
-                      acc[0] = fma(pjk, kq[j], acc[0]);
-                      acc[1] = fma(pjk, xy[j], acc[1]);
-                    },
-                    [&](int k, double* acc) {
-                      const double a = fma(pi[k], kq[k], acc[0]);
-                      const double b = fma(pi[k], xy[k], acc[1]);
-                      pkq[k] = a;
-                      px[k] = b;
-                      sm[1] = fma(kq[k], a, sm[1]);
-                      sm[3] = fma(xy[k], b, sm[3]);
-                      sm[4] = fma(b, kq[k], sm[4]);
-                    });
+          auto epi = [&](int k, double pq, double pxk) {
+            const double a = fma(pi[k], kq[k], pq);
+            const double b = fma(pi[k], xy[k], pxk);
+            pkq[k] = a;
+            px[k] = b;
+            sm[1] = fma(kq[k], a, sm[1]);
+            sm[3] = fma(xy[k], b, sm[3]);
+            sm[4] = fma(b, kq[k], sm[4]);
+          };
+          if constexpr (FMT == kFmtBand) {
+            for (int k = tid; k < n; k += NT) epi(k, band_poff_row(kq, k), band_poff_row(xy, k));
+          } else {
+            const double* Pp = P;
+            const int lp = ldp;
+            rowdot<2>(n, n,
+                      [&](int k, int j, double* acc) {
+                        const double pjk = Pp[j * lp + k];
+                        acc[0] = fma(pjk, kq[j], acc[0]);
+                        acc[1] = fma(pjk, xy[j], acc[1]);
+                      },
+                      [&](int k, double* acc) { epi(k, acc[0], acc[1]); });
+          }
         }
         block_reduce<NT, 5, 0>(sm, dummy, red, phase);
         ic.kqq = sm[0];
@@ -1479,6 +1552,317 @@ struct DenseIpm {
       }
     }
   }
+  // ==========================================================================
+  // Banded backend (FMT == kFmtBand): sparse A and P, and the Gram matrix
+  // G = P_off + diag(Rx) + A^T diag(1/Ry) A of half-bandwidth bw (e.g. the
+  // block-tridiagonal Gram of a stage-ordered MPC problem).  Everything lives
+  // in the instance's global workspace slot.
+  // ==========================================================================
+  __device__ void bind_band(int n_, int m_, int bw_, int nnz_a_, int nnz_p_, char* gmem) {
+    tid = threadIdx.x;
+    n = n_;
+    m = m_;
+    N = n + m;
+    bw = bw_;
+    nnz_a = nnz_a_;
+    nnz_p = nnz_p_;
+    const BandLayout L = plan_band_layout(n, m, bw, nnz_a, nnz_p);
+    np = L.np;
+    V = reinterpret_cast<double*>(gmem);
+    Lb = reinterpret_cast<double*>(gmem + L.v_bytes);
+    G = Lb;
+    av = reinterpret_cast<double*>(gmem + L.v_bytes + L.l_bytes);
+    at = av + nnz_a;
+    pv = at + nnz_a;
+    A = P = nullptr;
+    lda = ldp = ldg = 0;
+  }
+
+#define QTQP_BAND_LOCALS                                                        \
+  const int tid = this->tid, n = this->n, m = this->m, N = this->N;             \
+  const int bw = this->bw, ldl = this->bw + 1;                                  \
+  const int* const ip = this->ip;                                               \
+  const int* const ix = this->ix;                                               \
+  const int* const jp = this->jp;                                               \
+  const int* const jx = this->jx;                                               \
+  const int* const pp = this->pp;                                               \
+  const int* const px = this->px;                                               \
+  double* const av = this->av;                                                  \
+  double* const at = this->at;                                                  \
+  double* const pv = this->pv;                                                  \
+  const bool has_p = this->has_p;                                               \
+  (void)tid; (void)n; (void)m; (void)N; (void)bw; (void)ldl; (void)ip; (void)ix; \
+  (void)jp; (void)jx; (void)pp; (void)px; (void)av; (void)at; (void)pv; (void)has_p
+
+  // Ruiz equilibration on the CSR (A), CSC (A) and CSR (P) value arrays, with
+  // the reference's arithmetic: a_ij *= (d_i * e_j), p_ij *= (e_i * e_j).
+  __device__ void band_load_and_equilibrate(bool equilibrate, double& nb, double& nc) {
+    QTQP_BAND_LOCALS;
+    double* de = vec(kDE);
+    double* sc = vec(kTMP);
+    for (int q = tid; q < nnz_a; q += NT) {
+      av[q] = av0[q];
+      at[q] = at0[q];
+    }
+    for (int q = tid; q < nnz_p; q += NT) pv[q] = has_p ? pv0[q] : 0.0;
+    for (int k = tid; k < N; k += NT) de[k] = 1.0;
+    group_sync<NT>();
+    auto scale_of = [](double mx) {
+      if (mx == 0.0) mx = 1.0;
+      return fmin(fmax(1.0 / sqrt(mx), 1e-3), 1e3);
+    };
+    if (equilibrate) {
+      for (int sweep = 0; sweep < 10; ++sweep) {
+        for (int k = tid; k < N; k += NT) {
+          double mx = 0.0;
+          if (k < n) {
+            for (int q = jp[k]; q < jp[k + 1]; ++q) mx = fmax(mx, fabs(at[q]));
+            if (has_p)
+              for (int q = pp[k]; q < pp[k + 1]; ++q) mx = fmax(mx, fabs(pv[q]));
+          } else {
+            for (int q = ip[k - n]; q < ip[k - n + 1]; ++q) mx = fmax(mx, fabs(av[q]));
+          }
+          sc[k] = scale_of(mx);
+        }
+        group_sync<NT>();
+        for (int r = tid; r < m; r += NT) {
+          const double dr = sc[n + r];
+          for (int q = ip[r]; q < ip[r + 1]; ++q) av[q] *= dr * sc[ix[q]];
+        }
+        for (int j = tid; j < n; j += NT) {
+          const double ej = sc[j];
+          for (int q = jp[j]; q < jp[j + 1]; ++q) at[q] *= sc[n + jx[q]] * ej;
+        }
+        if (has_p) {
+          for (int i = tid; i < n; i += NT) {
+            const double ei = sc[i];
+            for (int q = pp[i]; q < pp[i + 1]; ++q) pv[q] *= ei * sc[px[q]];
+          }
+        }
+        for (int k = tid; k < N; k += NT) de[k] *= sc[k];
+        group_sync<NT>();
+      }
+    }
+    double* q = vec(kQ);
+    double* pi = vec(kPI);
+    double mx[2] = {0.0, 0.0};
+    double dummy[1] = {0.0};
+    for (int k = tid; k < N; k += NT) {
+      if (k < n) {
+        q[k] = c0[k] * de[k];
+        double d = 0.0;
+        if (has_p) {
+          for (int qq = pp[k]; qq < pp[k + 1]; ++qq) {
+            if (px[qq] == k) {  // diag(P_eq); pv keeps only the off-diagonal
+              d = pv[qq];
+              pv[qq] = 0.0;
+            }
+          }
+        }
+        pi[k] = d;
+        mx[1] = nanmax(mx[1], fabs(c0[k]));
+      } else {
+        q[k] = b0[k - n] * de[k];
+        mx[0] = nanmax(mx[0], fabs(b0[k - n]));
+      }
+    }
+    block_reduce<NT, 0, 2>(dummy, mx, red, phase);
+    nb = mx[0];
+    nc = mx[1];
+    group_sync<NT>();
+  }
+
+  // (P_off v)_k for the owner of row k (P symmetric, so row k = column k).
+  __device__ __forceinline__ double band_poff_row(const double* v, int k) const {
+    double t = 0.0;
+    if (has_p)
+      for (int q = pp[k]; q < pp[k + 1]; ++q) t = fma(pv[q], v[px[q]], t);
+    return t;
+  }
+  // (A^T y)_k with y at v[n + i].
+  __device__ __forceinline__ double band_at_col(const double* v, int k) const {
+    double t = 0.0;
+    for (int q = jp[k]; q < jp[k + 1]; ++q) t = fma(at[q], v[n + jx[q]], t);
+    return t;
+  }
+  // (A x)_i.
+  __device__ __forceinline__ double band_a_row(const double* v, int i) const {
+    double t = 0.0;
+    for (int q = ip[i]; q < ip[i + 1]; ++q) t = fma(av[q], v[ix[q]], t);
+    return t;
+  }
+
+  // Gram matrix in column band storage, then Cholesky (one barrier per
+  // column, the unscaled column k updates the trailing band and column k-1
+  // is finished in the same phase); the diagonal keeps 1 / l_kk.
+  template <typename T>
+  __device__ int band_factorize() {
+    QTQP_BAND_LOCALS;
+    QTQP_TIC();
+    T* L = reinterpret_cast<T*>(Lb);
+    const double* reg = vec(kREG);
+    const double* wsc = vec(kPW);
+    double dmax[1] = {0.0};
+    double dummy[1] = {0.0};
+    for (int j = tid; j < n; j += NT) {
+      T* col = L + size_t(j) * ldl;
+      for (int d = 0; d <= bw; ++d) col[d] = T(0);
+      for (int q = jp[j]; q < jp[j + 1]; ++q) {
+        const int r = jx[q];
+        const double w = wsc[n + r];
+        const T arj = T(at[q] * w);
+        for (int q2 = ip[r]; q2 < ip[r + 1]; ++q2) {
+          const int i = ix[q2];
+          if (i >= j && i - j <= bw) col[i - j] = fma(arj, T(av[q2] * w), col[i - j]);
+        }
+      }
+      if (has_p) {
+        for (int q = pp[j]; q < pp[j + 1]; ++q) {
+          const int i = px[q];
+          if (i > j && i - j <= bw) col[i - j] = T(pv[q]) + col[i - j];
+        }
+      }
+      col[0] = T(reg[j]) + col[0];
+      dmax[0] = nanmax(dmax[0], double(col[0]));
+    }
+    block_reduce<NT, 0, 1>(dummy, dmax, red, phase);
+    const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
+    for (int j = tid; j < n; j += NT) L[size_t(j) * ldl] = T(double(L[size_t(j) * ldl]) + jit);
+    group_sync<NT>();
+    QTQP_TOC(kPhGram);
+    QTQP_RETIC();
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NW = NT / 32;
+    T d_prev = T(1);
+    int info = 0;
+    for (int k = 0; k <= n; ++k) {
+      if (k > 0) {  // finish column k-1
+        T* ck = L + size_t(k - 1) * ldl;
+        const T il = rsqrt(d_prev);
+        const int rows = min(bw, n - k);
+        for (int d = 1 + tid; d <= rows; d += NT) ck[d] *= il;
+        if (tid == NT - 1) ck[0] = il;
+      }
+      if (k == n) break;
+      const T* ck = L + size_t(k) * ldl;
+      const T d = ck[0];
+      if (!(d > T(0))) {
+        info = k + 1;
+        break;
+      }
+      const T inv_d = T(1) / d;
+      const int last = min(n - 1, k + bw);
+      for (int j = k + 1 + warp; j <= last; j += NW) {
+        const T t = ck[j - k] * inv_d;
+        T* cj = L + size_t(j) * ldl;
+        for (int i = j + lane; i <= last; i += 32) cj[i - j] = fma(-ck[i - k], t, cj[i - j]);
+      }
+      d_prev = d;
+      group_sync<NT>();
+    }
+    group_sync<NT>();
+    QTQP_TOC(kPhChol);
+    return info;
+  }
+
+  // Solves L L^T v = v (column band storage, reciprocal diagonal) with one
+  // warp: forward z_k = v_k / l_kk, v_i -= l_ik z_k (i in (k, k+bw]) into w;
+  // backward x_k = w_k / l_kk, w_i -= l_ki x_k (i in [k-bw, k)) into v.
+  template <typename T>
+  __device__ void band_chol_solve(T* v, T* w) {
+    QTQP_BAND_LOCALS;
+    const T* L = reinterpret_cast<const T*>(Lb);
+    if (tid < 32) {
+      const int lane = tid;
+      for (int k = 0; k < n; ++k) {
+        const T* ck = L + size_t(k) * ldl;
+        const T zk = v[k] * ck[0];
+        const int rows = min(bw, n - 1 - k);
+        for (int d = 1 + lane; d <= rows; d += 32) v[k + d] = fma(-ck[d], zk, v[k + d]);
+        if (lane == 0) w[k] = zk;
+        __syncwarp();
+      }
+      for (int k = n - 1; k >= 0; --k) {
+        const T xk = w[k] * L[size_t(k) * ldl];
+        const int rows = min(bw, k);
+        for (int d = 1 + lane; d <= rows; d += 32) {
+          const int i = k - d;
+          w[i] = fma(-L[size_t(i) * ldl + d], xk, w[i]);
+        }
+        if (lane == 0) v[k] = xk;
+        __syncwarp();
+      }
+    }
+    group_sync<NT>();
+  }
+
+  __device__ void band_kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
+    QTQP_BAND_LOCALS;
+    QTQP_TIC();
+    const double* iry = vec(kPI);
+    double* tmp = vec(kTMP);
+    float* t32 = this->t32();
+    for (int j = tid; j < n; j += NT) {
+      double acc = 0.0;
+      for (int q = jp[j]; q < jp[j + 1]; ++q) {
+        const int i = jx[q];
+        acc = fma(at[q], iry[n + i] * r[n + i], acc);
+      }
+      const double g = r[j] + acc;
+      if (fp64) {
+        tmp[j] = g;
+      } else {
+        t32[j] = float(g);
+      }
+    }
+    group_sync<NT>();
+    if (fp64) {
+      band_chol_solve<double>(tmp, vec(kW));
+    } else {
+      band_chol_solve<float>(t32, t32 + n);
+    }
+    for (int k = tid; k < N; k += NT) {
+      double val;
+      if (k < n) {
+        val = fp64 ? tmp[k] : double(t32[k]);
+      } else {
+        const int i = k - n;
+        double ax = 0.0;
+        if (fp64) {
+          for (int q = ip[i]; q < ip[i + 1]; ++q) ax = fma(av[q], tmp[ix[q]], ax);
+        } else {
+          for (int q = ip[i]; q < ip[i + 1]; ++q) ax = fma(av[q], double(t32[ix[q]]), ax);
+        }
+        val = iry[k] * (ax - r[k]);
+      }
+      out[k] = accumulate ? out[k] + val : val;
+    }
+    QTQP_TOC(kPhSolve);
+  }
+
+  __device__ void band_kkt_residual(const double* v, const double* krhs, double* res,
+                                    double& mres, double& vnan) const {
+    QTQP_BAND_LOCALS;
+    const double* reg = vec(kREG);
+    const double* corr = vec(kCORR);
+    for (int k = tid; k < N; k += NT) {
+      double kv;
+      if (k < n) {
+        double t = band_poff_row(v, k);
+        t += reg[k] * v[k];
+        kv = t + band_at_col(v, k);
+      } else {
+        kv = band_a_row(v, k - n) - (-reg[k]) * v[k];
+      }
+      const double rk = krhs[k] - kv + corr[k] * v[k];
+      res[k] = rk;
+      mres = nanmax(mres, fabs(rk));
+      vnan = fmax(vnan, (v[k] != v[k]) ? 1.0 : 0.0);
+    }
+  }
 };
+
+template <int NT>
+using DenseIpm = Ipm<NT, kFmtDense>;
 
 }  // namespace qtqp

@@ -128,14 +128,18 @@ def mpc_structure(horizon: int, nx: int = 40, nu: int = 20, seed: int = 1003):
   return a, z, p, ub
 
 
-def mpc_feasible(horizon: int, seed: int = 1003, active_frac: float = 0.1):
+def mpc_feasible(horizon: int, seed: int = 1003, active_frac: float = 0.1,
+                 free_initial: bool = False):
   """MPC QP with b, c from a feasible pair: x_bar strictly inside the boxes
-  except a fraction `active_frac` at +-bound (with positive duals there)."""
+  except a fraction `active_frac` at +-bound (with positive duals there).
+  free_initial keeps the first stage's variables off the bounds."""
   a, z, p, ub = mpc_structure(horizon, seed=seed)
   rng = np.random.default_rng([seed, 1])
   n = p.shape[0]
   xbar = rng.uniform(-0.5, 0.5, size=n) * ub
   act = rng.random(n) < active_frac
+  if free_initial:
+    act[:60] = False
   sgn = np.where(rng.random(n) < 0.5, 1.0, -1.0)
   xbar = np.where(act, sgn * ub, xbar)
   ybar = np.zeros(a.shape[0])
@@ -152,16 +156,37 @@ def config3():
   return mpc_feasible(500)
 
 
+CFG4_NX = 40  # initial-state rows of b carry the parameter
+
+
 def config4_family(count: int = 20000, horizon: int = 50, dim: int = 32, seed: int = 1004):
   """Parametric family: fixed (A, P) of the T=50 MPC QP; (b, c) = (b_bar,
-  c_bar) + W theta, theta ~ N(0, I_dim), W ~ N(0, 0.1^2) fixed.
-  Returns (a, z, p, b_bar, c_bar, W, thetas)."""
-  a, b_bar, c_bar, z, p = mpc_feasible(horizon, seed=seed)
+  c_bar) + W theta, theta ~ N(0, I_dim), W with N(0, 0.1^2) entries (std 0.1).
+
+  W is non-zero on the rows of b that fix the initial state (the first nx
+  equality rows) and on every entry of c; its rows for the dynamics offsets
+  and the box bounds are zero.  Perturbing those as well makes almost every
+  instance infeasible (2045 of 2048 measured): the state is pinned at t=0 and
+  random dynamics offsets drift it out of the |x| <= 5 box faster than the
+  |u| <= 1 inputs can steer.  The base point keeps the initial state inside
+  the box.  Returns (a, z, p, b_bar, c_bar, W, thetas).
+  """
+  a, b_bar, c_bar, z, p = mpc_feasible(horizon, seed=seed, free_initial=True)
   rng = np.random.default_rng(seed)
   mtot, n = a.shape
-  w = rng.normal(scale=0.1, size=(mtot + n, dim))
+  w = np.zeros((mtot + n, dim))
+  w[:CFG4_NX] = rng.normal(scale=0.1, size=(CFG4_NX, dim))
+  w[mtot:] = rng.normal(scale=0.1, size=(n, dim))
   thetas = np.random.default_rng([seed, 2]).normal(size=(count, dim))
   return a, z, p, b_bar, c_bar, w, thetas
+
+
+def config4_instance(family, i: int):
+  """(a, b, c, z, p) of instance i of a family from config4_family."""
+  a, z, p, b_bar, c_bar, w, thetas = family
+  d = w @ thetas[i]
+  m = a.shape[0]
+  return a, b_bar + d[:m], c_bar + d[m:], z, p
 
 
 # ---------------------------------------------------------------------------
