@@ -341,7 +341,7 @@ def run_ours(args) -> None:
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": chosen["clocks"],
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * int(hb.plan.num_groups),
     }
     print(json.dumps(line), flush=True)
   if dist is not None:
