@@ -58,6 +58,10 @@ typedef struct {
   int32_t collect_stats; /* 1: write one qtqp_iter_stats record per iteration */
   int32_t tau_mode;      /* 0: quadratic with linearised fallback; 1: always
                             linearised (__init__.py:736-752)                 */
+  int32_t warm_corrections; /* learned warm start only (no reference
+                            counterpart): primal-dual active-set corrections
+                            after the first reduced KKT solve; 0 = exactly
+                            one reduced solve                                */
 } qtqp_options;
 
 /* One QP of a batch.  Offsets are element offsets into the caller's pools. */
@@ -80,6 +84,8 @@ typedef struct {
   int32_t fp32_factorizations;
   int32_t fp64_factorizations;
   int32_t ir_solves;        /* backend solves summed over all KKT solves       */
+  int32_t warm_started;     /* 1: the learned warm start was accepted          */
+  int32_t reserved;
   double tau;               /* final tau                                       */
   double pcost, dcost, pres, dres, gap;
 } qtqp_result;
@@ -212,7 +218,65 @@ int qtqp_band_batch_solve(const qtqp_band_instance* d_inst,
                           double* d_x_pool, double* d_y_pool, double* d_s_pool,
                           qtqp_result* d_results, qtqp_iter_stats* d_stats,
                           void* d_workspace, size_t workspace_bytes,
-                          const qtqp_options* opt, void* stream);
+                          const qtqp_options* opt, const double* d_warm_x,
+                          const double* d_warm_y, const uint8_t* d_warm_active,
+                          void* stream);
+/* d_warm_x / d_warm_y / d_warm_active (no reference counterpart): null for
+ * the plain method, or a learned warm start laid out like the x / y pools
+ * (original scaling) plus one active flag per constraint row.  Each instance
+ * then first solves the KKT system of the equality QP on its active rows
+ * (opt->warm_corrections primal-dual corrections of the set at most) and
+ * keeps that point only if the plain termination test reports SOLVED for it;
+ * otherwise the plain method runs from its usual start.
+ * qtqp_result.warm_started tells which. */
+
+/* ---- learned warm start: MLP kernels (no reference counterpart) --------- *
+ * theta -> 256 -> 256 -> (n + m) MLP, FP32, all matrices row-major.  Used to
+ * train the network on plain-method solutions of a parametric family and to
+ * produce warm starts for qtqp_band_batch_solve. */
+/* C = alpha op(A) op(B) + beta C (+ bias per column) (ReLU if relu != 0);
+ * op(A) is M x K (A stored K x M if trans_a), op(B) is K x N (B stored
+ * N x K if trans_b).  C is not read when beta == 0. */
+int qtqp_mlp_gemm(int32_t M, int32_t N, int32_t K, float alpha, const float* d_a,
+                  int32_t lda, int32_t trans_a, const float* d_b, int32_t ldb,
+                  int32_t trans_b, float beta, float* d_c, int32_t ldc,
+                  const float* d_bias, int32_t relu, void* stream);
+/* dh[i] = h[i] > 0 ? dh[i] : 0 (backward of the ReLU whose output is h). */
+int qtqp_mlp_relu_grad(float* d_dh, const float* d_h, int64_t count, void* stream);
+/* db[j] = sum_i d[i * cols + j]. */
+int qtqp_mlp_colsum(const float* d_d, int32_t rows, int32_t cols, float* d_db,
+                    void* stream);
+/* dy = 2 (y - t) / count and *d_loss = sum (y - t)^2 (overwritten). */
+int qtqp_mlp_mse_grad(const float* d_y, const float* d_t, int64_t count,
+                      float* d_dy, double* d_loss, void* stream);
+/* One Adam step (bias-corrected, step >= 1). */
+int qtqp_mlp_adam(float* d_p, const float* d_g, float* d_m, float* d_v,
+                  int64_t count, float lr, float beta1, float beta2, float eps,
+                  int32_t step, void* stream);
+/* Network outputs (count x (n+m), standardised) -> warm-start x / y pools
+ * and the active mask.  v = pred * scale + shift; v[0:n] is x, v[n:n+z] the
+ * equality duals, and on inequality row i the signed v = y_i - s_i (at a
+ * solution at most one of the two is non-zero), decoded as y_i = max(v, 0),
+ * active[i] = (v > threshold); active is 1 on the z equality rows. */
+int qtqp_mlp_decode(const float* d_pred, const double* d_scale,
+                    const double* d_shift, int32_t n, int32_t m, int32_t z,
+                    int32_t count, double threshold, double* d_x, double* d_y,
+                    uint8_t* d_active, void* stream);
+
+/* ---- tensor-core building blocks of the large dense KKT factorisation ---- *
+ * (the Gram term A^T D A of src/qtqp/solvers_dense.py:99-116 on tcgen05).
+ * qtqp_tc_split_tf32: hi = x rounded to TF32 (nearest), lo = x - hi.
+ * qtqp_tc_gram_f32: the lower 128 x 128 tiles of C = X X^T (FP32, row-major,
+ * leading dimension ldc; other tiles untouched) for X n x k row-major (ld),
+ * on tcgen05 kind::tf32 with FP32 accumulation: X = hi when split == 0, and
+ * hi hi^T + hi lo^T + lo hi^T (FP32-level accuracy) when split == 1.  n a
+ * multiple of 128, k of 32, ld and ldc multiples of 4, 16-byte aligned
+ * pointers.  *d_err (device int32) is set to 1 if a pipeline wait gave up. */
+int qtqp_tc_split_tf32(const float* d_x, int64_t count, float* d_hi, float* d_lo,
+                       void* stream);
+int qtqp_tc_gram_f32(int32_t n, int32_t k, const float* d_hi, const float* d_lo,
+                     int32_t ld, float* d_c, int32_t ldc, int32_t split,
+                     int32_t* d_err, void* stream);
 
 /* ---- dense KKT backend (the direct.LinearSolver plugin) ------------------ *
  * Replaces one backend of the plugin interface src/qtqp/direct.py:49-109

@@ -266,14 +266,18 @@ def _log_iteration(st: Dict[str, Any]) -> None:
 
 
 def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: str = "auto",
-                _opts=None,
+                warm_start=None, _opts=None,
                 _verbose: bool = False, _start: float | None = None,
                 **solve_kwargs) -> List[Solution]:
   """Solves independent QPs in one persistent GPU launch.
 
-  Accepts the keyword arguments of QTQP.solve (verbose defaults to False).
-  storage: 'auto' (per problem: banded when the Gram matrix is narrow-banded,
-  else dense), 'dense' or 'band'.  Returns one Solution per problem, in order.
+  Accepts the keyword arguments of QTQP.solve (verbose defaults to False)
+  plus warm_corrections.  storage: 'auto' (per problem: banded when the Gram
+  matrix is narrow-banded, else dense), 'dense' or 'band'.  warm_start:
+  (WarmStartMLP, thetas) for instances of a parametric family, all on the
+  banded path -- each instance first solves the KKT system on the predicted
+  active set and keeps that point only if the plain termination test passes,
+  else the plain method runs.  Returns one Solution per problem, in order.
   """
   start = timeit.default_timer() if _start is None else _start
   if _opts is None:
@@ -302,7 +306,15 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
       db = _band.DeviceBandBatch(hb, records=records)
     db.upload()
     t_launch = timeit.default_timer() - start
-    db.launch()
+    if warm_start is not None:
+      model, thetas = warm_start
+      if kind != "band" or len(idx) != len(problems):
+        raise ValueError("warm_start needs every problem on the banded path")
+      if any((q.n, q.m) != (model.n, model.m) for q in problems):
+        raise ValueError("warm_start: every problem must have the model's (n, m)")
+      db.launch(warm=model.predict_device(np.asarray(thetas)))
+    else:
+      db.launch()
     per[kind] = (idx, *db.fetch(), hb.inst)
   where = {}
   for kind, (idx, res, xp, yp, sp_, st, inst) in per.items():

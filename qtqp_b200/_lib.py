@@ -44,6 +44,14 @@ EXPORTS = (
     "qtqp_kkt_dense_factorize",
     "qtqp_kkt_dense_solve",
     "qtqp_kkt_dense_matvec",
+    "qtqp_mlp_gemm",
+    "qtqp_mlp_relu_grad",
+    "qtqp_mlp_colsum",
+    "qtqp_mlp_mse_grad",
+    "qtqp_mlp_adam",
+    "qtqp_mlp_decode",
+    "qtqp_tc_split_tf32",
+    "qtqp_tc_gram_f32",
 )
 
 
@@ -63,6 +71,7 @@ class Options(ctypes.Structure):
       ("precision", ctypes.c_int32),
       ("collect_stats", ctypes.c_int32),
       ("tau_mode", ctypes.c_int32),
+      ("warm_corrections", ctypes.c_int32),
   ]
 
 
@@ -89,6 +98,8 @@ class Result(ctypes.Structure):
       ("fp32_factorizations", ctypes.c_int32),
       ("fp64_factorizations", ctypes.c_int32),
       ("ir_solves", ctypes.c_int32),
+      ("warm_started", ctypes.c_int32),
+      ("reserved", ctypes.c_int32),
       ("tau", ctypes.c_double),
       ("pcost", ctypes.c_double),
       ("dcost", ctypes.c_double),
@@ -161,7 +172,17 @@ def load() -> ctypes.CDLL:
                                          ctypes.POINTER(BatchPlan)]
     lib.qtqp_band_batch_solve.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp, vp,
                                           vp, vp, vp, vp, vp, vp, sz,
-                                          ctypes.POINTER(Options), vp]
+                                          ctypes.POINTER(Options), vp, vp, vp, vp]
+    f32, f64, i64 = ctypes.c_float, ctypes.c_double, ctypes.c_int64
+    lib.qtqp_mlp_gemm.argtypes = [i32, i32, i32, f32, vp, i32, i32, vp, i32, i32, f32, vp, i32,
+                                  vp, i32, vp]
+    lib.qtqp_mlp_relu_grad.argtypes = [vp, vp, i64, vp]
+    lib.qtqp_mlp_colsum.argtypes = [vp, i32, i32, vp, vp]
+    lib.qtqp_mlp_mse_grad.argtypes = [vp, vp, i64, vp, vp, vp]
+    lib.qtqp_mlp_adam.argtypes = [vp, vp, vp, vp, i64, f32, f32, f32, f32, i32, vp]
+    lib.qtqp_mlp_decode.argtypes = [vp, vp, vp, i32, i32, i32, i32, f64, vp, vp, vp, vp]
+    lib.qtqp_tc_split_tf32.argtypes = [vp, i64, vp, vp, vp]
+    lib.qtqp_tc_gram_f32.argtypes = [i32, i32, vp, vp, i32, vp, i32, i32, vp, vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz
     lib.qtqp_kkt_dense_workspace_bytes.argtypes = [i32, i32]
     lib.qtqp_kkt_dense_set.argtypes = [i32, i32, vp, vp, vp, vp]

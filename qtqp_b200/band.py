@@ -37,10 +37,11 @@ def gram_bandwidth(a: sp.spmatrix, p: sp.spmatrix | None) -> int:
   return bw
 
 
-class BandProblem:
-  """One presolved sparse QP (A, P as scipy matrices; P may be None)."""
+class _Structure:
+  """CSR / CSC / P arrays and bandwidth of one (A, P) pair."""
 
-  def __init__(self, a: sp.spmatrix, b, c, z: int, p: sp.spmatrix | None = None):
+  def __init__(self, a: sp.spmatrix, p: sp.spmatrix | None):
+    self.src = (a, p)  # keeps the sources alive while the cache refers to them
     self.a = sp.csr_matrix(a, dtype=np.float64)
     self.a.sort_indices()
     self.at = sp.csr_matrix(self.a.T)  # CSC of A = CSR of A^T
@@ -49,10 +50,37 @@ class BandProblem:
     if p is not None and sp.csr_matrix(p).nnz:
       self.p = sp.csr_matrix(p, dtype=np.float64)
       self.p.sort_indices()
+    self.bw = gram_bandwidth(self.a, self.p)
+
+
+_STRUCT_CACHE: dict = {}
+
+
+def _structure(a, p) -> _Structure:
+  """Converted structure of (a, p), shared by every problem built from the
+  same matrix objects (a parametric family converts A and P once)."""
+  key = (id(a), id(p))
+  hit = _STRUCT_CACHE.get(key)
+  if hit is not None and hit.src[0] is a and hit.src[1] is p:
+    return hit
+  if len(_STRUCT_CACHE) > 64:
+    _STRUCT_CACHE.clear()
+  st = _Structure(a, p)
+  _STRUCT_CACHE[key] = st
+  return st
+
+
+class BandProblem:
+  """One presolved sparse QP (A, P as scipy matrices; P may be None).
+  Problems built from the same A and P objects share one packed copy."""
+
+  def __init__(self, a: sp.spmatrix, b, c, z: int, p: sp.spmatrix | None = None):
+    self.structure = _structure(a, p)
+    self.a, self.at, self.p = self.structure.a, self.structure.at, self.structure.p
     self.b = np.asarray(b, dtype=np.float64)
     self.c = np.asarray(c, dtype=np.float64)
     self.z = int(z)
-    self.bw = gram_bandwidth(self.a, self.p)
+    self.bw = self.structure.bw
 
 
 class HostBandBatch:
@@ -80,6 +108,7 @@ class HostBandBatch:
       voff += len(arr)
       return o
 
+    packed = {}  # id(structure) -> offsets of its shared A / P arrays
     for i, pr in enumerate(problems):
       m, n = pr.a.shape
       d = inst[i]
@@ -87,16 +116,20 @@ class HostBandBatch:
       d["has_p"] = int(pr.p is not None)
       d["bw"] = min(pr.bw, n - 1)
       d["nnz_a"] = pr.a.nnz
-      d["a_ptr"], d["a_idx"], d["a_val"] = (put_i(pr.a.indptr), put_i(pr.a.indices),
-                                            put_v(pr.a.data))
-      d["at_ptr"], d["at_idx"], d["at_val"] = (put_i(pr.at.indptr), put_i(pr.at.indices),
-                                               put_v(pr.at.data))
-      if pr.p is not None:
-        d["nnz_p"] = pr.p.nnz
-        d["p_ptr"], d["p_idx"], d["p_val"] = (put_i(pr.p.indptr), put_i(pr.p.indices),
-                                              put_v(pr.p.data))
-      else:
-        d["p_ptr"] = put_i(np.zeros(n + 1, dtype=np.int32))
+      d["nnz_p"] = pr.p.nnz if pr.p is not None else 0
+      key = id(pr.structure)
+      if key not in packed:
+        offs = {"a_ptr": put_i(pr.a.indptr), "a_idx": put_i(pr.a.indices),
+                "a_val": put_v(pr.a.data), "at_ptr": put_i(pr.at.indptr),
+                "at_idx": put_i(pr.at.indices), "at_val": put_v(pr.at.data)}
+        if pr.p is not None:
+          offs.update(p_ptr=put_i(pr.p.indptr), p_idx=put_i(pr.p.indices),
+                      p_val=put_v(pr.p.data))
+        else:
+          offs.update(p_ptr=put_i(np.zeros(n + 1, dtype=np.int32)), p_idx=0, p_val=0)
+        packed[key] = offs
+      for name, off in packed[key].items():
+        d[name] = off
       d["n_off"], d["m_off"] = n_off, m_off
       d["st_off"] = i * opts.max_iter
       n_off += n
@@ -153,17 +186,28 @@ class DeviceBandBatch:
       for dst, src in zip((self.ipool, self.vpool, self.b, self.c), self.h_pools):
         dst.copy_(src, non_blocking=True)
 
-  def launch(self, stream=None) -> None:
+  def launch(self, stream=None, warm=None) -> None:
+    """Enqueues the batch solve.  warm = (x, y, active) device tensors laid
+    out like the x / y pools (FP64, FP64, uint8) enables the learned warm
+    start; None runs the plain method."""
     torch = self.torch
     lib = _lib.load()
     st = stream or torch.cuda.current_stream(self.device)
     hb = self.hb
+    wx = wy = wa = None
+    if warm is not None:
+      for t, numel, dt in zip(warm, (hb.n_total, hb.m_total, hb.m_total),
+                              (torch.float64, torch.float64, torch.uint8)):
+        if t.dtype != dt or t.numel() < numel or not t.is_contiguous() or not t.is_cuda:
+          raise ValueError("warm start tensors must be contiguous (x f64, y f64, active u8) "
+                           "on the batch's device, sized like the x / y pools")
+      wx, wy, wa = (t.data_ptr() for t in warm)
     _lib.check(lib.qtqp_band_batch_solve(
         self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan),
         self.ipool.data_ptr(), self.vpool.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
         self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
         self.stats.data_ptr() if self.stats is not None else None,
-        self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts),
+        self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts), wx, wy, wa,
         _lib.stream_handle(st)))
 
   def fetch(self):

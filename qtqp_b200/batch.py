@@ -38,6 +38,7 @@ class SolveOptions:
   collect_stats: bool = False
   precision: str = "fp64"  # "fp64" or "mixed"
   tau_mode: int = 0
+  warm_corrections: int = 0  # learned warm start: active-set corrections
 
   def validate(self) -> None:
     """The reference's argument checks (__init__.py:403-412)."""
@@ -51,6 +52,7 @@ class SolveOptions:
     assert self.max_iterative_refinement_steps >= 1
     assert self.linear_solver_atol >= 0
     assert self.linear_solver_rtol >= 0
+    assert 0 <= self.warm_corrections <= 64
     if self.precision not in ("fp64", "mixed"):
       raise ValueError(f"precision must be 'fp64' or 'mixed', got {self.precision!r}")
 
@@ -61,7 +63,7 @@ class SolveOptions:
         self.linear_solver_atol, self.linear_solver_rtol, int(self.max_iter),
         int(self.max_iterative_refinement_steps), int(bool(self.equilibrate)),
         _lib.PREC_FP64 if self.precision == "fp64" else _lib.PREC_MIXED,
-        int(bool(self.collect_stats)), int(self.tau_mode))
+        int(bool(self.collect_stats)), int(self.tau_mode), int(self.warm_corrections))
 
 
 @dataclasses.dataclass

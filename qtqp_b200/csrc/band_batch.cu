@@ -29,6 +29,9 @@ struct BandParams {
   size_t slot_bytes;
   int32_t num_slots;
   int* counter;
+  const double* warm_x;  // learned warm start (null: plain method)
+  const double* warm_y;
+  const unsigned char* warm_act;
   qtqp_options opt;
 };
 
@@ -64,7 +67,12 @@ __global__ void __launch_bounds__(kBandThreads) band_batch_kernel(const BandPara
     s.phase = 0;
     s.o = &sopt;
     double* st = p.stats ? reinterpret_cast<double*>(p.stats + d.st_off) : nullptr;
-    s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off);
+    if (p.warm_act != nullptr) {
+      s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off,
+              p.warm_x + d.n_off, p.warm_y + d.m_off, p.warm_act + d.m_off);
+    } else {
+      s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off);
+    }
     __syncthreads();
     if (threadIdx.x == 0) next_idx = atomicAdd(p.counter, 1) + p.num_slots;
     __syncthreads();
@@ -124,7 +132,8 @@ extern "C" int qtqp_band_batch_solve(const qtqp_band_instance* d_inst, const int
                                      double* d_s_pool, qtqp_result* d_results,
                                      qtqp_iter_stats* d_stats, void* d_workspace,
                                      size_t workspace_bytes, const qtqp_options* opt,
-                                     void* stream) {
+                                     const double* d_warm_x, const double* d_warm_y,
+                                     const uint8_t* d_warm_active, void* stream) {
   if (plan == nullptr || opt == nullptr)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_band_batch_solve: null plan/options");
   if (plan->num_groups == 0) return QTQP_OK;
@@ -141,6 +150,10 @@ extern "C" int qtqp_band_batch_solve(const qtqp_band_instance* d_inst, const int
   if (opt->max_iter < 1 || opt->max_iterative_refinement_steps < 1 ||
       !(opt->step_size_scale > 0.0 && opt->step_size_scale < 1.0))
     return fail(QTQP_ERR_BAD_ARG, "qtqp_band_batch_solve: invalid options");
+  if (d_warm_active != nullptr && (d_warm_x == nullptr || d_warm_y == nullptr))
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_band_batch_solve: warm start needs x, y and active");
+  if (opt->warm_corrections < 0 || opt->warm_corrections > 64)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_band_batch_solve: warm_corrections must be in [0, 64]");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc = cuda_check(cudaMemsetAsync(d_workspace, 0, kBandHeader, st), "cudaMemsetAsync");
   if (rc) return rc;
@@ -167,6 +180,9 @@ extern "C" int qtqp_band_batch_solve(const qtqp_band_instance* d_inst, const int
   p.slots = static_cast<char*>(d_workspace) + G.slot_off;
   p.slot_bytes = G.slot_bytes;
   p.counter = static_cast<int*>(d_workspace);
+  p.warm_x = d_warm_x;
+  p.warm_y = d_warm_y;
+  p.warm_act = d_warm_active;
   p.opt = *opt;
   const int grid = std::max(1, std::min({G.count, G.slots, sms * std::max(per_sm, 1)}));
   p.num_slots = grid;

@@ -91,6 +91,124 @@ __device__ __forceinline__ void group_sync() {
   }
 }
 
+// ----------------------------------------------------------------------------
+// Grid-wide barrier and reductions of a cooperative launch (every block
+// resident), for one large QP solved by the whole GPU.  The barrier is a
+// generation counter in global memory; a wait that exceeds kGridWaitLimit
+// polls sets the sticky `err` flag, after which every barrier returns at once
+// (the solve then finishes its bounded loops and reports the error).
+// ----------------------------------------------------------------------------
+constexpr int kGridMaxBlocks = 256;
+constexpr int kGridBT = 256;  // threads per block of a grid-mode solve
+constexpr uint32_t kGridWaitLimit = 1u << 25;
+
+struct GridCtl {
+  unsigned int count;  // arrivals in the current generation
+  unsigned int gen;    // completed barriers
+  int err;             // 1: a barrier wait gave up
+  int pad;
+  double part[2][kGridMaxBlocks][kRedMax];  // per-block partials (double-buffered)
+};
+
+__device__ __forceinline__ void grid_sync(GridCtl* g) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile GridCtl* vg = g;
+    if (!vg->err) {
+      const unsigned int gen = vg->gen;
+      __threadfence();
+      const unsigned int arrived = atomicAdd(&g->count, 1u) + 1u;
+      if (arrived == gridDim.x) {
+        atomicExch(&g->count, 0u);
+        __threadfence();
+        atomicAdd(&g->gen, 1u);
+      } else {
+        uint32_t it = 0;
+        while (vg->gen == gen && !vg->err) {
+          if (++it > kGridWaitLimit) {
+            atomicExch(&g->err, 1);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+}
+
+// NS sums and NM maxima over every thread of the grid; all threads receive
+// the same values (the partials are combined in one fixed order in every
+// block, so control flow that depends on them agrees across blocks).  `red`
+// is shared scratch of 2 * (blockDim.x / 32) * kRedMax doubles; `phase`
+// alternates the global partial buffers (see block_reduce).
+template <int BT, int NS, int NM>
+__device__ __forceinline__ void grid_reduce(double (&sums)[NS > 0 ? NS : 1],
+                                            double (&maxs)[NM > 0 ? NM : 1], double* red,
+                                            GridCtl* g, int& phase) {
+  static_assert(NS + NM <= kRedMax, "too many reduction slots");
+  constexpr int NW = BT / 32;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) sums[k] += __shfl_xor_sync(0xffffffffu, sums[k], off);
+#pragma unroll
+    for (int k = 0; k < NM; ++k)
+      maxs[k] = nanmax(maxs[k], __shfl_xor_sync(0xffffffffu, maxs[k], off));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* wbuf = red;                // NW x kRedMax warp partials
+  double* res = red + NW * kRedMax;  // kRedMax results
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) wbuf[warp * kRedMax + k] = sums[k];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) wbuf[warp * kRedMax + NS + k] = maxs[k];
+  }
+  __syncthreads();
+  double* part = &g->part[phase][0][0];
+  phase ^= 1;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      double acc = 0.0;
+      for (int w = 0; w < NW; ++w) acc += wbuf[w * kRedMax + k];
+      part[blockIdx.x * kRedMax + k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+      double acc = wbuf[NS + k];
+      for (int w = 1; w < NW; ++w) acc = nanmax(acc, wbuf[w * kRedMax + NS + k]);
+      part[blockIdx.x * kRedMax + NS + k] = acc;
+    }
+  }
+  grid_sync(g);
+  if (warp == 0) {
+    const int nb = gridDim.x;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      double acc = 0.0;
+      for (int b = lane; b < nb; b += 32) acc += part[b * kRedMax + k];
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) res[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+      double acc = part[NS + k];  // block 0's partial starts every lane
+      for (int b = lane; b < nb; b += 32) acc = nanmax(acc, part[b * kRedMax + NS + k]);
+      for (int off = 16; off > 0; off >>= 1)
+        acc = nanmax(acc, __shfl_xor_sync(0xffffffffu, acc, off));
+      if (lane == 0) res[NS + k] = acc;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NS; ++k) sums[k] = res[k];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) maxs[k] = res[NS + k];
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

@@ -41,7 +41,7 @@ enum VecId : int {
   kPW,       // [P_eq K^{-1}q_x; 1/sqrt(Ry)]
   kRS,       // [P_eq K^{-1}r_x; s]
   kXD,       // [P_eq x; d_s]
-  kCT,       // [FP32 scratch (2n floats); Mehrotra correction]
+  kCT,       // [FP32 scratch (2n floats); Mehrotra correction / warm-start rows]
   kW,        // triangular-solve scratch (FP64)
   kNumVec
 };
@@ -179,6 +179,27 @@ struct Ipm {
   double* Lb;
   int bw, nnz_a, nnz_p;
 
+  // Grid mode (NT > 1024, FMT == kFmtLarge): the group is a cooperative grid
+  // of NT / kGridBT blocks; barriers and reductions go through gctl.
+  GridCtl* gctl;
+
+  __device__ __forceinline__ void sync() const {
+    if constexpr (NT > 1024) {
+      grid_sync(gctl);
+    } else {
+      sync();
+    }
+  }
+  template <int NS, int NM>
+  __device__ __forceinline__ void reduce(double (&sums)[NS > 0 ? NS : 1],
+                                         double (&maxs)[NM > 0 ? NM : 1]) {
+    if constexpr (NT > 1024) {
+      grid_reduce<kGridBT, NS, NM>(sums, maxs, red, gctl, phase);
+    } else {
+      reduce<NS, NM>(sums, maxs);
+    }
+  }
+
   __device__ __forceinline__ double* vec(int id) const { return V + size_t(id) * np; }
   // First index >= lo owned by this thread (k % NT == tid).
   __device__ __forceinline__ int own(int lo) const { return lo + ((tid - lo) & (NT - 1)); }
@@ -266,7 +287,7 @@ struct Ipm {
     for (int i = warp; i < n; i += NW)
       for (int j = lane; j < n; j += 32) P[i * ldp + j] = has_p ? P0[size_t(i) * n + j] : 0.0;
     for (int k = tid; k < N; k += NT) de[k] = 1.0;
-    group_sync<NT>();
+    sync();
     if (equilibrate) {
       const double* Ap = A;
       const double* Pp = P;
@@ -289,7 +310,7 @@ struct Ipm {
                           acc[0] = fmax(acc[0], fabs(Ap[k * la + j]));
                         },
                         [&](int k, double* acc) { sc[nn + k] = scale_of(acc[0]); });
-        group_sync<NT>();
+        sync();
         for (int i = warp; i < m; i += NW) {
           const double di = sc[n + i];
           for (int j = lane; j < n; j += 32) A[i * lda + j] *= di * sc[j];
@@ -301,7 +322,7 @@ struct Ipm {
           }
         }
         for (int k = tid; k < N; k += NT) de[k] *= sc[k];
-        group_sync<NT>();
+        sync();
       }
     }
     double* q = vec(kQ);
@@ -319,10 +340,10 @@ struct Ipm {
         mx[0] = nanmax(mx[0], fabs(b0[k - n]));
       }
     }
-    block_reduce<NT, 0, 2>(dummy, mx, red, phase);
+    reduce<0, 2>(dummy, mx);
     nb = mx[0];
     nc = mx[1];
-    group_sync<NT>();
+    sync();
   }
 
   // --------------------------------------------------------------------------
@@ -455,7 +476,7 @@ struct Ipm {
         }
       }
     }
-    block_reduce<NT, 0, 1>(dummy, dmax, red, phase);
+    reduce<0, 1>(dummy, dmax);
     const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -481,7 +502,7 @@ struct Ipm {
       }
     };
     publish(0, buf0);
-    group_sync<NT>();
+    sync();
     int info = 0;
     for (int k = 0; k < n; ++k) {
       T* buf = (k & 1) ? buf1 : buf0;
@@ -520,7 +541,7 @@ struct Ipm {
         }
       }
       if (k + 1 < n) publish(k + 1, (k & 1) ? buf0 : buf1);
-      group_sync<NT>();
+      sync();
     }
     if (info == 0 && mine) {
 #pragma unroll
@@ -531,7 +552,7 @@ struct Ipm {
           if (i < n && j <= i) g[i * ldg + j] = acc[a][b];
         }
     }
-    group_sync<NT>();
+    sync();
     if (info == 0) invert_diag_blocks<T>(g);
     QTQP_TOC(kPhChol);
     return info;
@@ -589,12 +610,12 @@ struct Ipm {
         }
       }
     }
-    block_reduce<NT, 0, 1>(dummy, dmax, red, phase);
+    reduce<0, 1>(dummy, dmax);
     // FP64: the reference's 1e-14 relative jitter (solvers_dense.py:112).
     // FP32: the same idea at FP32 resolution (2^-22 relative).
     const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
     for (int k = tid; k < n; k += NT) g[k * ldg + k] = T(double(g[k * ldg + k]) + jit);
-    group_sync<NT>();
+    sync();
     QTQP_TOC(kPhGram);
     QTQP_RETIC();
     const int info = cholesky<T>(g);
@@ -626,7 +647,7 @@ struct Ipm {
       if (k == n) break;
       const T d = g[k * ldg + k];
       if (!(d > T(0))) {
-        group_sync<NT>();
+        sync();
         return k + 1;
       }
       const T inv_d = T(1) / d;
@@ -635,9 +656,9 @@ struct Ipm {
         for (int i = j + lane; i < n; i += 32) g[i * ldg + j] = fma(-g[i * ldg + k], t, g[i * ldg + j]);
       }
       d_prev = d;
-      group_sync<NT>();
+      sync();
     }
-    group_sync<NT>();
+    sync();
     invert_diag_blocks<T>(g);
     return 0;
   }
@@ -672,7 +693,7 @@ struct Ipm {
         __syncwarp();
       }
     }
-    group_sync<NT>();
+    sync();
   }
 
   // Solves L L^T v = v in place with the block-inverted factor: forward
@@ -690,7 +711,7 @@ struct Ipm {
         for (int k = 0; k <= r; ++k) acc = fma(row[k], v[kb + k], acc);
         w[kb + r] = acc;
       }
-      group_sync<NT>();
+      sync();
       if (kb + bs < n) {
         for (int i = kb + bs + tid; i < n; i += NT) {
           const T* li = g + i * ldg + kb;
@@ -698,7 +719,7 @@ struct Ipm {
           for (int k = 0; k < bs; ++k) acc = fma(-li[k], w[kb + k], acc);
           v[i] = acc;
         }
-        group_sync<NT>();
+        sync();
       }
     }
     for (int blk = nblk - 1; blk >= 0; --blk) {
@@ -708,14 +729,14 @@ struct Ipm {
         for (int k = r; k < bs; ++k) acc = fma(g[(kb + k) * ldg + kb + r], w[kb + k], acc);
         v[kb + r] = acc;
       }
-      group_sync<NT>();
+      sync();
       if (kb > 0) {
         for (int i = tid; i < kb; i += NT) {
           T acc = w[i];
           for (int k = 0; k < bs; ++k) acc = fma(-g[(kb + k) * ldg + i], v[kb + k], acc);
           w[i] = acc;
         }
-        group_sync<NT>();
+        sync();
       }
     }
   }
@@ -750,7 +771,7 @@ struct Ipm {
                   t32[k] = float(g);
                 }
               });
-    group_sync<NT>();
+    sync();
     if (fp64) {
       chol_solve<double>(G, tmp, vec(kW));
     } else {
@@ -863,11 +884,11 @@ struct Ipm {
         krhs[k] = r;
         mx[0] = nanmax(mx[0], fabs(r));
       }
-      group_sync<NT>();
+      sync();
       QTQP_TIC();
       kkt_residual(sol, krhs, res, mx[1], mx[2]);
-      block_reduce<NT, 0, 3>(dummy, mx, red, phase);
-      group_sync<NT>();
+      reduce<0, 3>(dummy, mx);
+      sync();
       QTQP_TOC(kPhResidual);
       out.rhs_norm = mx[0];
       out.final_res = mx[1];
@@ -881,12 +902,12 @@ struct Ipm {
       out.solves = it;
       const double prev = rn;
       kkt_solve(res, sol, true, fp64);
-      group_sync<NT>();
+      sync();
       QTQP_TIC();
       double mx[2] = {0.0, 0.0};
       kkt_residual(sol, krhs, res, mx[0], mx[1]);
-      block_reduce<NT, 0, 2>(dummy, mx, red, phase);
-      group_sync<NT>();
+      reduce<0, 2>(dummy, mx);
+      sync();
       QTQP_TOC(kPhResidual);
       rn = mx[0];
       out.nan = mx[1] > 0.0;
@@ -911,7 +932,7 @@ struct Ipm {
   __device__ IrOutcome ir_solve_policy(RhsF rhs_k, WarmF warm_k, double* sol, bool& fp64,
                                        int& n32, int& n64, int& err) {
     for (int k = tid; k < N; k += NT) sol[k] = warm_k(k);
-    group_sync<NT>();
+    sync();
     IrOutcome r = ir_solve(rhs_k, sol, fp64);
     if (!fp64 && r.status != 1) {
       fp64 = true;
@@ -922,7 +943,7 @@ struct Ipm {
         return r;
       }
       for (int k = tid; k < N; k += NT) sol[k] = warm_k(k);
-      group_sync<NT>();
+      sync();
       r = ir_solve(rhs_k, sol, fp64);
     }
     return r;
@@ -974,7 +995,7 @@ struct Ipm {
                   [&](int k, double* acc) { epi(k, acc[0]); });
       }
     }
-    block_reduce<NT, 5, 0>(sm, dummy, red, phase);
+    reduce<5, 0>(sm, dummy);
     const bool accurate = irr.status == 1 || irr.final_res < 1e-7;
     if (o->tau_mode == 0 && accurate) {
       double ta = mu + ic.kqq;
@@ -1040,7 +1061,7 @@ struct Ipm {
       if (ds < -kEps) mx[0] = fmax(mx[0], -(-s[k] / ds));
       if (dy < -kEps) mx[0] = fmax(mx[0], -(-xy[k] / dy));
     }
-    block_reduce<NT, 0, 1>(dummy, mx, red, phase);
+    reduce<0, 1>(dummy, mx);
     return fmin(1.0, -mx[0]);
   }
 
@@ -1107,7 +1128,7 @@ struct Ipm {
       rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], xy[j], acc[0]); },
                 [&](int k, double* acc) { epi_y(k, acc[0]); });
     }
-    block_reduce<NT, 3, 9>(sm, mx, red, phase);
+    reduce<3, 9>(sm, mx);
     const double ctx = sm[0], bty = sm[1], xpx = has_p ? sm[2] : 0.0;
     const double pcost = (ctx + 0.5 * xpx * inv_tau) * inv_tau;
     const double dcost = (-bty - 0.5 * xpx * inv_tau) * inv_tau;
@@ -1171,7 +1192,7 @@ struct Ipm {
           b[3] = fmax(b[3], -soy);
         }
       }
-      block_reduce<NT, 5, 5>(a, b, red, phase);
+      reduce<5, 5>(a, b);
       const int cnt = m - z;
       const double mean_sy = a[1] / cnt, mean_soy = a[2] / cnt;
       double v[2] = {0, 0};
@@ -1182,7 +1203,7 @@ struct Ipm {
         v[0] += (sy - mean_sy) * (sy - mean_sy);
         v[1] += (soy - mean_soy) * (soy - mean_soy);
       }
-      block_reduce<NT, 2, 0>(v, dummy, red, phase);
+      reduce<2, 0>(v, dummy);
       if (tid == 0) {
         st[kStCompl] = fabs(a[0] * inv_tau * inv_tau);
         st[kStNormS] = mx[6];
@@ -1217,11 +1238,145 @@ struct Ipm {
     b[kLinPrec] = fp64 ? 64 : 32;
   }
 
+  // out[n + i] = (A v)_i (equilibrated A).  Exit: needs a barrier before
+  // other threads read out.
+  __device__ void a_times(const double* v, double* out) const {
+    if constexpr (FMT == kFmtBand) {
+      for (int k = own(n); k < N; k += NT) out[k] = band_a_row(v, k - n);
+    } else {
+      const double* Ap = A;
+      const int la = lda, nn = n;
+      rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], v[j], acc[0]); },
+                [&](int k, double* acc) { out[nn + k] = acc[0]; });
+    }
+  }
+
   // --------------------------------------------------------------------------
-  // The whole solve (QTQP._solve_impl, __init__.py:429-614).
+  // Learned warm start (no reference counterpart).  Given a predicted point
+  // (wx, wy) in the original scaling and a predicted active set (act[i] for
+  // the inequality rows), solve the KKT system of the equality QP
+  //   min 1/2 x'Px + c'x  s.t.  a_i x = b_i for i < z or i active
+  // (free rows carry a huge D, i.e. y_i = 0) by the IPM's own regularised
+  // factorisation and FP64 refinement; then y_i = 0 on free rows and
+  // s = b - A x.  Each solution is projected onto the cone (y[z:] >= 0,
+  // s[z:] >= 0) and accepted only if the plain termination test reports
+  // SOLVED for it at tau = 1.  Up to options.warm_corrections primal-dual
+  // active-set corrections may follow a rejected solution (tight rows whose
+  // dual came out negative leave, free rows whose slack came out negative
+  // enter, and the reduced system is solved again) while the set changes;
+  // 0 keeps exactly one reduced solve.  On false the caller runs the plain
+  // method from its usual starting point.
+  // --------------------------------------------------------------------------
+  __device__ bool warm_try(const double* wx, const double* wy, const unsigned char* act,
+                           double nb, double nc, bool& fp64, int& n32, int& n64, int& nsolves) {
+    const qtqp_options& op = *o;
+    double* xy = vec(kXY);
+    double* s = vec(kRS);
+    double* xyc = vec(kXYC);
+    double* reg = vec(kREG);
+    double* corr = vec(kCORR);
+    double* pi = vec(kPI);
+    double* pw = vec(kPW);
+    double* tight = vec(kCT);  // at [n, N): 1.0 where the row is held tight
+    const double* de = vec(kDE);
+    const double* q = vec(kQ);
+    const double dmin = fmax(op.min_static_regularization, 1e-10);
+    const double big = 1e10;
+    for (int k = tid; k < N; k += NT) {
+      if (k < n) {
+        xy[k] = wx[k] / de[k];
+      } else {
+        const int i = k - n;
+        tight[k] = (i < z || act[i] != 0) ? 1.0 : 0.0;
+        xy[k] = wy[i] / de[k];
+      }
+    }
+    double dummy[1] = {0.0};
+    const int rounds = 1 + max(0, min(op.warm_corrections, 64));
+    for (int round = 0; round < rounds; ++round) {
+      for (int k = tid; k < N; k += NT) {
+        if (k < n) {
+          const double t = pi[k];
+          const double r = fmax(t, op.min_static_regularization);
+          reg[k] = r;
+          corr[k] = r - t;
+        } else {
+          const bool tk = tight[k] != 0.0;
+          const double t = -(tk ? 0.0 : big), r = -(tk ? dmin : big);
+          reg[k] = r;
+          corr[k] = r - t;
+          pi[k] = 1.0 / (-r);
+          pw[k] = 1.0 / sqrt(-r);
+        }
+      }
+      sync();
+      int info;
+      if (fp64) {
+        ++n64;
+        info = factorize<double>();
+      } else {
+        ++n32;
+        info = factorize<float>();
+        if (info != 0) {
+          fp64 = true;
+          ++n64;
+          info = factorize<double>();
+        }
+      }
+      if (info != 0) return false;  // not an error of the problem: fall back
+      int err = 0;
+      IrOutcome r = ir_solve_policy([&](int k) { return -q[k]; }, [&](int k) { return xy[k]; },
+                                    xyc, fp64, n32, n64, err);
+      nsolves += r.solves;
+      if (err || r.nan) return false;
+      a_times(xyc, s);  // s[n + i] = (A x)_i
+      sync();
+      double v[1] = {0.0};  // 1 when a row changes
+      for (int k = tid; k < N; k += NT) {
+        if (k < n) {
+          xy[k] = xyc[k];
+          continue;
+        }
+        const int i = k - n;
+        const double sk = q[k] - s[k];
+        if (i < z) {
+          xy[k] = xyc[k];
+          s[k] = 0.0;
+        } else if (tight[k] != 0.0) {
+          xy[k] = fmax(xyc[k], 0.0);
+          if (xyc[k] < 0.0) {
+            tight[k] = 0.0;
+            v[0] = 1.0;
+          }
+          s[k] = fmax(sk, 0.0);
+        } else {
+          xy[k] = 0.0;
+          if (sk < 0.0) {
+            tight[k] = 1.0;
+            v[0] = 1.0;
+          }
+          s[k] = fmax(sk, 0.0);
+        }
+      }
+      reduce<0, 1>(dummy, v);
+      // The plain test judges the projected point: clipped duals and slacks
+      // show up in its residuals.
+      if (termination(1.0, nb, nc, nullptr, false) == QTQP_STATUS_SOLVED) return true;
+      if (!(v[0] > 0.0)) return false;  // the set is stable yet not acceptable
+      sync();
+    }
+    return false;
+  }
+
+  // --------------------------------------------------------------------------
+  // The whole solve (QTQP._solve_impl, __init__.py:429-614).  warm_*: the
+  // learned warm start of this instance (x and y in the original scaling,
+  // active-row mask), or null for the plain method.
   // --------------------------------------------------------------------------
   __device__ void solve(qtqp_result* result, double* stats, double* x_out, double* y_out,
-                        double* s_out) {
+                        double* s_out, const double* warm_x = nullptr,
+                        const double* warm_y = nullptr,
+                        const unsigned char* warm_act = nullptr) {
     const qtqp_options& op = *o;
     const uint64_t t_start = globaltimer_ns();
     double nb, nc;
@@ -1229,6 +1384,31 @@ struct Ipm {
       QTQP_TIC();
       load_and_equilibrate(op.equilibrate != 0, nb, nc);
       QTQP_TOC(kPhLoad);
+    }
+    int w32 = 0, w64 = 0, wsolves = 0;  // work of a rejected warm start counts too
+    if (warm_act != nullptr) {
+      bool fp64w = op.precision == QTQP_PREC_FP64;
+      const bool ok = warm_try(warm_x, warm_y, warm_act, nb, nc, fp64w, w32, w64, wsolves);
+      sync();
+      if (ok) {
+        finish(QTQP_STATUS_SOLVED, 1.0, x_out, y_out, s_out);
+        if (tid == 0) {
+          result->status = QTQP_STATUS_SOLVED;
+          result->iterations = 0;
+          result->error = 0;
+          result->fp32_factorizations = w32;
+          result->fp64_factorizations = w64;
+          result->ir_solves = wsolves;
+          result->warm_started = 1;
+          result->tau = 1.0;
+          result->pcost = last_pcost;
+          result->dcost = last_dcost;
+          result->pres = last_pres;
+          result->dres = last_dres;
+          result->gap = last_gap;
+        }
+        return;
+      }
     }
     double* xy = vec(kXY);
     double* s = vec(kRS);
@@ -1256,10 +1436,10 @@ struct Ipm {
       ds[k] = 0.0;
       ct[k] = 0.0;
     }
-    group_sync<NT>();
+    sync();
     double tau = 1.0, alpha = 0.0, sigma = 0.0, mu = 0.0;
     bool fp64 = op.precision == QTQP_PREC_FP64;
-    int n32 = 0, n64 = 0, nsolves = 0, err = 0;
+    int n32 = w32, n64 = w64, nsolves = wsolves, err = 0;
     int status = QTQP_STATUS_UNFINISHED;
     int it = 0, taken = 0;
     const double cnt = double(m - z);
@@ -1274,7 +1454,7 @@ struct Ipm {
           sm[0] = fma(xy[k], xy[k], sm[0]);
           if (k >= n) sm[1] = fma(xy[k], s[k], sm[1]);
         }
-        block_reduce<NT, 2, 0>(sm, dummy, red, phase);
+        reduce<2, 0>(sm, dummy);
         const double scale = sqrt(double(m - z + 1)) / fmax(kEps, sqrt(sm[0] + tau * tau));
         for (int k = tid; k < N; k += NT) {
           xy[k] *= scale;
@@ -1286,7 +1466,7 @@ struct Ipm {
       }
       // DirectKktSolver.update (direct.py:183-216).
       kkt_diag(mu, op.min_static_regularization);
-      group_sync<NT>();
+      sync();
       {
         int info;
         if (fp64) {
@@ -1352,7 +1532,7 @@ struct Ipm {
                       [&](int k, double* acc) { epi(k, acc[0], acc[1]); });
           }
         }
-        block_reduce<NT, 5, 0>(sm, dummy, red, phase);
+        reduce<5, 0>(sm, dummy);
         ic.kqq = sm[0];
         ic.kqpkq = sm[1];
         ic.qz = sm[2];
@@ -1404,7 +1584,7 @@ struct Ipm {
             sm[2] = fma(va, sa, sm[2]);
           }
         }
-        block_reduce<NT, 3, 0>(sm, dummy, red, phase);
+        reduce<3, 0>(sm, dummy);
         const double ta = tau + alpha_p * dtp;
         const double nrm2 = sm[0] + sm[1] + ta * ta;
         const double scale_sq = double(m - z + 1) / fmax(kEps * kEps, nrm2);
@@ -1428,7 +1608,7 @@ struct Ipm {
         }
         return r;
       };
-      group_sync<NT>();  // x_p, y_p complete before the corrector reads them
+      sync();  // x_p, y_p complete before the corrector reads them
       IrOutcome rc = ir_solve_policy(rhs_corr, [&](int k) { return xyp[k]; }, xyc, fp64, n32,
                                      n64, err);
       nsolves += rc.solves;
@@ -1463,7 +1643,7 @@ struct Ipm {
         tau += stp * (tau_c - tau);
         tau = fmax(tau, 1e-30);
       }
-      group_sync<NT>();
+      sync();
       {
         QTQP_TIC();
         status = termination(tau, nb, nc, st, op.collect_stats != 0);
@@ -1485,7 +1665,7 @@ struct Ipm {
       if (stats != nullptr && tid == 0)
         stats[size_t(taken - 1) * QTQP_STATS_DOUBLES + kStStatus] = status;
     }
-    group_sync<NT>();
+    sync();
     finish(status, tau, x_out, y_out, s_out);
     if (tid == 0) {
       result->status = err ? QTQP_STATUS_FAILED : status;
@@ -1494,6 +1674,7 @@ struct Ipm {
       result->fp32_factorizations = n32;
       result->fp64_factorizations = n64;
       result->ir_solves = nsolves;
+      result->warm_started = 0;
       result->tau = tau;
       result->pcost = last_pcost;
       result->dcost = last_dcost;
@@ -1520,7 +1701,7 @@ struct Ipm {
           sm[0] = fma(b0[k - n], de[k] * xy[k], sm[0]);
         }
       }
-      block_reduce<NT, 2, 0>(sm, dummy, red, phase);
+      reduce<2, 0>(sm, dummy);
     }
     for (int k = tid; k < N; k += NT) {
       if (k < n) {
@@ -1606,7 +1787,7 @@ struct Ipm {
     }
     for (int q = tid; q < nnz_p; q += NT) pv[q] = has_p ? pv0[q] : 0.0;
     for (int k = tid; k < N; k += NT) de[k] = 1.0;
-    group_sync<NT>();
+    sync();
     auto scale_of = [](double mx) {
       if (mx == 0.0) mx = 1.0;
       return fmin(fmax(1.0 / sqrt(mx), 1e-3), 1e3);
@@ -1624,7 +1805,7 @@ struct Ipm {
           }
           sc[k] = scale_of(mx);
         }
-        group_sync<NT>();
+        sync();
         for (int r = tid; r < m; r += NT) {
           const double dr = sc[n + r];
           for (int q = ip[r]; q < ip[r + 1]; ++q) av[q] *= dr * sc[ix[q]];
@@ -1640,7 +1821,7 @@ struct Ipm {
           }
         }
         for (int k = tid; k < N; k += NT) de[k] *= sc[k];
-        group_sync<NT>();
+        sync();
       }
     }
     double* q = vec(kQ);
@@ -1666,10 +1847,10 @@ struct Ipm {
         mx[0] = nanmax(mx[0], fabs(b0[k - n]));
       }
     }
-    block_reduce<NT, 0, 2>(dummy, mx, red, phase);
+    reduce<0, 2>(dummy, mx);
     nb = mx[0];
     nc = mx[1];
-    group_sync<NT>();
+    sync();
   }
 
   // (P_off v)_k for the owner of row k (P symmetric, so row k = column k).
@@ -1725,10 +1906,10 @@ struct Ipm {
       col[0] = T(reg[j]) + col[0];
       dmax[0] = nanmax(dmax[0], double(col[0]));
     }
-    block_reduce<NT, 0, 1>(dummy, dmax, red, phase);
+    reduce<0, 1>(dummy, dmax);
     const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
     for (int j = tid; j < n; j += NT) L[size_t(j) * ldl] = T(double(L[size_t(j) * ldl]) + jit);
-    group_sync<NT>();
+    sync();
     QTQP_TOC(kPhGram);
     QTQP_RETIC();
     const int warp = tid >> 5, lane = tid & 31;
@@ -1758,9 +1939,9 @@ struct Ipm {
         for (int i = j + lane; i <= last; i += 32) cj[i - j] = fma(-ck[i - k], t, cj[i - j]);
       }
       d_prev = d;
-      group_sync<NT>();
+      sync();
     }
-    group_sync<NT>();
+    sync();
     QTQP_TOC(kPhChol);
     return info;
   }
@@ -1793,7 +1974,7 @@ struct Ipm {
         __syncwarp();
       }
     }
-    group_sync<NT>();
+    sync();
   }
 
   __device__ void band_kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
@@ -1815,7 +1996,7 @@ struct Ipm {
         t32[j] = float(g);
       }
     }
-    group_sync<NT>();
+    sync();
     if (fp64) {
       band_chol_solve<double>(tmp, vec(kW));
     } else {
