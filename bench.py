@@ -38,9 +38,10 @@ CPU_SAMPLE = 1024          # instances in the CPU-baseline sample
 REF_SAMPLE = 1024          # instances per step of the reference arm
 HBM_FALLBACK_GBS = 6650.0  # only if MEASURED_PEAKS.json is absent
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), nominal; for context only
-# DRAM traffic of one dense_batch_kernel launch on this workload, from an ncu
-# capture (profiles/dense_batch_kernel_config1.md); None until captured.
-NCU_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) of one batch solve (its 8 group launches, mixed
+# precision) on this workload, from an ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum (profiles/dense_batch_kernel_config1.md).
+NCU_TRAFFIC_BYTES = 171.6e6
 
 
 def _args():
