@@ -187,7 +187,7 @@ struct Ipm {
     if constexpr (NT > 1024) {
       grid_sync(gctl);
     } else {
-      sync();
+      group_sync<NT>();
     }
   }
   template <int NS, int NM>
@@ -196,7 +196,7 @@ struct Ipm {
     if constexpr (NT > 1024) {
       grid_reduce<kGridBT, NS, NM>(sums, maxs, red, gctl, phase);
     } else {
-      reduce<NS, NM>(sums, maxs);
+      block_reduce<NT, NS, NM>(sums, maxs, red, phase);
     }
   }
 
