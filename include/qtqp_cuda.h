@@ -263,6 +263,28 @@ int qtqp_mlp_decode(const float* d_pred, const double* d_scale,
                     int32_t count, double threshold, double* d_x, double* d_y,
                     uint8_t* d_active, void* stream);
 
+/* ---- one large dense QP on the whole GPU ---------------------------------- *
+ * Replaces QTQP._solve_impl (src/qtqp/__init__.py:351-614) with the dense
+ * KKT backend (src/qtqp/solvers_dense.py:25-145) for a single large QP: the
+ * same device IPM as the batch, run by one cooperative launch of 128 blocks
+ * (grid barriers and reductions), with a blocked Gram + Cholesky factor
+ * (Gram on tcgen05 tensor cores, TF32 hi + lo split, when opt->precision is
+ * QTQP_PREC_MIXED; FP64 otherwise) and blocked triangular solves.
+ * A: m x n row-major FP64, P: n x n row-major FP64 (null if has_p == 0);
+ * b, c inputs; x, y, s, *d_result outputs (as the batch); d_stats:
+ * qtqp_iter_stats[max_iter] or NULL.  The workspace (>=
+ * qtqp_dense_large_workspace_bytes(n, m), 1024-byte aligned) is private.
+ * m * n < 2^31.  A grid barrier that waits too long ends the solve with
+ * status FAILED and error QTQP_ERR_TIMEOUT. */
+size_t qtqp_dense_large_workspace_bytes(int32_t n, int32_t m);
+int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t has_p,
+                           const double* d_a, const double* d_p,
+                           const double* d_b, const double* d_c, double* d_x,
+                           double* d_y, double* d_s, qtqp_result* d_result,
+                           qtqp_iter_stats* d_stats, void* d_workspace,
+                           size_t workspace_bytes, const qtqp_options* opt,
+                           void* stream);
+
 /* ---- tensor-core building blocks of the large dense KKT factorisation ---- *
  * (the Gram term A^T D A of src/qtqp/solvers_dense.py:99-116 on tcgen05).
  * qtqp_tc_split_tf32: hi = x rounded to TF32 (nearest), lo = x - hi.

@@ -29,6 +29,12 @@ from . import direct
 
 __version__ = "0.0.5+b200"
 
+# Dense QPs with at least this many variables are solved one at a time by the
+# whole GPU (grid mode) instead of one thread block each; a QP solved on its
+# own switches earlier.
+LARGE_N = 1024
+LARGE_N_SINGLE = 256
+
 _HEADER = ("| iter |      pcost |      dcost |     pres |     dres |      gap |"
            "   infeas |       mu |  q, p, c |     time |")
 _SEPARA = ("|------|------------|------------|----------|----------|----------|"
@@ -183,14 +189,18 @@ class QTQP:
     from . import band as _band  # pylint: disable=g-import-not-at-top
     return _band.BandProblem(self.a, self.b, self.c, self.z, self.p if self.p.nnz else None)
 
-  def storage_format(self) -> str:
+  def storage_format(self, single: bool = False) -> str:
     """'band' when the Gram matrix P + A^T D A is narrow-banded (its
-    half-bandwidth at most n/4) and n > 96, else 'dense'."""
+    half-bandwidth at most n/4) and n > 96; otherwise 'large' (the whole GPU
+    on one QP) when n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on
+    its own; else 'dense' (one thread block per QP)."""
     if self.n <= 96:
       return "dense"
     from . import band as _band  # pylint: disable=g-import-not-at-top
     bw = _band.gram_bandwidth(self.a, self.p if self.p.nnz else None)
-    return "band" if 4 * (bw + 1) <= self.n else "dense"
+    if 4 * (bw + 1) <= self.n:
+      return "band"
+    return "large" if self.n >= (LARGE_N_SINGLE if single else LARGE_N) else "dense"
 
   def solve(self, *, atol: float = 1e-7, rtol: float = 1e-8, atol_infeas: float = 1e-8,
             rtol_infeas: float = 1e-9, max_iter: int = 100, step_size_scale: float = 0.99,
@@ -217,7 +227,8 @@ class QTQP:
     if verbose:
       print(f"| QTQP v{__version__}: m={self.m}, n={self.n}, z={self.z}, "
             f"nnz(A)={self.a.nnz}, nnz(P)={self.p.nnz}, linear_solver=CUDA")
-    out = solve_batch([self], _opts=opts, _verbose=verbose, _start=start)[0]
+    out = solve_batch([self], storage=self.storage_format(single=True), _opts=opts,
+                      _verbose=verbose, _start=start)[0]
     return out
 
 
@@ -289,10 +300,25 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     opts, verbose = _opts, _verbose
   _lib.require_device()
   records = bool(verbose or opts.collect_stats)
-  # Dense and banded problems go to their own device batches.
+  # Dense and banded problems go to their own device batches; each large
+  # problem gets the whole GPU in turn.
   kinds = [q.storage_format() if storage == "auto" else storage for q in problems]
+  if any(k not in ("dense", "band", "large") for k in kinds):
+    raise ValueError(f"storage must be 'auto', 'dense', 'band' or 'large', got {storage!r}")
   per = {}  # kind -> (indices, results, x, y, s, stats, inst)
+  where = {}
   t_launch = 0.0
+  if warm_start is not None and any(k != "band" for k in kinds):
+    raise ValueError("warm_start needs every problem on the banded path")
+  for i in [i for i, k in enumerate(kinds) if k == "large"]:
+    from . import large as _large  # pylint: disable=g-import-not-at-top
+    dl = _large.DeviceLarge(problems[i].dense_problem(), opts, records=records)
+    dl.upload()
+    t_launch = timeit.default_timer() - start
+    dl.launch()
+    res, xp, yp, sp_, st = dl.fetch()
+    inst = np.zeros(1, dtype=[("n_off", np.int64), ("m_off", np.int64)])
+    where[i] = (res[0], xp, yp, sp_, None if st is None else st[0], inst[0])
   for kind in ("dense", "band"):
     idx = [i for i, k in enumerate(kinds) if k == kind]
     if not idx:
@@ -308,15 +334,12 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     t_launch = timeit.default_timer() - start
     if warm_start is not None:
       model, thetas = warm_start
-      if kind != "band" or len(idx) != len(problems):
-        raise ValueError("warm_start needs every problem on the banded path")
       if any((q.n, q.m) != (model.n, model.m) for q in problems):
         raise ValueError("warm_start: every problem must have the model's (n, m)")
       db.launch(warm=model.predict_device(np.asarray(thetas)))
     else:
       db.launch()
     per[kind] = (idx, *db.fetch(), hb.inst)
-  where = {}
   for kind, (idx, res, xp, yp, sp_, st, inst) in per.items():
     for j, i in enumerate(idx):
       where[i] = (res[j], xp, yp, sp_, None if st is None else st[j], inst[j])
@@ -327,6 +350,8 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
       raise np.linalg.LinAlgError("Cholesky failed: the KKT Gram matrix is not positive definite")
     if int(r["error"]) == _lib.QTQP_ERR_NAN:
       raise ValueError("Linear solver returned NaNs.")
+    if int(r["error"]) == _lib.QTQP_ERR_TIMEOUT:
+      raise RuntimeError("qtqp_b200: a grid barrier of the large solve timed out")
     n0, m0 = int(d["n_off"]), int(d["m_off"])
     x = x_pool[n0:n0 + q.n].copy()
     y = y_pool[m0:m0 + q.m].copy()

@@ -50,6 +50,8 @@ EXPORTS = (
     "qtqp_mlp_mse_grad",
     "qtqp_mlp_adam",
     "qtqp_mlp_decode",
+    "qtqp_dense_large_workspace_bytes",
+    "qtqp_dense_large_solve",
     "qtqp_tc_split_tf32",
     "qtqp_tc_gram_f32",
 )
@@ -181,6 +183,10 @@ def load() -> ctypes.CDLL:
     lib.qtqp_mlp_mse_grad.argtypes = [vp, vp, i64, vp, vp, vp]
     lib.qtqp_mlp_adam.argtypes = [vp, vp, vp, vp, i64, f32, f32, f32, f32, i32, vp]
     lib.qtqp_mlp_decode.argtypes = [vp, vp, vp, i32, i32, i32, i32, f64, vp, vp, vp, vp]
+    lib.qtqp_dense_large_workspace_bytes.restype = sz
+    lib.qtqp_dense_large_workspace_bytes.argtypes = [i32, i32]
+    lib.qtqp_dense_large_solve.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp,
+                                           vp, vp, sz, ctypes.POINTER(Options), vp]
     lib.qtqp_tc_split_tf32.argtypes = [vp, i64, vp, vp, vp]
     lib.qtqp_tc_gram_f32.argtypes = [i32, i32, vp, vp, i32, vp, i32, i32, vp, vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz

@@ -134,12 +134,20 @@ struct IrOutcome {
 enum MatFormat : int {
   kFmtDense = 0,  // dense A (m x n), dense P, dense Gram G / Cholesky factor
   kFmtBand = 1,   // sparse A (CSR + CSC), sparse P (CSR), banded Gram / factor
+  kFmtLarge = 2,  // one large dense QP on the whole GPU (grid mode, NT > 1024):
+                  // dense A / P in global memory, blocked Gram + Cholesky
 };
 
 // ----------------------------------------------------------------------------
 // The solver state of one instance, replicated in every thread of the block.
 // FMT selects the matrix backend; the interior-point logic is shared.
 // ----------------------------------------------------------------------------
+// Large-format phases (large_ipm.cuh), called from the Ipm dispatch points.
+template <typename T, class S>
+__device__ int large_factorize(S& s);
+template <typename T, class S>
+__device__ void large_chol_solve(S& s, T* v, T* w);
+
 template <int NT, int FMT = kFmtDense>
 struct Ipm {
   int tid;
@@ -182,6 +190,25 @@ struct Ipm {
   // Grid mode (NT > 1024, FMT == kFmtLarge): the group is a cooperative grid
   // of NT / kGridBT blocks; barriers and reductions go through gctl.
   GridCtl* gctl;
+  // Large format: padded sizes (multiples of 128 / 32), the factor in FP64
+  // (g64) or FP32 (g32), both npad x npad row-major (lower triangle), the
+  // inverses of its 128 x 128 diagonal blocks (linv, in the factor's
+  // precision), the split TF32 operands X = (diag(1/sqrt(Ry)) A)^T
+  // (xhi / xlo, npad x mpad), their tensor maps, the CTA's shared-memory
+  // arena (tensor-core ring / staging tiles), its TMEM accumulator and the
+  // per-thread pipeline counters of the tensor-core ring.
+  int npad, mpad;
+  int* linfo;  // factorisation status shared by the grid
+  double* g64;
+  float* g32l;
+  double* linv;
+  float* xhi;
+  float* xlo;
+  const void* map_hi;
+  const void* map_lo;
+  unsigned char* arena;
+  uint32_t tmem;
+  uint32_t tc_load, tc_mma, tc_tiles;
 
   __device__ __forceinline__ void sync() const {
     if constexpr (NT > 1024) {
@@ -409,10 +436,15 @@ struct Ipm {
   // --------------------------------------------------------------------------
   template <typename T>
   QTQP_PHASE int factorize() {
-    if constexpr (FMT == kFmtBand) return band_factorize<T>();
-    const int nb = (n + 3) >> 2;
-    if (nb * (nb + 1) / 2 <= NT) return factorize_regs<T>();
-    return factorize_mem<T>();
+    if constexpr (FMT == kFmtBand) {
+      return band_factorize<T>();
+    } else if constexpr (FMT == kFmtLarge) {
+      return large_factorize<T>(*this);
+    } else {
+      const int nb = (n + 3) >> 2;
+      if (nb * (nb + 1) / 2 <= NT) return factorize_regs<T>();
+      return factorize_mem<T>();
+    }
   }
 
   // One thread per 4x4 tile of the lower triangle of G: the tile is formed
@@ -701,6 +733,10 @@ struct Ipm {
   // sum_{c>b} L_cb^T x_c), two barriers per 32-block; w is n scratch entries.
   template <typename T>
   QTQP_PHASE void chol_solve(const T* g, T* v, T* w) {
+    if constexpr (FMT == kFmtLarge) {
+      large_chol_solve<T>(*this, v, w);
+      return;
+    }
     QTQP_LOCALS;
     const int nblk = (n + 31) >> 5;
     for (int blk = 0; blk < nblk; ++blk) {

@@ -1,0 +1,571 @@
+// Large-format phases of the device IPM (FMT == kFmtLarge): one large dense QP
+// solved by a cooperative grid of kLargeBlocks blocks.  The interior-point
+// logic is the shared Ipm code; here are the KKT factorisation and the
+// triangular solves, blocked for the whole GPU:
+//
+//   Gram      G = P_off + diag(Rx) + A^T diag(1/Ry) A  (solvers_dense.py:99-116)
+//             FP32 factor: X = (diag(1/sqrt(Ry)) A)^T split into TF32 hi + lo,
+//             lower 128 x 128 tiles of X X^T on tcgen05 (three TF32 products,
+//             FP32 accumulation in TMEM).  FP64 factor: 64 x 64 SIMT tiles.
+//   Cholesky  right-looking with 128-wide panels: the diagonal block by one
+//             CTA in shared memory, the panel by row-wise substitution (one
+//             warp per row), the trailing update in 64 x 64 SIMT tiles; then
+//             the inverse of every diagonal block.
+//   Solves    block forward / backward substitution with the inverted
+//             diagonal blocks, one grid barrier per 128-block step.
+//
+// Padding: the factor is npad x npad (npad = n rounded up to 128) with an
+// identity on the padded diagonal; X is npad x mpad with zero padding.
+#pragma once
+
+#include "dense_ipm.cuh"
+#include "tc_common.cuh"
+
+namespace qtqp {
+
+constexpr int kLB = 128;                          // panel / diagonal block size
+constexpr int kLargeBlocks = 128;                 // CTAs of the cooperative grid
+constexpr int kLargeNT = kLargeBlocks * kGridBT;  // 32768 threads
+constexpr int kTcStages = 3;
+constexpr uint32_t kTcTileBytes = kLB * 32 * 4;        // 128 rows x 32 FP32
+constexpr uint32_t kTcStageBytes = 4 * kTcTileBytes;   // A hi, B hi, A lo, B lo
+constexpr size_t kArenaBytes = kTcStages * kTcStageBytes;  // 192 KB
+constexpr size_t kLargeSmem = 1024 + kArenaBytes + 256;    // + alignment + barriers
+
+__host__ __device__ inline int round_up(int v, int q) { return (v + q - 1) / q * q; }
+
+// Global workspace of a large solve.
+struct LargeLayout {
+  int n, m, npad, mpad, nblk, np;
+  size_t ctl_off, info_off, v_off, a_off, p_off, g64_off, g32_off, linv_off, xhi_off, xlo_off,
+      total;
+};
+__host__ __device__ inline LargeLayout plan_large_layout(int n, int m) {
+  LargeLayout L;
+  L.n = n;
+  L.m = m;
+  L.npad = round_up(n, kLB);
+  L.mpad = round_up(m, 32);
+  L.nblk = L.npad / kLB;
+  L.np = (max(n + m, n + 4) + 1) & ~1;
+  auto al = [](size_t b) { return (b + 1023) & ~size_t(1023); };
+  size_t off = 0;
+  L.ctl_off = off;
+  off += al(sizeof(GridCtl));
+  L.info_off = off;
+  off += al(16);
+  L.v_off = off;
+  off += al(size_t(kNumVec) * L.np * 8);
+  L.a_off = off;
+  off += al(size_t(m) * n * 8);
+  L.p_off = off;
+  off += al(size_t(n) * n * 8);
+  L.g64_off = off;
+  off += al(size_t(L.npad) * L.npad * 8);
+  L.g32_off = off;
+  off += al(size_t(L.npad) * L.npad * 4);
+  L.linv_off = off;
+  off += al(size_t(L.nblk) * kLB * kLB * 8);
+  L.xhi_off = off;
+  off += al(size_t(L.npad) * L.mpad * 4);
+  L.xlo_off = off;
+  off += al(size_t(L.npad) * L.mpad * 4);
+  L.total = off;
+  return L;
+}
+
+// ---------------------------------------------------------------------------
+// Gram of the FP32 factor on tcgen05.
+// ---------------------------------------------------------------------------
+// X = (diag(w) A)^T split into TF32 hi + lo (w = 1/sqrt(Ry) at vec(kPW)[n+i]),
+// by 32 x 32 tiles transposed through shared memory.
+template <class S>
+__device__ void large_scale_split(S& s) {
+  const int n = s.n, m = s.m, npad = s.npad, mpad = s.mpad;
+  const double* A = s.A;
+  const double* w = s.vec(kPW) + n;
+  float* t = reinterpret_cast<float*>(s.arena);  // 32 x 33
+  const int tr = threadIdx.x >> 5, tc = threadIdx.x & 31;  // 8 rows per pass
+  const int tiles_i = mpad / 32, tiles_j = npad / 32;
+  for (int t_id = blockIdx.x; t_id < tiles_i * tiles_j; t_id += gridDim.x) {
+    const int i0 = (t_id % tiles_i) * 32, j0 = (t_id / tiles_i) * 32;
+    for (int r = tr; r < 32; r += 8) {  // rows i of A, columns j coalesced
+      const int i = i0 + r, j = j0 + tc;
+      t[r * 33 + tc] = (i < m && j < n) ? float(A[size_t(i) * n + j] * w[i]) : 0.0f;
+    }
+    __syncthreads();
+    for (int r = tr; r < 32; r += 8) {  // rows j of X, columns i coalesced
+      const float v = t[tc * 33 + r];
+      uint32_t h;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(v));
+      const size_t o = size_t(j0 + r) * mpad + i0 + tc;
+      s.xhi[o] = __uint_as_float(h);
+      s.xlo[o] = v - __uint_as_float(h);
+    }
+    __syncthreads();
+  }
+}
+
+// Lower 128 x 128 tiles of X X^T (three TF32 products) into g32.  Warp 0
+// lane 0 loads (TMA, 3-stage ring), warp 1 lane 0 issues the MMAs, all
+// eight warps drain TMEM (warp w: lanes 32 (w % 4), columns 64 (w / 4)).
+// The ring counters continue across tiles and calls (s.tc_load / s.tc_mma /
+// s.tc_tiles are per-thread copies; each role advances its own).
+template <class S>
+__device__ void large_gram_tc(S& s) {
+  const int npad = s.npad, k_tiles = s.mpad / 32, nt = npad / kLB;
+  uint8_t* ring = s.arena;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kArenaBytes);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + kTcStages;
+  uint64_t* done = bars + 2 * kTcStages;
+  int* failed = reinterpret_cast<int*>(done + 1);
+  const CUtensorMap* mh = static_cast<const CUtensorMap*>(s.map_hi);
+  const CUtensorMap* ml = static_cast<const CUtensorMap*>(s.map_lo);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr uint32_t idesc = tc::idesc_f32acc(kLB, kLB, false);
+  const int tiles = nt * (nt + 1) / 2;
+  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+    int ti = 0;
+    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    const int tj = t - ti * (ti + 1) / 2;
+    if (warp == 0 && lane == 0) {
+      for (int kt = 0; kt < k_tiles; ++kt) {
+        const uint32_t g = s.tc_load++;
+        const int st = int(g % kTcStages);
+        const uint32_t use = g / kTcStages;
+        if (use > 0 && !tc::mbar_wait(&empty[st], (use - 1) & 1)) {
+          atomicExch(failed, 1);
+          break;
+        }
+        uint8_t* sb = ring + st * kTcStageBytes;
+        tc::mbar_arrive_expect_tx(&full[st], kTcStageBytes);
+        tc::tma_load_2d(sb, mh, kt * 32, ti * kLB, &full[st]);
+        tc::tma_load_2d(sb + kTcTileBytes, mh, kt * 32, tj * kLB, &full[st]);
+        tc::tma_load_2d(sb + 2 * kTcTileBytes, ml, kt * 32, ti * kLB, &full[st]);
+        tc::tma_load_2d(sb + 3 * kTcTileBytes, ml, kt * 32, tj * kLB, &full[st]);
+      }
+    } else if (warp == 1 && lane == 0) {
+      for (int kt = 0; kt < k_tiles; ++kt) {
+        const uint32_t g = s.tc_mma++;
+        const int st = int(g % kTcStages);
+        const uint32_t use = g / kTcStages;
+        if (!tc::mbar_wait(&full[st], use & 1)) {
+          atomicExch(failed, 1);
+          break;
+        }
+        tc::fence_after_sync();
+        const uint32_t a_hi = tc::smem_u32(ring + st * kTcStageBytes);
+        const uint32_t b_hi = a_hi + kTcTileBytes, a_lo = a_hi + 2 * kTcTileBytes,
+                       b_lo = a_hi + 3 * kTcTileBytes;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const uint32_t off = kk * 32;
+          tc::mma_tf32(s.tmem, tc::desc_kmajor_sw128(a_hi + off), tc::desc_kmajor_sw128(b_hi + off),
+                       idesc, (kt | kk) != 0);
+          tc::mma_tf32(s.tmem, tc::desc_kmajor_sw128(a_hi + off), tc::desc_kmajor_sw128(b_lo + off),
+                       idesc, 1);
+          tc::mma_tf32(s.tmem, tc::desc_kmajor_sw128(a_lo + off), tc::desc_kmajor_sw128(b_hi + off),
+                       idesc, 1);
+        }
+        tc::mma_commit(&empty[st]);
+      }
+      tc::mma_commit(done);
+    }
+    __syncwarp();
+    if (!tc::mbar_wait(done, s.tc_tiles & 1)) atomicExch(failed, 1);
+    s.tc_tiles++;
+    tc::fence_after_sync();
+    __syncthreads();
+    if (*failed == 0) {
+      const int q = warp & 3, half = warp >> 2;
+      const int row = ti * kLB + q * 32 + lane;
+      float* grow = s.g32l + size_t(row) * npad + size_t(tj) * kLB + half * 64;
+#pragma unroll 1
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        float v[32];
+        tc::tmem_ld32(s.tmem + (uint32_t(q * 32) << 16) + uint32_t(half * 64 + c0), v);
+#pragma unroll
+        for (int e = 0; e < 32; e += 4)
+          *reinterpret_cast<float4*>(grow + c0 + e) = make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
+      }
+    }
+    tc::fence_before_sync();
+    __syncthreads();  // TMEM free for the next tile's MMAs
+  }
+  if (threadIdx.x == 0 && *failed) atomicExch(&s.gctl->err, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Gram of the FP64 factor: 64 x 64 tiles, 4 x 4 outputs per thread, A rows
+// staged 32 at a time (scaled by w_i) in shared memory.
+// ---------------------------------------------------------------------------
+template <class S>
+__device__ void large_gram_simt(S& s) {
+  const int n = s.n, m = s.m, npad = s.npad;
+  const double* A = s.A;
+  const double* w = s.vec(kPW) + n;
+  double* sa = reinterpret_cast<double*>(s.arena);  // [32][64]
+  double* sb = sa + 32 * 64;                         // [32][64]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int nt = npad / 64, tiles = nt * (nt + 1) / 2;
+  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+    int ti = 0;
+    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    const int tj = t - ti * (ti + 1) / 2;
+    const int i0 = ti * 64, j0 = tj * 64;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int r0 = 0; r0 < m; r0 += 32) {
+      for (int e = threadIdx.x; e < 32 * 64; e += blockDim.x) {
+        const int r = e >> 6, c = e & 63, i = r0 + r;
+        const double wi = i < m ? w[i] : 0.0;
+        sa[e] = (i < m && i0 + c < n) ? A[size_t(i) * n + i0 + c] * wi : 0.0;
+        sb[e] = (i < m && j0 + c < n) ? A[size_t(i) * n + j0 + c] * wi : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          av[a] = sa[r * 64 + ty * 4 + a];
+          bv[a] = sb[r * 64 + tx * 4 + a];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) s.g64[size_t(i0 + ty * 4 + a) * npad + j0 + tx * 4 + b] = acc[a][b];
+  }
+}
+
+// G += P_off + diag(Rx) on the lower triangle, identity padding, then the
+// relative diagonal jitter (1e-14 in FP64 as solvers_dense.py:112; 2^-22 at
+// FP32 resolution).
+template <typename T, class S>
+__device__ void large_finish_gram(S& s, T* g) {
+  const int n = s.n, npad = s.npad, tid = s.tid;
+  const double* P = s.P;
+  const double* reg = s.vec(kREG);
+  double dmax[1] = {0.0};
+  double dummy[1] = {0.0};
+  const size_t total = size_t(npad) * npad;
+  for (size_t e = tid; e < total; e += kLargeNT) {
+    const int i = int(e / npad), j = int(e % npad);
+    if (j > i) continue;
+    if (i >= n || j >= n) {
+      g[e] = (i == j) ? T(1) : T(0);
+      continue;
+    }
+    double base = P[size_t(i) * n + j];
+    if (i == j) base += reg[i];
+    const T v = T(base) + g[e];
+    g[e] = v;
+    if (i == j) dmax[0] = nanmax(dmax[0], double(v));
+  }
+  s.template reduce<0, 1>(dummy, dmax);
+  const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
+  for (int k = tid; k < n; k += kLargeNT) g[size_t(k) * npad + k] = T(double(g[size_t(k) * npad + k]) + jit);
+  s.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Blocked Cholesky of the lower triangle of g (npad x npad), then the
+// inverses of the diagonal blocks into linv.  Returns 0 or the 1-based index
+// of the first non-positive pivot (uniform over the grid).
+// ---------------------------------------------------------------------------
+template <typename T, class S>
+__device__ int large_cholesky(S& s, T* g) {
+  const int npad = s.npad, nblk = npad / kLB;
+  int* info = s.linfo;
+  T* sm = reinterpret_cast<T*>(s.arena);  // diagonal block [128][129] / staging
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gwarp = blockIdx.x * (kGridBT / 32) + warp, nwarps = gridDim.x * (kGridBT / 32);
+  if (s.tid == 0) *info = 0;
+  s.sync();
+  for (int k = 0; k < nblk; ++k) {
+    const int k0 = k * kLB;
+    // (a) diagonal block: one CTA, one barrier per column.
+    if (int(blockIdx.x) == k % int(gridDim.x)) {
+      for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
+        const int r = e >> 7, c = e & 127;
+        sm[r * 129 + c] = c <= r ? g[size_t(k0 + r) * npad + k0 + c] : T(0);
+      }
+      __syncthreads();
+      T d_prev = T(1);
+      int bad = 0;
+      for (int c = 0; c <= kLB; ++c) {
+        if (c > 0) {  // finish column c-1
+          const T l = sqrt(d_prev), il = T(1) / l;
+          for (int r = c + int(threadIdx.x); r < kLB; r += blockDim.x) sm[r * 129 + c - 1] *= il;
+          if (threadIdx.x == 0) sm[(c - 1) * 129 + c - 1] = l;
+        }
+        if (c == kLB) break;
+        const T d = sm[c * 129 + c];
+        if (!(d > T(0))) {
+          bad = c + 1;
+          break;
+        }
+        const T inv_d = T(1) / d;
+        for (int j = c + 1 + warp; j < kLB; j += blockDim.x / 32) {
+          const T t = sm[j * 129 + c] * inv_d;
+          for (int r = j + lane; r < kLB; r += 32) sm[r * 129 + j] = fma(-sm[r * 129 + c], t, sm[r * 129 + j]);
+        }
+        d_prev = d;
+        __syncthreads();
+      }
+      __syncthreads();
+      if (bad) {
+        if (threadIdx.x == 0) atomicCAS(info, 0, k0 + bad);
+      } else {
+        for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
+          const int r = e >> 7, c = e & 127;
+          if (c <= r) g[size_t(k0 + r) * npad + k0 + c] = sm[r * 129 + c];
+        }
+      }
+    }
+    s.sync();
+    if (*reinterpret_cast<volatile int*>(info) != 0) break;
+    const int rest = npad - k0 - kLB;
+    if (rest == 0) break;
+    // (b) panel rows: x L_kk^T = g_i, one warp per row, lane owns columns
+    // 4 lane .. 4 lane + 3.  L_kk is staged in shared memory by every CTA.
+    for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
+      const int r = e >> 7, c = e & 127;
+      sm[r * 129 + c] = c <= r ? g[size_t(k0 + r) * npad + k0 + c] : T(0);
+    }
+    __syncthreads();
+    for (int row = k0 + kLB + gwarp; row < npad; row += nwarps) {
+      T* gr = g + size_t(row) * npad + k0;
+      T x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = gr[4 * lane + q];
+      for (int c = 0; c < kLB; ++c) {
+        const int owner = c >> 2, slot = c & 3;
+        T xc = T(0);
+        if (lane == owner) {
+          T v = x[0];
+          if (slot == 1) v = x[1];
+          if (slot == 2) v = x[2];
+          if (slot == 3) v = x[3];
+          xc = v / sm[c * 129 + c];
+          if (slot == 0) x[0] = xc;
+          if (slot == 1) x[1] = xc;
+          if (slot == 2) x[2] = xc;
+          if (slot == 3) x[3] = xc;
+        }
+        xc = __shfl_sync(0xffffffffu, xc, owner);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int l = 4 * lane + q;
+          if (l > c) x[q] = fma(-xc, sm[l * 129 + c], x[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) gr[4 * lane + q] = x[q];
+    }
+    s.sync();
+    // (c) trailing update of the lower 64 x 64 tiles right of the panel:
+    // g_ij -= L_ik L_jk^T (K = 128), panels staged k-major in shared memory.
+    {
+      T* pa = sm;             // [128][64]: pa[kk * 64 + r] = L[i0 + r][k0 + kk]
+      T* pb = sm + kLB * 64;  // [128][64]
+      const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+      const int nt = rest / 64, tiles = nt * (nt + 1) / 2;
+      const int base = k0 + kLB;
+      for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        int ti = 0;
+        while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+        const int tj = t - ti * (ti + 1) / 2;
+        const int i0 = base + ti * 64, j0 = base + tj * 64;
+        for (int e = threadIdx.x; e < 64 * kLB; e += blockDim.x) {
+          const int r = e >> 7, kk = e & 127;
+          pa[kk * 64 + r] = g[size_t(i0 + r) * npad + k0 + kk];
+          pb[kk * 64 + r] = g[size_t(j0 + r) * npad + k0 + kk];
+        }
+        __syncthreads();
+        T acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+#pragma unroll 4
+        for (int kk = 0; kk < kLB; ++kk) {
+          T av[4], bv[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            av[a] = pa[kk * 64 + ty * 4 + a];
+            bv[a] = pb[kk * 64 + tx * 4 + a];
+          }
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int i = i0 + ty * 4 + a;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int j = j0 + tx * 4 + b;
+            if (j <= i) g[size_t(i) * npad + j] -= acc[a][b];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    s.sync();
+  }
+  const int rc = *reinterpret_cast<volatile int*>(info);
+  if (rc != 0) return rc;
+  // Inverses of the diagonal blocks: column c of inv(L_bb) by thread c.
+  T* lv = reinterpret_cast<T*>(s.linv);
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
+    const int b0 = b * kLB;
+    for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
+      const int r = e >> 7, c = e & 127;
+      sm[r * 129 + c] = c <= r ? g[size_t(b0 + r) * npad + b0 + c] : T(0);
+    }
+    __syncthreads();
+    T* inv = lv + size_t(b) * kLB * kLB;
+    if (threadIdx.x < kLB) {
+      const int c = threadIdx.x;
+      // x_c = 1 / L_cc; x_r = -(sum_{c <= l < r} L_rl x_l) / L_rr, in place in
+      // the output column (rows r >= c), upper part zero.
+      for (int r = 0; r < c; ++r) inv[r * kLB + c] = T(0);
+      inv[c * kLB + c] = T(1) / sm[c * 129 + c];
+      for (int r = c + 1; r < kLB; ++r) {
+        T acc = T(0);
+        for (int l = c; l < r; ++l) acc = fma(sm[r * 129 + l], inv[l * kLB + c], acc);
+        inv[r * kLB + c] = -acc / sm[r * 129 + r];
+      }
+    }
+    __syncthreads();
+  }
+  s.sync();
+  return 0;
+}
+
+template <typename T, class S>
+__device__ int large_factorize(S& s) {
+  if constexpr (sizeof(T) == 4) {
+    large_scale_split(s);
+    s.sync();
+    large_gram_tc(s);
+    s.sync();
+    large_finish_gram<float>(s, s.g32l);
+    return large_cholesky<float>(s, s.g32l);
+  } else {
+    large_gram_simt(s);
+    s.sync();
+    large_finish_gram<double>(s, s.g64);
+    return large_cholesky<double>(s, s.g64);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// L L^T v = v in place (v, w: n entries of T; w is scratch).  Forward:
+// z_b = inv(L_bb) (v_b - sum_{c<b} L_bc z_c) into w; backward:
+// x_b = inv(L_bb)^T (z_b - sum_{c>b} L_cb^T x_c) into v.  Step b: the CTA that
+// owns block b+1 (b-1 backward) applies z_b to that block and immediately
+// forms its next z, while the other CTAs apply z_b to the remaining rows;
+// one grid barrier per step.
+// ---------------------------------------------------------------------------
+template <typename T, class S>
+__device__ void large_chol_solve(S& s, T* v, T* w) {
+  const int n = s.n, npad = s.npad;
+  const int nb = (n + kLB - 1) / kLB;
+  const T* g = sizeof(T) == 4 ? reinterpret_cast<const T*>(s.g32l)
+                              : reinterpret_cast<const T*>(s.g64);
+  const T* lv = reinterpret_cast<const T*>(s.linv);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int WPB = kGridBT / 32;
+  const int G = gridDim.x;
+  auto bsz = [&](int b) { return min(kLB, n - b * kLB); };
+  // z_b = inv(L_bb) v_b by the calling CTA (thread r < bs: row r).
+  auto diag_fwd = [&](int b) {
+    const int b0 = b * kLB, bs = bsz(b);
+    const T* inv = lv + size_t(b) * kLB * kLB;
+    if (int(threadIdx.x) < bs) {
+      const int r = threadIdx.x;
+      T acc = T(0);
+      for (int c = 0; c <= r; ++c) acc = fma(inv[r * kLB + c], v[b0 + c], acc);
+      w[b0 + r] = acc;
+    }
+  };
+  // x_b = inv(L_bb)^T w_b (thread r < bs: row r).
+  auto diag_bwd = [&](int b) {
+    const int b0 = b * kLB, bs = bsz(b);
+    const T* inv = lv + size_t(b) * kLB * kLB;
+    if (int(threadIdx.x) < bs) {
+      const int r = threadIdx.x;
+      T acc = T(0);
+      for (int c = r; c < bs; ++c) acc = fma(inv[c * kLB + r], w[b0 + c], acc);
+      v[b0 + r] = acc;
+    }
+  };
+  // v_i -= L_ib z_b for rows [lo, hi), one warp per row (lanes split k).
+  auto fwd_rows = [&](int b, int lo, int hi, int wfirst, int wcount) {
+    const int b0 = b * kLB, bs = bsz(b);
+    for (int i = lo + wfirst; i < hi; i += wcount) {
+      const T* li = g + size_t(i) * npad + b0;
+      T acc = T(0);
+      for (int c = lane; c < bs; c += 32) acc = fma(li[c], w[b0 + c], acc);
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) v[i] -= acc;
+    }
+  };
+  // w_i -= sum_{l in b} L_li x_l for columns [lo, hi), one lane per column.
+  auto bwd_cols = [&](int b, int lo, int hi, int tfirst, int tcount) {
+    const int b0 = b * kLB, bs = bsz(b);
+    for (int i = lo + tfirst; i < hi; i += tcount) {
+      T acc = T(0);
+      for (int l = 0; l < bs; ++l) acc = fma(g[size_t(b0 + l) * npad + i], v[b0 + l], acc);
+      w[i] -= acc;
+    }
+  };
+  // Forward.
+  if (blockIdx.x == 0) diag_fwd(0);
+  s.sync();
+  for (int b = 0; b + 1 < nb; ++b) {
+    const int own = (b + 1) % G;
+    const int nxt0 = (b + 1) * kLB, nxt1 = min(n, nxt0 + kLB);
+    if (int(blockIdx.x) == own) {
+      fwd_rows(b, nxt0, nxt1, warp, WPB);
+      __syncthreads();
+      diag_fwd(b + 1);
+    } else {
+      const int cta = (int(blockIdx.x) - own - 1 + G) % G;  // 0 .. G-2
+      fwd_rows(b, nxt1, n, cta * WPB + warp, (G - 1) * WPB);
+    }
+    s.sync();
+  }
+  // Backward.
+  if (int(blockIdx.x) == (nb - 1) % G) diag_bwd(nb - 1);
+  s.sync();
+  for (int b = nb - 1; b > 0; --b) {
+    const int own = (b - 1) % G;
+    const int prv0 = (b - 1) * kLB;
+    if (int(blockIdx.x) == own) {
+      bwd_cols(b, prv0, prv0 + kLB, threadIdx.x, blockDim.x);
+      __syncthreads();
+      diag_bwd(b - 1);
+    } else {
+      const int cta = (int(blockIdx.x) - own - 1 + G) % G;
+      bwd_cols(b, 0, prv0, cta * kGridBT + threadIdx.x, (G - 1) * kGridBT);
+    }
+    s.sync();
+  }
+}
+
+}  // namespace qtqp
