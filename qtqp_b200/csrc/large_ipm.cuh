@@ -458,19 +458,27 @@ __device__ int large_cholesky(S& s, T* g) {
 
 template <typename T, class S>
 __device__ int large_factorize(S& s) {
+  QTQP_TIC();
+  int info;
   if constexpr (sizeof(T) == 4) {
     large_scale_split(s);
     s.sync();
     large_gram_tc(s);
     s.sync();
     large_finish_gram<float>(s, s.g32l);
-    return large_cholesky<float>(s, s.g32l);
+    QTQP_TOC(kPhGram);
+    QTQP_RETIC();
+    info = large_cholesky<float>(s, s.g32l);
   } else {
     large_gram_simt(s);
     s.sync();
     large_finish_gram<double>(s, s.g64);
-    return large_cholesky<double>(s, s.g64);
+    QTQP_TOC(kPhGram);
+    QTQP_RETIC();
+    info = large_cholesky<double>(s, s.g64);
   }
+  QTQP_TOC(kPhChol);
+  return info;
 }
 
 // ---------------------------------------------------------------------------
