@@ -220,7 +220,9 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 // g_phase_cycles[phase].  Default builds compile these to nothing.
 enum Phase : int {
   kPhLoad = 0, kPhNormalize, kPhGram, kPhChol, kPhSolve, kPhResidual, kPhTau, kPhStep,
-  kPhTerm, kPhOther, kNumPhases
+  kPhTerm, kPhOther,
+  // Sub-phases of the large (grid-mode) factorisation and solves.
+  kPhLgDiag, kPhLgPanel, kPhLgTrail, kPhLgInv, kPhLgFwd, kPhLgBwd, kNumPhases
 };
 #ifdef QTQP_PHASE_TIMERS
 extern __device__ unsigned long long g_phase_cycles[kNumPhases];

@@ -258,7 +258,31 @@ struct Ipm {
 #pragma unroll
       for (int a = 0; a < NACC; ++a) acc[a] = 0.0;
       if (k < K) {
-        for (int i = s; i < len; i += S) body(k, i, acc);
+        if constexpr (NT > 1024) {
+          // Grid mode streams A and P from HBM: U independent partial sums
+          // keep U loads in flight per lane.
+          constexpr int U = 8;
+          double part[U][NACC];
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int a = 0; a < NACC; ++a) part[u][a] = 0.0;
+          int i = s;
+          for (; i + (U - 1) * S < len; i += U * S) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) body(k, i + u * S, part[u]);
+          }
+          for (; i < len; i += S) body(k, i, part[0]);
+#pragma unroll
+          for (int a = 0; a < NACC; ++a) {
+            double t = part[0][a];
+#pragma unroll
+            for (int u = 1; u < U; ++u) t = MAXOP ? fmax(t, part[u][a]) : t + part[u][a];
+            acc[a] = t;
+          }
+        } else {
+          for (int i = s; i < len; i += S) body(k, i, acc);
+        }
       }
       for (int off = 16; off >= per_warp; off >>= 1) {
 #pragma unroll

@@ -65,7 +65,7 @@ __host__ __device__ inline LargeLayout plan_large_layout(int n, int m) {
   L.g32_off = off;
   off += al(size_t(L.npad) * L.npad * 4);
   L.linv_off = off;
-  off += al(size_t(L.nblk) * kLB * kLB * 8);
+  off += al(2 * size_t(L.nblk) * kLB * kLB * 8);  // inverses and their transposes
   L.xhi_off = off;
   off += al(size_t(L.npad) * L.mpad * 4);
   L.xlo_off = off;
@@ -197,55 +197,101 @@ __device__ void large_gram_tc(S& s) {
 }
 
 // ---------------------------------------------------------------------------
-// Gram of the FP64 factor: 64 x 64 tiles, 4 x 4 outputs per thread, A rows
-// staged 32 at a time (scaled by w_i) in shared memory.
+// Gram of the FP64 factor: lower 128 x 128 tiles of A^T diag(1/Ry) A, 8 x 8
+// outputs per thread (rows ty + 16a, columns tx + 16b: conflict-free shared
+// memory reads).  Slices of 16 rows of A (and their 1/Ry) are copied to
+// shared memory with cp.async, double-buffered: slice k+1 is in flight while
+// slice k is multiplied.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(tc::smem_u32(dst)),
+               "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <class S>
 __device__ void large_gram_simt(S& s) {
   const int n = s.n, m = s.m, npad = s.npad;
   const double* A = s.A;
-  const double* w = s.vec(kPW) + n;
-  double* sa = reinterpret_cast<double*>(s.arena);  // [32][64]
-  double* sb = sa + 32 * 64;                         // [32][64]
+  const double* iry = s.vec(kPI) + n;               // 1 / Ry
+  constexpr int KS = 16;                            // rows per slice
+  constexpr int SL = 2 * KS * kLB + KS;             // doubles per buffer
+  double* smem = reinterpret_cast<double*>(s.arena);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int nt = npad / 64, tiles = nt * (nt + 1) / 2;
+  const int nt = npad / kLB, tiles = nt * (nt + 1) / 2;
+  auto issue = [&](int r0, int i0, int j0, int buf) {
+    double* sa = smem + buf * SL;
+    double* sb = sa + KS * kLB;
+    double* sw = sb + KS * kLB;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = threadIdx.x + q * kGridBT, r = e >> 7, c = e & 127, i = r0 + r;
+      const bool ok = i < m;
+      cp_async8(sa + e, A + (ok && i0 + c < n ? size_t(i) * n + i0 + c : 0),
+                ok && i0 + c < n);
+      cp_async8(sb + e, A + (ok && j0 + c < n ? size_t(i) * n + j0 + c : 0),
+                ok && j0 + c < n);
+    }
+    if (threadIdx.x < KS) {
+      const int i = r0 + threadIdx.x;
+      cp_async8(sw + threadIdx.x, iry + (i < m ? i : 0), i < m);
+    }
+    cp_async_commit();
+  };
   for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
     int ti = 0;
     while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
     const int tj = t - ti * (ti + 1) / 2;
-    const int i0 = ti * 64, j0 = tj * 64;
-    double acc[4][4];
+    const int i0 = ti * kLB, j0 = tj * kLB;
+    double acc[8][8];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int r0 = 0; r0 < m; r0 += 32) {
-      for (int e = threadIdx.x; e < 32 * 64; e += blockDim.x) {
-        const int r = e >> 6, c = e & 63, i = r0 + r;
-        const double wi = i < m ? w[i] : 0.0;
-        sa[e] = (i < m && i0 + c < n) ? A[size_t(i) * n + i0 + c] * wi : 0.0;
-        sb[e] = (i < m && j0 + c < n) ? A[size_t(i) * n + j0 + c] * wi : 0.0;
+      for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+    issue(0, i0, j0, 0);
+    int buf = 0;
+    for (int r0 = 0; r0 < m; r0 += KS) {
+      // Slice r0 landed in `buf`; the other buffer was last read before the
+      // previous barrier, so the next slice may be issued into it now.
+      if (r0 + KS < m) {
+        issue(r0 + KS, i0, j0, buf ^ 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
       }
       __syncthreads();
-#pragma unroll 4
-      for (int r = 0; r < 32; ++r) {
-        double av[4], bv[4];
+      const double* sa = smem + buf * SL;
+      const double* sb = sa + KS * kLB;
+      const double* sw = sb + KS * kLB;
+#pragma unroll 2
+      for (int r = 0; r < KS; ++r) {
+        const double wr = sw[r];
+        double av[8], bv[8];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          av[a] = sa[r * 64 + ty * 4 + a];
-          bv[a] = sb[r * 64 + tx * 4 + a];
+        for (int a = 0; a < 8; ++a) {
+          av[a] = sa[r * kLB + ty + 16 * a] * wr;
+          bv[a] = sb[r * kLB + tx + 16 * a];
         }
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < 8; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+          for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
       }
-      __syncthreads();
+      __syncthreads();  // everyone is done with `buf` before it is refilled
+      buf ^= 1;
     }
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) s.g64[size_t(i0 + ty * 4 + a) * npad + j0 + tx * 4 + b] = acc[a][b];
+      for (int b = 0; b < 8; ++b)
+        s.g64[size_t(i0 + ty + 16 * a) * npad + j0 + tx + 16 * b] = acc[a][b];
   }
 }
 
@@ -293,8 +339,10 @@ __device__ int large_cholesky(S& s, T* g) {
   const int gwarp = blockIdx.x * (kGridBT / 32) + warp, nwarps = gridDim.x * (kGridBT / 32);
   if (s.tid == 0) *info = 0;
   s.sync();
+  QTQP_TIC();
   for (int k = 0; k < nblk; ++k) {
     const int k0 = k * kLB;
+    QTQP_RETIC();
     // (a) diagonal block: one CTA, one barrier per column.
     if (int(blockIdx.x) == k % int(gridDim.x)) {
       for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
@@ -335,6 +383,8 @@ __device__ int large_cholesky(S& s, T* g) {
       }
     }
     s.sync();
+    QTQP_TOC(kPhLgDiag);
+    QTQP_RETIC();
     if (*reinterpret_cast<volatile int*>(info) != 0) break;
     const int rest = npad - k0 - kLB;
     if (rest == 0) break;
@@ -375,11 +425,14 @@ __device__ int large_cholesky(S& s, T* g) {
       for (int q = 0; q < 4; ++q) gr[4 * lane + q] = x[q];
     }
     s.sync();
+    QTQP_TOC(kPhLgPanel);
+    QTQP_RETIC();
     // (c) trailing update of the lower 64 x 64 tiles right of the panel:
     // g_ij -= L_ik L_jk^T (K = 128), panels staged k-major in shared memory.
     {
-      T* pa = sm;             // [128][64]: pa[kk * 64 + r] = L[i0 + r][k0 + kk]
-      T* pb = sm + kLB * 64;  // [128][64]
+      constexpr int PP = 65;  // pitch: conflict-free transposed staging
+      T* pa = sm;             // [128][PP]: pa[kk * PP + r] = L[i0 + r][k0 + kk]
+      T* pb = sm + kLB * PP;  // [128][PP]
       const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
       const int nt = rest / 64, tiles = nt * (nt + 1) / 2;
       const int base = k0 + kLB;
@@ -390,8 +443,8 @@ __device__ int large_cholesky(S& s, T* g) {
         const int i0 = base + ti * 64, j0 = base + tj * 64;
         for (int e = threadIdx.x; e < 64 * kLB; e += blockDim.x) {
           const int r = e >> 7, kk = e & 127;
-          pa[kk * 64 + r] = g[size_t(i0 + r) * npad + k0 + kk];
-          pb[kk * 64 + r] = g[size_t(j0 + r) * npad + k0 + kk];
+          pa[kk * PP + r] = g[size_t(i0 + r) * npad + k0 + kk];
+          pb[kk * PP + r] = g[size_t(j0 + r) * npad + k0 + kk];
         }
         __syncthreads();
         T acc[4][4];
@@ -404,8 +457,8 @@ __device__ int large_cholesky(S& s, T* g) {
           T av[4], bv[4];
 #pragma unroll
           for (int a = 0; a < 4; ++a) {
-            av[a] = pa[kk * 64 + ty * 4 + a];
-            bv[a] = pb[kk * 64 + tx * 4 + a];
+            av[a] = pa[kk * PP + ty * 4 + a];
+            bv[a] = pb[kk * PP + tx * 4 + a];
           }
 #pragma unroll
           for (int a = 0; a < 4; ++a)
@@ -425,9 +478,11 @@ __device__ int large_cholesky(S& s, T* g) {
       }
     }
     s.sync();
+    QTQP_TOC(kPhLgTrail);
   }
   const int rc = *reinterpret_cast<volatile int*>(info);
   if (rc != 0) return rc;
+  QTQP_RETIC();
   // Inverses of the diagonal blocks: column c of inv(L_bb) by thread c.
   T* lv = reinterpret_cast<T*>(s.linv);
   for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
@@ -437,22 +492,35 @@ __device__ int large_cholesky(S& s, T* g) {
       sm[r * 129 + c] = c <= r ? g[size_t(b0 + r) * npad + b0 + c] : T(0);
     }
     __syncthreads();
-    T* inv = lv + size_t(b) * kLB * kLB;
+    T* inv = lv + size_t(b) * kLB * kLB;                 // inv(L_bb), row-major
+    T* invt = lv + size_t(nblk + b) * kLB * kLB;         // its transpose
     if (threadIdx.x < kLB) {
       const int c = threadIdx.x;
-      // x_c = 1 / L_cc; x_r = -(sum_{c <= l < r} L_rl x_l) / L_rr, in place in
-      // the output column (rows r >= c), upper part zero.
-      for (int r = 0; r < c; ++r) inv[r * kLB + c] = T(0);
-      inv[c * kLB + c] = T(1) / sm[c * 129 + c];
+      // Column c of inv(L_bb) = row c of its transpose (contiguous for this
+      // thread): x_c = 1 / L_cc; x_r = -(sum_{c <= l < r} L_rl x_l) / L_rr.
+      T* xc = invt + size_t(c) * kLB;
+      for (int r = 0; r < c; ++r) xc[r] = T(0);
+      xc[c] = T(1) / sm[c * 129 + c];
       for (int r = c + 1; r < kLB; ++r) {
-        T acc = T(0);
-        for (int l = c; l < r; ++l) acc = fma(sm[r * 129 + l], inv[l * kLB + c], acc);
-        inv[r * kLB + c] = -acc / sm[r * 129 + r];
+        T acc0 = T(0), acc1 = T(0);
+        int l = c;
+        for (; l + 1 < r; l += 2) {
+          acc0 = fma(sm[r * 129 + l], xc[l], acc0);
+          acc1 = fma(sm[r * 129 + l + 1], xc[l + 1], acc1);
+        }
+        if (l < r) acc0 = fma(sm[r * 129 + l], xc[l], acc0);
+        xc[r] = -(acc0 + acc1) / sm[r * 129 + r];
       }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
+      const int r = e >> 7, c = e & 127;
+      inv[e] = invt[size_t(c) * kLB + r];
     }
     __syncthreads();
   }
   s.sync();
+  QTQP_TOC(kPhLgInv);
   return 0;
 }
 
@@ -487,62 +555,112 @@ __device__ int large_factorize(S& s) {
 // x_b = inv(L_bb)^T (z_b - sum_{c>b} L_cb^T x_c) into v.  Step b: the CTA that
 // owns block b+1 (b-1 backward) applies z_b to that block and immediately
 // forms its next z, while the other CTAs apply z_b to the remaining rows;
-// one grid barrier per step.
+// one grid barrier per step.  Every inner loop keeps several independent
+// loads in flight (the factor streams from HBM / L2).
 // ---------------------------------------------------------------------------
 template <typename T, class S>
 __device__ void large_chol_solve(S& s, T* v, T* w) {
   const int n = s.n, npad = s.npad;
   const int nb = (n + kLB - 1) / kLB;
+  const int nblk = npad / kLB;
   const T* g = sizeof(T) == 4 ? reinterpret_cast<const T*>(s.g32l)
                               : reinterpret_cast<const T*>(s.g64);
   const T* lv = reinterpret_cast<const T*>(s.linv);
+  T* red = reinterpret_cast<T*>(s.arena);  // [kLB] partials of the owner
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int WPB = kGridBT / 32;
   const int G = gridDim.x;
   auto bsz = [&](int b) { return min(kLB, n - b * kLB); };
-  // z_b = inv(L_bb) v_b by the calling CTA (thread r < bs: row r).
+  // z_b = inv(L_bb) v_b: thread r < bs, reading the transposed inverse
+  // (coalesced over r).
   auto diag_fwd = [&](int b) {
     const int b0 = b * kLB, bs = bsz(b);
-    const T* inv = lv + size_t(b) * kLB * kLB;
+    const T* it = lv + size_t(nblk + b) * kLB * kLB;
     if (int(threadIdx.x) < bs) {
       const int r = threadIdx.x;
-      T acc = T(0);
-      for (int c = 0; c <= r; ++c) acc = fma(inv[r * kLB + c], v[b0 + c], acc);
-      w[b0 + r] = acc;
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+      int c = 0;
+      for (; c + 3 <= r; c += 4) {
+        a0 = fma(it[(c + 0) * kLB + r], v[b0 + c + 0], a0);
+        a1 = fma(it[(c + 1) * kLB + r], v[b0 + c + 1], a1);
+        a2 = fma(it[(c + 2) * kLB + r], v[b0 + c + 2], a2);
+        a3 = fma(it[(c + 3) * kLB + r], v[b0 + c + 3], a3);
+      }
+      for (; c <= r; ++c) a0 = fma(it[c * kLB + r], v[b0 + c], a0);
+      w[b0 + r] = (a0 + a1) + (a2 + a3);
     }
   };
-  // x_b = inv(L_bb)^T w_b (thread r < bs: row r).
+  // x_b = inv(L_bb)^T w_b: thread r < bs (coalesced over r).
   auto diag_bwd = [&](int b) {
     const int b0 = b * kLB, bs = bsz(b);
     const T* inv = lv + size_t(b) * kLB * kLB;
     if (int(threadIdx.x) < bs) {
       const int r = threadIdx.x;
-      T acc = T(0);
-      for (int c = r; c < bs; ++c) acc = fma(inv[c * kLB + r], w[b0 + c], acc);
-      v[b0 + r] = acc;
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+      int c = r;
+      for (; c + 3 < bs; c += 4) {
+        a0 = fma(inv[(c + 0) * kLB + r], w[b0 + c + 0], a0);
+        a1 = fma(inv[(c + 1) * kLB + r], w[b0 + c + 1], a1);
+        a2 = fma(inv[(c + 2) * kLB + r], w[b0 + c + 2], a2);
+        a3 = fma(inv[(c + 3) * kLB + r], w[b0 + c + 3], a3);
+      }
+      for (; c < bs; ++c) a0 = fma(inv[c * kLB + r], w[b0 + c], a0);
+      v[b0 + r] = (a0 + a1) + (a2 + a3);
     }
   };
-  // v_i -= L_ib z_b for rows [lo, hi), one warp per row (lanes split k).
+  // v_i -= L_ib z_b for rows [lo, hi): each warp takes 4 rows at a time,
+  // lanes split the 128 columns (4 each), then 4 shuffle reductions.
   auto fwd_rows = [&](int b, int lo, int hi, int wfirst, int wcount) {
     const int b0 = b * kLB, bs = bsz(b);
-    for (int i = lo + wfirst; i < hi; i += wcount) {
-      const T* li = g + size_t(i) * npad + b0;
-      T acc = T(0);
-      for (int c = lane; c < bs; c += 32) acc = fma(li[c], w[b0 + c], acc);
-      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-      if (lane == 0) v[i] -= acc;
+    T z[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = lane + 32 * q;
+      z[q] = c < bs ? w[b0 + c] : T(0);
+    }
+    for (int i = lo + 4 * wfirst; i < hi; i += 4 * wcount) {
+      T acc[4];
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr) {
+        acc[rr] = T(0);
+        if (i + rr < hi) {
+          const T* li = g + size_t(i + rr) * npad + b0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int c = lane + 32 * q;
+            if (c < bs) acc[rr] = fma(li[c], z[q], acc[rr]);
+          }
+        }
+      }
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr)
+        for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
+      if (lane < 4 && i + lane < hi) {
+        T a = acc[0];
+        if (lane == 1) a = acc[1];
+        if (lane == 2) a = acc[2];
+        if (lane == 3) a = acc[3];
+        v[i + lane] -= a;
+      }
     }
   };
-  // w_i -= sum_{l in b} L_li x_l for columns [lo, hi), one lane per column.
-  auto bwd_cols = [&](int b, int lo, int hi, int tfirst, int tcount) {
-    const int b0 = b * kLB, bs = bsz(b);
-    for (int i = lo + tfirst; i < hi; i += tcount) {
-      T acc = T(0);
-      for (int l = 0; l < bs; ++l) acc = fma(g[size_t(b0 + l) * npad + i], v[b0 + l], acc);
-      w[i] -= acc;
+  // w_i -= sum_{l in [l0, l1)} L_li x_l for column i (one thread per column,
+  // coalesced over i), returned as the partial sum.
+  auto bwd_col = [&](int b, int i, int l0, int l1) {
+    const int b0 = b * kLB;
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+    int l = l0;
+    for (; l + 3 < l1; l += 4) {
+      a0 = fma(g[size_t(b0 + l + 0) * npad + i], v[b0 + l + 0], a0);
+      a1 = fma(g[size_t(b0 + l + 1) * npad + i], v[b0 + l + 1], a1);
+      a2 = fma(g[size_t(b0 + l + 2) * npad + i], v[b0 + l + 2], a2);
+      a3 = fma(g[size_t(b0 + l + 3) * npad + i], v[b0 + l + 3], a3);
     }
+    for (; l < l1; ++l) a0 = fma(g[size_t(b0 + l) * npad + i], v[b0 + l], a0);
+    return (a0 + a1) + (a2 + a3);
   };
   // Forward.
+  QTQP_TIC();
   if (blockIdx.x == 0) diag_fwd(0);
   s.sync();
   for (int b = 0; b + 1 < nb; ++b) {
@@ -558,22 +676,32 @@ __device__ void large_chol_solve(S& s, T* v, T* w) {
     }
     s.sync();
   }
+  QTQP_TOC(kPhLgFwd);
+  QTQP_RETIC();
   // Backward.
   if (int(blockIdx.x) == (nb - 1) % G) diag_bwd(nb - 1);
   s.sync();
   for (int b = nb - 1; b > 0; --b) {
     const int own = (b - 1) % G;
-    const int prv0 = (b - 1) * kLB;
+    const int prv0 = (b - 1) * kLB, bs = bsz(b);
     if (int(blockIdx.x) == own) {
-      bwd_cols(b, prv0, prv0 + kLB, threadIdx.x, blockDim.x);
+      // 128 columns x 2 halves of the block's rows, combined in shared memory.
+      const int col = threadIdx.x & (kLB - 1), half = threadIdx.x >> 7;
+      const int mid = bs / 2;
+      const T part = bwd_col(b, prv0 + col, half ? mid : 0, half ? bs : mid);
+      if (half) red[col] = part;
+      __syncthreads();
+      if (!half) w[prv0 + col] -= part + red[col];
       __syncthreads();
       diag_bwd(b - 1);
     } else {
       const int cta = (int(blockIdx.x) - own - 1 + G) % G;
-      bwd_cols(b, 0, prv0, cta * kGridBT + threadIdx.x, (G - 1) * kGridBT);
+      for (int i = cta * kGridBT + threadIdx.x; i < prv0; i += (G - 1) * kGridBT)
+        w[i] -= bwd_col(b, i, 0, bs);
     }
     s.sync();
   }
+  QTQP_TOC(kPhLgBwd);
 }
 
 }  // namespace qtqp
