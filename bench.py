@@ -50,7 +50,14 @@ def _args():
   ap.add_argument("--steps", type=int, default=5)
   ap.add_argument("--warmup", type=int, default=3)
   ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-  ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+  ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
+                  help="form whose throughput is the headline value (both are measured)")
+  ap.add_argument("--workload", default="batch_small",
+                  choices=["batch_small", "dense_large", "parametric"],
+                  help="batch_small: 4096 uneven small dense QPs (default); dense_large: "
+                       "one n=4096, m=8192 dense QP on the whole GPU; parametric: a T=50 "
+                       "MPC family with the learned warm start")
+  ap.add_argument("--train", type=int, default=4096, help="parametric: training instances")
   ap.add_argument("--count", type=int, default=COUNT)
   ap.add_argument("--no-cpu-baseline", action="store_true")
   return ap.parse_args()
@@ -254,7 +261,7 @@ def run_ours(args) -> None:
 
   # Plain FP64 form (comparator), then the chosen form.
   forms = {}
-  for precision in ("fp64", args.precision) if args.precision != "fp64" else ("fp64",):
+  for precision in ("fp64", "mixed"):
     hb, db = prepare(precision)
     barrier()
     clocks = _Clocks(local) if precision == args.precision else None
@@ -332,6 +339,9 @@ def run_ours(args) -> None:
                    " inputs also exceed L2",
                    "launch_groups": [list(g) for g in hb.groups]},
         "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
+        "mixed_value": forms["mixed"]["solved"] * world * args.steps / forms["mixed"]["time"],
+        "mixed_statuses_identical_to_fp64": bool(np.array_equal(
+            forms["fp64"]["res"]["status"], forms["mixed"]["res"]["status"])),
         "statuses_identical_to_fp64": same_status,
         "solved_per_step": solved_total, "instances_per_step": args.count * world,
         "mean_iterations": float(np.mean(iters)),
@@ -349,9 +359,264 @@ def run_ours(args) -> None:
     dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Other workloads (not the default line): one large dense QP, and the
+# parametric MPC family with the learned warm start.
+# ---------------------------------------------------------------------------
+LARGE_WORKLOAD = "one large dense QP: n=4096, m=8192, z=1024 (A ~ N(0,1/n), P = U diag(d) U^T + 1e-4 I)"
+PARAM_WORKLOAD = "parametric MPC family T=50 (n=3000, m=8000, z=2000): (b, c) = (b0, c0) + W theta"
+
+
+def _bf16_peak():
+  path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+  if os.path.exists(path):
+    with open(path) as f:
+      return float(json.load(f)["bf16_tflops"]), "measured"
+  return 1590.0, "fallback"
+
+
+def _ev_time(stream, fn):
+  import torch
+  e0 = torch.cuda.Event(enable_timing=True)
+  e1 = torch.cuda.Event(enable_timing=True)
+  e0.record(stream)
+  fn()
+  e1.record(stream)
+  e1.synchronize()
+  return e0.elapsed_time(e1) * 1e-3
+
+
+def run_dense_large(args):
+  """One large dense QP per step on the whole GPU (replicas only for N > 1)."""
+  rank = int(os.environ.get("RANK", "0"))
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  from qtqp_b200 import problems
+  a, b, c, z, p = problems.config2(seed=1002 + rank)
+  m, n = a.shape
+  flops = m * n * (n + 1) + n ** 3 / 3.0  # one factorisation (Gram + Cholesky)
+  if args.impl == "reference":
+    if rank != 0:
+      return
+    import scipy.sparse as sp
+    from oracle import qtqp_oracle as orc
+    times = []
+    for _ in range(args.steps):
+      t0 = time.perf_counter()
+      r = orc.solve(sp.csc_matrix(a), b, c, z, sp.csc_matrix(p), backend="dense")
+      times.append(time.perf_counter() - t0)
+    value = len(times) / sum(times)
+    cores = os.cpu_count() or 1
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": LARGE_WORKLOAD, "status": r.status},
+        "cpu_baseline": {"value": value, "unit": "QPs/s", "cores": cores, "kind": "port",
+                         "sample": "the whole QP, oracle restatement (dense Gram/Cholesky, "
+                                   "multithreaded BLAS)"},
+        "e2e": {"value": value, "unit": "QPs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}), flush=True)
+    return
+  cpu = None
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    import scipy.sparse as sp
+    from oracle import qtqp_oracle as orc
+    t0 = time.perf_counter()
+    orc.solve(sp.csc_matrix(a), b, c, z, sp.csc_matrix(p), backend="dense")
+    t = time.perf_counter() - t0
+    cpu = {"value": 1.0 / t, "unit": "QPs/s", "cores": os.cpu_count() or 1, "kind": "port",
+           "sample": "one whole solve of the QP, oracle restatement (dense Gram/Cholesky, "
+                     "multithreaded BLAS)"}
+  import numpy as np
+  import torch
+  from qtqp_b200 import batch, large
+  torch.cuda.set_device(local)
+  dev = torch.device("cuda", local)
+  stream = torch.cuda.current_stream(dev)
+  dist = None
+  if world > 1:
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+  prob = batch.DenseProblem(a=a, b=b, c=c, z=z, p=p)
+  forms = {}
+  for precision in ("fp64", "mixed"):
+    dl = large.DeviceLarge(prob, batch.SolveOptions(precision=precision), device=dev)
+    dl.upload(stream)
+    for _ in range(args.warmup):
+      dl.launch(stream)
+    torch.cuda.synchronize(dev)
+    clocks = _Clocks(local) if precision == args.precision else None
+    t = sum(_ev_time(stream, lambda: dl.launch(stream)) for _ in range(args.steps))
+    ck = clocks.stop() if clocks else None
+    res = dl.fetch()[0][0]
+    if dist is not None:
+      tt = torch.tensor([t], dtype=torch.float64, device=dev)
+      dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+      t = float(tt.item())
+    forms[precision] = dict(dl=dl, time=t, res=res, clocks=ck)
+  chosen = forms[args.precision]
+  dl, res = chosen["dl"], chosen["res"]
+  solved = int(res["status"] == 0)
+  value = solved * world * args.steps / chosen["time"]
+  fp64 = forms["fp64"]
+  fp64_value = int(fp64["res"]["status"] == 0) * world * args.steps / fp64["time"]
+  mixed = forms["mixed"]
+  mixed_value = int(mixed["res"]["status"] == 0) * world * args.steps / mixed["time"]
+  # End to end: host inputs -> device, solve, outputs -> host, every step.
+  h_out = [torch.empty_like(t_, device="cpu").pin_memory() for t_ in (dl.x, dl.y, dl.s,
+                                                                      dl.result)]
+
+  def e2e_step():
+    dl.upload(stream)
+    dl.launch(stream)
+    with torch.cuda.stream(stream):
+      for dst, src in zip(h_out, (dl.x, dl.y, dl.s, dl.result)):
+        dst.copy_(src, non_blocking=True)
+  e2e_step()
+  e_total = sum(_ev_time(stream, e2e_step) for _ in range(args.steps))
+  t_launch = chosen["time"] / args.steps
+  nfact = int(res["fp32_factorizations"] + res["fp64_factorizations"])
+  achieved = flops * nfact / t_launch / 1e12
+  peak, peak_kind = _bf16_peak()
+  if rank == 0:
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_launch,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator of the workload's distribution)",
+        "config": {"workload": LARGE_WORKLOAD, "precision": args.precision,
+                   "l2": "inputs (A 268 MB, P 134 MB) exceed L2",
+                   "parallelism": "replicas" if world > 1 else "one QP per GPU"},
+        "fp64_value": fp64_value, "mixed_value": mixed_value,
+        "chosen_over_fp64": value / fp64_value if fp64_value else None,
+        "statuses_identical": bool(fp64["res"]["status"] == mixed["res"]["status"]),
+        "iterations": int(res["iterations"]),
+        "factorizations": {"fp32": int(res["fp32_factorizations"]),
+                           "fp64": int(res["fp64_factorizations"])},
+        "kkt_tflops": achieved,
+        "e2e": {"value": solved * args.steps / e_total, "unit": "QPs/s",
+                "h2d_bytes_per_step": dl.input_bytes,
+                "d2h_bytes_per_step": sum(int(t_.numel() * t_.element_size()) for t_ in h_out)},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "kernel": "large_solve_kernel",
+                     "algorithmic_flops_per_launch": flops * nfact,
+                     "note": "algorithmic KKT factorisation flops (m n (n+1) + n^3/3 per "
+                             "factorisation) over the whole solve's time"},
+        "cpu_baseline": cpu, "clocks": chosen["clocks"], "gpu_launches": args.steps}),
+          flush=True)
+  if dist is not None:
+    dist.destroy_process_group()
+
+
+def run_parametric(args):
+  """Plain FP64 batch vs mixed precision + learned warm start on held-out
+  instances of the parametric family (training is outside the timed region)."""
+  rank = int(os.environ.get("RANK", "0"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  if rank != 0:
+    return
+  test_count = args.count if args.count != COUNT else 512
+  from qtqp_b200 import problems
+  fam = problems.config4_family(count=args.train + test_count)
+  thetas = fam[-1]
+  insts = [problems.config4_instance(fam, i) for i in range(args.train + test_count)]
+  if args.impl == "reference":
+    import scipy.sparse as sp
+    from oracle import qtqp_oracle as orc
+    cores = os.cpu_count() or 1
+    sample = list(range(args.train, args.train + min(test_count, 4)))
+    t0 = time.perf_counter()
+    for i in sample:
+      a, b, c, z, p = insts[i]
+      orc.solve(a, b, c, z, p, backend="superlu")
+    t = time.perf_counter() - t0
+    value = len(sample) / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": PARAM_WORKLOAD},
+        "cpu_baseline": {"value": value, "unit": "QPs/s", "cores": 1, "kind": "port",
+                         "sample": f"{len(sample)} held-out instances, oracle (sparse LU)"},
+        "e2e": {"value": value, "unit": "QPs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}), flush=True)
+    return
+  import numpy as np
+  import torch
+  import qtqp_b200 as qb
+  from qtqp_b200 import band, batch, warmstart
+  torch.cuda.set_device(local)
+  dev = torch.device("cuda", local)
+  stream = torch.cuda.current_stream(dev)
+  qps = [qb.QTQP(a=a, b=b, c=c, z=z, p=p) for a, b, c, z, p in insts]
+  train = list(range(args.train))
+  test = list(range(args.train, args.train + test_count))
+  t0 = time.perf_counter()
+  sols = qb.solve_batch([qps[i] for i in train], storage="band")
+  t_label = time.perf_counter() - t0
+  keep = [i for i, s_ in zip(train, sols) if s_.status == qb.SolutionStatus.SOLVED]
+  sols = [s_ for s_ in sols if s_.status == qb.SolutionStatus.SOLVED]
+  q0 = qps[0]
+  targets = warmstart.targets_from(q0.n, q0.z, [s_.x for s_ in sols], [s_.y for s_ in sols],
+                                   [s_.s for s_ in sols])
+  net = warmstart.WarmStartMLP(dim=thetas.shape[1], n=q0.n, m=q0.m, z=q0.z, seed=0, device=dev)
+  t0 = time.perf_counter()
+  rep = net.train(thetas[keep], targets, epochs=30, batch=64, lr=2e-3)
+  torch.cuda.synchronize(dev)
+  t_train = time.perf_counter() - t0
+  net.calibrate(thetas[keep], targets)
+  probs = [qps[i].band_problem() for i in test]
+
+  def timed(opts, warm_fn):
+    hb = band.HostBandBatch(probs, opts)
+    db = band.DeviceBandBatch(hb, device=dev)
+    db.upload(stream)
+    for _ in range(args.warmup):
+      db.launch(stream, warm=warm_fn())
+    torch.cuda.synchronize(dev)
+    t = sum(_ev_time(stream, lambda: db.launch(stream, warm=warm_fn()))
+            for _ in range(args.steps))
+    return t, db.fetch()[0]
+  t_plain, r_plain = timed(batch.SolveOptions(precision="fp64"), lambda: None)
+  corr = 16
+  t_warm, r_warm = timed(batch.SolveOptions(precision="mixed", warm_corrections=corr),
+                         lambda: net.predict_device(thetas[test]))
+  solved_w = int(np.sum(r_warm["status"] == 0))
+  solved_p = int(np.sum(r_plain["status"] == 0))
+  value = solved_w * args.steps / t_warm
+  fp64_value = solved_p * args.steps / t_plain
+  hidden = net.hidden
+  params = thetas.shape[1] * hidden + hidden * hidden + hidden * net.out + 2 * hidden + net.out
+  train_flops = 3 * 2 * params * len(keep) * rep.epochs
+  print(json.dumps({
+      "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": 1, "steps": args.steps,
+      "warmup": args.warmup, "ms_per_step": 1e3 * t_warm / args.steps, "higher_is_better": True,
+      "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+      "data": "synthetic (seeded generator of the family)",
+      "config": {"workload": PARAM_WORKLOAD, "test_instances": test_count,
+                 "train_instances": len(keep), "warm_corrections": corr,
+                 "chosen": "mixed precision + learned warm start; fp64_value: plain FP64"},
+      "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
+      "statuses_identical": bool(np.array_equal(r_plain["status"], r_warm["status"])),
+      "warm_accepted": int(r_warm["warm_started"].sum()),
+      "iterations": {"plain": int(r_plain["iterations"].sum()),
+                     "warm": int(r_warm["iterations"].sum())},
+      "mlp": {"train_seconds": t_train, "label_seconds": t_label, "epochs": rep.epochs,
+              "final_loss": rep.final_loss, "row_error_rate": net.row_error_rate,
+              "train_tflops": train_flops / t_train / 1e12},
+      "cpu_baseline": None, "gpu_launches": args.steps * 5}), flush=True)
+
+
 def main():
   args = _args()
-  if args.impl == "reference":
+  if args.workload == "dense_large":
+    run_dense_large(args)
+  elif args.workload == "parametric":
+    run_parametric(args)
+  elif args.impl == "reference":
     run_reference(args)
   else:
     run_ours(args)
