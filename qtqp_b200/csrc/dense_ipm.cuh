@@ -202,6 +202,7 @@ struct Ipm {
   double* g64;
   float* g32l;
   double* linv;
+  double* sinv;  // sub-block inverses of the current panel step
   float* xhi;
   float* xlo;
   const void* map_hi;

@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(kGridBT, 1)
   s.g64 = reinterpret_cast<double*>(p.ws + L.g64_off);
   s.g32l = reinterpret_cast<float*>(p.ws + L.g32_off);
   s.linv = reinterpret_cast<double*>(p.ws + L.linv_off);
+  s.sinv = reinterpret_cast<double*>(p.ws + L.sinv_off);
   s.xhi = reinterpret_cast<float*>(p.ws + L.xhi_off);
   s.xlo = reinterpret_cast<float*>(p.ws + L.xlo_off);
   s.map_hi = &map_hi;
@@ -118,6 +119,9 @@ extern "C" int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t h
                                       const qtqp_options* opt, void* stream) {
   if (n < 1 || m < 1 || z < 0 || z >= m)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_large_solve: needs n, m >= 1 and 0 <= z < m");
+  if (n > kLB * kLargeBlocks)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_large_solve: n must be at most " +
+                                      std::to_string(kLB * kLargeBlocks));
   if (size_t(m) * size_t(n) >= (size_t(1) << 31) || size_t(round_up(n, kLB)) * round_up(m, 32) >=
                                                         (size_t(1) << 31))
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_large_solve: m * n must stay below 2^31");

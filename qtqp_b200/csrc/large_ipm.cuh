@@ -37,8 +37,8 @@ __host__ __device__ inline int round_up(int v, int q) { return (v + q - 1) / q *
 // Global workspace of a large solve.
 struct LargeLayout {
   int n, m, npad, mpad, nblk, np;
-  size_t ctl_off, info_off, v_off, a_off, p_off, g64_off, g32_off, linv_off, xhi_off, xlo_off,
-      total;
+  size_t ctl_off, info_off, v_off, a_off, p_off, g64_off, g32_off, linv_off, sinv_off, xhi_off,
+      xlo_off, total;
 };
 __host__ __device__ inline LargeLayout plan_large_layout(int n, int m) {
   LargeLayout L;
@@ -66,6 +66,8 @@ __host__ __device__ inline LargeLayout plan_large_layout(int n, int m) {
   off += al(size_t(L.npad) * L.npad * 4);
   L.linv_off = off;
   off += al(2 * size_t(L.nblk) * kLB * kLB * 8);  // inverses and their transposes
+  L.sinv_off = off;
+  off += al(4 * 32 * 33 * 8);                      // sub-block inverses of one step
   L.xhi_off = off;
   off += al(size_t(L.npad) * L.mpad * 4);
   L.xlo_off = off;
@@ -211,6 +213,10 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tc::smem_u32(dst)), "l"(src)
+               : "memory");
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -327,14 +333,99 @@ __device__ void large_finish_gram(S& s, T* g) {
 
 // ---------------------------------------------------------------------------
 // Blocked Cholesky of the lower triangle of g (npad x npad), then the
-// inverses of the diagonal blocks into linv.  Returns 0 or the 1-based index
-// of the first non-positive pivot (uniform over the grid).
+// inverses of the diagonal blocks into linv (and, resident in each CTA's
+// shared memory, the inverse of the block the CTA owns in the solves).
+// Returns 0 or the 1-based index of the first non-positive pivot (uniform
+// over the grid).
+//
+// Step k (panel width 128):
+//   (a) one CTA factors the diagonal block in shared memory, in four 32-wide
+//       steps: one warp factors the 32 x 32 diagonal sub-block in registers
+//       and inverts it, the rows below are solved with that inverse, and the
+//       trailing part of the block is updated;
+//   (b) every warp takes panel rows and solves x L_kk^T = g_i with the four
+//       sub-block inverses (one lane per column, broadcasts by shuffle);
+//   (c) the lower 128 x 128 tiles right of the panel get g_ij -= L_ik L_jk^T
+//       with 8 x 8 outputs per thread and cp.async double-buffered slices.
 // ---------------------------------------------------------------------------
+constexpr int kPitch = kLB + 1;   // shared-memory pitch of a staged 128 x 128 block
+constexpr int kSubPitch = 33;     // pitch of a staged 32 x 32 block
+
+// 128 x 128 block of g at (r0, c0) into dst[r * kPitch + c], eight loads in
+// flight per thread; the strict upper part is zero when lower_only.
+template <typename T>
+__device__ __forceinline__ void stage_block(T* dst, const T* g, size_t ld, int r0, int c0,
+                                            bool lower_only) {
+  for (int base = threadIdx.x; base < kLB * kLB; base += 8 * kGridBT) {
+    T v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = base + q * kGridBT, r = e >> 7, c = e & 127;
+      v[q] = (!lower_only || c <= r) ? g[size_t(r0 + r) * ld + c0 + c] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = base + q * kGridBT;
+      dst[(e >> 7) * kPitch + (e & 127)] = v[q];
+    }
+  }
+}
+
+// One warp factors the 32 x 32 lower block at sm[o][o] (pitch kPitch) in
+// registers (lane r holds row r), writes L back and its inverse to
+// inv32[r * kSubPitch + c].  Returns 0 or the 1-based failing pivot (the
+// same in every lane).
+template <typename T>
+__device__ __noinline__ int warp_chol32(T* sm, int o, T* inv32, int lane) {
+  T a[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) a[j] = (j <= lane) ? sm[(o + lane) * kPitch + o + j] : T(0);
+  int bad = 0;  // no early exit: the loops stay fully unrolled, a[] in registers
+#pragma unroll
+  for (int c = 0; c < 32; ++c) {
+    const T piv = __shfl_sync(0xffffffffu, a[c], c);
+    if (!(piv > T(0)) && bad == 0) bad = c + 1;
+    const T lcc = sqrt(piv);
+    const T l = lane == c ? lcc : (lane > c ? a[c] / lcc : T(0));
+    a[c] = l;
+#pragma unroll
+    for (int j = c + 1; j < 32; ++j) {
+      const T lj = __shfl_sync(0xffffffffu, l, j);
+      if (lane >= j) a[j] = fma(-l, lj, a[j]);
+    }
+  }
+  if (bad) return bad;
+#pragma unroll
+  for (int j = 0; j < 32; ++j)
+    if (j <= lane) sm[(o + lane) * kPitch + o + j] = a[j];
+  __syncwarp();
+  // Inverse, one column per lane (c = lane): x_c = 1 / L_cc,
+  // x_r = -(sum_{c <= k < r} L_rk x_k) / L_rr; L read back from shared
+  // memory (the same address in every lane: broadcasts).
+  T x[32];
+  const T* L = sm + o * kPitch + o;
+#pragma unroll
+  for (int r = 0; r < 32; ++r) {
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < r; ++k)
+      if (k >= lane) acc = fma(L[r * kPitch + k], x[k], acc);
+    const T lrr = L[r * kPitch + r];
+    x[r] = r < lane ? T(0) : (r == lane ? T(1) / lrr : -acc / lrr);
+  }
+#pragma unroll
+  for (int r = 0; r < 32; ++r) inv32[r * kSubPitch + lane] = x[r];
+  return 0;
+}
+
 template <typename T, class S>
 __device__ int large_cholesky(S& s, T* g) {
   const int npad = s.npad, nblk = npad / kLB;
   int* info = s.linfo;
-  T* sm = reinterpret_cast<T*>(s.arena);  // diagonal block [128][129] / staging
+  T* sm = reinterpret_cast<T*>(s.arena);   // staged 128 x 128 block (pitch kPitch)
+  T* sinv = sm + kLB * kPitch;              // 4 sub-block inverses (pitch kSubPitch)
+  volatile int* sflag = reinterpret_cast<volatile int*>(sinv + 4 * 32 * kSubPitch);
+  T* ginv = reinterpret_cast<T*>(s.sinv);   // the same inverses in global memory
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gwarp = blockIdx.x * (kGridBT / 32) + warp, nwarps = gridDim.x * (kGridBT / 32);
   if (s.tid == 0) *info = 0;
@@ -343,43 +434,70 @@ __device__ int large_cholesky(S& s, T* g) {
   for (int k = 0; k < nblk; ++k) {
     const int k0 = k * kLB;
     QTQP_RETIC();
-    // (a) diagonal block: one CTA, one barrier per column.
+    // (a) diagonal block.
     if (int(blockIdx.x) == k % int(gridDim.x)) {
-      for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
-        const int r = e >> 7, c = e & 127;
-        sm[r * 129 + c] = c <= r ? g[size_t(k0 + r) * npad + k0 + c] : T(0);
-      }
+      QTQP_TIC();
+      stage_block(sm, g, npad, k0, k0, true);
       __syncthreads();
-      T d_prev = T(1);
+      QTQP_TOC(kPhNormalize);
       int bad = 0;
-      for (int c = 0; c <= kLB; ++c) {
-        if (c > 0) {  // finish column c-1
-          const T l = sqrt(d_prev), il = T(1) / l;
-          for (int r = c + int(threadIdx.x); r < kLB; r += blockDim.x) sm[r * 129 + c - 1] *= il;
-          if (threadIdx.x == 0) sm[(c - 1) * 129 + c - 1] = l;
+      for (int q = 0; q < 4 && !bad; ++q) {
+        const int o = 32 * q;
+        QTQP_RETIC();
+        if (warp == 0) {
+          const int b = warp_chol32(sm, o, sinv + q * 32 * kSubPitch, lane);
+          if (lane == 0) *sflag = b ? o + b : 0;
         }
-        if (c == kLB) break;
-        const T d = sm[c * 129 + c];
-        if (!(d > T(0))) {
-          bad = c + 1;
-          break;
-        }
-        const T inv_d = T(1) / d;
-        for (int j = c + 1 + warp; j < kLB; j += blockDim.x / 32) {
-          const T t = sm[j * 129 + c] * inv_d;
-          for (int r = j + lane; r < kLB; r += 32) sm[r * 129 + j] = fma(-sm[r * 129 + c], t, sm[r * 129 + j]);
-        }
-        d_prev = d;
         __syncthreads();
+        QTQP_TOC(kPhStep);
+        QTQP_RETIC();
+        bad = *sflag;
+        if (bad) break;
+        // Rows below the sub-block: x = row inv(L_qq)^T (thread per row).
+        const T* iq = sinv + q * 32 * kSubPitch;
+        const int rows = kLB - o - 32;
+        if (int(threadIdx.x) < rows) {
+          T* row = sm + (o + 32 + threadIdx.x) * kPitch + o;
+          T v[32];
+#pragma unroll
+          for (int l = 0; l < 32; ++l) v[l] = row[l];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            T acc = T(0);
+#pragma unroll
+            for (int l = 0; l <= j; ++l) acc = fma(v[l], iq[j * kSubPitch + l], acc);
+            row[j] = acc;
+          }
+        }
+        __syncthreads();
+        // Trailing lower part of the block: a_ij -= sum_l a_il a_jl.
+        const int t0 = o + 32, tn = kLB - t0, cnt = tn * (tn + 1) / 2;
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+          int i = int((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+          while (i * (i + 1) / 2 > e) --i;
+          while ((i + 1) * (i + 2) / 2 <= e) ++i;
+          const int j = e - i * (i + 1) / 2;
+          const T* ri = sm + (t0 + i) * kPitch + o;
+          const T* rj = sm + (t0 + j) * kPitch + o;
+          T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+          for (int l = 0; l < 32; l += 2) {
+            acc0 = fma(ri[l], rj[l], acc0);
+            acc1 = fma(ri[l + 1], rj[l + 1], acc1);
+          }
+          sm[(t0 + i) * kPitch + t0 + j] -= acc0 + acc1;
+        }
+        __syncthreads();
+        QTQP_TOC(kPhOther);
       }
-      __syncthreads();
       if (bad) {
         if (threadIdx.x == 0) atomicCAS(info, 0, k0 + bad);
       } else {
         for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
           const int r = e >> 7, c = e & 127;
-          if (c <= r) g[size_t(k0 + r) * npad + k0 + c] = sm[r * 129 + c];
+          if (c <= r) g[size_t(k0 + r) * npad + k0 + c] = sm[r * kPitch + c];
         }
+        for (int e = threadIdx.x; e < 4 * 32 * kSubPitch; e += blockDim.x) ginv[e] = sinv[e];
       }
     }
     s.sync();
@@ -388,93 +506,109 @@ __device__ int large_cholesky(S& s, T* g) {
     if (*reinterpret_cast<volatile int*>(info) != 0) break;
     const int rest = npad - k0 - kLB;
     if (rest == 0) break;
-    // (b) panel rows: x L_kk^T = g_i, one warp per row, lane owns columns
-    // 4 lane .. 4 lane + 3.  L_kk is staged in shared memory by every CTA.
-    for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
-      const int r = e >> 7, c = e & 127;
-      sm[r * 129 + c] = c <= r ? g[size_t(k0 + r) * npad + k0 + c] : T(0);
-    }
-    __syncthreads();
-    for (int row = k0 + kLB + gwarp; row < npad; row += nwarps) {
-      T* gr = g + size_t(row) * npad + k0;
-      T x[4];
+    // (b) panel rows.
+    if (k0 + kLB + int(blockIdx.x) * (kGridBT / 32) < npad) {  // this CTA has rows
+      stage_block(sm, g, npad, k0, k0, true);
+      for (int e = threadIdx.x; e < 4 * 32 * kSubPitch; e += blockDim.x) sinv[e] = ginv[e];
+      __syncthreads();
+      for (int row = k0 + kLB + gwarp; row < npad; row += nwarps) {
+        T* gr = g + size_t(row) * npad + k0;
+        T v[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) x[q] = gr[4 * lane + q];
-      for (int c = 0; c < kLB; ++c) {
-        const int owner = c >> 2, slot = c & 3;
-        T xc = T(0);
-        if (lane == owner) {
-          T v = x[0];
-          if (slot == 1) v = x[1];
-          if (slot == 2) v = x[2];
-          if (slot == 3) v = x[3];
-          xc = v / sm[c * 129 + c];
-          if (slot == 0) x[0] = xc;
-          if (slot == 1) x[1] = xc;
-          if (slot == 2) x[2] = xc;
-          if (slot == 3) x[3] = xc;
-        }
-        xc = __shfl_sync(0xffffffffu, xc, owner);
+        for (int q = 0; q < 4; ++q) v[q] = gr[32 * q + lane];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const int l = 4 * lane + q;
-          if (l > c) x[q] = fma(-xc, sm[l * 129 + c], x[q]);
-        }
-      }
+          const T* iq = sinv + q * 32 * kSubPitch;
+          T x = T(0);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) gr[4 * lane + q] = x[q];
+          for (int l = 0; l < 32; ++l)
+            x = fma(__shfl_sync(0xffffffffu, v[q], l), iq[lane * kSubPitch + l], x);
+          v[q] = x;
+#pragma unroll
+          for (int q2 = q + 1; q2 < 4; ++q2) {
+            const T* lr = sm + (32 * q2 + lane) * kPitch + 32 * q;
+#pragma unroll
+            for (int l = 0; l < 32; ++l) v[q2] = fma(-__shfl_sync(0xffffffffu, x, l), lr[l], v[q2]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gr[32 * q + lane] = v[q];
+      }
     }
     s.sync();
     QTQP_TOC(kPhLgPanel);
     QTQP_RETIC();
-    // (c) trailing update of the lower 64 x 64 tiles right of the panel:
-    // g_ij -= L_ik L_jk^T (K = 128), panels staged k-major in shared memory.
+    // (c) trailing update.
     {
-      constexpr int PP = 65;  // pitch: conflict-free transposed staging
-      T* pa = sm;             // [128][PP]: pa[kk * PP + r] = L[i0 + r][k0 + kk]
-      T* pb = sm + kLB * PP;  // [128][PP]
+      constexpr int KS = 16;
+      constexpr int SP = kLB + 1;                     // slice pitch
+      constexpr int SL = 2 * KS * SP;                 // elements per buffer
       const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-      const int nt = rest / 64, tiles = nt * (nt + 1) / 2;
+      const int nt = rest / kLB, tiles = nt * (nt + 1) / 2;
       const int base = k0 + kLB;
+      auto issue = [&](int kk0, int i0, int j0, int buf) {
+        T* pa = sm + buf * SL;
+        T* pb = pa + KS * SP;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int e = threadIdx.x + q * kGridBT, r = e >> 4, kk = e & 15;
+          if constexpr (sizeof(T) == 8) {
+            cp_async8(pa + kk * SP + r, g + size_t(i0 + r) * npad + k0 + kk0 + kk, true);
+            cp_async8(pb + kk * SP + r, g + size_t(j0 + r) * npad + k0 + kk0 + kk, true);
+          } else {
+            cp_async4(pa + kk * SP + r, g + size_t(i0 + r) * npad + k0 + kk0 + kk);
+            cp_async4(pb + kk * SP + r, g + size_t(j0 + r) * npad + k0 + kk0 + kk);
+          }
+        }
+        cp_async_commit();
+      };
       for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
         int ti = 0;
         while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
         const int tj = t - ti * (ti + 1) / 2;
-        const int i0 = base + ti * 64, j0 = base + tj * 64;
-        for (int e = threadIdx.x; e < 64 * kLB; e += blockDim.x) {
-          const int r = e >> 7, kk = e & 127;
-          pa[kk * PP + r] = g[size_t(i0 + r) * npad + k0 + kk];
-          pb[kk * PP + r] = g[size_t(j0 + r) * npad + k0 + kk];
-        }
-        __syncthreads();
-        T acc[4][4];
+        const int i0 = base + ti * kLB, j0 = base + tj * kLB;
+        T acc[8][8];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < 8; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-#pragma unroll 4
-        for (int kk = 0; kk < kLB; ++kk) {
-          T av[4], bv[4];
-#pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            av[a] = pa[kk * PP + ty * 4 + a];
-            bv[a] = pb[kk * PP + tx * 4 + a];
+          for (int b = 0; b < 8; ++b) acc[a][b] = T(0);
+        issue(0, i0, j0, 0);
+        int buf = 0;
+        for (int kk0 = 0; kk0 < kLB; kk0 += KS) {
+          if (kk0 + KS < kLB) {
+            issue(kk0 + KS, i0, j0, buf ^ 1);
+            cp_async_wait<1>();
+          } else {
+            cp_async_wait<0>();
           }
+          __syncthreads();
+          const T* pa = sm + buf * SL;
+          const T* pb = pa + KS * SP;
+#pragma unroll 2
+          for (int kk = 0; kk < KS; ++kk) {
+            T av[8], bv[8];
 #pragma unroll
-          for (int a = 0; a < 4; ++a)
+            for (int a = 0; a < 8; ++a) {
+              av[a] = pa[kk * SP + ty + 16 * a];
+              bv[a] = pb[kk * SP + tx + 16 * a];
+            }
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+              for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+          }
+          __syncthreads();
+          buf ^= 1;
         }
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int i = i0 + ty * 4 + a;
+        for (int a = 0; a < 8; ++a) {
+          const int i = i0 + ty + 16 * a;
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const int j = j0 + tx * 4 + b;
+          for (int b = 0; b < 8; ++b) {
+            const int j = j0 + tx + 16 * b;
             if (j <= i) g[size_t(i) * npad + j] -= acc[a][b];
           }
         }
-        __syncthreads();
       }
     }
     s.sync();
@@ -487,10 +621,7 @@ __device__ int large_cholesky(S& s, T* g) {
   T* lv = reinterpret_cast<T*>(s.linv);
   for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
     const int b0 = b * kLB;
-    for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
-      const int r = e >> 7, c = e & 127;
-      sm[r * 129 + c] = c <= r ? g[size_t(b0 + r) * npad + b0 + c] : T(0);
-    }
+    stage_block(sm, g, npad, b0, b0, true);
     __syncthreads();
     T* inv = lv + size_t(b) * kLB * kLB;                 // inv(L_bb), row-major
     T* invt = lv + size_t(nblk + b) * kLB * kLB;         // its transpose
@@ -500,16 +631,16 @@ __device__ int large_cholesky(S& s, T* g) {
       // thread): x_c = 1 / L_cc; x_r = -(sum_{c <= l < r} L_rl x_l) / L_rr.
       T* xc = invt + size_t(c) * kLB;
       for (int r = 0; r < c; ++r) xc[r] = T(0);
-      xc[c] = T(1) / sm[c * 129 + c];
+      xc[c] = T(1) / sm[c * kPitch + c];
       for (int r = c + 1; r < kLB; ++r) {
         T acc0 = T(0), acc1 = T(0);
         int l = c;
         for (; l + 1 < r; l += 2) {
-          acc0 = fma(sm[r * 129 + l], xc[l], acc0);
-          acc1 = fma(sm[r * 129 + l + 1], xc[l + 1], acc1);
+          acc0 = fma(sm[r * kPitch + l], xc[l], acc0);
+          acc1 = fma(sm[r * kPitch + l + 1], xc[l + 1], acc1);
         }
-        if (l < r) acc0 = fma(sm[r * 129 + l], xc[l], acc0);
-        xc[r] = -(acc0 + acc1) / sm[r * 129 + r];
+        if (l < r) acc0 = fma(sm[r * kPitch + l], xc[l], acc0);
+        xc[r] = -(acc0 + acc1) / sm[r * kPitch + r];
       }
     }
     __syncthreads();
@@ -520,6 +651,12 @@ __device__ int large_cholesky(S& s, T* g) {
     __syncthreads();
   }
   s.sync();
+  // Each CTA keeps the inverse of the block it owns in the solves resident
+  // in shared memory until the next factorisation.
+  if (int(blockIdx.x) < nblk) {
+    stage_block(sm, lv + size_t(blockIdx.x) * kLB * kLB, kLB, 0, 0, false);
+    __syncthreads();
+  }
   QTQP_TOC(kPhLgInv);
   return 0;
 }
@@ -562,51 +699,56 @@ template <typename T, class S>
 __device__ void large_chol_solve(S& s, T* v, T* w) {
   const int n = s.n, npad = s.npad;
   const int nb = (n + kLB - 1) / kLB;
-  const int nblk = npad / kLB;
   const T* g = sizeof(T) == 4 ? reinterpret_cast<const T*>(s.g32l)
                               : reinterpret_cast<const T*>(s.g64);
-  const T* lv = reinterpret_cast<const T*>(s.linv);
-  T* red = reinterpret_cast<T*>(s.arena);  // [kLB] partials of the owner
+  // CTA b owns block b (nb <= gridDim.x); inv(L_bb) is resident in its shared
+  // memory (pitch kPitch) since the factorisation.
+  const T* rinv = reinterpret_cast<const T*>(s.arena);
+  T* red = reinterpret_cast<T*>(s.arena) + kLB * kPitch;  // [kLB] partials of the owner
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int WPB = kGridBT / 32;
   const int G = gridDim.x;
   auto bsz = [&](int b) { return min(kLB, n - b * kLB); };
-  // z_b = inv(L_bb) v_b: thread r < bs, reading the transposed inverse
-  // (coalesced over r).
+  // z_b = inv(L_bb) v_b by CTA b (thread r < bs; v_b staged in red).
   auto diag_fwd = [&](int b) {
     const int b0 = b * kLB, bs = bsz(b);
-    const T* it = lv + size_t(nblk + b) * kLB * kLB;
+    if (int(threadIdx.x) < bs) red[threadIdx.x] = v[b0 + threadIdx.x];
+    __syncthreads();
     if (int(threadIdx.x) < bs) {
       const int r = threadIdx.x;
+      const T* ir = rinv + r * kPitch;
       T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
       int c = 0;
       for (; c + 3 <= r; c += 4) {
-        a0 = fma(it[(c + 0) * kLB + r], v[b0 + c + 0], a0);
-        a1 = fma(it[(c + 1) * kLB + r], v[b0 + c + 1], a1);
-        a2 = fma(it[(c + 2) * kLB + r], v[b0 + c + 2], a2);
-        a3 = fma(it[(c + 3) * kLB + r], v[b0 + c + 3], a3);
+        a0 = fma(ir[c + 0], red[c + 0], a0);
+        a1 = fma(ir[c + 1], red[c + 1], a1);
+        a2 = fma(ir[c + 2], red[c + 2], a2);
+        a3 = fma(ir[c + 3], red[c + 3], a3);
       }
-      for (; c <= r; ++c) a0 = fma(it[c * kLB + r], v[b0 + c], a0);
+      for (; c <= r; ++c) a0 = fma(ir[c], red[c], a0);
       w[b0 + r] = (a0 + a1) + (a2 + a3);
     }
+    __syncthreads();
   };
-  // x_b = inv(L_bb)^T w_b: thread r < bs (coalesced over r).
+  // x_b = inv(L_bb)^T w_b by CTA b (thread r < bs; w_b staged in red).
   auto diag_bwd = [&](int b) {
     const int b0 = b * kLB, bs = bsz(b);
-    const T* inv = lv + size_t(b) * kLB * kLB;
+    if (int(threadIdx.x) < bs) red[threadIdx.x] = w[b0 + threadIdx.x];
+    __syncthreads();
     if (int(threadIdx.x) < bs) {
       const int r = threadIdx.x;
       T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
       int c = r;
       for (; c + 3 < bs; c += 4) {
-        a0 = fma(inv[(c + 0) * kLB + r], w[b0 + c + 0], a0);
-        a1 = fma(inv[(c + 1) * kLB + r], w[b0 + c + 1], a1);
-        a2 = fma(inv[(c + 2) * kLB + r], w[b0 + c + 2], a2);
-        a3 = fma(inv[(c + 3) * kLB + r], w[b0 + c + 3], a3);
+        a0 = fma(rinv[(c + 0) * kPitch + r], red[c + 0], a0);
+        a1 = fma(rinv[(c + 1) * kPitch + r], red[c + 1], a1);
+        a2 = fma(rinv[(c + 2) * kPitch + r], red[c + 2], a2);
+        a3 = fma(rinv[(c + 3) * kPitch + r], red[c + 3], a3);
       }
-      for (; c < bs; ++c) a0 = fma(inv[c * kLB + r], w[b0 + c], a0);
+      for (; c < bs; ++c) a0 = fma(rinv[c * kPitch + r], red[c], a0);
       v[b0 + r] = (a0 + a1) + (a2 + a3);
     }
+    __syncthreads();
   };
   // v_i -= L_ib z_b for rows [lo, hi): each warp takes 4 rows at a time,
   // lanes split the 128 columns (4 each), then 4 shuffle reductions.
@@ -689,15 +831,29 @@ __device__ void large_chol_solve(S& s, T* v, T* w) {
       const int col = threadIdx.x & (kLB - 1), half = threadIdx.x >> 7;
       const int mid = bs / 2;
       const T part = bwd_col(b, prv0 + col, half ? mid : 0, half ? bs : mid);
-      if (half) red[col] = part;
+      if (half) red[kLB + col] = part;
       __syncthreads();
-      if (!half) w[prv0 + col] -= part + red[col];
+      if (!half) w[prv0 + col] -= part + red[kLB + col];
       __syncthreads();
       diag_bwd(b - 1);
     } else {
+      // 32 columns per CTA, the block's rows split over the 8 warps (16 each),
+      // partial sums combined in a fixed order.
       const int cta = (int(blockIdx.x) - own - 1 + G) % G;
-      for (int i = cta * kGridBT + threadIdx.x; i < prv0; i += (G - 1) * kGridBT)
-        w[i] -= bwd_col(b, i, 0, bs);
+      const int col = threadIdx.x & 31, part = threadIdx.x >> 5;
+      const int l0 = min(bs, 16 * part), l1 = min(bs, 16 * part + 16);
+      for (int c0 = 32 * cta; c0 < prv0; c0 += 32 * (G - 1)) {
+        const int i = c0 + col;
+        red[part * 32 + col] = i < prv0 ? bwd_col(b, i, l0, l1) : T(0);
+        __syncthreads();
+        if (part == 0 && i < prv0) {
+          T t = red[col];
+#pragma unroll
+          for (int q = 1; q < kGridBT / 32; ++q) t += red[q * 32 + col];
+          w[i] -= t;
+        }
+        __syncthreads();
+      }
     }
     s.sync();
   }
