@@ -58,6 +58,9 @@ def _args():
                        "one n=4096, m=8192 dense QP on the whole GPU; parametric: a T=50 "
                        "MPC family with the learned warm start")
   ap.add_argument("--train", type=int, default=4096, help="parametric: training instances")
+  ap.add_argument("--large-n", type=int, default=4096,
+                  help="dense_large: n (m = 2n, z = n/4); 4096 is the workload, smaller "
+                       "sizes are for profiling captures")
   ap.add_argument("--count", type=int, default=COUNT)
   ap.add_argument("--no-cpu-baseline", action="store_true")
   return ap.parse_args()
@@ -392,7 +395,9 @@ def run_dense_large(args):
   world = int(os.environ.get("WORLD_SIZE", "1"))
   local = int(os.environ.get("LOCAL_RANK", "0"))
   from qtqp_b200 import problems
-  a, b, c, z, p = problems.config2(seed=1002 + rank)
+  nl = args.large_n
+  a, b, c, z, p = problems.config2(seed=1002 + rank, n=nl, m=2 * nl, z=nl // 4,
+                                   rank=min(256, nl // 4))
   m, n = a.shape
   flops = m * n * (n + 1) + n ** 3 / 3.0  # one factorisation (Gram + Cholesky)
   if args.impl == "reference":
@@ -486,7 +491,9 @@ def run_dense_large(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_launch,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator of the workload's distribution)",
-        "config": {"workload": LARGE_WORKLOAD, "precision": args.precision,
+        "config": {"workload": LARGE_WORKLOAD if nl == 4096 else
+                   f"one dense QP: n={nl}, m={2 * nl}, z={nl // 4} (profiling size)",
+                   "precision": args.precision,
                    "l2": "inputs (A 268 MB, P 134 MB) exceed L2",
                    "parallelism": "replicas" if world > 1 else "one QP per GPU"},
         "fp64_value": fp64_value, "mixed_value": mixed_value,
