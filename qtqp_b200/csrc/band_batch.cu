@@ -29,6 +29,7 @@ struct BandParams {
   size_t slot_bytes;
   int32_t num_slots;
   int* counter;
+  size_t win_bytes;      // dynamic shared memory (0: no window)
   const double* warm_x;  // learned warm start (null: plain method)
   const double* warm_y;
   const unsigned char* warm_act;
@@ -37,6 +38,7 @@ struct BandParams {
 
 __global__ void __launch_bounds__(kBandThreads) band_batch_kernel(const BandParams p) {
   __shared__ double red[2 * (kBandThreads / 32) * kRedMax];
+  extern __shared__ double bwin[];  // window of the banded factorisation (win_bytes)
   __shared__ qtqp_options sopt;
   __shared__ int next_idx;
   if (threadIdx.x == 0) sopt = p.opt;
@@ -66,6 +68,10 @@ __global__ void __launch_bounds__(kBandThreads) band_batch_kernel(const BandPara
     s.red = red;
     s.phase = 0;
     s.o = &sopt;
+    s.bwin = (p.win_bytes > 0 && d.bw <= kBandWinMaxBw &&
+              band_win_bytes(d.bw, kBandThreads) <= p.win_bytes)
+                 ? bwin
+                 : nullptr;
     double* st = p.stats ? reinterpret_cast<double*>(p.stats + d.st_off) : nullptr;
     if (p.warm_act != nullptr) {
       s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off,
@@ -110,6 +116,10 @@ extern "C" int qtqp_band_batch_plan(qtqp_band_instance* h_inst, int32_t count,
   std::copy(ord.begin(), ord.end(), h_order);
   const int sms = num_sms > 0 ? num_sms : 148;
   const int slots = std::max(1, std::min(count, sms * kBandMaxBlocksPerSm));
+  size_t win = 0;  // the widest band that still fits the shared-memory window
+  for (int i = 0; i < count; ++i)
+    if (h_inst[i].bw <= kBandWinMaxBw)
+      win = std::max(win, band_win_bytes(std::min(h_inst[i].bw, h_inst[i].n - 1), kBandThreads));
   *plan = qtqp_batch_plan{};
   if (count == 0) return QTQP_OK;
   plan->num_groups = 1;
@@ -117,7 +127,7 @@ extern "C" int qtqp_band_batch_plan(qtqp_band_instance* h_inst, int32_t count,
   g.begin = 0;
   g.count = count;
   g.block_threads = kBandThreads;
-  g.smem_bytes = 0;
+  g.smem_bytes = int32_t(win);
   g.slots = slots;
   g.slot_off = kBandHeader;
   g.slot_bytes = slot;
@@ -160,8 +170,13 @@ extern "C" int qtqp_band_batch_solve(const qtqp_band_instance* d_inst, const int
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t win = size_t(std::max(G.smem_bytes, 0));
+  rc = cuda_check(cudaFuncSetAttribute(band_batch_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(win)),
+                  "cudaFuncSetAttribute(band_batch_kernel)");
+  if (rc) return rc;
   rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_batch_kernel,
-                                                                kBandThreads, 0),
+                                                                kBandThreads, win),
                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
   if (rc) return rc;
   BandParams p;
@@ -180,12 +195,13 @@ extern "C" int qtqp_band_batch_solve(const qtqp_band_instance* d_inst, const int
   p.slots = static_cast<char*>(d_workspace) + G.slot_off;
   p.slot_bytes = G.slot_bytes;
   p.counter = static_cast<int*>(d_workspace);
+  p.win_bytes = win;
   p.warm_x = d_warm_x;
   p.warm_y = d_warm_y;
   p.warm_act = d_warm_active;
   p.opt = *opt;
   const int grid = std::max(1, std::min({G.count, G.slots, sms * std::max(per_sm, 1)}));
   p.num_slots = grid;
-  band_batch_kernel<<<grid, kBandThreads, 0, st>>>(p);
+  band_batch_kernel<<<grid, kBandThreads, win, st>>>(p);
   return cuda_check(cudaGetLastError(), "band_batch_kernel launch");
 }

@@ -93,6 +93,22 @@ __host__ __device__ inline BandLayout plan_band_layout(int n, int m, int bw, int
   return L;
 }
 
+// Shared-memory window of the banded factorisation / solves: bands up to
+// kBandWinMaxBw use it (the (bw+2)^2 window, the per-thread Gram columns and
+// the 128-slot solve window must fit).
+constexpr int kBandWinMaxBw = 126;
+constexpr int kBandRing = 32;  // factor columns / rows in flight in the band solves
+__host__ __device__ inline size_t band_win_bytes(int bw, int nt) {
+  const size_t b2 = (size_t(bw) + 2) * (size_t(bw) + 2) * sizeof(double);
+  const size_t pairs = size_t(bw) * (size_t(bw) + 1) / 2 * sizeof(uint32_t);
+  const size_t cols = size_t(nt) * (size_t(bw) + 1) * sizeof(double);
+  const size_t solve = (128 + kBandRing * 128 + kBandRing) * sizeof(double);
+  size_t e = b2 + pairs;
+  if (cols > e) e = cols;
+  if (solve > e) e = solve;
+  return (e + 15) & ~size_t(15);
+}
+
 // Fields of one qtqp_iter_stats record.
 enum StatField : int {
   kStIter = 0, kStCtx, kStBty, kStPcost, kStDcost, kStPres, kStDres, kStGap,
@@ -186,6 +202,9 @@ struct Ipm {
   double* pv;
   double* Lb;
   int bw, nnz_a, nnz_p;
+  // Shared-memory window of the banded factorisation and solves (null: the
+  // band is too wide for it and the global-memory variants run).
+  double* bwin;
 
   // Grid mode (NT > 1024, FMT == kFmtLarge): the group is a cooperative grid
   // of NT / kGridBT blocks; barriers and reductions go through gctl.
@@ -1934,11 +1953,144 @@ struct Ipm {
     return t;
   }
 
-  // Gram matrix in column band storage, then Cholesky (one barrier per
-  // column, the unscaled column k updates the trailing band and column k-1
-  // is finished in the same phase); the diagonal keeps 1 / l_kk.
+  // Gram matrix in column band storage, then Cholesky.  With the shared-
+  // memory window (bw <= kBandWinMaxBw): each thread accumulates its Gram
+  // column in shared memory, and the factorisation keeps the active
+  // (bw+2) x (bw+2) part of the band in shared memory (band_chol_window).
+  // Otherwise the global-memory variant below runs.  The diagonal of the
+  // factor keeps 1 / l_kk.
   template <typename T>
   __device__ int band_factorize() {
+    if (bwin == nullptr) return band_factorize_global<T>();
+    QTQP_BAND_LOCALS;
+    QTQP_TIC();
+    T* L = reinterpret_cast<T*>(Lb);
+    const double* reg = vec(kREG);
+    const double* wsc = vec(kPW);
+    double dmax[1] = {0.0};
+    double dummy[1] = {0.0};
+    T* acc = reinterpret_cast<T*>(bwin) + size_t(tid) * ldl;  // this thread's column
+    for (int j0 = 0; j0 < n; j0 += NT) {
+      const int j = j0 + tid;
+      if (j < n) {
+        for (int d = 0; d <= bw; ++d) acc[d] = T(0);
+        for (int q = jp[j]; q < jp[j + 1]; ++q) {
+          const int r = jx[q];
+          const double w = wsc[n + r];
+          const T arj = T(at[q] * w);
+          const int q1 = ip[r + 1];
+          int q2 = ip[r];
+#pragma unroll 4
+          for (; q2 < q1; ++q2) {
+            const int i = ix[q2];
+            if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(av[q2] * w), acc[i - j]);
+          }
+        }
+        if (has_p) {
+          for (int q = pp[j]; q < pp[j + 1]; ++q) {
+            const int i = px[q];
+            if (i > j && i - j <= bw) acc[i - j] = T(pv[q]) + acc[i - j];
+          }
+        }
+        acc[0] = T(reg[j]) + acc[0];
+        dmax[0] = nanmax(dmax[0], double(acc[0]));
+        T* col = L + size_t(j) * ldl;
+        for (int d = 0; d <= bw; ++d) col[d] = acc[d];
+      }
+    }
+    reduce<0, 1>(dummy, dmax);
+    const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
+    for (int j = tid; j < n; j += NT) L[size_t(j) * ldl] = T(double(L[size_t(j) * ldl]) + jit);
+    sync();
+    QTQP_TOC(kPhGram);
+    QTQP_RETIC();
+    const int info = band_chol_window<T>();
+    QTQP_TOC(kPhChol);
+    return info;
+  }
+
+  // Band Cholesky with the active part of the band in shared memory.  Rows
+  // and columns k .. k+bw+1 live in a (bw+2) x (bw+2) window with circular
+  // indices (slot = index mod (bw+2)); step k reads the still-unscaled
+  // column k, writes the finished column k of L to global memory, updates
+  // the window, and stores row k+bw+1 of the Gram matrix (prefetched into
+  // registers during the previous step) into the slots that row k-1 and
+  // column k-1 have freed.  One barrier per column.
+  template <typename T>
+  __device__ int band_chol_window() {
+    QTQP_BAND_LOCALS;
+    T* L = reinterpret_cast<T*>(Lb);
+    T* W = reinterpret_cast<T*>(bwin);
+    const int B = bw + 2;
+    // Offsets (oi, oj), 1 <= oj <= oi <= bw, of the trailing update relative
+    // to k, the same every step; thread t handles pairs t, t + NT, ...
+    uint32_t* pairs = reinterpret_cast<uint32_t*>(bwin + (size_t(B) * B * sizeof(T) + 7) / 8);
+    const int npairs = bw * (bw + 1) / 2;
+    for (int oi = 1 + tid; oi <= bw; oi += NT)
+      for (int oj = 1; oj <= oi; ++oj) pairs[(oi - 1) * oi / 2 + oj - 1] = uint32_t(oi) | (uint32_t(oj) << 16);
+    // Rows 0 .. min(bw, n-1): entries (i, j), j <= i.
+    for (int e = tid; e < B * B; e += NT) {
+      const int i = e / B, j = e - i * B;
+      W[e] = (j <= i && i <= bw && i < n) ? L[size_t(j) * ldl + (i - j)] : T(0);
+    }
+    // Prefetch of the row that enters at step k: r = k + bw + 1, entries
+    // (r, j) for j in [r - bw, r]; thread t takes j = r - bw + t.
+    auto fetch = [&](int k) {
+      const int r = k + bw + 1, j = r - bw + tid;
+      return (r < n && tid <= bw) ? L[size_t(j) * ldl + (r - j)] : T(0);
+    };
+    T pre = fetch(0);
+    sync();
+    int info = 0;
+    for (int k = 0; k < n; ++k) {
+      const int ks = k % B;
+      const T d = W[ks * B + ks];
+      if (!(d > T(0))) {
+        info = k + 1;
+        break;
+      }
+      const T inv_d = T(1) / d, il = rsqrt(d);
+      const int last = min(n - 1, k + bw);
+      auto slot = [&](int i) {  // i % B for i in [k, k + B)
+        const int t = ks + (i - k);
+        return t >= B ? t - B : t;
+      };
+      // Finished column k of L (global); the window keeps it unscaled.
+      for (int i = k + 1 + tid; i <= last; i += NT) L[size_t(k) * ldl + (i - k)] = W[slot(i) * B + ks] * il;
+      if (tid == 0) L[size_t(k) * ldl] = il;
+      // Trailing update: W_ij -= W_ik W_jk / d for k < j <= i <= last.
+      const int span = last - k;
+#pragma unroll 4
+      for (int pi = tid; pi < npairs; pi += NT) {
+        const uint32_t pr = pairs[pi];
+        const int oi = int(pr & 0xffffu), oj = int(pr >> 16);
+        if (oi <= span) {
+          const int is = slot(k + oi), js = slot(k + oj);
+          W[is * B + js] = fma(-W[is * B + ks] * inv_d, W[js * B + ks], W[is * B + js]);
+        }
+      }
+      // Row r = k + bw + 1 enters: row slot (k-1) mod B, column slots of
+      // j in [k+1, r] (never ks; the diagonal lands in column k-1's slot).
+      {
+        const int r = k + bw + 1;
+        if (r < n && tid <= bw) {
+          const int rs = ks == 0 ? B - 1 : ks - 1;  // (k - 1) mod B
+          const int j = r - bw + tid;               // in [k + 1, r]
+          W[rs * B + (j - k == B - 1 ? rs : slot(j))] = pre;
+        }
+        pre = fetch(k + 1);
+      }
+      sync();
+    }
+    sync();
+    return info;
+  }
+
+  // Global-memory variant (wide bands): Gram in column band storage, then
+  // Cholesky with one barrier per column (the unscaled column k updates the
+  // trailing band and column k-1 is finished in the same phase).
+  template <typename T>
+  __device__ int band_factorize_global() {
     QTQP_BAND_LOCALS;
     QTQP_TIC();
     T* L = reinterpret_cast<T*>(Lb);
@@ -2010,8 +2162,107 @@ struct Ipm {
   // Solves L L^T v = v (column band storage, reciprocal diagonal) with one
   // warp: forward z_k = v_k / l_kk, v_i -= l_ik z_k (i in (k, k+bw]) into w;
   // backward x_k = w_k / l_kk, w_i -= l_ki x_k (i in [k-bw, k)) into v.
+  // With the window, the bw+1 active entries of the vector live in shared
+  // memory (128 circular slots) and the factor entries of the next step are
+  // loaded into registers while the current step runs.
   template <typename T>
   __device__ void band_chol_solve(T* v, T* w) {
+    if (bwin == nullptr) {
+      band_chol_solve_global<T>(v, w);
+      return;
+    }
+    QTQP_BAND_LOCALS;
+    const T* L = reinterpret_cast<const T*>(Lb);
+    T* win = reinterpret_cast<T*>(bwin);        // 128 circular vector slots
+    T* ring = win + 128;                        // kBandRing x 128 factor entries
+    T* vring = ring + kBandRing * 128;          // kBandRing entering vector values
+    constexpr int D = kBandRing;
+    if (tid < 32) {
+      const int lane = tid;
+      // Forward.  Group c (one per step, issued D-1 steps ahead) copies column
+      // c of L (offsets 0..bw; 0 = 1 / l_cc) and v[c + bw + 1] into the rings.
+      auto issue_fwd = [&](int c) {
+        T* rc = ring + (c % D) * 128;
+        const int rows = min(bw, n - 1 - c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int d = lane + 32 * q;
+          const bool ok = c < n && d <= rows;
+          cp_async_elem(rc + d, L + (ok ? size_t(c) * ldl + d : 0), ok);
+        }
+        if (lane == 0) {
+          const bool ok = c + bw + 1 < n;
+          cp_async_elem(vring + c % D, v + (ok ? c + bw + 1 : 0), ok);
+        }
+        cp_async_commit();
+      };
+      for (int i = lane; i <= min(bw, n - 1); i += 32) win[i & 127] = v[i];
+      for (int c = 0; c < D - 1; ++c) issue_fwd(c);
+      for (int k = 0; k < n; ++k) {
+        issue_fwd(k + D - 1);
+        cp_async_wait<D - 1>();
+        __syncwarp();
+        const T* ck = ring + (k % D) * 128;
+        const T zk = win[k & 127] * ck[0];
+        const int rows = min(bw, n - 1 - k);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int d = lane + 1 + 32 * q;
+          if (d <= rows) win[(k + d) & 127] = fma(-ck[d], zk, win[(k + d) & 127]);
+        }
+        if (lane == 0) {
+          w[k] = zk;
+          if (k + bw + 1 < n) win[(k + bw + 1) & 127] = vring[k % D];
+        }
+        __syncwarp();
+      }
+      cp_async_wait<0>();
+      __threadfence_block();  // z (written to w above) before the copies read it
+      __syncwarp();
+      // Backward.  Group c copies row c of L (l_c,c-d at column c-d, offset
+      // d; offset 0 = 1 / l_cc) and w[c - bw - 1].
+      auto issue_bwd = [&](int c) {
+        T* rc = ring + ((c % D + D) % D) * 128;
+        const int rows = min(bw, c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int d = lane + 32 * q;
+          const bool ok = c >= 0 && d <= rows;
+          cp_async_elem(rc + d, L + (ok ? size_t(c - d) * ldl + d : 0), ok);
+        }
+        if (lane == 0) {
+          const bool ok = c - bw - 1 >= 0;
+          cp_async_elem(vring + (c % D + D) % D, w + (ok ? c - bw - 1 : 0), ok);
+        }
+        cp_async_commit();
+      };
+      for (int i = lane; i <= min(bw, n - 1); i += 32) win[(n - 1 - i) & 127] = w[n - 1 - i];
+      for (int c = n - 1; c > n - D; --c) issue_bwd(c);
+      for (int k = n - 1; k >= 0; --k) {
+        issue_bwd(k - D + 1);
+        cp_async_wait<D - 1>();
+        __syncwarp();
+        const T* rk = ring + ((k % D + D) % D) * 128;
+        const T xk = win[k & 127] * rk[0];
+        const int rows = min(bw, k);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int d = lane + 1 + 32 * q;
+          if (d <= rows) win[(k - d) & 127] = fma(-rk[d], xk, win[(k - d) & 127]);
+        }
+        if (lane == 0) {
+          v[k] = xk;
+          if (k - bw - 1 >= 0) win[(k - bw - 1) & 127] = vring[(k % D + D) % D];
+        }
+        __syncwarp();
+      }
+      cp_async_wait<0>();
+    }
+    sync();
+  }
+
+  template <typename T>
+  __device__ void band_chol_solve_global(T* v, T* w) {
     QTQP_BAND_LOCALS;
     const T* L = reinterpret_cast<const T*>(Lb);
     if (tid < 32) {
