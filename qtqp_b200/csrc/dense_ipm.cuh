@@ -1467,7 +1467,9 @@ struct Ipm {
     }
     int w32 = 0, w64 = 0, wsolves = 0;  // work of a rejected warm start counts too
     if (warm_act != nullptr) {
-      bool fp64w = op.precision == QTQP_PREC_FP64;
+      // FP64 factor: the reduced system is as ill-conditioned as the last
+      // interior-point iterations, where an FP32 factor is refused anyway.
+      bool fp64w = true;
       const bool ok = warm_try(warm_x, warm_y, warm_act, nb, nc, fp64w, w32, w64, wsolves);
       sync();
       if (ok) {
