@@ -12,10 +12,11 @@ namespace qtqp {
 
 static int launch_nt(int nt, const BatchParams& p, int smem_total, cudaStream_t st) {
   switch (nt) {
+    case 32: return launch_group_32(p, smem_total, st);
     case 64: return launch_group_64(p, smem_total, st);
     case 128: return launch_group_128(p, smem_total, st);
     case 256: return launch_group_256(p, smem_total, st);
-    default: return fail(QTQP_ERR_BAD_ARG, "block_threads must be 64, 128 or 256");
+    default: return fail(QTQP_ERR_BAD_ARG, "block_threads must be 32, 64, 128 or 256");
   }
 }
 
@@ -66,9 +67,9 @@ extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
   if (h_inst == nullptr || h_order == nullptr || opt == nullptr || plan == nullptr ||
       count < 0)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_plan: null argument or negative count");
-  if (block_threads != 0 && block_threads != 64 && block_threads != 128 &&
-      block_threads != 256)
-    return fail(QTQP_ERR_BAD_ARG, "block_threads must be 0, 64, 128 or 256");
+  if (block_threads != 0 && block_threads != 32 && block_threads != 64 &&
+      block_threads != 128 && block_threads != 256)
+    return fail(QTQP_ERR_BAD_ARG, "block_threads must be 0, 32, 64, 128 or 256");
   for (int i = 0; i < count; ++i) {
     const qtqp_dense_instance& d = h_inst[i];
     if (d.n < 1 || d.m < 1 || d.z < 0 || d.z >= d.m)
@@ -139,8 +140,15 @@ extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
       if (size_t(smem_bytes) < red || size_t(smem_bytes) > kSmemBlockMax)
         return fail(QTQP_ERR_BAD_ARG, "smem_bytes outside [reduction scratch, 227 KiB]");
       cap = size_t(smem_bytes) - red;
-    } else if (max_all + red <= kSmemBlockMax) {
+    } else if (max_all + red <= kSmemBlockMax &&
+               (r.cls > 1 || 2 * (max_gv + red + kSmemReserved) > kSmemPerSm)) {
       cap = max_all;  // everything on chip
+    } else if (max_all + red <= kSmemBlockMax) {
+      // One block per SM if A and P stay on chip: keeping only G and the
+      // vectors there (A and P through L2) fits two or more QPs per SM,
+      // which is faster for these latency-bound solves (measured: n 49..64,
+      // m = 2n: 16.8 -> 14.7 ms per 1172 QPs).
+      cap = max_gv;
     } else if (max_gv + red <= kSmemBlockMax) {
       cap = max_gv;   // G + vectors on chip, A and P through L2
     } else {

@@ -39,6 +39,7 @@ __host__ __device__ constexpr size_t red_bytes() {
 
 inline size_t red_bytes_rt(int nt) {
   switch (nt) {
+    case 32: return red_bytes<32>();
     case 64: return red_bytes<64>();
     case 128: return red_bytes<128>();
     default: return red_bytes<256>();
@@ -101,6 +102,7 @@ inline int launch_group(const BatchParams& p, int smem_total, cudaStream_t strea
 }
 
 
+int launch_group_32(const BatchParams& p, int smem_total, cudaStream_t stream);
 int launch_group_64(const BatchParams& p, int smem_total, cudaStream_t stream);
 int launch_group_128(const BatchParams& p, int smem_total, cudaStream_t stream);
 int launch_group_256(const BatchParams& p, int smem_total, cudaStream_t stream);

@@ -740,9 +740,11 @@ struct Ipm {
   }
 
   // In-place inverse of each 32x32 lower-triangular diagonal block of L, one
-  // warp per block, column by column from the last: for i > j,
-  // X_ij = -(sum_{j<k<=i} X_ik L_kj) / L_jj, X_jj = 1 / L_jj.  Both Cholesky
-  // variants already store 1 / L_jj on the diagonal.
+  // warp per block, lane c computing column c in registers (top-down):
+  // X_cc = 1 / L_cc, X_rc = -(sum_{c<=k<r} L_rk X_kc) / L_rr for r > c, with
+  // L read from shared memory (the same entry in every lane: a broadcast).
+  // Both Cholesky variants already store 1 / L_jj on the diagonal, which is
+  // also the inverse's diagonal.
   template <typename T>
   QTQP_PHASE void invert_diag_blocks(T* g) {
     QTQP_LOCALS;
@@ -752,22 +754,31 @@ struct Ipm {
     for (int blk = warp; blk < nblk; blk += NW) {
       const int kb = blk * 32, bs = min(32, n - kb);
       T* L = g + kb * ldg + kb;
-      for (int j = bs - 1; j >= 0; --j) {
-        const T inv_jj = L[j * ldg + j];  // the factor's diagonal holds 1 / L_jj
-        T w0 = T(0), w1 = T(0);
-        if (lane > j && lane < bs) {
-          const T* row = L + lane * ldg;
-          int k = j + 1;
-          for (; k + 1 <= lane; k += 2) {
-            w0 = fma(row[k], L[k * ldg + j], w0);
-            w1 = fma(row[k + 1], L[(k + 1) * ldg + j], w1);
+      const int c = lane;
+      T x[32];
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        T a0 = T(0), a1 = T(0);
+#pragma unroll
+        for (int k = 0; k < r; ++k) {
+          if (k >= c && r < bs) {  // rows past the block are never read
+            if (k & 1) {
+              a1 = fma(L[r * ldg + k], x[k], a1);
+            } else {
+              a0 = fma(L[r * ldg + k], x[k], a0);
+            }
           }
-          if (k <= lane) w0 = fma(row[k], L[k * ldg + j], w0);
         }
-        __syncwarp();
-        if (lane > j && lane < bs) L[lane * ldg + j] = -(w0 + w1) * inv_jj;
-        __syncwarp();
+        const T idg = r < bs ? L[r * ldg + r] : T(0);
+        x[r] = r < c ? T(0) : (r == c ? idg : -(a0 + a1) * idg);
       }
+      __syncwarp();
+      if (c < bs) {
+#pragma unroll
+        for (int r = 0; r < 32; ++r)
+          if (r > c && r < bs) L[r * ldg + c] = x[r];
+      }
+      __syncwarp();
     }
     sync();
   }
