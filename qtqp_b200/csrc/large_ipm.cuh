@@ -354,47 +354,69 @@ __device__ __forceinline__ void stage_block(T* dst, const T* g, size_t ld, int r
   }
 }
 
-// One warp factors the 32 x 32 lower block at sm[o][o] (pitch kPitch) in
-// registers (lane r holds row r), writes L back and its inverse to
-// inv32[r * kSubPitch + c].  Returns 0 or the 1-based failing pivot (the
-// same in every lane).
+// One warp factors the 32 x 32 lower block at sm[o][o] (pitch kPitch) and
+// writes its inverse to inv32[r * kSubPitch + c].  Returns 0 or the 1-based
+// failing pivot (the same in every lane).
+//
+// Factor: Crout order, lane r holds row r in registers; step c forms
+// s_r = a_rc - sum_{k<c} l_rk l_ck (row c of L read back from shared memory,
+// the same address in every lane), l_cc = sqrt(s_c), l_rc = s_r / l_cc.
+// Inverse: lane c forms column c top-down, X_rc = -(sum_{c<=k<r} L_rk X_kc)
+// / l_rr.  Every division and square root goes through one reciprocal
+// square root per pivot (1 / l_cc = rsqrt(s_c)), kept for the inverse:
+// these are the long-latency operations of this sequential chain.
 template <typename T>
 __device__ __noinline__ int warp_chol32(T* sm, int o, T* inv32, int lane) {
-  T a[32];
+  T* Lr = sm + (o + lane) * kPitch + o;  // this lane's row
+  T idg[32];                              // 1 / l_cc (the same in every lane)
+  int bad = 0;
+  {
+    T a[32];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) a[j] = (j <= lane) ? sm[(o + lane) * kPitch + o + j] : T(0);
-  int bad = 0;  // no early exit: the loops stay fully unrolled, a[] in registers
+    for (int j = 0; j < 32; ++j) a[j] = (j <= lane) ? Lr[j] : T(0);
 #pragma unroll
-  for (int c = 0; c < 32; ++c) {
-    const T piv = __shfl_sync(0xffffffffu, a[c], c);
-    if (!(piv > T(0)) && bad == 0) bad = c + 1;
-    const T lcc = sqrt(piv);
-    const T l = lane == c ? lcc : (lane > c ? a[c] / lcc : T(0));
-    a[c] = l;
+    for (int c = 0; c < 32; ++c) {
+      const T* Lc = sm + (o + c) * kPitch + o;
+      T s0 = a[c], s1 = T(0);
 #pragma unroll
-    for (int j = c + 1; j < 32; ++j) {
-      const T lj = __shfl_sync(0xffffffffu, l, j);
-      if (lane >= j) a[j] = fma(-l, lj, a[j]);
+      for (int k = 0; k < c; ++k) {
+        if (k & 1) {
+          s1 = fma(-a[k], Lc[k], s1);
+        } else {
+          s0 = fma(-a[k], Lc[k], s0);
+        }
+      }
+      const T sr = s0 + s1;
+      const T piv = __shfl_sync(0xffffffffu, sr, c);
+      if (!(piv > T(0)) && bad == 0) bad = c + 1;
+      const T il = rsqrt(piv);
+      idg[c] = il;
+      if (lane == c) {
+        a[c] = piv * il;
+      } else if (lane > c) {
+        a[c] = sr * il;
+      }
+      if (lane >= c) Lr[c] = a[c];
+      __syncwarp();
     }
   }
   if (bad) return bad;
-#pragma unroll
-  for (int j = 0; j < 32; ++j)
-    if (j <= lane) sm[(o + lane) * kPitch + o + j] = a[j];
-  __syncwarp();
-  // Inverse, one column per lane (c = lane): x_c = 1 / L_cc,
-  // x_r = -(sum_{c <= k < r} L_rk x_k) / L_rr; L read back from shared
-  // memory (the same address in every lane: broadcasts).
   T x[32];
   const T* L = sm + o * kPitch + o;
 #pragma unroll
   for (int r = 0; r < 32; ++r) {
-    T acc = T(0);
+    T a0 = T(0), a1 = T(0);
 #pragma unroll
-    for (int k = 0; k < r; ++k)
-      if (k >= lane) acc = fma(L[r * kPitch + k], x[k], acc);
-    const T lrr = L[r * kPitch + r];
-    x[r] = r < lane ? T(0) : (r == lane ? T(1) / lrr : -acc / lrr);
+    for (int k = 0; k < r; ++k) {
+      if (k >= lane) {
+        if (k & 1) {
+          a1 = fma(L[r * kPitch + k], x[k], a1);
+        } else {
+          a0 = fma(L[r * kPitch + k], x[k], a0);
+        }
+      }
+    }
+    x[r] = r < lane ? T(0) : (r == lane ? idg[r] : -(a0 + a1) * idg[r]);
   }
 #pragma unroll
   for (int r = 0; r < 32; ++r) inv32[r * kSubPitch + lane] = x[r];
@@ -608,13 +630,16 @@ __device__ int large_cholesky(S& s, T* g) {
     __syncthreads();
     T* inv = lv + size_t(b) * kLB * kLB;                 // inv(L_bb), row-major
     T* invt = lv + size_t(nblk + b) * kLB * kLB;         // its transpose
+    T* rdiag = sm + kLB * kPitch;  // 1 / L_rr
+    if (threadIdx.x < kLB) rdiag[threadIdx.x] = T(1) / sm[threadIdx.x * kPitch + threadIdx.x];
+    __syncthreads();
     if (threadIdx.x < kLB) {
       const int c = threadIdx.x;
       // Column c of inv(L_bb) = row c of its transpose (contiguous for this
       // thread): x_c = 1 / L_cc; x_r = -(sum_{c <= l < r} L_rl x_l) / L_rr.
       T* xc = invt + size_t(c) * kLB;
       for (int r = 0; r < c; ++r) xc[r] = T(0);
-      xc[c] = T(1) / sm[c * kPitch + c];
+      xc[c] = rdiag[c];
       for (int r = c + 1; r < kLB; ++r) {
         T acc0 = T(0), acc1 = T(0);
         int l = c;
@@ -623,7 +648,7 @@ __device__ int large_cholesky(S& s, T* g) {
           acc1 = fma(sm[r * kPitch + l + 1], xc[l + 1], acc1);
         }
         if (l < r) acc0 = fma(sm[r * kPitch + l], xc[l], acc0);
-        xc[r] = -(acc0 + acc1) / sm[r * kPitch + r];
+        xc[r] = -(acc0 + acc1) * rdiag[r];
       }
     }
     __syncthreads();
