@@ -712,11 +712,10 @@ struct Ipm {
     QTQP_LOCALS;
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    T d_prev = T(1);
+    T il_prev = T(1);  // 1 / sqrt(d) of the previous pivot
     for (int k = 0; k <= n; ++k) {
       if (k > 0) {  // finish column k-1
-        const T lkk = sqrt(d_prev);
-        const T inv = T(1) / lkk;
+        const T inv = il_prev;
         for (int i = k + tid; i < n; i += NT) g[i * ldg + k - 1] *= inv;
         if (tid == NT - 1) g[(k - 1) * ldg + k - 1] = inv;  // diagonal keeps 1/l_kk
       }
@@ -726,12 +725,15 @@ struct Ipm {
         sync();
         return k + 1;
       }
-      const T inv_d = T(1) / d;
+      // One reciprocal square root per pivot, no divisions on this chain:
+      // 1 / l_kk = rsqrt(d), 1 / d = (1 / l_kk)^2.
+      const T il = rsqrt(d);
+      const T inv_d = il * il;
       for (int j = k + 1 + warp; j < n; j += NW) {
         const T t = g[j * ldg + k] * inv_d;
         for (int i = j + lane; i < n; i += 32) g[i * ldg + j] = fma(-g[i * ldg + k], t, g[i * ldg + j]);
       }
-      d_prev = d;
+      il_prev = il;
       sync();
     }
     sync();
@@ -2062,7 +2064,7 @@ struct Ipm {
         info = k + 1;
         break;
       }
-      const T inv_d = T(1) / d, il = rsqrt(d);
+      const T il = rsqrt(d), inv_d = il * il;  // no division on this chain
       const int last = min(n - 1, k + bw);
       auto slot = [&](int i) {  // i % B for i in [k, k + B)
         const int t = ks + (i - k);
@@ -2140,12 +2142,12 @@ struct Ipm {
     QTQP_RETIC();
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    T d_prev = T(1);
+    T il_prev = T(1);
     int info = 0;
     for (int k = 0; k <= n; ++k) {
       if (k > 0) {  // finish column k-1
         T* ck = L + size_t(k - 1) * ldl;
-        const T il = rsqrt(d_prev);
+        const T il = il_prev;
         const int rows = min(bw, n - k);
         for (int d = 1 + tid; d <= rows; d += NT) ck[d] *= il;
         if (tid == NT - 1) ck[0] = il;
@@ -2157,14 +2159,14 @@ struct Ipm {
         info = k + 1;
         break;
       }
-      const T inv_d = T(1) / d;
+      const T il = rsqrt(d), inv_d = il * il;
       const int last = min(n - 1, k + bw);
       for (int j = k + 1 + warp; j <= last; j += NW) {
         const T t = ck[j - k] * inv_d;
         T* cj = L + size_t(j) * ldl;
         for (int i = j + lane; i <= last; i += 32) cj[i - j] = fma(-ck[i - k], t, cj[i - j]);
       }
-      d_prev = d;
+      il_prev = il;
       sync();
     }
     sync();
