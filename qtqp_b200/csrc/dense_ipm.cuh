@@ -1989,16 +1989,50 @@ struct Ipm {
       const int j = j0 + tid;
       if (j < n) {
         for (int d = 0; d <= bw; ++d) acc[d] = T(0);
-        for (int q = jp[j]; q < jp[j + 1]; ++q) {
-          const int r = jx[q];
-          const double w = wsc[n + r];
-          const T arj = T(at[q] * w);
-          const int q1 = ip[r + 1];
-          int q2 = ip[r];
-#pragma unroll 4
-          for (; q2 < q1; ++q2) {
-            const int i = ix[q2];
-            if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(av[q2] * w), acc[i - j]);
+        // The loads of every level are issued in batches of 8 before they are
+        // used (column j's rows and their scalings, then each row's entries),
+        // so that this latency-bound gather keeps several loads in flight.
+        const int qa = jp[j], qb = jp[j + 1];
+        for (int q0 = qa; q0 < qb; q0 += 8) {
+          int rr[8], r0[8], r1[8];
+          double ww[8], aq[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const bool ok = q0 + u < qb;
+            rr[u] = ok ? jx[q0 + u] : 0;
+            aq[u] = ok ? at[q0 + u] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const bool ok = q0 + u < qb;
+            ww[u] = ok ? wsc[n + rr[u]] : 0.0;
+            r0[u] = ok ? ip[rr[u]] : 0;
+            r1[u] = ok ? ip[rr[u] + 1] : 0;
+          }
+#pragma unroll 1
+          for (int u = 0; u < 8 && q0 + u < qb; ++u) {
+            const double w = ww[u];
+            const T arj = T(aq[u] * w);
+            const int q1 = r1[u];
+            int q2 = r0[u];
+            for (; q2 + 8 <= q1; q2 += 8) {
+              int ii[8];
+              double aa[8];
+#pragma unroll
+              for (int e = 0; e < 8; ++e) {
+                ii[e] = ix[q2 + e];
+                aa[e] = av[q2 + e];
+              }
+#pragma unroll
+              for (int e = 0; e < 8; ++e) {
+                const int i = ii[e];
+                if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(aa[e] * w), acc[i - j]);
+              }
+            }
+            for (; q2 < q1; ++q2) {
+              const int i = ix[q2];
+              if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(av[q2] * w), acc[i - j]);
+            }
           }
         }
         if (has_p) {
