@@ -1948,24 +1948,44 @@ struct Ipm {
     sync();
   }
 
+  // sum_{q0 <= q < q1} val[q] v[voff + idx[q]]: indices and values are
+  // loaded 8 at a time, then the 8 gathers, so that several loads are in
+  // flight per thread (these sparse dots are latency-bound).
+  __device__ __forceinline__ static double sparse_dot(const int* idx, const double* val,
+                                                      const double* v, int voff, int q0,
+                                                      int q1) {
+    double t0 = 0.0, t1 = 0.0;
+    int q = q0;
+    for (; q + 8 <= q1; q += 8) {
+      int ii[8];
+      double aa[8], xx[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        ii[e] = idx[q + e];
+        aa[e] = val[q + e];
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) xx[e] = v[voff + ii[e]];
+#pragma unroll
+      for (int e = 0; e < 8; e += 2) {
+        t0 = fma(aa[e], xx[e], t0);
+        t1 = fma(aa[e + 1], xx[e + 1], t1);
+      }
+    }
+    for (; q < q1; ++q) t0 = fma(val[q], v[voff + idx[q]], t0);
+    return t0 + t1;
+  }
   // (P_off v)_k for the owner of row k (P symmetric, so row k = column k).
   __device__ __forceinline__ double band_poff_row(const double* v, int k) const {
-    double t = 0.0;
-    if (has_p)
-      for (int q = pp[k]; q < pp[k + 1]; ++q) t = fma(pv[q], v[px[q]], t);
-    return t;
+    return has_p ? sparse_dot(px, pv, v, 0, pp[k], pp[k + 1]) : 0.0;
   }
   // (A^T y)_k with y at v[n + i].
   __device__ __forceinline__ double band_at_col(const double* v, int k) const {
-    double t = 0.0;
-    for (int q = jp[k]; q < jp[k + 1]; ++q) t = fma(at[q], v[n + jx[q]], t);
-    return t;
+    return sparse_dot(jx, at, v, n, jp[k], jp[k + 1]);
   }
   // (A x)_i.
   __device__ __forceinline__ double band_a_row(const double* v, int i) const {
-    double t = 0.0;
-    for (int q = ip[i]; q < ip[i + 1]; ++q) t = fma(av[q], v[ix[q]], t);
-    return t;
+    return sparse_dot(ix, av, v, 0, ip[i], ip[i + 1]);
   }
 
   // Gram matrix in column band storage, then Cholesky.  With the shared-
