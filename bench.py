@@ -53,11 +53,14 @@ def _args():
   ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
                   help="form whose throughput is the headline value (both are measured)")
   ap.add_argument("--workload", default="batch_small",
-                  choices=["batch_small", "dense_large", "parametric"],
+                  choices=["batch_small", "dense_large", "mpc", "parametric"],
                   help="batch_small: 4096 uneven small dense QPs (default); dense_large: "
                        "one n=4096, m=8192 dense QP on the whole GPU; parametric: a T=50 "
                        "MPC family with the learned warm start")
   ap.add_argument("--train", type=int, default=4096, help="parametric: training instances")
+  ap.add_argument("--mpc-horizon", type=int, default=500,
+                  help="mpc: horizon T (n = 60 T); 500 is the workload, smaller horizons are "
+                       "for profiling captures")
   ap.add_argument("--large-n", type=int, default=4096,
                   help="dense_large: n (m = 2n, z = n/4); 4096 is the workload, smaller "
                        "sizes are for profiling captures")
@@ -518,6 +521,110 @@ def run_dense_large(args):
     dist.destroy_process_group()
 
 
+MPC_WORKLOAD = ("one MPC-structured QP: horizon T, nx=40, nu=20 (n=60T, z=40T, m=z+2n), "
+                "box bounds 5 / 1, 10% of the boxes active")
+
+
+def run_mpc(args):
+  """One banded MPC QP per step (replicas only for N > 1)."""
+  rank = int(os.environ.get("RANK", "0"))
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  from qtqp_b200 import problems
+  T = args.mpc_horizon
+  a, b, c, z, p = problems.mpc_feasible(T)
+  workload = MPC_WORKLOAD.replace("horizon T", f"horizon T={T}")
+  if args.impl == "reference" or (rank == 0 and world == 1 and not args.no_cpu_baseline):
+    from oracle import qtqp_oracle as orc
+    t0 = time.perf_counter()
+    r = orc.solve(a, b, c, z, p, backend="superlu")
+    t_cpu = time.perf_counter() - t0
+    cpu = {"value": 1.0 / t_cpu, "unit": "QPs/s", "cores": 1, "kind": "port",
+           "sample": "one whole solve, oracle restatement (SuperLU KKT)"}
+    if args.impl == "reference":
+      if rank == 0:
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": 1.0 / t_cpu, "unit": "QPs/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * t_cpu,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": workload, "status": r.status},
+            "cpu_baseline": cpu, "e2e": {"value": 1.0 / t_cpu, "unit": "QPs/s",
+                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+      return
+  else:
+    cpu = None
+  import numpy as np
+  import torch
+  import qtqp_b200 as qb
+  from qtqp_b200 import band, batch
+  torch.cuda.set_device(local)
+  dev = torch.device("cuda", local)
+  stream = torch.cuda.current_stream(dev)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  forms = {}
+  for precision in ("fp64", "mixed"):
+    hb = band.HostBandBatch([q.band_problem()], batch.SolveOptions(precision=precision))
+    db = band.DeviceBandBatch(hb, device=dev)
+    db.upload(stream)
+    for _ in range(args.warmup):
+      db.launch(stream)
+    torch.cuda.synchronize(dev)
+    clocks = _Clocks(local) if precision == args.precision else None
+    t = sum(_ev_time(stream, lambda: db.launch(stream)) for _ in range(args.steps))
+    ck = clocks.stop() if clocks else None
+    forms[precision] = dict(hb=hb, db=db, time=t, res=db.fetch()[0][0], clocks=ck)
+  chosen = forms[args.precision]
+  hb, db, res = chosen["hb"], chosen["db"], chosen["res"]
+  value = int(res["status"] == 0) * args.steps / chosen["time"]
+  fp64 = forms["fp64"]
+  mixed = forms["mixed"]
+  h_out = [torch.empty_like(t_, device="cpu").pin_memory() for t_ in (db.x, db.y, db.s)]
+
+  def e2e_step():
+    db.upload(stream)
+    db.launch(stream)
+    with torch.cuda.stream(stream):
+      for dst, src in zip(h_out, (db.x, db.y, db.s)):
+        dst.copy_(src, non_blocking=True)
+  e2e_step()
+  e_total = sum(_ev_time(stream, e2e_step) for _ in range(args.steps))
+  t_launch = chosen["time"] / args.steps
+  nnz = int(hb.inst["nnz_a"][0])
+  n_, m_ = int(hb.inst["n"][0]), int(hb.inst["m"][0])
+  iters = int(res["iterations"])
+  # Algorithmic bytes per IPM iteration: the survey's SpMV bytes of A x (CSR:
+  # 12 nnz + 4 (rows + 1) + 8 (cols + rows)), twice (A x and A^T y), plus the
+  # band factor written and read (8 n (bw + 1) each).
+  bw = int(hb.inst["bw"][0])
+  per_iter = 2 * (12 * nnz + 4 * (m_ + 1) + 8 * (n_ + m_)) + 2 * 8 * n_ * (bw + 1)
+  achieved = per_iter * iters / t_launch / 1e9
+  peak, peak_kind = _peaks()
+  if rank == 0:
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_launch, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator of the workload's distribution)",
+        "config": {"workload": workload, "precision": args.precision, "bandwidth": bw,
+                   "parallelism": "replicas" if world > 1 else "one QP per GPU"},
+        "fp64_value": int(fp64["res"]["status"] == 0) * args.steps / fp64["time"],
+        "mixed_value": int(mixed["res"]["status"] == 0) * args.steps / mixed["time"],
+        "statuses_identical": bool(fp64["res"]["status"] == mixed["res"]["status"]),
+        "iterations": iters,
+        "factorizations": {"fp32": int(res["fp32_factorizations"]),
+                           "fp64": int(res["fp64_factorizations"])},
+        "e2e": {"value": int(res["status"] == 0) * args.steps / e_total, "unit": "QPs/s",
+                "h2d_bytes_per_step": hb.input_bytes,
+                "d2h_bytes_per_step": sum(int(t_.numel() * t_.element_size()) for t_ in h_out)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "kernel": "band_batch_kernel",
+                     "algorithmic_bytes_per_launch": per_iter * iters},
+        "cpu_baseline": cpu, "clocks": chosen["clocks"], "gpu_launches": args.steps}),
+          flush=True)
+
+
 def run_parametric(args):
   """Plain FP64 batch vs mixed precision + learned warm start on held-out
   instances of the parametric family (training is outside the timed region)."""
@@ -623,6 +730,8 @@ def main():
     run_dense_large(args)
   elif args.workload == "parametric":
     run_parametric(args)
+  elif args.workload == "mpc":
+    run_mpc(args)
   elif args.impl == "reference":
     run_reference(args)
   else:
