@@ -230,6 +230,33 @@ int qtqp_band_batch_solve(const qtqp_band_instance* d_inst,
  * otherwise the plain method runs from its usual start.
  * qtqp_result.warm_started tells which. */
 
+/* ---- one large banded QP on the whole GPU -------------------------------- *
+ * The banded device IPM of qtqp_band_batch_solve (same algorithm, options
+ * and outputs; QTQP._solve_impl, src/qtqp/__init__.py:351-614, with the KKT
+ * layer of src/qtqp/direct.py:112-311) for a single large QP, run by one
+ * cooperative launch of 128 blocks: Gram matrix, residuals and sparse
+ * products over the whole grid, and a partitioned band Cholesky (`parts`
+ * interiors factorised in parallel, a block-tridiagonal Cholesky over the
+ * parts-1 separators of bw columns between them) with the matching
+ * partitioned triangular solves.  h_inst: host pointer to the instance's
+ * descriptor (offsets into the device pools as in the batch).  parts in
+ * [1, min(128, (n + bw) / (2 bw))]; qtqp_band_grid_default_parts gives the
+ * default.  bw <= 117 (the separator blocks are staged in shared memory);
+ * wider bands return QTQP_ERR_BAD_ARG.  The workspace (>=
+ * qtqp_band_grid_workspace_bytes, 256-byte aligned) is private.  A grid
+ * barrier that waits too long ends the solve with status FAILED and error
+ * QTQP_ERR_TIMEOUT. */
+int32_t qtqp_band_grid_default_parts(const qtqp_band_instance* h_inst);
+size_t qtqp_band_grid_workspace_bytes(const qtqp_band_instance* h_inst,
+                                      int32_t parts);
+int qtqp_band_grid_solve(const qtqp_band_instance* h_inst, int32_t parts,
+                         const int32_t* d_ipool, const double* d_vpool,
+                         const double* d_b_pool, const double* d_c_pool,
+                         double* d_x_pool, double* d_y_pool, double* d_s_pool,
+                         qtqp_result* d_result, qtqp_iter_stats* d_stats,
+                         void* d_workspace, size_t workspace_bytes,
+                         const qtqp_options* opt, void* stream);
+
 /* ---- learned warm start: MLP kernels (no reference counterpart) --------- *
  * theta -> 256 -> 256 -> (n + m) MLP, FP32, all matrices row-major.  Used to
  * train the network on plain-method solutions of a parametric family and to

@@ -34,6 +34,7 @@ __version__ = "0.0.5+b200"
 # own switches earlier.
 LARGE_N = 1024
 LARGE_N_SINGLE = 256
+BAND_GRID_N = 1024  # a banded QP solved on its own from this size: the whole GPU
 
 _HEADER = ("| iter |      pcost |      dcost |     pres |     dres |      gap |"
            "   infeas |       mu |  q, p, c |     time |")
@@ -191,14 +192,18 @@ class QTQP:
 
   def storage_format(self, single: bool = False) -> str:
     """'band' when the Gram matrix P + A^T D A is narrow-banded (its
-    half-bandwidth at most n/4) and n > 96; otherwise 'large' (the whole GPU
-    on one QP) when n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on
-    its own; else 'dense' (one thread block per QP)."""
+    half-bandwidth at most n/4) and n > 96 -- 'band_grid' (the whole GPU,
+    partitioned band factorisation) instead for a QP solved on its own with
+    n >= BAND_GRID_N; otherwise 'large' (the whole GPU on one dense QP) when
+    n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on its own; else
+    'dense' (one thread block per QP)."""
     if self.n <= 96:
       return "dense"
     from . import band as _band  # pylint: disable=g-import-not-at-top
     bw = _band.gram_bandwidth(self.a, self.p if self.p.nnz else None)
     if 4 * (bw + 1) <= self.n:
+      if single and self.n >= BAND_GRID_N and _band.grid_supported(bw, self.n):
+        return "band_grid"
       return "band"
     return "large" if self.n >= (LARGE_N_SINGLE if single else LARGE_N) else "dense"
 
@@ -303,8 +308,9 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   # Dense and banded problems go to their own device batches; each large
   # problem gets the whole GPU in turn.
   kinds = [q.storage_format() if storage == "auto" else storage for q in problems]
-  if any(k not in ("dense", "band", "large") for k in kinds):
-    raise ValueError(f"storage must be 'auto', 'dense', 'band' or 'large', got {storage!r}")
+  if any(k not in ("dense", "band", "large", "band_grid") for k in kinds):
+    raise ValueError("storage must be 'auto', 'dense', 'band', 'large' or 'band_grid', "
+                     f"got {storage!r}")
   per = {}  # kind -> (indices, results, x, y, s, stats, inst)
   where = {}
   t_launch = 0.0
@@ -319,6 +325,15 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     res, xp, yp, sp_, st = dl.fetch()
     inst = np.zeros(1, dtype=[("n_off", np.int64), ("m_off", np.int64)])
     where[i] = (res[0], xp, yp, sp_, None if st is None else st[0], inst[0])
+  for i in [i for i, k in enumerate(kinds) if k == "band_grid"]:
+    from . import band as _band  # pylint: disable=g-import-not-at-top
+    hb = _band.HostBandBatch([problems[i].band_problem()], opts)
+    dg = _band.DeviceBandGrid(hb, records=records)
+    dg.upload()
+    t_launch = timeit.default_timer() - start
+    dg.launch()
+    res, xp, yp, sp_, st = dg.fetch()
+    where[i] = (res[0], xp, yp, sp_, None if st is None else st[0], hb.inst[0])
   for kind in ("dense", "band"):
     idx = [i for i, k in enumerate(kinds) if k == kind]
     if not idx:
@@ -351,7 +366,7 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     if int(r["error"]) == _lib.QTQP_ERR_NAN:
       raise ValueError("Linear solver returned NaNs.")
     if int(r["error"]) == _lib.QTQP_ERR_TIMEOUT:
-      raise RuntimeError("qtqp_b200: a grid barrier of the large solve timed out")
+      raise RuntimeError("qtqp_b200: a grid barrier of a whole-GPU solve timed out")
     n0, m0 = int(d["n_off"]), int(d["m_off"])
     x = x_pool[n0:n0 + q.n].copy()
     y = y_pool[m0:m0 + q.m].copy()

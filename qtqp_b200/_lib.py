@@ -54,6 +54,9 @@ EXPORTS = (
     "qtqp_dense_large_solve",
     "qtqp_tc_split_tf32",
     "qtqp_tc_gram_f32",
+    "qtqp_band_grid_default_parts",
+    "qtqp_band_grid_workspace_bytes",
+    "qtqp_band_grid_solve",
 )
 
 
@@ -187,6 +190,12 @@ def load() -> ctypes.CDLL:
     lib.qtqp_dense_large_workspace_bytes.argtypes = [i32, i32]
     lib.qtqp_dense_large_solve.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp,
                                            vp, vp, sz, ctypes.POINTER(Options), vp]
+    lib.qtqp_band_grid_default_parts.restype = i32
+    lib.qtqp_band_grid_default_parts.argtypes = [vp]
+    lib.qtqp_band_grid_workspace_bytes.restype = sz
+    lib.qtqp_band_grid_workspace_bytes.argtypes = [vp, i32]
+    lib.qtqp_band_grid_solve.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz,
+                                         ctypes.POINTER(Options), vp]
     lib.qtqp_tc_split_tf32.argtypes = [vp, i64, vp, vp, vp]
     lib.qtqp_tc_gram_f32.argtypes = [i32, i32, vp, vp, i32, vp, i32, i32, vp, vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz

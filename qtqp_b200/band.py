@@ -218,3 +218,84 @@ class DeviceBandBatch:
       stats = self.stats.cpu().numpy().reshape(self.hb.count, self.hb.opts.max_iter,
                                                 _lib.STATS_DOUBLES)
     return (res, self.x.cpu().numpy(), self.y.cpu().numpy(), self.s.cpu().numpy(), stats)
+
+
+# Widest band of the whole-GPU path (two bw x (bw+1) FP64 separator blocks
+# staged in 225 KiB of shared memory).
+GRID_MAX_BW = 117
+
+
+def grid_supported(bw: int, n: int) -> bool:
+  """Whether one banded QP of half-bandwidth bw can use the whole-GPU
+  partitioned solve (the separator blocks must fit in shared memory)."""
+  return 1 <= bw <= GRID_MAX_BW and n >= 2 * bw + 2
+
+
+class DeviceBandGrid:
+  """One banded QP solved by the whole GPU (cooperative grid launch with the
+  partitioned band factorisation).  Takes a single-problem HostBandBatch for
+  the packed pools and descriptor; same outputs as DeviceBandBatch."""
+
+  def __init__(self, hb: HostBandBatch, device=None, records: bool | None = None,
+               parts: int | None = None):
+    if hb.count != 1:
+      raise ValueError("DeviceBandGrid solves exactly one problem")
+    torch = _lib.require_device()
+    self.torch, self.hb = torch, hb
+    dev = torch.device(device or "cuda")
+    self.device = dev
+    lib = _lib.load()
+    self._inst = np.ascontiguousarray(hb.inst[:1])
+    self.parts = int(lib.qtqp_band_grid_default_parts(self._inst.ctypes.data)
+                     if parts is None else parts)
+    self.ws_bytes = int(lib.qtqp_band_grid_workspace_bytes(self._inst.ctypes.data, self.parts))
+    if self.ws_bytes == 0:
+      msg = lib.qtqp_last_error()
+      raise ValueError(msg.decode() if msg else "qtqp_band_grid_workspace_bytes failed")
+    f64 = dict(dtype=torch.float64, device=dev)
+    self.h_pools = [torch.from_numpy(x).pin_memory() for x in
+                    (hb.ipool, hb.vpool, hb.b_pool, hb.c_pool)]
+    self.ipool = torch.empty(hb.ipool.size, dtype=torch.int32, device=dev)
+    self.vpool = torch.empty(hb.vpool.size, **f64)
+    self.b = torch.empty(hb.b_pool.size, **f64)
+    self.c = torch.empty(hb.c_pool.size, **f64)
+    self.x = torch.empty(max(hb.n_total, 1), **f64)
+    self.y = torch.empty(max(hb.m_total, 1), **f64)
+    self.s = torch.empty(max(hb.m_total, 1), **f64)
+    self.result = torch.zeros(_lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    self.stats = None
+    if records or (records is None and hb.opts.collect_stats):
+      self.stats = torch.empty(hb.opts.max_iter * _lib.STATS_DOUBLES, **f64)
+    self._ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=dev)
+    self.ws_ptr = (self._ws.data_ptr() + 255) & ~255
+    self._copts = hb.opts.to_c()
+
+  @property
+  def input_bytes(self) -> int:
+    return self.hb.input_bytes
+
+  def upload(self, stream=None) -> None:
+    torch = self.torch
+    with torch.cuda.stream(stream or torch.cuda.current_stream(self.device)):
+      for dst, src in zip((self.ipool, self.vpool, self.b, self.c), self.h_pools):
+        dst.copy_(src, non_blocking=True)
+
+  def launch(self, stream=None) -> None:
+    torch = self.torch
+    st = stream or torch.cuda.current_stream(self.device)
+    lib = _lib.load()
+    _lib.check(lib.qtqp_band_grid_solve(
+        self._inst.ctypes.data, self.parts, self.ipool.data_ptr(), self.vpool.data_ptr(),
+        self.b.data_ptr(), self.c.data_ptr(), self.x.data_ptr(), self.y.data_ptr(),
+        self.s.data_ptr(), self.result.data_ptr(),
+        self.stats.data_ptr() if self.stats is not None else None, self.ws_ptr, self.ws_bytes,
+        ctypes.byref(self._copts), _lib.stream_handle(st)))
+
+  def fetch(self):
+    """(results[1], x, y, s, stats or None) on the host, like the batches."""
+    self.torch.cuda.synchronize(self.device)
+    res = self.result.cpu().numpy().view(_lib.RESULT_DTYPE)[:1]
+    stats = None
+    if self.stats is not None:
+      stats = self.stats.cpu().numpy().reshape(1, self.hb.opts.max_iter, _lib.STATS_DOUBLES)
+    return res, self.x.cpu().numpy(), self.y.cpu().numpy(), self.s.cpu().numpy(), stats

@@ -163,6 +163,11 @@ template <typename T, class S>
 __device__ int large_factorize(S& s);
 template <typename T, class S>
 __device__ void large_chol_solve(S& s, T* v, T* w);
+// Partitioned banded factorisation / solve of grid mode (band_grid.cuh).
+template <typename T, class S>
+__device__ int bandp_factorize(S& s);
+template <typename T, class S>
+__device__ void bandp_solve(S& s, T* v, T* w);
 
 template <int NT, int FMT = kFmtDense>
 struct Ipm {
@@ -205,6 +210,13 @@ struct Ipm {
   // Shared-memory window of the banded factorisation and solves (null: the
   // band is too wide for it and the global-memory variants run).
   double* bwin;
+  size_t bwin_bytes;
+  // Banded backend in grid mode: the number of partitions of the columns,
+  // the partitions' spikes, the separator blocks and the separator vectors.
+  int nparts;
+  double* bp_wl;
+  double* bp_sep;
+  double* bp_vec;
 
   // Grid mode (NT > 1024, FMT == kFmtLarge): the group is a cooperative grid
   // of NT / kGridBT blocks; barriers and reductions go through gctl.
@@ -1988,130 +2000,160 @@ struct Ipm {
     return sparse_dot(ix, av, v, 0, ip[i], ip[i + 1]);
   }
 
-  // Gram matrix in column band storage, then Cholesky.  With the shared-
-  // memory window (bw <= kBandWinMaxBw): each thread accumulates its Gram
-  // column in shared memory, and the factorisation keeps the active
-  // (bw+2) x (bw+2) part of the band in shared memory (band_chol_window).
-  // Otherwise the global-memory variant below runs.  The diagonal of the
-  // factor keeps 1 / l_kk.
+  // Column j of the Gram matrix G = P_off + diag(Rx) + A^T diag(1/Ry) A,
+  // rows j .. j + bw, into acc[0 .. bw].  The loads of every level are issued
+  // in batches of 8 before they are used (column j's rows and their
+  // scalings, then each row's entries), so that this latency-bound gather
+  // keeps several loads in flight.
   template <typename T>
-  __device__ int band_factorize() {
-    if (bwin == nullptr) return band_factorize_global<T>();
+  __device__ __forceinline__ void band_gram_column(int j, T* acc) const {
     QTQP_BAND_LOCALS;
-    QTQP_TIC();
-    T* L = reinterpret_cast<T*>(Lb);
     const double* reg = vec(kREG);
     const double* wsc = vec(kPW);
+    for (int d = 0; d <= bw; ++d) acc[d] = T(0);
+    const int qa = jp[j], qb = jp[j + 1];
+    for (int q0 = qa; q0 < qb; q0 += 8) {
+      int rr[8], r0[8], r1[8];
+      double ww[8], aq[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool ok = q0 + u < qb;
+        rr[u] = ok ? jx[q0 + u] : 0;
+        aq[u] = ok ? at[q0 + u] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool ok = q0 + u < qb;
+        ww[u] = ok ? wsc[n + rr[u]] : 0.0;
+        r0[u] = ok ? ip[rr[u]] : 0;
+        r1[u] = ok ? ip[rr[u] + 1] : 0;
+      }
+#pragma unroll 1
+      for (int u = 0; u < 8 && q0 + u < qb; ++u) {
+        const double w = ww[u];
+        const T arj = T(aq[u] * w);
+        const int q1 = r1[u];
+        int q2 = r0[u];
+        for (; q2 + 8 <= q1; q2 += 8) {
+          int ii[8];
+          double aa[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            ii[e] = ix[q2 + e];
+            aa[e] = av[q2 + e];
+          }
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int i = ii[e];
+            if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(aa[e] * w), acc[i - j]);
+          }
+        }
+        for (; q2 < q1; ++q2) {
+          const int i = ix[q2];
+          if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(av[q2] * w), acc[i - j]);
+        }
+      }
+    }
+    if (has_p) {
+      for (int q = pp[j]; q < pp[j + 1]; ++q) {
+        const int i = px[q];
+        if (i > j && i - j <= bw) acc[i - j] = T(pv[q]) + acc[i - j];
+      }
+    }
+    acc[0] = T(reg[j]) + acc[0];
+  }
+
+  // The Gram matrix in column band storage (Lb) plus the relative diagonal
+  // jitter of the dense backend.  acc_smem: this thread's column scratch in
+  // shared memory (bw + 1 entries), or null to accumulate in place.
+  template <typename T>
+  __device__ void band_gram(T* acc_smem) {
+    const int ldl = bw + 1;
+    T* L = reinterpret_cast<T*>(Lb);
     double dmax[1] = {0.0};
     double dummy[1] = {0.0};
-    T* acc = reinterpret_cast<T*>(bwin) + size_t(tid) * ldl;  // this thread's column
     for (int j0 = 0; j0 < n; j0 += NT) {
       const int j = j0 + tid;
       if (j < n) {
-        for (int d = 0; d <= bw; ++d) acc[d] = T(0);
-        // The loads of every level are issued in batches of 8 before they are
-        // used (column j's rows and their scalings, then each row's entries),
-        // so that this latency-bound gather keeps several loads in flight.
-        const int qa = jp[j], qb = jp[j + 1];
-        for (int q0 = qa; q0 < qb; q0 += 8) {
-          int rr[8], r0[8], r1[8];
-          double ww[8], aq[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const bool ok = q0 + u < qb;
-            rr[u] = ok ? jx[q0 + u] : 0;
-            aq[u] = ok ? at[q0 + u] : 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const bool ok = q0 + u < qb;
-            ww[u] = ok ? wsc[n + rr[u]] : 0.0;
-            r0[u] = ok ? ip[rr[u]] : 0;
-            r1[u] = ok ? ip[rr[u] + 1] : 0;
-          }
-#pragma unroll 1
-          for (int u = 0; u < 8 && q0 + u < qb; ++u) {
-            const double w = ww[u];
-            const T arj = T(aq[u] * w);
-            const int q1 = r1[u];
-            int q2 = r0[u];
-            for (; q2 + 8 <= q1; q2 += 8) {
-              int ii[8];
-              double aa[8];
-#pragma unroll
-              for (int e = 0; e < 8; ++e) {
-                ii[e] = ix[q2 + e];
-                aa[e] = av[q2 + e];
-              }
-#pragma unroll
-              for (int e = 0; e < 8; ++e) {
-                const int i = ii[e];
-                if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(aa[e] * w), acc[i - j]);
-              }
-            }
-            for (; q2 < q1; ++q2) {
-              const int i = ix[q2];
-              if (i >= j && i - j <= bw) acc[i - j] = fma(arj, T(av[q2] * w), acc[i - j]);
-            }
-          }
-        }
-        if (has_p) {
-          for (int q = pp[j]; q < pp[j + 1]; ++q) {
-            const int i = px[q];
-            if (i > j && i - j <= bw) acc[i - j] = T(pv[q]) + acc[i - j];
-          }
-        }
-        acc[0] = T(reg[j]) + acc[0];
-        dmax[0] = nanmax(dmax[0], double(acc[0]));
         T* col = L + size_t(j) * ldl;
-        for (int d = 0; d <= bw; ++d) col[d] = acc[d];
+        T* acc = acc_smem != nullptr ? acc_smem : col;
+        band_gram_column<T>(j, acc);
+        dmax[0] = nanmax(dmax[0], double(acc[0]));
+        if (acc_smem != nullptr)
+          for (int d = 0; d <= bw; ++d) col[d] = acc[d];
       }
     }
     reduce<0, 1>(dummy, dmax);
     const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
     for (int j = tid; j < n; j += NT) L[size_t(j) * ldl] = T(double(L[size_t(j) * ldl]) + jit);
     sync();
-    QTQP_TOC(kPhGram);
-    QTQP_RETIC();
-    const int info = band_chol_window<T>();
-    QTQP_TOC(kPhChol);
-    return info;
   }
 
-  // Band Cholesky with the active part of the band in shared memory.  Rows
-  // and columns k .. k+bw+1 live in a (bw+2) x (bw+2) window with circular
-  // indices (slot = index mod (bw+2)); step k reads the still-unscaled
-  // column k, writes the finished column k of L to global memory, updates
-  // the window, and stores row k+bw+1 of the Gram matrix (prefetched into
-  // registers during the previous step) into the slots that row k-1 and
-  // column k-1 have freed.  One barrier per column.
+  // Gram matrix in column band storage, then Cholesky.  With the shared-
+  // memory window (bw <= kBandWinMaxBw): each thread accumulates its Gram
+  // column in shared memory, and the factorisation keeps the active
+  // (bw+2) x (bw+2) part of the band in shared memory (band_chol_window_range).
+  // Otherwise the global-memory variant below runs.  In grid mode the
+  // partitioned factorisation runs (band_grid.cuh).  The diagonal of the
+  // factor keeps 1 / l_kk.
   template <typename T>
-  __device__ int band_chol_window() {
-    QTQP_BAND_LOCALS;
-    T* L = reinterpret_cast<T*>(Lb);
+  __device__ int band_factorize() {
+    if constexpr (NT > 1024) {
+      return bandp_factorize<T>(*this);
+    } else {
+      if (bwin == nullptr) return band_factorize_global<T>();
+      QTQP_TIC();
+      band_gram<T>(reinterpret_cast<T*>(bwin) + size_t(tid) * (bw + 1));
+      QTQP_TOC(kPhGram);
+      QTQP_RETIC();
+      const int info = band_chol_window_range<T, NT>(tid, 0, n, n, nullptr, 0);
+      QTQP_TOC(kPhChol);
+      return info;
+    }
+  }
+
+  // Band Cholesky with the active part of the band in shared memory, over
+  // the principal submatrix of rows / columns [lo, lo + nsub) of which the
+  // first ne columns are eliminated (ne == nsub: the whole factorisation).
+  // Local rows and columns k .. k+bw+1 live in a (bw+2) x (bw+2) window with
+  // circular indices (slot = index mod (bw+2)); step k reads the still-
+  // unscaled column k, writes the finished column k of L to global memory,
+  // updates the window, and stores row k+bw+1 of the Gram matrix (prefetched
+  // into registers during the previous step) into the slots that row k-1
+  // and column k-1 have freed.  One barrier per column.  Columns before lo
+  // are not part of the submatrix.  tail (when ne < nsub): the lower
+  // triangle of the trailing (nsub-ne)^2 block after the elimination (the
+  // Schur complement of the eliminated columns), row-major with leading
+  // dimension ldt.  lt: this thread's index among the BT threads of the
+  // group.  Returns 0 or the 1-based global column of the first
+  // non-positive pivot.
+  template <typename T, int BT>
+  __device__ int band_chol_window_range(int lt, int lo, int nsub, int ne, T* tail, int ldt) {
+    const int bw = this->bw, ldl = bw + 1;
+    T* L = reinterpret_cast<T*>(Lb) + size_t(lo) * ldl;
     T* W = reinterpret_cast<T*>(bwin);
     const int B = bw + 2;
     // Offsets (oi, oj), 1 <= oj <= oi <= bw, of the trailing update relative
-    // to k, the same every step; thread t handles pairs t, t + NT, ...
+    // to k, the same every step; thread t handles pairs t, t + BT, ...
     uint32_t* pairs = reinterpret_cast<uint32_t*>(bwin + (size_t(B) * B * sizeof(T) + 7) / 8);
     const int npairs = bw * (bw + 1) / 2;
-    for (int oi = 1 + tid; oi <= bw; oi += NT)
+    for (int oi = 1 + lt; oi <= bw; oi += BT)
       for (int oj = 1; oj <= oi; ++oj) pairs[(oi - 1) * oi / 2 + oj - 1] = uint32_t(oi) | (uint32_t(oj) << 16);
-    // Rows 0 .. min(bw, n-1): entries (i, j), j <= i.
-    for (int e = tid; e < B * B; e += NT) {
+    // Rows 0 .. min(bw, nsub-1): entries (i, j), j <= i.
+    for (int e = lt; e < B * B; e += BT) {
       const int i = e / B, j = e - i * B;
-      W[e] = (j <= i && i <= bw && i < n) ? L[size_t(j) * ldl + (i - j)] : T(0);
+      W[e] = (j <= i && i <= bw && i < nsub) ? L[size_t(j) * ldl + (i - j)] : T(0);
     }
     // Prefetch of the row that enters at step k: r = k + bw + 1, entries
     // (r, j) for j in [r - bw, r]; thread t takes j = r - bw + t.
     auto fetch = [&](int k) {
-      const int r = k + bw + 1, j = r - bw + tid;
-      return (r < n && tid <= bw) ? L[size_t(j) * ldl + (r - j)] : T(0);
+      const int r = k + bw + 1, j = r - bw + lt;
+      return (r < nsub && lt <= bw) ? L[size_t(j) * ldl + (r - j)] : T(0);
     };
     T pre = fetch(0);
-    sync();
+    group_sync<BT>();
     int info = 0;
-    for (int k = 0; k < n; ++k) {
+    for (int k = 0; k < ne; ++k) {
       const int ks = k % B;
       const T d = W[ks * B + ks];
       if (!(d > T(0))) {
@@ -2119,18 +2161,18 @@ struct Ipm {
         break;
       }
       const T il = rsqrt(d), inv_d = il * il;  // no division on this chain
-      const int last = min(n - 1, k + bw);
+      const int last = min(nsub - 1, k + bw);
       auto slot = [&](int i) {  // i % B for i in [k, k + B)
         const int t = ks + (i - k);
         return t >= B ? t - B : t;
       };
       // Finished column k of L (global); the window keeps it unscaled.
-      for (int i = k + 1 + tid; i <= last; i += NT) L[size_t(k) * ldl + (i - k)] = W[slot(i) * B + ks] * il;
-      if (tid == 0) L[size_t(k) * ldl] = il;
+      for (int i = k + 1 + lt; i <= last; i += BT) L[size_t(k) * ldl + (i - k)] = W[slot(i) * B + ks] * il;
+      if (lt == 0) L[size_t(k) * ldl] = il;
       // Trailing update: W_ij -= W_ik W_jk / d for k < j <= i <= last.
       const int span = last - k;
 #pragma unroll 4
-      for (int pi = tid; pi < npairs; pi += NT) {
+      for (int pi = lt; pi < npairs; pi += BT) {
         const uint32_t pr = pairs[pi];
         const int oi = int(pr & 0xffffu), oj = int(pr >> 16);
         if (oi <= span) {
@@ -2142,17 +2184,24 @@ struct Ipm {
       // j in [k+1, r] (never ks; the diagonal lands in column k-1's slot).
       {
         const int r = k + bw + 1;
-        if (r < n && tid <= bw) {
+        if (r < nsub && lt <= bw) {
           const int rs = ks == 0 ? B - 1 : ks - 1;  // (k - 1) mod B
-          const int j = r - bw + tid;               // in [k + 1, r]
+          const int j = r - bw + lt;                // in [k + 1, r]
           W[rs * B + (j - k == B - 1 ? rs : slot(j))] = pre;
         }
         pre = fetch(k + 1);
       }
-      sync();
+      group_sync<BT>();
     }
-    sync();
-    return info;
+    group_sync<BT>();
+    if (tail != nullptr && info == 0) {
+      const int t = nsub - ne;
+      for (int e = lt; e < t * t; e += BT) {
+        const int i = e / t, j = e - i * t;
+        if (j <= i) tail[size_t(i) * ldt + j] = W[((ne + i) % B) * B + (ne + j) % B];
+      }
+    }
+    return info == 0 ? 0 : lo + info;
   }
 
   // Global-memory variant (wide bands): Gram in column band storage, then
@@ -2232,102 +2281,134 @@ struct Ipm {
   // warp: forward z_k = v_k / l_kk, v_i -= l_ik z_k (i in (k, k+bw]) into w;
   // backward x_k = w_k / l_kk, w_i -= l_ki x_k (i in [k-bw, k)) into v.
   // With the window, the bw+1 active entries of the vector live in shared
-  // memory (128 circular slots) and the factor entries of the next step are
-  // loaded into registers while the current step runs.
+  // memory (128 circular slots) and the factor entries of the next steps are
+  // copied into a ring while the current step runs.  In grid mode the
+  // partitioned solve runs (band_grid.cuh).
   template <typename T>
   __device__ void band_chol_solve(T* v, T* w) {
-    if (bwin == nullptr) {
-      band_chol_solve_global<T>(v, w);
-      return;
+    if constexpr (NT > 1024) {
+      bandp_solve<T>(*this, v, w);
+    } else {
+      if (bwin == nullptr) {
+        band_chol_solve_global<T>(v, w);
+        return;
+      }
+      if (tid < 32) {
+        band_fwd_range<T>(v, w, 0, n, n, tid);
+        band_bwd_range<T>(v, w, 0, n, n, tid);
+      }
+      sync();
     }
-    QTQP_BAND_LOCALS;
+  }
+
+  // Forward substitution over the columns [lo, lo + ne) of the rows
+  // [lo, R) by one warp (lane): z_k into w[k]; the rows [lo + ne, R) of v
+  // receive their updates v_i -= l_ik z_k.  Group c of the ring (one per
+  // step, issued kBandRing-1 steps ahead) copies column c of L (offsets
+  // 0..bw; 0 = 1 / l_cc) and v[c + bw + 1].
+  template <typename T>
+  __device__ void band_fwd_range(T* v, T* w, int lo, int ne, int R, int lane) {
+    const int bw = this->bw, ldl = bw + 1, hi = lo + ne;
     const T* L = reinterpret_cast<const T*>(Lb);
-    T* win = reinterpret_cast<T*>(bwin);        // 128 circular vector slots
-    T* ring = win + 128;                        // kBandRing x 128 factor entries
-    T* vring = ring + kBandRing * 128;          // kBandRing entering vector values
+    T* win = reinterpret_cast<T*>(bwin);  // 128 circular vector slots
+    T* ring = win + 128;                  // kBandRing x 128 factor entries
+    T* vring = ring + kBandRing * 128;    // kBandRing entering vector values
     constexpr int D = kBandRing;
-    if (tid < 32) {
-      const int lane = tid;
-      // Forward.  Group c (one per step, issued D-1 steps ahead) copies column
-      // c of L (offsets 0..bw; 0 = 1 / l_cc) and v[c + bw + 1] into the rings.
-      auto issue_fwd = [&](int c) {
-        T* rc = ring + (c % D) * 128;
-        const int rows = min(bw, n - 1 - c);
+    auto issue_fwd = [&](int c) {
+      T* rc = ring + (c % D) * 128;
+      const int rows = min(bw, R - 1 - c);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int d = lane + 32 * q;
-          const bool ok = c < n && d <= rows;
-          cp_async_elem(rc + d, L + (ok ? size_t(c) * ldl + d : 0), ok);
-        }
-        if (lane == 0) {
-          const bool ok = c + bw + 1 < n;
-          cp_async_elem(vring + c % D, v + (ok ? c + bw + 1 : 0), ok);
-        }
-        cp_async_commit();
-      };
-      for (int i = lane; i <= min(bw, n - 1); i += 32) win[i & 127] = v[i];
-      for (int c = 0; c < D - 1; ++c) issue_fwd(c);
-      for (int k = 0; k < n; ++k) {
-        issue_fwd(k + D - 1);
-        cp_async_wait<D - 1>();
-        __syncwarp();
-        const T* ck = ring + (k % D) * 128;
-        const T zk = win[k & 127] * ck[0];
-        const int rows = min(bw, n - 1 - k);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int d = lane + 1 + 32 * q;
-          if (d <= rows) win[(k + d) & 127] = fma(-ck[d], zk, win[(k + d) & 127]);
-        }
-        if (lane == 0) {
-          w[k] = zk;
-          if (k + bw + 1 < n) win[(k + bw + 1) & 127] = vring[k % D];
-        }
-        __syncwarp();
+      for (int q = 0; q < 4; ++q) {
+        const int d = lane + 32 * q;
+        const bool ok = c < hi && d <= rows;
+        cp_async_elem(rc + d, L + (ok ? size_t(c) * ldl + d : 0), ok);
       }
-      cp_async_wait<0>();
-      __threadfence_block();  // z (written to w above) before the copies read it
+      if (lane == 0) {
+        const bool ok = c + bw + 1 < R;
+        cp_async_elem(vring + c % D, v + (ok ? c + bw + 1 : 0), ok);
+      }
+      cp_async_commit();
+    };
+    for (int i = lane; i <= min(bw, R - 1 - lo); i += 32) win[(lo + i) & 127] = v[lo + i];
+    for (int c = lo; c < lo + D - 1; ++c) issue_fwd(c);
+    for (int k = lo; k < hi; ++k) {
+      issue_fwd(k + D - 1);
+      cp_async_wait<D - 1>();
       __syncwarp();
-      // Backward.  Group c copies row c of L (l_c,c-d at column c-d, offset
-      // d; offset 0 = 1 / l_cc) and w[c - bw - 1].
-      auto issue_bwd = [&](int c) {
-        T* rc = ring + ((c % D + D) % D) * 128;
-        const int rows = min(bw, c);
+      const T* ck = ring + (k % D) * 128;
+      const T zk = win[k & 127] * ck[0];
+      const int rows = min(bw, R - 1 - k);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int d = lane + 32 * q;
-          const bool ok = c >= 0 && d <= rows;
-          cp_async_elem(rc + d, L + (ok ? size_t(c - d) * ldl + d : 0), ok);
-        }
-        if (lane == 0) {
-          const bool ok = c - bw - 1 >= 0;
-          cp_async_elem(vring + (c % D + D) % D, w + (ok ? c - bw - 1 : 0), ok);
-        }
-        cp_async_commit();
-      };
-      for (int i = lane; i <= min(bw, n - 1); i += 32) win[(n - 1 - i) & 127] = w[n - 1 - i];
-      for (int c = n - 1; c > n - D; --c) issue_bwd(c);
-      for (int k = n - 1; k >= 0; --k) {
-        issue_bwd(k - D + 1);
-        cp_async_wait<D - 1>();
-        __syncwarp();
-        const T* rk = ring + ((k % D + D) % D) * 128;
-        const T xk = win[k & 127] * rk[0];
-        const int rows = min(bw, k);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int d = lane + 1 + 32 * q;
-          if (d <= rows) win[(k - d) & 127] = fma(-rk[d], xk, win[(k - d) & 127]);
-        }
-        if (lane == 0) {
-          v[k] = xk;
-          if (k - bw - 1 >= 0) win[(k - bw - 1) & 127] = vring[(k % D + D) % D];
-        }
-        __syncwarp();
+      for (int q = 0; q < 4; ++q) {
+        const int d = lane + 1 + 32 * q;
+        if (d <= rows) win[(k + d) & 127] = fma(-ck[d], zk, win[(k + d) & 127]);
       }
-      cp_async_wait<0>();
+      if (lane == 0) {
+        w[k] = zk;
+        if (k + bw + 1 < R) win[(k + bw + 1) & 127] = vring[k % D];
+      }
+      __syncwarp();
     }
-    sync();
+    cp_async_wait<0>();
+    __syncwarp();
+    for (int i = hi + lane; i < R; i += 32) v[i] = win[i & 127];
+  }
+
+  // Backward substitution by one warp over the rows [lo, R): x_k =
+  // (w_k - sum_d l_{k+d,k} x_{k+d}) / l_kk for k in [lo, hi), into v[k];
+  // the rows [hi, R) hold known values of x in v (the separator that
+  // follows a partition) and only contribute.  Group c of the ring copies
+  // row c of L (l_{c,c-d} at column c-d, offset d; offset 0 = 1 / l_cc) and
+  // w[c - bw - 1].
+  template <typename T>
+  __device__ void band_bwd_range(T* v, T* w, int lo, int hi, int R, int lane) {
+    const int bw = this->bw, ldl = bw + 1;
+    const T* L = reinterpret_cast<const T*>(Lb);
+    T* win = reinterpret_cast<T*>(bwin);
+    T* ring = win + 128;
+    T* vring = ring + kBandRing * 128;
+    constexpr int D = kBandRing;
+    __threadfence_block();  // w (plain stores) before the copies read it
+    __syncwarp();
+    auto issue_bwd = [&](int c) {
+      T* rc = ring + ((c % D + D) % D) * 128;
+      const int rows = min(bw, c - lo);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int d = lane + 32 * q;
+        const bool ok = c >= lo && d <= rows;
+        cp_async_elem(rc + d, L + (ok ? size_t(c - d) * ldl + d : 0), ok);
+      }
+      if (lane == 0) {
+        const bool ok = c - bw - 1 >= lo;
+        cp_async_elem(vring + (c % D + D) % D, w + (ok ? c - bw - 1 : 0), ok);
+      }
+      cp_async_commit();
+    };
+    for (int i = lane; i <= min(bw, R - 1 - lo); i += 32) {
+      const int r = R - 1 - i;
+      win[r & 127] = r >= hi ? v[r] : w[r];
+    }
+    for (int c = R - 1; c > R - D; --c) issue_bwd(c);
+    for (int k = R - 1; k >= lo; --k) {
+      issue_bwd(k - D + 1);
+      cp_async_wait<D - 1>();
+      __syncwarp();
+      const T* rk = ring + ((k % D + D) % D) * 128;
+      const T xk = k >= hi ? win[k & 127] : win[k & 127] * rk[0];
+      const int rows = min(bw, k - lo);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int d = lane + 1 + 32 * q;
+        if (d <= rows && k - d < hi) win[(k - d) & 127] = fma(-rk[d], xk, win[(k - d) & 127]);
+      }
+      if (lane == 0) {
+        if (k < hi) v[k] = xk;
+        if (k - bw - 1 >= lo) win[(k - bw - 1) & 127] = vring[(k % D + D) % D];
+      }
+      __syncwarp();
+    }
+    cp_async_wait<0>();
   }
 
   template <typename T>

@@ -129,11 +129,11 @@ def mpc_structure(horizon: int, nx: int = 40, nu: int = 20, seed: int = 1003):
 
 
 def mpc_feasible(horizon: int, seed: int = 1003, active_frac: float = 0.1,
-                 free_initial: bool = False):
+                 free_initial: bool = False, nx: int = 40, nu: int = 20):
   """MPC QP with b, c from a feasible pair: x_bar strictly inside the boxes
   except a fraction `active_frac` at +-bound (with positive duals there).
   free_initial keeps the first stage's variables off the bounds."""
-  a, z, p, ub = mpc_structure(horizon, seed=seed)
+  a, z, p, ub = mpc_structure(horizon, nx=nx, nu=nu, seed=seed)
   rng = np.random.default_rng([seed, 1])
   n = p.shape[0]
   xbar = rng.uniform(-0.5, 0.5, size=n) * ub

@@ -90,3 +90,30 @@ def test_kkt_workspace_size(lib):
 def _dense(prob):
   a, b, c, z, p = prob
   return a.toarray(), b, c, z, p.toarray()
+
+
+def _band_inst(n, bw, m=None):
+  inst = np.zeros(1, dtype=_lib.BAND_DTYPE)
+  inst["n"], inst["m"], inst["z"], inst["bw"] = n, m or 2 * n, n // 4, bw
+  inst["nnz_a"] = 4 * n
+  return inst
+
+
+def test_band_grid_partition_limits(lib):
+  """Partition counts keep every interior at least bw long and stay within
+  the grid; too-wide bands are refused."""
+  inst = _band_inst(30000, 99)
+  dp = lib.qtqp_band_grid_default_parts(inst.ctypes.data)
+  assert 1 <= dp <= min(128, (30000 + 99) // 198)
+  assert lib.qtqp_band_grid_workspace_bytes(inst.ctypes.data, dp) > 8 * 30000 * 100
+  assert lib.qtqp_band_grid_workspace_bytes(inst.ctypes.data, 1) > 0
+  assert lib.qtqp_band_grid_workspace_bytes(inst.ctypes.data, 128) > 0
+  assert lib.qtqp_band_grid_workspace_bytes(inst.ctypes.data, 129) == 0
+  assert lib.qtqp_band_grid_workspace_bytes(inst.ctypes.data, 0) == 0
+  small = _band_inst(1000, 99)
+  assert lib.qtqp_band_grid_workspace_bytes(small.ctypes.data, (1000 + 99) // 198) > 0
+  assert lib.qtqp_band_grid_workspace_bytes(small.ctypes.data, (1000 + 99) // 198 + 1) == 0
+  assert b"parts must be" in lib.qtqp_last_error()
+  wide = _band_inst(30000, 127)
+  assert lib.qtqp_band_grid_workspace_bytes(wide.ctypes.data, 4) == 0
+  assert b"too wide" in lib.qtqp_last_error()
