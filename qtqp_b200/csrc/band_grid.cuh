@@ -636,14 +636,18 @@ __device__ int bandp_factorize(S& s) {
     }
   }
   s.sync();
+  QTQP_TOC(kPhBpInterior);
+  QTQP_RETIC();
   if (k == 0 && *info == 0) {
     const int bad = bandp_chain<T>(s, bp);
     if (bad != 0 && threadIdx.x == 0) atomicMax(const_cast<int*>(info), bad);
   }
   s.sync();
+  QTQP_TOC(kPhBpChain);
+  QTQP_RETIC();
   if (*info == 0 && k < bp.P - 1) bandp_sep_inverse<T>(s, bp, k);
   s.sync();
-  QTQP_TOC(kPhChol);
+  QTQP_TOC(kPhBpSepInv);
   return *info;
 }
 
@@ -659,6 +663,7 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
   constexpr int kNW = kGridBT / 32;
   // Scratch after the solve rings (band_fwd_range / band_bwd_range).
   T* scr = reinterpret_cast<T*>(s.bwin) + (128 + kBandRing * 128 + kBandRing);
+  QTQP_TIC();
   // Forward per interior; t_k's spike term W_L^T y of interior k+1.
   if (k < P) {
     const int lo = bp.lo(k), li = bp.li(k), hi = lo + li, R = hi + (k < P - 1 ? bw : 0);
@@ -676,6 +681,8 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
     }
   }
   s.sync();
+  QTQP_TOC(kPhBpFwd);
+  QTQP_RETIC();
   // u_k = Li_k (v[S_k] - W_L^T y).
   if (k < P - 1) {
     const int hi = bp.lo(k) + bp.li(k);
@@ -751,6 +758,8 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
     }
   }
   s.sync();
+  QTQP_TOC(kPhBpChains);
+  QTQP_RETIC();
   // Backward per interior after removing W_L x_{S_{k-1}}.
   if (k < P) {
     const int lo = bp.lo(k), li = bp.li(k), hi = lo + li, R = hi + (k < P - 1 ? bw : 0);
@@ -769,6 +778,7 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
     if (warp == 0) s.template band_bwd_range<T>(v, w, lo, hi, R, lane);
   }
   s.sync();
+  QTQP_TOC(kPhBpBwd);
 }
 
 }  // namespace qtqp

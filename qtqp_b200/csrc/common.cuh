@@ -258,7 +258,9 @@ enum Phase : int {
   kPhLoad = 0, kPhNormalize, kPhGram, kPhChol, kPhSolve, kPhResidual, kPhTau, kPhStep,
   kPhTerm, kPhOther,
   // Sub-phases of the large (grid-mode) factorisation and solves.
-  kPhLgDiag, kPhLgPanel, kPhLgTrail, kPhLgInv, kPhLgFwd, kPhLgBwd, kNumPhases
+  kPhLgDiag, kPhLgPanel, kPhLgTrail, kPhLgInv, kPhLgFwd, kPhLgBwd,
+  // Sub-phases of the partitioned banded factorisation and solves.
+  kPhBpInterior, kPhBpChain, kPhBpSepInv, kPhBpFwd, kPhBpChains, kPhBpBwd, kNumPhases
 };
 #ifdef QTQP_PHASE_TIMERS
 extern __device__ unsigned long long g_phase_cycles[kNumPhases];
