@@ -61,6 +61,9 @@ def _args():
   ap.add_argument("--mpc-horizon", type=int, default=500,
                   help="mpc: horizon T (n = 60 T); 500 is the workload, smaller horizons are "
                        "for profiling captures")
+  ap.add_argument("--mpc-parts", type=int, default=None,
+                  help="mpc: partitions of the banded factorisation (default: the library's "
+                       "choice for the band)")
   ap.add_argument("--large-n", type=int, default=4096,
                   help="dense_large: n (m = 2n, z = n/4); 4096 is the workload, smaller "
                        "sizes are for profiling captures")
@@ -565,7 +568,7 @@ def run_mpc(args):
   forms = {}
   for precision in ("fp64", "mixed"):
     hb = band.HostBandBatch([q.band_problem()], batch.SolveOptions(precision=precision))
-    db = band.DeviceBandBatch(hb, device=dev)
+    db = band.DeviceBandGrid(hb, device=dev, parts=args.mpc_parts)
     db.upload(stream)
     for _ in range(args.warmup):
       db.launch(stream)
@@ -607,6 +610,7 @@ def run_mpc(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator of the workload's distribution)",
         "config": {"workload": workload, "precision": args.precision, "bandwidth": bw,
+                   "partitions": db.parts,
                    "parallelism": "replicas" if world > 1 else "one QP per GPU"},
         "fp64_value": int(fp64["res"]["status"] == 0) * args.steps / fp64["time"],
         "mixed_value": int(mixed["res"]["status"] == 0) * args.steps / mixed["time"],
@@ -619,7 +623,7 @@ def run_mpc(args):
                 "d2h_bytes_per_step": sum(int(t_.numel() * t_.element_size()) for t_ in h_out)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                     "kernel": "band_batch_kernel",
+                     "kernel": "band_grid_kernel",
                      "algorithmic_bytes_per_launch": per_iter * iters},
         "cpu_baseline": cpu, "clocks": chosen["clocks"], "gpu_launches": args.steps}),
           flush=True)
