@@ -241,7 +241,7 @@ int qtqp_band_batch_solve(const qtqp_band_instance* d_inst,
  * partitioned triangular solves.  h_inst: host pointer to the instance's
  * descriptor (offsets into the device pools as in the batch).  parts in
  * [1, min(128, (n + bw) / (2 bw))]; qtqp_band_grid_default_parts gives the
- * default.  bw <= 117 (the separator blocks are staged in shared memory);
+ * default.  bw <= 118 (the separator blocks are staged in shared memory);
  * wider bands return QTQP_ERR_BAD_ARG.  The workspace (>=
  * qtqp_band_grid_workspace_bytes, 256-byte aligned) is private.  A grid
  * barrier that waits too long ends the solve with status FAILED and error

@@ -220,9 +220,9 @@ class DeviceBandBatch:
     return (res, self.x.cpu().numpy(), self.y.cpu().numpy(), self.s.cpu().numpy(), stats)
 
 
-# Widest band of the whole-GPU path (two bw x (bw+1) FP64 separator blocks
+# Widest band of the whole-GPU path (two bw x bw FP64 separator blocks
 # staged in 225 KiB of shared memory).
-GRID_MAX_BW = 117
+GRID_MAX_BW = 118
 
 
 def grid_supported(bw: int, n: int) -> bool:

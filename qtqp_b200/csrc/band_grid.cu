@@ -93,10 +93,10 @@ using namespace qtqp;
 
 extern "C" int32_t qtqp_band_grid_default_parts(const qtqp_band_instance* h_inst) {
   if (h_inst == nullptr || h_inst->bw < 1 || h_inst->n < 2) return 1;
-  // About six half-bandwidths of columns per partition balance the
-  // parallel interiors against the sequential separator chain.
-  const int want = std::max(1, h_inst->n / (6 * h_inst->bw));
-  return std::max(1, std::min({want, kBandGridBlocks, band_grid_max_parts(h_inst->n, h_inst->bw)}));
+  // The separators are reduced in log2(parts) parallel levels, so the most
+  // partitions (the shortest interiors) are the fastest: one per block, as
+  // far as every interior stays at least bw long.
+  return std::max(1, std::min(kBandGridBlocks, band_grid_max_parts(h_inst->n, h_inst->bw)));
 }
 
 extern "C" size_t qtqp_band_grid_workspace_bytes(const qtqp_band_instance* h_inst, int32_t parts) {

@@ -21,17 +21,21 @@
 //   C = G_SS - L_SI L_SI^T: block tridiagonal over the separators,
 //     D_k = G[S_k,S_k] - W_R^T W_R (of I_k) - W_L^T W_L (of I_{k+1}),
 //     E_k = C[S_{k+1}, S_k] = -W_R^T W_L (both of I_{k+1}),
-//   chol(C): one block's chain over the separators, Lc_k = chol(D_k -
-//     F_{k-1} F_{k-1}^T), F_k = E_k Lc_k^{-T} (the panel below Lc_k in one
-//     Cholesky of the stacked [D_k; E_k]),
-//   then, in parallel per separator, Li_k = Lc_k^{-1}, G_k = Li_k F_{k-1}
-//     and H_k = (F_k Li_k)^T, so that the two chains of a solve are one
-//     bw x bw product per separator each.
+//   C^{-1} by block cyclic reduction over the separators (1-based j):
+//     level l eliminates the j with lowest set bit 2^l, in parallel (one
+//     block each): Di_j = D_j^{-1} by a symmetric sweep (in-place
+//     Gauss-Jordan on the SPD block, one pivot per step), Yl_j = Di_j Cl_j
+//     and Yr_j = Di_j Cr_j^T for the couplings Cl_j = C[j, j - 2^l], Cr_j =
+//     C[j + 2^l, j]; then every surviving j' (multiple of 2^(l+1)) takes
+//     D_j' -= Cr Yr (of its left neighbour) + Cl^T Yl (of its right
+//     neighbour) and its new left coupling -Cr Yl of the left neighbour, in
+//     parallel.
 // Solve of G x = v: forward per interior (y = L_I^{-1} v_I, which also
-// forms v_S - W_R^T y in the separator rows), t_k = v_S - W_L^T y,
-// u_k = Li_k t_k, z_k = u_k - G_k z_{k-1} (chain), v_k = Li_k^T z_k,
-// x_k = v_k - H_k x_{k+1} (chain), then backward per interior with the
-// separators' x known and the left spike's contribution removed first.
+// forms v_S - W_R^T y in the separator rows), t = v_S - W_L^T y, then the
+// reduction levels forward (z_j = Di_j t_j, neighbours' t -= C z_j) and
+// backward (x_j = z_j - Yl_j x_left - Yr_j x_right), then backward per
+// interior with the separators' x known and the left spike's contribution
+// removed first.
 #pragma once
 
 #include "dense_ipm.cuh"
@@ -43,9 +47,13 @@ constexpr int kBandGridNT = kBandGridBlocks * kGridBT;
 // Dynamic shared memory available to one block of the grid solve.
 constexpr size_t kBandGridSmemCap = 225 * 1024;
 
-// bw x bw blocks kept per separator and bw-vectors per separator.
-enum SepBlock : int { kSbD = 0, kSbQ, kSbE, kSbL, kSbF, kSbI, kSbG, kSbH, kSepBlocks };
-enum SepVec : int { kSvCL = 0, kSvU, kSvZ, kSvV, kSepVecs };
+// bw x bw blocks kept per separator (row-major): D (Schur complement, lower),
+// Q (W_L^T W_L of the next interior), E (coupling with the next separator
+// from the interiors), C (left coupling created by the reduction), Di
+// (inverse of D at elimination), Yl, Yr (reduced couplings) and R (the
+// right coupling at elimination); and bw-vectors.
+enum SepBlock : int { kSbD = 0, kSbQ, kSbE, kSbC, kSbI, kSbXl, kSbXr, kSbR, kSepBlocks };
+enum SepVec : int { kSvCL = 0, kSvT, kSvZ, kSepVecs };
 
 // The partition of the columns 0 .. n-1 into P interiors and P-1 separators.
 struct BandParts {
@@ -67,12 +75,14 @@ __host__ __device__ inline int band_grid_max_parts(int n, int bw) {
   return p < 1 ? 1 : p;
 }
 
-// Pitch (elements) of a staged bw x bw separator block in shared memory.
-__host__ __device__ inline int sep_pitch(int bw) { return bw + 1; }
+// Pitch (elements) of a staged bw x bw separator block in shared memory
+// (column-major, S(i, j) = buf[j * pitch + i]): odd, so that both rows and
+// columns are read without bank conflicts.
+__host__ __device__ inline int sep_pitch(int bw) { return bw | 1; }
 
 // Dynamic shared memory of one block (sized for FP64): the largest of the
 // band window (band_chol_window_range), the spike window, the products'
-// staging, the separator chain and inverse, and the solve rings; plus the
+// staging, the separator reduction, and the solve rings; plus the
 // per-thread Gram columns when they also fit.
 __host__ __device__ inline size_t band_grid_smem_need(int bw) {
   const size_t e = sizeof(double);
@@ -80,7 +90,7 @@ __host__ __device__ inline size_t band_grid_smem_need(int bw) {
   size_t need = ((B * B * e + 7) & ~size_t(7)) + size_t(bw) * (bw + 1) / 2 * 4;
   const size_t spike = (size_t(bw) + 1) * bw * e + 256 * e;
   const size_t prod = size_t(bw) * bw * e + 32 * 4 * ((size_t(bw) + 3) / 4) * e;
-  const size_t chain = 2 * size_t(bw) * sep_pitch(bw) * e + 32 * 33 * e + 64;
+  const size_t chain = (2 * (size_t(bw) * sep_pitch(bw) + 4) + 3 * 128 + 256 + 2 * 16) * e;
   const size_t solve = (128 + kBandRing * 128 + kBandRing) * e + 512 * e;
   if (spike > need) need = spike;
   if (prod > need) need = prod;
@@ -156,7 +166,7 @@ __device__ __forceinline__ void tri_tile(int u, int& a, int& b) {
 // while the current one is applied.
 // ---------------------------------------------------------------------------
 template <typename T, class S>
-__device__ void bandp_spike(S& s, const BandParts& bp, int k) {
+__device__ __noinline__ void bandp_spike(S& s, const BandParts& bp, int k) {
   const int bw = s.bw, ldl = bw + 1, B1 = bw + 1;
   const int lo = bp.lo(k), li = bp.li(k);
   const T* L = reinterpret_cast<const T*>(s.Lb);
@@ -198,7 +208,7 @@ __device__ void bandp_spike(S& s, const BandParts& bp, int k) {
 // lower triangle over 32-row chunks of W_L staged in shared memory.
 // ---------------------------------------------------------------------------
 template <typename T, class S>
-__device__ void bandp_products(S& s, const BandParts& bp, int k) {
+__device__ __noinline__ void bandp_products(S& s, const BandParts& bp, int k) {
   const int bw = s.bw, ldl = bw + 1;
   const int lo = bp.lo(k), li = bp.li(k);
   const T* WL = part_wl<T>(s, bp, k);
@@ -277,336 +287,344 @@ __device__ void bandp_products(S& s, const BandParts& bp, int k) {
 }
 
 // ---------------------------------------------------------------------------
-// One warp factors the pw x pw (pw <= 32) diagonal block at M[o][o] (pitch
-// ldm) in place, rows and columns beyond pw taken as the identity, and
-// writes the inverse of the factor to inv32 (32 x 33).  Crout order: lane
-// r holds row r; one reciprocal square root per pivot.  Returns 0 or the
-// 1-based column of a non-positive pivot.
+// Staged separator blocks.  A row-major bw x bw block is staged in shared
+// memory column-major with an odd pitch ldm: S(i, j) = buf[j * ldm + i]
+// (trans: S(i, j) = src[j][i]), by asynchronous copies that are all in
+// flight at once (one commit group); stage_wait ends the group for the
+// whole block.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __noinline__ int warp_chol_panel(T* M, int ldm, int o, int pw, T* inv32, int lane) {
-  const bool live = lane < pw;
-  T* Lr = M + size_t(o + (live ? lane : 0)) * ldm + o;
-  T idg[32];
-  int bad = 0;
-  {
-    T a[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) a[j] = (live && j <= lane) ? Lr[j] : (j == lane ? T(1) : T(0));
-#pragma unroll
-    for (int c = 0; c < 32; ++c) {
-      T sr = a[c];
-      if (c < pw) {
-        const T* Lc = M + size_t(o + c) * ldm + o;
-        T s0 = a[c], s1 = T(0);
-#pragma unroll
-        for (int q = 0; q < c; ++q) {
-          if (q & 1) {
-            s1 = fma(-a[q], Lc[q], s1);
-          } else {
-            s0 = fma(-a[q], Lc[q], s0);
-          }
-        }
-        sr = s0 + s1;
-      }
-      const T piv = __shfl_sync(0xffffffffu, sr, c);
-      if (c < pw && !(piv > T(0)) && bad == 0) bad = c + 1;
-      const T il = c < pw ? rsqrt(piv) : T(1);
-      idg[c] = il;
-      if (lane == c) {
-        a[c] = piv * il;
-      } else if (lane > c) {
-        a[c] = sr * il;
-      }
-      if (live && lane >= c && c < pw) Lr[c] = a[c];
-      __syncwarp();
-    }
+__device__ void stage_async(T* buf, int ldm, const T* src, int bw, bool trans) {
+  for (int e = threadIdx.x; e < bw * bw; e += kGridBT) {
+    const int r = e / bw, c = e - r * bw;
+    cp_async_elem(trans ? buf + r * ldm + c : buf + c * ldm + r, src + e, true);
   }
-  if (bad) return bad;
-  T x[32];
-#pragma unroll
-  for (int r = 0; r < 32; ++r) {
-    if (r < pw) {
-      const T* Lrow = M + size_t(o + r) * ldm + o;
-      T a0 = T(0), a1 = T(0);
-#pragma unroll
-      for (int q = 0; q < r; ++q) {
-        if (q >= lane) {
-          if (q & 1) {
-            a1 = fma(Lrow[q], x[q], a1);
-          } else {
-            a0 = fma(Lrow[q], x[q], a0);
-          }
-        }
-      }
-      x[r] = r < lane ? T(0) : (r == lane ? idg[r] : -(a0 + a1) * idg[r]);
-    } else {
-      x[r] = r == lane ? T(1) : T(0);
-    }
+}
+__device__ __forceinline__ void stage_wait() {
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+}
+template <typename T>
+__device__ void unstage(T* dst, const T* buf, int ldm, int bw) {
+  for (int e = threadIdx.x; e < bw * bw; e += kGridBT) {
+    const int r = e / bw, c = e - r * bw;
+    dst[e] = buf[c * ldm + r];
   }
-#pragma unroll
-  for (int r = 0; r < 32; ++r) inv32[r * 33 + lane] = x[r];
-  return 0;
 }
 
-// ---------------------------------------------------------------------------
-// The separator chain (one block): for k = 0 .. P-2, D_k = Dp_k - Q_k -
-// F_{k-1} F_{k-1}^T, then the blocked Cholesky of the stacked [D_k; E_k]
-// (32-column panels: warp_chol_panel on the diagonal block, the rows below
-// times its inverse, a rank-32 update of the trailing columns in 4 x 4
-// register tiles) gives Lc_k (top, lower, l_cc on the diagonal) and F_k
-// (bottom).  F_k stays in shared memory for the next separator.
-// Returns 0 or the 1-based global column of a non-positive pivot.
-// ---------------------------------------------------------------------------
-template <typename T, class S>
-__device__ int bandp_chain(S& s, const BandParts& bp) {
-  const int bw = s.bw, ldm = sep_pitch(bw);
-  const int lt = threadIdx.x, warp = lt >> 5, lane = lt & 31;
-  T* Mt = reinterpret_cast<T*>(s.bwin);
-  T* Mb = Mt + size_t(bw) * ldm;
-  T* inv32 = Mb + size_t(bw) * ldm;
-  int* flag = reinterpret_cast<int*>(inv32 + 32 * 33);
-  const int nt4 = (bw + 3) / 4;
-  for (int k = 0; k < bp.P - 1; ++k) {
-    const T* Dg = sep_block<T>(s, k, kSbD);
-    const T* Qg = sep_block<T>(s, k, kSbQ);
-    // 1. Top block (lower triangle).
-    if (k == 0) {
-      for (int e = lt; e < bw * bw; e += kGridBT) {
-        const int i = e / bw, j = e - i * bw;
-        if (j <= i) Mt[i * ldm + j] = Dg[e] - Qg[e];
-      }
-    } else {
-      const int ntiles = nt4 * (nt4 + 1) / 2;
-      for (int u = lt; u < ntiles; u += kGridBT) {
-        int ta, tb;
-        tri_tile(u, ta, tb);
-        T acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-        int ra[4], rb[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          ra[i] = min(4 * ta + i, bw - 1) * ldm;
-          rb[i] = min(4 * tb + i, bw - 1) * ldm;
-        }
-        for (int c = 0; c < bw; ++c) {
-          T a[4], b[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            a[i] = Mb[ra[i] + c];
-            b[i] = Mb[rb[i] + c];
-          }
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int a = 4 * ta + i, b = 4 * tb + j;
-            if (a < bw && b <= a)
-              Mt[a * ldm + b] = Dg[size_t(a) * bw + b] - Qg[size_t(a) * bw + b] - acc[i][j];
-          }
-      }
-    }
-    __syncthreads();
-    // 2. Bottom block E_k.
-    const bool has_e = k < bp.P - 2;
-    const int nb = has_e ? bw : 0;
-    if (has_e) {
-      const T* Eg = sep_block<T>(s, k, kSbE);
-      for (int e = lt; e < bw * bw; e += kGridBT) {
-        const int i = e / bw, j = e - i * bw;
-        Mb[i * ldm + j] = Eg[e];
-      }
-    }
-    __syncthreads();
-    // 3. Blocked Cholesky of [Mt; Mb].
-    for (int o = 0; o < bw; o += 32) {
-      const int pw = min(32, bw - o);
-      if (warp == 0) {
-        const int bad = warp_chol_panel<T>(Mt, ldm, o, pw, inv32, lane);
-        if (lane == 0) *flag = bad ? o + bad : 0;
-      }
-      __syncthreads();
-      const int bad = *flag;
-      if (bad) return bp.lo(k) + bp.li(k) + bad;
-      // Rows below the diagonal block: row <- row inv^T (thread per row).
-      const int rows_top = bw - o - pw;
-      for (int r = lt; r < rows_top + nb; r += kGridBT) {
-        T* row = r < rows_top ? Mt + (o + pw + r) * ldm + o : Mb + (r - rows_top) * ldm + o;
-        T v[32];
-#pragma unroll
-        for (int l = 0; l < 32; ++l) v[l] = l < pw ? row[l] : T(0);
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          if (j < pw) {
-            T acc = T(0);
-#pragma unroll
-            for (int l = 0; l <= j; ++l) acc = fma(v[l], inv32[j * 33 + l], acc);
-            row[j] = acc;
-          }
-        }
-      }
-      __syncthreads();
-      // Trailing columns [t0, bw): top rows i >= j, all bottom rows.
-      const int t0 = o + pw;
-      if (t0 < bw) {
-        const int nt = (bw - t0 + 3) / 4;
-        const int ntop = nt * (nt + 1) / 2;
-        const int nbot = ((nb + 3) / 4) * nt;
-        for (int u = lt; u < ntop + nbot; u += kGridBT) {
-          int i0, j0, lim;
-          T* base;
-          if (u < ntop) {
-            int ta, tb;
-            tri_tile(u, ta, tb);
-            i0 = t0 + 4 * ta;
-            j0 = t0 + 4 * tb;
-            base = Mt;
-            lim = bw;
-          } else {
-            const int v = u - ntop;
-            const int ta = v / nt, tb = v - ta * nt;
-            i0 = 4 * ta;
-            j0 = t0 + 4 * tb;
-            base = Mb;
-            lim = nb;
-          }
-          T acc[4][4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-          int ra[4], rb[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            ra[i] = min(i0 + i, lim - 1) * ldm + o;
-            rb[i] = min(j0 + i, bw - 1) * ldm + o;
-          }
-          for (int l = 0; l < pw; ++l) {
-            T a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              a[i] = base[ra[i] + l];
-              b[i] = Mt[rb[i] + l];
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-              for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-          }
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const int a = i0 + i, b = j0 + j;
-              const bool ok = u < ntop ? (a < bw && b <= a) : (a < nb && b < bw);
-              if (ok) base[a * ldm + b] -= acc[i][j];
-            }
-        }
-      }
-      __syncthreads();
-    }
-    // 4. Lc_k and F_k to global memory.
-    T* Lg = sep_block<T>(s, k, kSbL);
-    T* Fg = sep_block<T>(s, k, kSbF);
-    for (int e = lt; e < bw * bw; e += kGridBT) {
-      const int i = e / bw, j = e - i * bw;
-      Lg[e] = j <= i ? Mt[i * ldm + j] : T(0);
-      if (has_e) Fg[e] = Mb[i * ldm + j];
-    }
-    __syncthreads();
-  }
-  return 0;
+// One FP64 tensor-core step d += a b (mma.sync m8n8k4, row.col): lane l
+// holds a = A[l/4][l%4], b = B[l%4][l/4] and the accumulator entries
+// (l/4, 2 (l%4)) and (l/4, 2 (l%4) + 1).
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
 }
 
-// ---------------------------------------------------------------------------
-// Per separator k (one block): Li_k = Lc_k^{-1} (thread per column), then
-// G_k = Li_k F_{k-1} (k >= 1) and H_k = (F_k Li_k)^T (k <= P-3).
-// ---------------------------------------------------------------------------
-template <typename T, class S>
-__device__ void bandp_sep_inverse(S& s, const BandParts& bp, int k) {
-  const int bw = s.bw, ldm = sep_pitch(bw);
+// The FP64 form of smem_gemm_nt on the FP64 tensor cores: each warp takes
+// 16 x 16 blocks of the output (2 x 2 independent 8 x 8 accumulators),
+// operands read straight from the staged blocks (zero beyond i1, j1, K).
+template <class Fn>
+__device__ __forceinline__ void smem_gemm_nt_dmma(const double* A, const double* B, int ldm, int K,
+                                                  int i0, int i1, int j0, int j1, bool lower,
+                                                  Fn fn) {
+  if (i1 <= i0 || j1 <= j0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gi = lane >> 2, tg = lane & 3;
+  const int ni = (i1 - i0 + 15) / 16, nj = (j1 - j0 + 15) / 16;
+  for (int t = warp; t < ni * nj; t += kGridBT / 32) {
+    const int ti = t % ni, tj = t / ni;
+    const int ib = i0 + 16 * ti, jb = j0 + 16 * tj;
+    if (lower && ib + 15 < jb) continue;  // above the diagonal
+    double acc[2][2][2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int n = 0; n < 2; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+    int ia[2], jc[2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      ia[m] = ib + 8 * m + gi;
+      jc[m] = jb + 8 * m + gi;
+    }
+#pragma unroll 2
+    for (int c0 = 0; c0 < K; c0 += 4) {
+      const int c = c0 + tg;
+      double a[2], b[2];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        a[m] = (c < K && ia[m] < i1) ? A[c * ldm + ia[m]] : 0.0;
+        b[m] = (c < K && jc[m] < j1) ? B[c * ldm + jc[m]] : 0.0;
+      }
+#pragma unroll
+      for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) dmma_8x8x4(acc[m][n], a[m], b[n]);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int n = 0; n < 2; ++n)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int i = ia[m], j = jb + 8 * n + 2 * tg + e;
+          if (i < i1 && j < j1 && (!lower || j <= i)) fn(i, j, acc[m][n][e]);
+        }
+  }
+}
+
+// acc(i, j) = sum_{c < K} A(i, c) B(j, c) for i in [i0, i1), j in [j0, j1)
+// (lower: j <= i only), A and B staged column-major (pitch ldm); fn(i, j,
+// acc) for each.  FP64: on the FP64 tensor cores (smem_gemm_nt_dmma).  4 x 4 register tiles: the tile's rows are strided across
+// the lanes (consecutive lanes, consecutive rows: no bank conflicts with an
+// odd pitch), its columns contiguous (the same for most of a warp).
+template <typename T, class Fn>
+__device__ __forceinline__ void smem_gemm_nt(const T* A, const T* B, int ldm, int K, int i0,
+                                             int i1, int j0, int j1, bool lower, Fn fn) {
+  if constexpr (sizeof(T) == 8) {
+    smem_gemm_nt_dmma(A, B, ldm, K, i0, i1, j0, j1, lower, fn);
+    return;
+  }
+  if (i1 <= i0 || j1 <= j0) return;
+  const int ni = (i1 - i0 + 3) / 4, nj = (j1 - j0 + 3) / 4;
+  for (int u = threadIdx.x; u < ni * nj; u += kGridBT) {
+    const int tj = u / ni, ti = u - tj * ni;
+    const int jb = j0 + 4 * tj;
+    if (lower && min(i0 + ti + 3 * ni, i1 - 1) < jb) continue;  // above the diagonal
+    int ia[4], jc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ia[q] = min(i0 + ti + ni * q, i1 - 1);
+      jc[q] = min(jb + q, j1 - 1);
+    }
+    T acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[p][q] = T(0);
+#pragma unroll 2
+    for (int c = 0; c < K; ++c) {
+      const T* ac = A + c * ldm;
+      const T* bc = B + c * ldm;
+      T a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = ac[ia[q]];
+        b[q] = bc[jc[q]];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int i = i0 + ti + ni * p;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = jb + q;
+        if (i < i1 && j < j1 && (!lower || j <= i)) fn(i, j, acc[p][q]);
+      }
+    }
+  }
+}
+
+// Panel width of the blocked Cholesky of a separator block.
+constexpr int kPanel = 16;
+
+// Blocked Cholesky of the stacked [Mt; Mb] (Mt: bw x bw, lower; Mb: nb x bw
+// rows below it), both staged column-major.  Each kPanel-column panel is
+// factorised tall-skinny in registers: thread r holds the panel's entries of
+// row r (top rows from the panel's diagonal down, then every bottom row); per
+// column the diagonal block's rows publish their entries (double-buffered),
+// one barrier, then every row scales its entry by one reciprocal square
+// root of the pivot and updates the rest of its panel row.  The trailing
+// columns then take a rank-kPanel update (tiled products).  Mt becomes L,
+// Mb becomes Mb L^{-T}; needs bw - o + nb <= kGridBT rows per panel.
+// pub: 2 x kPanel scratch.  Returns 0 or the 1-based column of a
+// non-positive pivot (the same in every thread).
+template <typename T>
+__device__ __noinline__ int smem_chol_stacked(T* Mt, T* Mb, int nb, int bw, int ldm, T* pub) {
   const int lt = threadIdx.x;
-  T* Ls = reinterpret_cast<T*>(s.bwin);
-  T* X = Ls + size_t(bw) * ldm;
-  T* idg = X + size_t(bw) * ldm;
-  const T* Lg = sep_block<T>(s, k, kSbL);
-  for (int e = lt; e < bw * bw; e += kGridBT) {
-    const int i = e / bw, j = e - i * bw;
-    Ls[i * ldm + j] = Lg[e];
-  }
-  __syncthreads();
-  if (lt < bw) idg[lt] = T(1) / Ls[lt * ldm + lt];
-  __syncthreads();
-  if (lt < bw) {
-    const int t = lt;
-    for (int r = 0; r < t; ++r) X[r * ldm + t] = T(0);
-    X[t * ldm + t] = idg[t];
-    for (int r = t + 1; r < bw; ++r) {
-      T a0 = T(0), a1 = T(0);
-      int c = t;
-      for (; c + 1 < r; c += 2) {
-        a0 = fma(Ls[r * ldm + c], X[c * ldm + t], a0);
-        a1 = fma(Ls[r * ldm + c + 1], X[(c + 1) * ldm + t], a1);
+  for (int o = 0; o < bw; o += kPanel) {
+    const int pw = min(kPanel, bw - o);
+    const int rows_top = bw - o;
+    const bool own = lt < rows_top + nb;
+    T* base = lt < rows_top ? Mt + o + lt : Mb + (lt - rows_top);
+    T v[kPanel];
+#pragma unroll
+    for (int l = 0; l < kPanel; ++l) v[l] = (own && l < pw) ? base[(o + l) * ldm] : T(0);
+    int bad = 0;
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) {
+      if (c < pw) {
+        T* pc = pub + (c & 1) * kPanel;
+        if (lt >= c && lt < pw) pc[lt] = v[c];
+        __syncthreads();
+        const T piv = pc[c];
+        if (!(piv > T(0))) {
+          bad = c + 1;
+          break;
+        }
+        const T il = rsqrt(piv);
+        if (own) {
+          if (lt == c) {
+            v[c] = piv * il;
+          } else if (lt > c) {
+            const T lic = v[c] * il;
+            v[c] = lic;
+#pragma unroll
+            for (int j = c + 1; j < kPanel; ++j)
+              if (j < pw) v[j] = fma(-lic, pc[j] * il, v[j]);
+          }
+        }
       }
-      if (c < r) a0 = fma(Ls[r * ldm + c], X[c * ldm + t], a0);
-      X[r * ldm + t] = -(a0 + a1) * idg[r];
     }
+    if (bad) return o + bad;
+    if (own) {
+#pragma unroll
+      for (int l = 0; l < kPanel; ++l)
+        if (l < pw) base[(o + l) * ldm] = v[l];
+    }
+    __syncthreads();
+    const int t0 = o + pw;
+    const T* Pt = Mt + o * ldm;
+    smem_gemm_nt<T>(Pt, Pt, ldm, pw, t0, bw, t0, bw, true,
+                    [&](int i, int j, T acc) { Mt[j * ldm + i] -= acc; });
+    smem_gemm_nt<T>(Mb + o * ldm, Pt, ldm, pw, 0, nb, t0, bw, false,
+                    [&](int i, int j, T acc) { Mb[j * ldm + i] -= acc; });
+    __syncthreads();
+  }
+  return 0;
+}
+
+// Shared-memory layout of the reduction phases: two staged blocks, three
+// vectors of 128, a 256-slot reduction scratch and the Cholesky panel's
+// publish slots.
+template <typename T>
+struct CrSmem {
+  T* Mt;
+  T* Mb;
+  T* vec;
+  T* red;
+  T* pub;
+  __device__ CrSmem(double* base, int bw, int ldm) {
+    Mt = reinterpret_cast<T*>(base);
+    Mb = Mt + bw * ldm + 4;
+    vec = Mb + bw * ldm + 4;
+    red = vec + 3 * 128;
+    pub = red + 256;
+  }
+};
+
+// The start and end of separator k (k < P - 1): [hi_k, hi_k + bw).
+__device__ __forceinline__ int sep_start(const BandParts& bp, int k) {
+  return bp.lo(k) + bp.li(k);
+}
+
+// Reduction level l, eliminated separator j = 2^l (2 b + 1) (1-based;
+// block b): the Cholesky of the stacked [D_j; I] gives L_j^{-T}, then Di_j =
+// L_j^{-T} L_j^{-1}, Yl_j = Di_j Cl_j, Yr_j = Di_j Cr_j^T (tiled products),
+// and a copy of Cr_j (its slot is rewritten at this level by j + 2^l).
+template <typename T, class S>
+__device__ __noinline__ int bandp_cr_eliminate(S& s, const BandParts& bp, int l, int j) {
+  const int bw = s.bw, ldm = sep_pitch(bw), N = bp.P - 1, h = 1 << l, k = j - 1;
+  CrSmem<T> sm(s.bwin, bw, ldm);
+  QTQP_TIC();
+  stage_async(sm.Mt, ldm, sep_block<T>(s, k, kSbD), bw, false);
+  if (l == 0) stage_async(sm.Mb, ldm, sep_block<T>(s, k, kSbQ), bw, false);
+  stage_wait();
+  for (int e = threadIdx.x; e < bw * bw; e += kGridBT) {
+    const int c = e / bw, i = e - c * bw;
+    if (l == 0 && i >= c) sm.Mt[c * ldm + i] -= sm.Mb[c * ldm + i];
   }
   __syncthreads();
+  for (int e = threadIdx.x; e < bw * bw; e += kGridBT) {
+    const int c = e / bw, i = e - c * bw;
+    sm.Mb[c * ldm + i] = i == c ? T(1) : T(0);
+  }
+  __syncthreads();
+  QTQP_TOC(kPhBpCrStage);
+  QTQP_RETIC();
+  const int bad = smem_chol_stacked<T>(sm.Mt, sm.Mb, bw, bw, ldm, sm.pub);
+  if (bad) return sep_start(bp, k) + bad;
+  QTQP_TOC(kPhBpCrSweep);
+  QTQP_RETIC();
+  // Mb(i, c) = (L^{-T})(i, c); Di(i, jj) = sum_c Mb(i, c) Mb(jj, c) into Mt.
   T* Ig = sep_block<T>(s, k, kSbI);
-  for (int e = lt; e < bw * bw; e += kGridBT) {
-    const int i = e / bw, j = e - i * bw;
-    Ig[e] = X[i * ldm + j];
-  }
-  if (k >= 1) {  // G_k = Li_k F_{k-1}: G[a][b] = sum_{c <= a} X[a][c] F[c][b]
-    const T* Fg = sep_block<T>(s, k - 1, kSbF);
+  smem_gemm_nt<T>(sm.Mb, sm.Mb, ldm, bw, 0, bw, 0, bw, true, [&](int i, int jj, T acc) {
+    sm.Mt[jj * ldm + i] = acc;
+    sm.Mt[i * ldm + jj] = acc;
+  });
+  __syncthreads();
+  unstage(Ig, sm.Mt, ldm, bw);
+  for (int side = 0; side < 2; ++side) {
+    const bool has = side == 0 ? j - h >= 1 : j + h <= N;
+    if (!has) continue;
+    // Staged so that Mb(jj, c) is column jj of Cl (side 0) or row jj of Cr.
+    const T* src = side == 0 ? (l == 0 ? sep_block<T>(s, k - 1, kSbE) : sep_block<T>(s, k, kSbC))
+                             : (l == 0 ? sep_block<T>(s, k, kSbE) : sep_block<T>(s, k + h, kSbC));
     __syncthreads();
-    for (int e = lt; e < bw * bw; e += kGridBT) {
-      const int i = e / bw, j = e - i * bw;
-      Ls[i * ldm + j] = Fg[e];
-    }
-    __syncthreads();
-    T* Gg = sep_block<T>(s, k, kSbG);
-    for (int e = lt; e < bw * bw; e += kGridBT) {
-      const int a = e / bw, b = e - a * bw;
-      T acc = T(0);
-      for (int c = 0; c <= a; ++c) acc = fma(X[a * ldm + c], Ls[c * ldm + b], acc);
-      Gg[e] = acc;
-    }
-  }
-  if (k <= bp.P - 3) {  // H_k = (F_k Li_k)^T: H[a][b] = sum_{c >= a} F[b][c] X[c][a]
-    const T* Fg = sep_block<T>(s, k, kSbF);
-    __syncthreads();
-    for (int e = lt; e < bw * bw; e += kGridBT) {
-      const int i = e / bw, j = e - i * bw;
-      Ls[i * ldm + j] = Fg[e];
-    }
-    __syncthreads();
-    T* Hg = sep_block<T>(s, k, kSbH);
-    for (int e = lt; e < bw * bw; e += kGridBT) {
-      const int a = e / bw, b = e - a * bw;
-      T acc = T(0);
-      for (int c = a; c < bw; ++c) acc = fma(Ls[b * ldm + c], X[c * ldm + a], acc);
-      Hg[e] = acc;
-    }
+    stage_async(sm.Mb, ldm, src, bw, side == 0);
+    stage_wait();
+    if (side == 1) unstage(sep_block<T>(s, k, kSbR), sm.Mb, ldm, bw);
+    T* Y = sep_block<T>(s, k, side == 0 ? kSbXl : kSbXr);
+    smem_gemm_nt<T>(sm.Mt, sm.Mb, ldm, bw, 0, bw, 0, bw, false,
+                    [&](int i, int jj, T acc) { Y[size_t(i) * bw + jj] = acc; });
   }
   __syncthreads();
+  QTQP_TOC(kPhBpCrGemm);
+  return 0;
+}
+
+// Reduction level l, surviving separator j' = 2^(l+1) (b + 1) (block b):
+// D_j' -= Cr Yr of the left neighbour jl = j' - 2^l (and Q at level 0),
+// its new left coupling -Cr Yl of jl, and D_j' -= Cl^T Yl of the right
+// neighbour jr = j' + 2^l.  D (lower, row-major) is updated in place.
+template <typename T, class S>
+__device__ __noinline__ void bandp_cr_gather(S& s, const BandParts& bp, int l, int jp) {
+  const int bw = s.bw, ldm = sep_pitch(bw), N = bp.P - 1, h = 1 << l, k = jp - 1;
+  CrSmem<T> sm(s.bwin, bw, ldm);
+  QTQP_TIC();
+  const int kl = jp - h - 1;
+  T* D = sep_block<T>(s, k, kSbD);
+  const T* Q = sep_block<T>(s, k, kSbQ);
+  stage_async(sm.Mt, ldm, sep_block<T>(s, kl, kSbR), bw, false);
+  stage_async(sm.Mb, ldm, sep_block<T>(s, kl, kSbXr), bw, true);
+  stage_wait();
+  smem_gemm_nt<T>(sm.Mt, sm.Mb, ldm, bw, 0, bw, 0, bw, true, [&](int i, int jj, T acc) {
+    const size_t e = size_t(i) * bw + jj;
+    D[e] -= l == 0 ? acc + Q[e] : acc;
+  });
+  __syncthreads();
+  if (jp - 2 * h >= 1) {
+    stage_async(sm.Mb, ldm, sep_block<T>(s, kl, kSbXl), bw, true);
+    stage_wait();
+    T* Cn = sep_block<T>(s, k, kSbC);
+    smem_gemm_nt<T>(sm.Mt, sm.Mb, ldm, bw, 0, bw, 0, bw, false,
+                    [&](int i, int jj, T acc) { Cn[size_t(i) * bw + jj] = -acc; });
+    __syncthreads();
+  }
+  if (jp + h <= N) {
+    const int kr = jp + h - 1;
+    stage_async(sm.Mt, ldm, l == 0 ? sep_block<T>(s, k, kSbE) : sep_block<T>(s, kr, kSbC), bw,
+                true);
+    stage_async(sm.Mb, ldm, sep_block<T>(s, kr, kSbXl), bw, true);
+    stage_wait();
+    smem_gemm_nt<T>(sm.Mt, sm.Mb, ldm, bw, 0, bw, 0, bw, true,
+                    [&](int i, int jj, T acc) { D[size_t(i) * bw + jj] -= acc; });
+    __syncthreads();
+  }
+  QTQP_TOC(kPhBpCrGather);
 }
 
 // ---------------------------------------------------------------------------
 // The partitioned factorisation (grid mode).  Every block of the grid takes
 // part in the Gram matrix; block k < P eliminates interior k (and forms its
-// spike products), block 0 runs the separator chain, block k < P-1 inverts
-// separator k.  Returns the same value in every thread: 0 or the 1-based
-// column of a non-positive pivot.
+// spike products); the separators are reduced level by level.  Returns the
+// same value in every thread: 0 or the 1-based column of a non-positive
+// pivot.
 // ---------------------------------------------------------------------------
 template <typename T, class S>
 __device__ int bandp_factorize(S& s) {
@@ -638,17 +656,47 @@ __device__ int bandp_factorize(S& s) {
   s.sync();
   QTQP_TOC(kPhBpInterior);
   QTQP_RETIC();
-  if (k == 0 && *info == 0) {
-    const int bad = bandp_chain<T>(s, bp);
-    if (bad != 0 && threadIdx.x == 0) atomicMax(const_cast<int*>(info), bad);
+  const int N = bp.P - 1;
+  for (int l = 0; (1 << l) <= N; ++l) {
+    const int h = 1 << l;
+    const int j = h * (2 * k + 1);
+    // Another block may record a failure during this phase: the block
+    // agrees on one reading of the status before it branches.
+    const bool ok = __syncthreads_and(*info == 0) != 0;
+    if (j <= N && ok) {
+      const int bad = bandp_cr_eliminate<T>(s, bp, l, j);
+      if (bad != 0 && threadIdx.x == 0) atomicMax(const_cast<int*>(info), bad);
+    }
+    s.sync();
+    const int jp = 2 * h * (k + 1);
+    if (jp <= N && *info == 0) bandp_cr_gather<T>(s, bp, l, jp);
+    s.sync();
   }
-  s.sync();
   QTQP_TOC(kPhBpChain);
-  QTQP_RETIC();
-  if (*info == 0 && k < bp.P - 1) bandp_sep_inverse<T>(s, bp, k);
-  s.sync();
-  QTQP_TOC(kPhBpSepInv);
   return *info;
+}
+
+// Row / column matrix-vector products with a staged block, two halves of
+// the block over the inner index, combined through red (256 slots):
+// rows: y[i] = sum_c S(i, c) x[c]; cols: y[c] = sum_i S(i, c) x[i].
+// Thread i (< bw) receives y[i].
+template <typename T>
+__device__ __forceinline__ T smem_matvec(const T* S, int ldm, int bw, const T* x, bool cols,
+                                         T* red) {
+  const int i = threadIdx.x & 127, half = threadIdx.x >> 7;
+  T acc = T(0);
+  if (i < bw) {
+    if (cols) {
+      for (int c = half; c < bw; c += 2) acc = fma(S[i * ldm + c], x[c], acc);
+    } else {
+      for (int c = half; c < bw; c += 2) acc = fma(S[c * ldm + i], x[c], acc);
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  const T y = threadIdx.x < 128 ? red[threadIdx.x] + red[threadIdx.x + 128] : T(0);
+  __syncthreads();
+  return y;
 }
 
 // ---------------------------------------------------------------------------
@@ -657,14 +705,16 @@ __device__ int bandp_factorize(S& s) {
 // ---------------------------------------------------------------------------
 template <typename T, class S>
 __device__ void bandp_solve(S& s, T* v, T* w) {
-  const int bw = s.bw;
+  const int bw = s.bw, ldm = sep_pitch(bw);
   const BandParts bp(s.n, bw, s.nparts);
-  const int P = bp.P, k = blockIdx.x, lt = threadIdx.x, lane = lt & 31, warp = lt >> 5;
+  const int P = bp.P, N = P - 1, k = blockIdx.x, lt = threadIdx.x, lane = lt & 31,
+            warp = lt >> 5;
   constexpr int kNW = kGridBT / 32;
   // Scratch after the solve rings (band_fwd_range / band_bwd_range).
   T* scr = reinterpret_cast<T*>(s.bwin) + (128 + kBandRing * 128 + kBandRing);
   QTQP_TIC();
-  // Forward per interior; t_k's spike term W_L^T y of interior k+1.
+  // Forward per interior; the spike term W_L^T y of interior k for
+  // separator k - 1.
   if (k < P) {
     const int lo = bp.lo(k), li = bp.li(k), hi = lo + li, R = hi + (k < P - 1 ? bw : 0);
     if (warp == 0) s.template band_fwd_range<T>(v, w, lo, li, R, lane);
@@ -683,81 +733,71 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
   s.sync();
   QTQP_TOC(kPhBpFwd);
   QTQP_RETIC();
-  // u_k = Li_k (v[S_k] - W_L^T y).
-  if (k < P - 1) {
-    const int hi = bp.lo(k) + bp.li(k);
-    const T* cl = sep_vec<T>(s, k, kSvCL);
-    if (lt < bw) scr[lt] = v[hi + lt] - cl[lt];
-    __syncthreads();
-    const T* Li = sep_block<T>(s, k, kSbI);
-    T* u = sep_vec<T>(s, k, kSvU);
-    for (int a = warp; a < bw; a += kNW) {
-      T acc = T(0);
-      for (int c = lane; c <= a; c += 32) acc = fma(Li[size_t(a) * bw + c], scr[c], acc);
-      acc = warp_sum(acc);
-      if (lane == 0) u[a] = acc;
+  CrSmem<T> sm(s.bwin, bw, ldm);
+  T* t = sm.vec;
+  T* xa = sm.vec + 128;
+  T* xb = sm.vec + 256;
+  T* red = sm.red;
+  // t_j at level 0 is v[S] - W_L^T y; later levels keep it in kSvT.
+  auto load_t = [&](int l, int kk) {
+    if (lt < bw)
+      t[lt] = l == 0 ? v[sep_start(bp, kk) + lt] - sep_vec<T>(s, kk, kSvCL)[lt]
+                     : sep_vec<T>(s, kk, kSvT)[lt];
+  };
+  int levels = 0;
+  while ((1 << levels) <= N) ++levels;
+  for (int l = 0; l < levels; ++l) {
+    const int h = 1 << l;
+    const int j = h * (2 * k + 1);
+    if (j <= N) {  // z_j = Di_j t_j
+      load_t(l, j - 1);
+      stage_async(sm.Mt, ldm, sep_block<T>(s, j - 1, kSbI), bw, false);
+      stage_wait();
+      const T z = smem_matvec(sm.Mt, ldm, bw, t, false, red);
+      if (lt < bw) sep_vec<T>(s, j - 1, kSvZ)[lt] = z;
     }
-  }
-  s.sync();
-  // Chain z_k = u_k - G_k z_{k-1} (block 0).
-  if (k == 0) {
-    for (int j = 0; j < P - 1; ++j) {
-      T* zs = scr + (j & 1) * 128;
-      const T* zp = scr + ((j + 1) & 1) * 128;
-      const T* u = sep_vec<T>(s, j, kSvU);
-      const T* G = sep_block<T>(s, j, kSbG);
-      T* z = sep_vec<T>(s, j, kSvZ);
-      for (int a = warp; a < bw; a += kNW) {
-        T acc = T(0);
-        if (j > 0)
-          for (int c = lane; c < bw; c += 32) acc = fma(G[size_t(a) * bw + c], zp[c], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) {
-          const T zv = u[a] - acc;
-          zs[a] = zv;
-          z[a] = zv;
-        }
+    s.sync();
+    const int jp = 2 * h * (k + 1);
+    if (jp <= N) {  // t_j' -= Cr z (left neighbour) + Cl^T z (right neighbour)
+      load_t(l, jp - 1);
+      const int kl = jp - h - 1, kr = jp + h - 1;
+      if (lt < bw) xa[lt] = sep_vec<T>(s, kl, kSvZ)[lt];
+      stage_async(sm.Mt, ldm, sep_block<T>(s, kl, kSbR), bw, false);
+      stage_wait();
+      T acc = smem_matvec(sm.Mt, ldm, bw, xa, false, red);
+      if (jp + h <= N) {
+        if (lt < bw) xb[lt] = sep_vec<T>(s, kr, kSvZ)[lt];
+        stage_async(sm.Mt, ldm, l == 0 ? sep_block<T>(s, jp - 1, kSbE) : sep_block<T>(s, kr, kSbC),
+                    bw, false);
+        stage_wait();
+        acc += smem_matvec(sm.Mt, ldm, bw, xb, true, red);
       }
-      __syncthreads();
+      if (lt < bw) sep_vec<T>(s, jp - 1, kSvT)[lt] = t[lt] - acc;
     }
+    s.sync();
   }
-  s.sync();
-  // v_k = Li_k^T z_k.
-  if (k < P - 1) {
-    const T* Li = sep_block<T>(s, k, kSbI);
-    const T* z = sep_vec<T>(s, k, kSvZ);
-    const int a = lt & 127, g = lt >> 7;
-    T acc = T(0);
-    if (a < bw)
-      for (int c = a + g; c < bw; c += 2) acc = fma(Li[size_t(c) * bw + a], z[c], acc);
-    scr[lt] = acc;
-    __syncthreads();
-    if (lt < bw) sep_vec<T>(s, k, kSvV)[lt] = scr[lt] + scr[lt + 128];
-  }
-  s.sync();
-  // Chain x_k = v_k - H_k x_{k+1} (block 0), into the separator rows of v.
-  if (k == 0) {
-    for (int j = P - 2; j >= 0; --j) {
-      T* xs = scr + (j & 1) * 128;
-      const T* xn = scr + ((j + 1) & 1) * 128;
-      const T* vv = sep_vec<T>(s, j, kSvV);
-      const T* H = sep_block<T>(s, j, kSbH);
-      const int hi = bp.lo(j) + bp.li(j);
-      for (int a = warp; a < bw; a += kNW) {
-        T acc = T(0);
-        if (j < P - 2)
-          for (int c = lane; c < bw; c += 32) acc = fma(H[size_t(a) * bw + c], xn[c], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) {
-          const T xv = vv[a] - acc;
-          xs[a] = xv;
-          v[hi + a] = xv;
-        }
+  for (int l = levels - 1; l >= 0; --l) {
+    const int h = 1 << l;
+    const int j = h * (2 * k + 1);
+    if (j <= N) {  // x_j = z_j - Yl_j x_left - Yr_j x_right
+      const int kk = j - 1;
+      T r = lt < bw ? sep_vec<T>(s, kk, kSvZ)[lt] : T(0);
+      if (j - h >= 1) {
+        if (lt < bw) xa[lt] = v[sep_start(bp, j - h - 1) + lt];
+        stage_async(sm.Mt, ldm, sep_block<T>(s, kk, kSbXl), bw, false);
+        stage_wait();
+        r -= smem_matvec(sm.Mt, ldm, bw, xa, false, red);
       }
-      __syncthreads();
+      if (j + h <= N) {
+        if (lt < bw) xb[lt] = v[sep_start(bp, j + h - 1) + lt];
+        stage_async(sm.Mt, ldm, sep_block<T>(s, kk, kSbXr), bw, false);
+        stage_wait();
+        r -= smem_matvec(sm.Mt, ldm, bw, xb, false, red);
+      }
+      if (lt < bw) v[sep_start(bp, kk) + lt] = r;
     }
+    s.sync();
   }
-  s.sync();
   QTQP_TOC(kPhBpChains);
   QTQP_RETIC();
   // Backward per interior after removing W_L x_{S_{k-1}}.

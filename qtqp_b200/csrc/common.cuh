@@ -260,7 +260,9 @@ enum Phase : int {
   // Sub-phases of the large (grid-mode) factorisation and solves.
   kPhLgDiag, kPhLgPanel, kPhLgTrail, kPhLgInv, kPhLgFwd, kPhLgBwd,
   // Sub-phases of the partitioned banded factorisation and solves.
-  kPhBpInterior, kPhBpChain, kPhBpSepInv, kPhBpFwd, kPhBpChains, kPhBpBwd, kNumPhases
+  kPhBpInterior, kPhBpChain, kPhBpFwd, kPhBpChains, kPhBpBwd,
+  // Steps of one reduction level (per participating block).
+  kPhBpCrStage, kPhBpCrSweep, kPhBpCrGemm, kPhBpCrGather, kNumPhases
 };
 #ifdef QTQP_PHASE_TIMERS
 extern __device__ unsigned long long g_phase_cycles[kNumPhases];
