@@ -313,15 +313,6 @@ __device__ void unstage(T* dst, const T* buf, int ldm, int bw) {
   }
 }
 
-// One FP64 tensor-core step d += a b (mma.sync m8n8k4, row.col): lane l
-// holds a = A[l/4][l%4], b = B[l%4][l/4] and the accumulator entries
-// (l/4, 2 (l%4)) and (l/4, 2 (l%4) + 1).
-__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
-}
-
 // The FP64 form of smem_gemm_nt on the FP64 tensor cores: each warp takes
 // 16 x 16 blocks of the output (2 x 2 independent 8 x 8 accumulators),
 // operands read straight from the staged blocks (zero beyond i1, j1, K).

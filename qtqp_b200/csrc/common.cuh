@@ -245,6 +245,15 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 
+// One FP64 tensor-core step d += a b (mma.sync m8n8k4, row.col; tcgen05 has
+// no FP64 kind): lane l holds a = A[l/4][l%4], b = B[l%4][l/4] and the
+// accumulator entries (l/4, 2 (l%4)) and (l/4, 2 (l%4) + 1).
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

@@ -198,34 +198,39 @@ __device__ void large_gram_tc(S& s) {
   if (threadIdx.x == 0 && *failed) atomicExch(&s.gctl->err, 1);
 }
 
-// ---------------------------------------------------------------------------
-// Gram of the FP64 factor: lower 128 x 128 tiles of A^T diag(1/Ry) A, 8 x 8
-// outputs per thread (rows ty + 16a, columns tx + 16b: conflict-free shared
-// memory reads).  Slices of 16 rows of A (and their 1/Ry) are copied to
-// shared memory with cp.async, double-buffered: slice k+1 is in flight while
-// slice k is multiplied.
-// ---------------------------------------------------------------------------
+// G_lower = A^T diag(1/Ry) A in FP64 on the FP64 tensor cores (DMMA,
+// mma.sync m8n8k4): one CTA per 128 x 128 lower tile; K-slices of 16 rows of
+// A (both column panels) and their weights staged by cp.async in a ring of
+// four buffers (three slices in flight), with a row pitch of 132 so that each half-warp's fragment loads
+// hit 16 different banks; warp w computes the 64 x 32 block (w / 4, w % 4)
+// of the tile with 8 x 4 accumulators of 8 x 8.  Rows and columns beyond
+// m, n are zero-filled.
 template <class S>
-__device__ void large_gram_simt(S& s) {
+__device__ __noinline__ void large_gram_dmma(S& s) {
   const int n = s.n, m = s.m, npad = s.npad;
   const double* A = s.A;
-  const double* iry = s.vec(kPI) + n;               // 1 / Ry
-  constexpr int KS = 16;                            // rows per slice
-  constexpr int SL = 2 * KS * kLB + KS;             // doubles per buffer
+  const double* iry = s.vec(kPI) + n;  // 1 / Ry
+  constexpr int KS = 16;               // rows per slice
+  constexpr int LP = kLB + 4;          // staged row pitch
+  constexpr int SL = 2 * KS * LP + KS; // doubles per buffer
+  constexpr int NS = 4;                // slices in flight (ring of NS buffers)
+  static_assert(NS * SL * sizeof(double) <= kArenaBytes, "Gram ring exceeds the arena");
   double* smem = reinterpret_cast<double*>(s.arena);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gi = lane >> 2, tg = lane & 3;
+  const int wr = warp >> 2, wc = warp & 3;
   const int nt = npad / kLB, tiles = nt * (nt + 1) / 2;
   auto issue = [&](int r0, int i0, int j0, int buf) {
     double* sa = smem + buf * SL;
-    double* sb = sa + KS * kLB;
-    double* sw = sb + KS * kLB;
+    double* sb = sa + KS * LP;
+    double* sw = sb + KS * LP;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int e = threadIdx.x + q * kGridBT, r = e >> 7, c = e & 127, i = r0 + r;
       const bool ok = i < m;
-      cp_async8(sa + e, A + (ok && i0 + c < n ? size_t(i) * n + i0 + c : 0),
+      cp_async8(sa + r * LP + c, A + (ok && i0 + c < n ? size_t(i) * n + i0 + c : 0),
                 ok && i0 + c < n);
-      cp_async8(sb + e, A + (ok && j0 + c < n ? size_t(i) * n + j0 + c : 0),
+      cp_async8(sb + r * LP + c, A + (ok && j0 + c < n ? size_t(i) * n + j0 + c : 0),
                 ok && j0 + c < n);
     }
     if (threadIdx.x < KS) {
@@ -239,48 +244,60 @@ __device__ void large_gram_simt(S& s) {
     while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
     const int tj = t - ti * (ti + 1) / 2;
     const int i0 = ti * kLB, j0 = tj * kLB;
-    double acc[8][8];
+    double acc[8][4][2];
 #pragma unroll
     for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
-    issue(0, i0, j0, 0);
-    int buf = 0;
-    for (int r0 = 0; r0 < m; r0 += KS) {
-      // Slice r0 landed in `buf`; the other buffer was last read before the
-      // previous barrier, so the next slice may be issued into it now.
-      if (r0 + KS < m) {
-        issue(r0 + KS, i0, j0, buf ^ 1);
-        cp_async_wait<1>();
+      for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    const int nsl = (m + KS - 1) / KS;
+    // Slices 0 .. NS-2 in flight (empty groups past the end keep the count).
+#pragma unroll
+    for (int q = 0; q < NS - 1; ++q) {
+      if (q < nsl) {
+        issue(q * KS, i0, j0, q);
       } else {
-        cp_async_wait<0>();
+        cp_async_commit();
       }
+    }
+    for (int q = 0; q < nsl; ++q) {
+      // Slice q + NS - 1 goes into the buffer read at step q - 1 (released by
+      // that step's closing barrier); then slice q has landed.
+      const int nx = q + NS - 1;
+      if (nx < nsl) {
+        issue(nx * KS, i0, j0, nx % NS);
+      } else {
+        cp_async_commit();
+      }
+      cp_async_wait<NS - 1>();
       __syncthreads();
-      const double* sa = smem + buf * SL;
-      const double* sb = sa + KS * kLB;
-      const double* sw = sb + KS * kLB;
-#pragma unroll 2
-      for (int r = 0; r < KS; ++r) {
-        const double wr = sw[r];
-        double av[8], bv[8];
+      const int buf = q % NS;
+      const double* sa = smem + buf * SL + wr * 64 + gi;
+      const double* sb = smem + buf * SL + KS * LP + wc * 32 + gi;
+      const double* sw = smem + buf * SL + 2 * KS * LP;
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          av[a] = sa[r * kLB + ty + 16 * a] * wr;
-          bv[a] = sb[r * kLB + tx + 16 * a];
-        }
+      for (int k0 = 0; k0 < KS; k0 += 4) {
+        const int r = k0 + tg;
+        const double w = sw[r];
+        double a[8], b[4];
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
+        for (int mi = 0; mi < 8; ++mi) a[mi] = sa[r * LP + mi * 8] * w;
 #pragma unroll
-          for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        for (int ni = 0; ni < 4; ++ni) b[ni] = sb[r * LP + ni * 8];
+#pragma unroll
+        for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) dmma_8x8x4(acc[mi][ni], a[mi], b[ni]);
       }
       __syncthreads();  // everyone is done with `buf` before it is refilled
-      buf ^= 1;
     }
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+    for (int mi = 0; mi < 8; ++mi)
 #pragma unroll
-      for (int b = 0; b < 8; ++b)
-        s.g64[size_t(i0 + ty + 16 * a) * npad + j0 + tx + 16 * b] = acc[a][b];
+      for (int ni = 0; ni < 4; ++ni) {
+        const int i = i0 + wr * 64 + mi * 8 + gi, j = j0 + wc * 32 + ni * 8 + 2 * tg;
+        s.g64[size_t(i) * npad + j] = acc[mi][ni][0];
+        s.g64[size_t(i) * npad + j + 1] = acc[mi][ni][1];
+      }
   }
 }
 
@@ -543,10 +560,11 @@ __device__ int large_cholesky(S& s, T* g) {
     s.sync();
     QTQP_TOC(kPhLgPanel);
     QTQP_RETIC();
-    // (c) trailing update.
+    // (c) trailing update (FP64: on the FP64 tensor cores, DMMA m8n8k4, warp w
+    // on the 64 x 32 block (w / 4, w % 4) of the tile; FP32: 8 x 8 SIMT tiles).
     {
       constexpr int KS = 16;
-      constexpr int SP = kLB + 1;                     // slice pitch
+      constexpr int SP = sizeof(T) == 8 ? kLB + 4 : kLB + 1;  // slice pitch
       constexpr int SL = 2 * KS * SP;                 // elements per buffer
       const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
       const int nt = rest / kLB, tiles = nt * (nt + 1) / 2;
@@ -589,29 +607,66 @@ __device__ int large_cholesky(S& s, T* g) {
           __syncthreads();
           const T* pa = sm + buf * SL;
           const T* pb = pa + KS * SP;
-#pragma unroll 2
-          for (int kk = 0; kk < KS; ++kk) {
-            T av[8], bv[8];
+          if constexpr (sizeof(T) == 8) {
+            // acc[mi][ni / 2][...]: the 8 x 4 DMMA accumulators of this warp.
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            const int gi = lane >> 2, tg = lane & 3, wr = warp >> 2, wc = warp & 3;
 #pragma unroll
-            for (int a = 0; a < 8; ++a) {
-              av[a] = pa[kk * SP + ty + 16 * a];
-              bv[a] = pb[kk * SP + tx + 16 * a];
+            for (int k4 = 0; k4 < KS; k4 += 4) {
+              const double* ra = reinterpret_cast<const double*>(pa) + (k4 + tg) * SP + wr * 64 + gi;
+              const double* rb = reinterpret_cast<const double*>(pb) + (k4 + tg) * SP + wc * 32 + gi;
+              double a[8], b[4];
+#pragma unroll
+              for (int mi = 0; mi < 8; ++mi) a[mi] = ra[mi * 8];
+#pragma unroll
+              for (int ni = 0; ni < 4; ++ni) b[ni] = rb[ni * 8];
+#pragma unroll
+              for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                  dmma_8x8x4(reinterpret_cast<double(&)[2]>(acc[mi][2 * ni]), a[mi], b[ni]);
             }
+          } else {
+#pragma unroll 2
+            for (int kk = 0; kk < KS; ++kk) {
+              T av[8], bv[8];
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
+              for (int a = 0; a < 8; ++a) {
+                av[a] = pa[kk * SP + ty + 16 * a];
+                bv[a] = pb[kk * SP + tx + 16 * a];
+              }
 #pragma unroll
-              for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+              for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+            }
           }
           __syncthreads();
           buf ^= 1;
         }
+        if constexpr (sizeof(T) == 8) {
+          const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+          const int gi = lane >> 2, tg = lane & 3, wr = warp >> 2, wc = warp & 3;
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const int i = i0 + ty + 16 * a;
+          for (int mi = 0; mi < 8; ++mi) {
+            const int i = i0 + wr * 64 + mi * 8 + gi;
 #pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            const int j = j0 + tx + 16 * b;
-            if (j <= i) g[size_t(i) * npad + j] -= acc[a][b];
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int j = j0 + wc * 32 + ni * 8 + 2 * tg + e;
+                if (j <= i) g[size_t(i) * npad + j] -= acc[mi][2 * ni + e];
+              }
+          }
+        } else {
+#pragma unroll
+          for (int a = 0; a < 8; ++a) {
+            const int i = i0 + ty + 16 * a;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+              const int j = j0 + tx + 16 * b;
+              if (j <= i) g[size_t(i) * npad + j] -= acc[a][b];
+            }
           }
         }
       }
@@ -683,7 +738,7 @@ __device__ int large_factorize(S& s) {
     QTQP_RETIC();
     info = large_cholesky<float>(s, s.g32l);
   } else {
-    large_gram_simt(s);
+    large_gram_dmma(s);
     s.sync();
     large_finish_gram<double>(s, s.g64);
     QTQP_TOC(kPhGram);
