@@ -276,9 +276,9 @@ struct Ipm {
   // s * (32/S) + g) so that neighbouring lanes work on neighbouring outputs;
   // their partial sums are combined with xor shuffles, and lane s == 0 calls
   // epi(k, sum).  NACC independent sums per output.  No barrier inside.
-  template <int NACC, bool MAXOP = false, typename Body, typename Epi>
+  template <int NACC, bool MAXOP = false, int FORCE_S = 0, typename Body, typename Epi>
   __device__ __forceinline__ void rowdot(int K, int len, Body body, Epi epi) const {
-    const int S = lanes_for(K);
+    const int S = FORCE_S > 0 ? FORCE_S : lanes_for(K);
     const int per_warp = 32 / S;
     const int tid = this->tid;
     const int lane = tid & 31, warp = tid >> 5;
@@ -326,6 +326,9 @@ struct Ipm {
       if (k < K && s == 0) epi(k, acc);
     }
   }
+  // Lanes per output of a row dot (body reads element (k, j)): a whole warp
+  // per output in grid mode (coalesced rows), the automatic split otherwise.
+  static constexpr int kRowS = NT > 1024 ? 32 : 0;
   __device__ __forceinline__ float* t32() const { return reinterpret_cast<float*>(vec(kCT)); }
 
   // --------------------------------------------------------------------------
@@ -887,7 +890,7 @@ struct Ipm {
       out[k] = accumulate ? out[k] + val : val;
     }
     // y = (A x - r_y) / Ry
-    rowdot<1>(m, n,
+    rowdot<1, false, kRowS>(m, n,
               [&](int k, int j, double* acc) {
                 const double xj = fp64 ? tmp[j] : double(t32[j]);
                 acc[0] = fma(Ap[k * ld + j], xj, acc[0]);
@@ -932,7 +935,7 @@ struct Ipm {
                 mres = nanmax(mres, fabs(rk));
                 vnan = fmax(vnan, (v[k] != v[k]) ? 1.0 : 0.0);
               });
-    rowdot<1>(m, n,
+    rowdot<1, false, kRowS>(m, n,
               [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], v[j], acc[0]); },
               [&](int k, double* acc) {
                 const int kk = nn + k;
@@ -1230,7 +1233,7 @@ struct Ipm {
                   }
                 },
                 [&](int k, double* acc) { epi_x(k, acc[0], acc[1]); });
-      rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], xy[j], acc[0]); },
+      rowdot<1, false, kRowS>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], xy[j], acc[0]); },
                 [&](int k, double* acc) { epi_y(k, acc[0]); });
     }
     reduce<3, 9>(sm, mx);
@@ -1351,7 +1354,7 @@ struct Ipm {
     } else {
       const double* Ap = A;
       const int la = lda, nn = n;
-      rowdot<1>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], v[j], acc[0]); },
+      rowdot<1, false, kRowS>(m, n, [&](int k, int j, double* acc) { acc[0] = fma(Ap[k * la + j], v[j], acc[0]); },
                 [&](int k, double* acc) { out[nn + k] = acc[0]; });
     }
   }
