@@ -88,6 +88,7 @@ __host__ __device__ inline size_t band_grid_smem_need(int bw) {
   const size_t e = sizeof(double);
   const size_t B = size_t(bw) + 2;
   size_t need = ((B * B * e + 7) & ~size_t(7)) + size_t(bw) * (bw + 1) / 2 * 4;
+  if (band_panel_bytes(bw) > need) need = band_panel_bytes(bw);
   const size_t spike = (size_t(bw) + 1) * bw * e + 256 * e;
   const size_t prod = size_t(bw) * bw * e + 32 * 4 * ((size_t(bw) + 3) / 4) * e;
   const size_t chain = (2 * (size_t(bw) * sep_pitch(bw) + 4) + 3 * 128 + 256 + 2 * 16) * e;
@@ -633,7 +634,7 @@ __device__ int bandp_factorize(S& s) {
   if (k < bp.P) {
     const int lo = bp.lo(k), li = bp.li(k);
     const bool has_sep = k < bp.P - 1;
-    const int bad = s.template band_chol_window_range<T, kGridBT>(
+    const int bad = s.template band_chol_panel_range<T, kGridBT>(
         threadIdx.x, lo, li + (has_sep ? bw : 0), li,
         has_sep ? sep_block<T>(s, k, kSbD) : static_cast<T*>(nullptr), bw);
     if (bad != 0) {

@@ -98,12 +98,22 @@ __host__ __device__ inline BandLayout plan_band_layout(int n, int m, int bw, int
 // the 128-slot solve window must fit).
 constexpr int kBandWinMaxBw = 126;
 constexpr int kBandRing = 32;  // factor columns / rows in flight in the band solves
+constexpr int kBandPanel = 8;  // columns per panel of the blocked band Cholesky
+// Shared memory of the blocked band Cholesky (band_chol_panel_range): the
+// circular (bw + kBandPanel)^2 window, the panel rows, the publish slots
+// and the 16-bit trailing-update offsets.
+__host__ __device__ inline size_t band_panel_bytes(int bw) {
+  const size_t B = size_t(bw) + kBandPanel;
+  const size_t elems = B * B + (size_t(bw) + kBandPanel) * (kBandPanel + 1) + 2 * kBandPanel;
+  return elems * sizeof(double) + size_t(bw) * (size_t(bw) + 1) / 2 * sizeof(uint16_t);
+}
 __host__ __device__ inline size_t band_win_bytes(int bw, int nt) {
   const size_t b2 = (size_t(bw) + 2) * (size_t(bw) + 2) * sizeof(double);
   const size_t pairs = size_t(bw) * (size_t(bw) + 1) / 2 * sizeof(uint32_t);
   const size_t cols = size_t(nt) * (size_t(bw) + 1) * sizeof(double);
   const size_t solve = (128 + kBandRing * 128 + kBandRing) * sizeof(double);
   size_t e = b2 + pairs;
+  if (bw + kBandPanel <= nt && band_panel_bytes(bw) > e) e = band_panel_bytes(bw);
   if (cols > e) e = cols;
   if (solve > e) e = solve;
   return (e + 15) & ~size_t(15);
@@ -2109,10 +2119,141 @@ struct Ipm {
       band_gram<T>(reinterpret_cast<T*>(bwin) + size_t(tid) * (bw + 1));
       QTQP_TOC(kPhGram);
       QTQP_RETIC();
-      const int info = band_chol_window_range<T, NT>(tid, 0, n, n, nullptr, 0);
+      const int info = bw + kBandPanel <= NT
+                           ? band_chol_panel_range<T, NT>(tid, 0, n, n, nullptr, 0)
+                           : band_chol_window_range<T, NT>(tid, 0, n, n, nullptr, 0);
       QTQP_TOC(kPhChol);
       return info;
     }
+  }
+
+  // Blocked form of band_chol_window_range (same arguments and results):
+  // kBandPanel-column panels.  Each panel is factorised tall-skinny in
+  // registers (thread r holds the panel's entries of row k + r, for the
+  // kBandPanel + bw rows the panel touches; per column the diagonal block's
+  // rows publish their entry, one barrier, then every row scales its entry
+  // by one reciprocal square root and updates the rest of its panel row),
+  // written to the factor, and applied to the active bw x bw window as one
+  // rank-kBandPanel update.  The window is circular with period B = bw +
+  // kBandPanel (lower triangle, shared memory); the kBandPanel rows that
+  // enter it are loaded from the Gram matrix during the panel, and the
+  // window columns left of an entering row's band are zeroed.  Needs
+  // kBandPanel + bw <= BT.
+  template <typename T, int BT>
+  __device__ int band_chol_panel_range(int lt, int lo, int nsub, int ne, T* tail, int ldt) {
+    constexpr int KP = kBandPanel, PP = KP + 1;
+    const int bw = this->bw, ldl = bw + 1, B = bw + KP;
+    T* L = reinterpret_cast<T*>(Lb) + size_t(lo) * ldl;
+    T* W = reinterpret_cast<T*>(bwin);
+    T* Pn = W + B * B;
+    T* pub = Pn + (KP + bw) * PP;
+    uint16_t* pairs = reinterpret_cast<uint16_t*>(pub + 2 * KP);
+    const int npairs = bw * (bw + 1) / 2;
+    for (int a = lt; a < bw; a += BT)
+      for (int b = 0; b <= a; ++b) pairs[a * (a + 1) / 2 + b] = uint16_t(a | (b << 8));
+    for (int e = lt; e < B * B; e += BT) {
+      const int i = e / B, j = e - i * B;
+      W[e] = (j <= i && i - j <= bw && i < nsub) ? L[size_t(j) * ldl + (i - j)] : T(0);
+    }
+    group_sync<BT>();
+    int bad = 0;
+    constexpr int MAXPRE = (KP * 128 + BT - 1) / BT;  // entering entries per thread (bw < 128)
+    for (int k = 0; k < ne; k += KP) {
+      const int pw = min(KP, ne - k);
+      const int nr = min(pw + bw, nsub - k);
+      const int sk = k % B;
+      auto sl = [&](int x) {  // slot of index k + x, 0 <= x < 2 B
+        int t = sk + x;
+        t = t >= B ? t - B : t;
+        return t >= B ? t - B : t;
+      };
+      // Rows k + B .. k + B + pw - 1 enter after this panel: prefetch their
+      // band entries (row r, column r - bw + d).
+      T pre[MAXPRE];
+#pragma unroll
+      for (int q = 0; q < MAXPRE; ++q) {
+        const int f = lt + BT * q, e = f / (bw + 1), d = f - e * (bw + 1);
+        const int r = k + B + e;
+        pre[q] = (e < pw && r < nsub) ? L[size_t(r - bw + d) * ldl + (bw - d)] : T(0);
+      }
+      T v[KP];
+#pragma unroll
+      for (int c = 0; c < KP; ++c)
+        v[c] = (lt < nr && c < pw && c <= lt) ? W[sl(lt) * B + sl(c)] : T(0);
+#pragma unroll
+      for (int c = 0; c < KP; ++c) {
+        if (c < pw) {
+          T* pc = pub + (c & 1) * KP;
+          if (lt >= c && lt < pw) pc[lt] = v[c];
+          group_sync<BT>();
+          const T piv = pc[c];
+          if (!(piv > T(0))) {
+            bad = k + c + 1;
+            break;
+          }
+          const T il = rsqrt(piv);
+          if (lt < nr) {
+            if (lt == c) {
+              v[c] = il;  // the factor keeps 1 / l_cc
+            } else if (lt > c) {
+              const T lic = v[c] * il;
+              v[c] = lic;
+#pragma unroll
+              for (int j = c + 1; j < KP; ++j)
+                if (j < pw) v[j] = fma(-lic, pc[j] * il, v[j]);
+            }
+          }
+        }
+      }
+      if (bad) break;
+      if (lt < nr) {
+#pragma unroll
+        for (int c = 0; c < KP; ++c)
+          if (c < pw && c <= lt && lt - c <= bw) L[size_t(k + c) * ldl + (lt - c)] = v[c];
+        if (lt >= pw) {
+#pragma unroll
+          for (int c = 0; c < KP; ++c) Pn[lt * PP + c] = v[c];
+        }
+      }
+      group_sync<BT>();
+      // Trailing update of the window: rows / columns k + pw .. k + pw + bw - 1.
+      for (int pi = lt; pi < npairs; pi += BT) {
+        const int pr = pairs[pi];
+        const int a = pr & 0xff, b = pr >> 8;
+        const int i = pw + a, j = pw + b;
+        if (k + i < nsub) {
+          const T* ri = Pn + i * PP;
+          const T* rj = Pn + j * PP;
+          T acc = T(0);
+#pragma unroll
+          for (int c = 0; c < KP; ++c) acc = fma(ri[c], rj[c], acc);
+          T* w = W + sl(i) * B + sl(j);
+          *w -= acc;
+        }
+      }
+      // Entering rows: band entries, and zeros left of the band.
+#pragma unroll
+      for (int q = 0; q < MAXPRE; ++q) {
+        const int f = lt + BT * q, e = f / (bw + 1), d = f - e * (bw + 1);
+        const int r = k + B + e;
+        if (e < pw && r < nsub) W[sl(B + e) * B + sl(KP + e + d)] = pre[q];
+      }
+      for (int f = lt; f < pw * (KP - 1); f += BT) {
+        const int e = f / (KP - 1), t = f - e * (KP - 1);
+        const int r = k + B + e, j = k + pw + t;  // columns k+pw .. r-bw-1
+        if (r < nsub && j < r - bw) W[sl(B + e) * B + sl(pw + t)] = T(0);
+      }
+      group_sync<BT>();
+    }
+    if (tail != nullptr && bad == 0) {
+      const int t = nsub - ne;
+      for (int e = lt; e < t * t; e += BT) {
+        const int i = e / t, j = e - i * t;
+        if (j <= i) tail[size_t(i) * ldt + j] = W[((ne + i) % B) * B + (ne + j) % B];
+      }
+    }
+    group_sync<BT>();
+    return bad == 0 ? 0 : lo + bad;
   }
 
   // Band Cholesky with the active part of the band in shared memory, over
