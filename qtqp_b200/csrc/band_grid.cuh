@@ -709,8 +709,7 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
   // separator k - 1.
   if (k < P) {
     const int lo = bp.lo(k), li = bp.li(k), hi = lo + li, R = hi + (k < P - 1 ? bw : 0);
-    if (warp == 0) s.template band_fwd_range<T>(v, w, lo, li, R, lane);
-    __syncthreads();
+    s.template band_fwd_blocked<T, kGridBT>(v, w, lo, li, R, lt);
     if (k >= 1) {
       const T* WL = part_wl<T>(s, bp, k);
       const int c = lt & 127, g = lt >> 7;
@@ -807,7 +806,7 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
       }
       __syncthreads();
     }
-    if (warp == 0) s.template band_bwd_range<T>(v, w, lo, hi, R, lane);
+    s.template band_bwd_blocked<T, kGridBT>(v, w, lo, hi, R, lt);
   }
   s.sync();
   QTQP_TOC(kPhBpBwd);

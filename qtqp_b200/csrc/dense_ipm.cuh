@@ -2437,12 +2437,158 @@ struct Ipm {
         band_chol_solve_global<T>(v, w);
         return;
       }
-      if (tid < 32) {
-        band_fwd_range<T>(v, w, 0, n, n, tid);
-        band_bwd_range<T>(v, w, 0, n, n, tid);
-      }
-      sync();
+      band_fwd_blocked<T, NT>(v, w, 0, n, n, tid);
+      band_bwd_blocked<T, NT>(v, w, 0, n, n, tid);
     }
+  }
+
+  // Blocked forms of band_fwd_range / band_bwd_range (same arguments and
+  // results), run by all BT threads of the group (lt: this thread's index):
+  // per block of 8 columns one thread solves the 8 x 8 diagonal block, then
+  // one thread per row applies the block's 8 values to the next bw rows, with
+  // the next block's factor entries copied in (cp.async) meanwhile.  The
+  // active vector entries live in 256 circular slots of shared memory.
+  static constexpr int kSolveBlk = 8;
+  template <typename T, int BT>
+  __device__ void band_fwd_blocked(T* v, T* w, int lo, int ne, int R, int lt) {
+    constexpr int KB = kSolveBlk;
+    const int bw = this->bw, ldl = bw + 1, hi = lo + ne;
+    const T* L = reinterpret_cast<const T*>(Lb);
+    T* win = reinterpret_cast<T*>(bwin);  // 256 slots: row r at r & 255
+    T* pan = win + 256;                   // 2 x (KB ldl): factor columns of a block
+    T* zz = pan + 2 * KB * ldl;           // the block's KB values
+    auto issue = [&](int k0, int buf) {
+      T* dst = pan + buf * KB * ldl;
+      const int nel = min(KB, hi - k0) * ldl;
+      for (int e = lt; e < KB * ldl; e += BT)
+        cp_async_elem(dst + e, L + (e < nel ? size_t(k0) * ldl + e : 0), e < nel);
+      cp_async_commit();
+    };
+    int loaded = min(R, lo + bw + KB);
+    for (int r = lo + lt; r < loaded; r += BT) win[r & 255] = v[r];
+    if (lo < hi) issue(lo, 0);
+    int buf = 0;
+    for (int k0 = lo; k0 < hi; k0 += KB, buf ^= 1) {
+      const int pw = min(KB, hi - k0);
+      // This block's columns have landed and every thread is done with the
+      // previous block: the next block's copies may now fill the other buffer.
+      cp_async_wait<0>();
+      group_sync<BT>();
+      if (k0 + KB < hi) issue(k0 + KB, buf ^ 1);
+      const T* pc = pan + buf * KB * ldl;  // column k0 + c: pc[c * ldl + d], d = row - column
+      if (lt == 0) {
+        T zl[KB];
+#pragma unroll
+        for (int c = 0; c < KB; ++c) {
+          if (c < pw) {
+            T t = win[(k0 + c) & 255];
+#pragma unroll
+            for (int c2 = 0; c2 < c; ++c2) t = fma(-pc[c2 * ldl + (c - c2)], zl[c2], t);
+            zl[c] = t * pc[c * ldl];
+            zz[c] = zl[c];
+            w[k0 + c] = zl[c];
+          }
+        }
+      }
+      group_sync<BT>();
+      const int rend = min(R, k0 + pw + bw);
+      for (int r = k0 + pw + lt; r < rend; r += BT) {
+        T t = win[r & 255];
+#pragma unroll
+        for (int c = 0; c < KB; ++c) {
+          const int d = r - k0 - c;
+          if (c < pw && d <= bw) t = fma(-pc[c * ldl + d], zz[c], t);
+        }
+        win[r & 255] = t;
+      }
+      const int nload = min(R, k0 + 2 * KB + bw);
+      for (int r = loaded + lt; r < nload; r += BT) win[r & 255] = v[r];
+      loaded = max(loaded, nload);
+    }
+    cp_async_wait<0>();
+    group_sync<BT>();
+    for (int r = hi + lt; r < R; r += BT) v[r] = win[r & 255];
+    group_sync<BT>();
+  }
+
+  template <typename T, int BT>
+  __device__ void band_bwd_blocked(T* v, T* w, int lo, int hi, int R, int lt) {
+    constexpr int KB = kSolveBlk;
+    const int bw = this->bw, ldl = bw + 1;
+    const T* L = reinterpret_cast<const T*>(Lb);
+    T* win = reinterpret_cast<T*>(bwin);
+    T* stg = win + 256;                   // 2 x ((bw + KB) x KB): entries L(kb + q, i)
+    T* xx = stg + 2 * (bw + KB) * KB;     // the block's KB values
+    const int SR = bw + KB;               // staged rows per block: i in [kb - bw, kb + KB)
+    // Stage, for the block of rows [kb, k1], the entries L(kb + q, i) (band
+    // column i, offset kb + q - i) for i in [kb - bw, k1].
+    auto issue = [&](int kb, int k1, int buf) {
+      T* dst = stg + buf * SR * KB;
+      for (int e = lt; e < SR * KB; e += BT) {
+        const int ii = e / KB, q = e - ii * KB, i = kb - bw + ii, d = kb + q - i;
+        const bool ok = i >= lo && i <= k1 && kb + q <= k1 && d >= 0 && d <= bw;
+        cp_async_elem(dst + e, L + (ok ? size_t(i) * ldl + d : 0), ok);
+      }
+      cp_async_commit();
+    };
+    // Window: w for rows [max(lo, hi - bw - KB), hi), the known x for [hi, R).
+    const int wlo = max(lo, hi - bw - KB);
+    for (int r = wlo + lt; r < R; r += BT) win[r & 255] = r >= hi ? v[r] : w[r];
+    int kb = max(lo, hi - KB);
+    if (lo < hi) issue(kb, hi - 1, 0);
+    group_sync<BT>();
+    // Known rows [hi, R): w_i -= sum_r L(r, i) x_r for i in [hi - bw, hi).
+    if (R > hi) {
+      for (int i = max(lo, hi - bw) + lt; i < hi; i += BT) {
+        T t = win[i & 255];
+        const int rmax = min(R - 1, i + bw);
+        for (int r = hi; r <= rmax; ++r) t = fma(-L[size_t(i) * ldl + (r - i)], win[r & 255], t);
+        win[i & 255] = t;
+      }
+    }
+    int loaded = wlo;  // rows [loaded, hi) are in the window
+    int buf = 0;
+    for (int k1 = hi - 1; k1 >= lo; k1 = kb - 1, buf ^= 1) {
+      kb = max(lo, k1 - KB + 1);
+      const int pw = k1 - kb + 1;
+      const int kbn = max(lo, kb - KB);
+      // As in the forward: this block's entries have landed and the other
+      // buffer is free once every thread has passed the barrier.
+      cp_async_wait<0>();
+      group_sync<BT>();
+      if (kb > lo) issue(kbn, kb - 1, buf ^ 1);
+      const T* sg = stg + buf * SR * KB;  // L(kb + q, i) at sg[(i - kb + bw) * KB + q]
+      if (lt == 0) {
+        T xl[KB];
+#pragma unroll
+        for (int c = KB - 1; c >= 0; --c) {
+          if (c < pw) {
+            const int r = kb + c;
+            T t = win[r & 255];
+#pragma unroll
+            for (int c2 = c + 1; c2 < KB; ++c2)
+              if (c2 < pw) t = fma(-sg[(c + bw) * KB + c2], xl[c2], t);
+            xl[c] = t * sg[(c + bw) * KB + c];
+            xx[c] = xl[c];
+            v[r] = xl[c];
+          }
+        }
+      }
+      group_sync<BT>();
+      for (int i = max(lo, kb - bw) + lt; i < kb; i += BT) {
+        T t = win[i & 255];
+        const T* si = sg + (i - kb + bw) * KB;
+#pragma unroll
+        for (int q = 0; q < KB; ++q)
+          if (q < pw) t = fma(-si[q], xx[q], t);
+        win[i & 255] = t;
+      }
+      const int nload = max(lo, kbn - bw);
+      for (int r = nload + lt; r < loaded; r += BT) win[r & 255] = w[r];
+      loaded = min(loaded, nload);
+    }
+    cp_async_wait<0>();
+    group_sync<BT>();
   }
 
   // Forward substitution over the columns [lo, lo + ne) of the rows
