@@ -699,8 +699,8 @@ def run_parametric(args):
             for _ in range(args.steps))
     return t, db.fetch()[0]
   t_plain, r_plain = timed(batch.SolveOptions(precision="fp64"), lambda: None)
-  corr = 16
-  t_warm, r_warm = timed(batch.SolveOptions(precision="mixed", warm_corrections=corr),
+  corr = 8  # the best measured budget of primal-dual corrections on this family
+  t_warm, r_warm = timed(batch.SolveOptions(precision=args.precision, warm_corrections=corr),
                          lambda: net.predict_device(thetas[test]))
   solved_w = int(np.sum(r_warm["status"] == 0))
   solved_p = int(np.sum(r_plain["status"] == 0))
@@ -716,7 +716,7 @@ def run_parametric(args):
       "data": "synthetic (seeded generator of the family)",
       "config": {"workload": PARAM_WORKLOAD, "test_instances": test_count,
                  "train_instances": len(keep), "warm_corrections": corr,
-                 "chosen": "mixed precision + learned warm start; fp64_value: plain FP64"},
+                 "chosen": f"{args.precision} + learned warm start; fp64_value: plain FP64"},
       "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
       "statuses_identical": bool(np.array_equal(r_plain["status"], r_warm["status"])),
       "warm_accepted": int(r_warm["warm_started"].sum()),
