@@ -702,7 +702,7 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
   const int P = bp.P, N = P - 1, k = blockIdx.x, lt = threadIdx.x, lane = lt & 31,
             warp = lt >> 5;
   constexpr int kNW = kGridBT / 32;
-  // Scratch after the solve rings (band_fwd_range / band_bwd_range).
+  // Scratch after the blocked band solves' window and staging.
   T* scr = reinterpret_cast<T*>(s.bwin) + (128 + kBandRing * 128 + kBandRing);
   QTQP_TIC();
   // Forward per interior; the spike term W_L^T y of interior k for

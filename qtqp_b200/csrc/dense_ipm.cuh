@@ -2421,13 +2421,11 @@ struct Ipm {
     return info;
   }
 
-  // Solves L L^T v = v (column band storage, reciprocal diagonal) with one
-  // warp: forward z_k = v_k / l_kk, v_i -= l_ik z_k (i in (k, k+bw]) into w;
-  // backward x_k = w_k / l_kk, w_i -= l_ki x_k (i in [k-bw, k)) into v.
-  // With the window, the bw+1 active entries of the vector live in shared
-  // memory (128 circular slots) and the factor entries of the next steps are
-  // copied into a ring while the current step runs.  In grid mode the
-  // partitioned solve runs (band_grid.cuh).
+  // Solves L L^T v = v (column band storage, reciprocal diagonal): forward
+  // into w, backward into v.  With the shared-memory window the blocked
+  // solves below run (the whole group); without it one warp walks the
+  // columns in global memory.  In grid mode the partitioned solve runs
+  // (band_grid.cuh).
   template <typename T>
   __device__ void band_chol_solve(T* v, T* w) {
     if constexpr (NT > 1024) {
@@ -2442,8 +2440,12 @@ struct Ipm {
     }
   }
 
-  // Blocked forms of band_fwd_range / band_bwd_range (same arguments and
-  // results), run by all BT threads of the group (lt: this thread's index):
+  // Blocked band triangular solves, run by all BT threads of the group (lt:
+  // this thread's index).  Forward: z_k = (v_k - sum_c l_kc z_c) / l_kk for
+  // the columns [lo, lo + ne) into w[k], the rows [lo + ne, R) of v receiving
+  // their updates.  Backward: x_k = (w_k - sum_d l_{k+d,k} x_{k+d}) / l_kk for
+  // k in [lo, hi) into v[k], the rows [hi, R) holding known values of x in v
+  // (the separator that follows a partition).
   // per block of 8 columns one thread solves the 8 x 8 diagonal block, then
   // one thread per row applies the block's 8 values to the next bw rows, with
   // the next block's factor entries copied in (cp.async) meanwhile.  The
@@ -2589,116 +2591,6 @@ struct Ipm {
     }
     cp_async_wait<0>();
     group_sync<BT>();
-  }
-
-  // Forward substitution over the columns [lo, lo + ne) of the rows
-  // [lo, R) by one warp (lane): z_k into w[k]; the rows [lo + ne, R) of v
-  // receive their updates v_i -= l_ik z_k.  Group c of the ring (one per
-  // step, issued kBandRing-1 steps ahead) copies column c of L (offsets
-  // 0..bw; 0 = 1 / l_cc) and v[c + bw + 1].
-  template <typename T>
-  __device__ void band_fwd_range(T* v, T* w, int lo, int ne, int R, int lane) {
-    const int bw = this->bw, ldl = bw + 1, hi = lo + ne;
-    const T* L = reinterpret_cast<const T*>(Lb);
-    T* win = reinterpret_cast<T*>(bwin);  // 128 circular vector slots
-    T* ring = win + 128;                  // kBandRing x 128 factor entries
-    T* vring = ring + kBandRing * 128;    // kBandRing entering vector values
-    constexpr int D = kBandRing;
-    auto issue_fwd = [&](int c) {
-      T* rc = ring + (c % D) * 128;
-      const int rows = min(bw, R - 1 - c);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int d = lane + 32 * q;
-        const bool ok = c < hi && d <= rows;
-        cp_async_elem(rc + d, L + (ok ? size_t(c) * ldl + d : 0), ok);
-      }
-      if (lane == 0) {
-        const bool ok = c + bw + 1 < R;
-        cp_async_elem(vring + c % D, v + (ok ? c + bw + 1 : 0), ok);
-      }
-      cp_async_commit();
-    };
-    for (int i = lane; i <= min(bw, R - 1 - lo); i += 32) win[(lo + i) & 127] = v[lo + i];
-    for (int c = lo; c < lo + D - 1; ++c) issue_fwd(c);
-    for (int k = lo; k < hi; ++k) {
-      issue_fwd(k + D - 1);
-      cp_async_wait<D - 1>();
-      __syncwarp();
-      const T* ck = ring + (k % D) * 128;
-      const T zk = win[k & 127] * ck[0];
-      const int rows = min(bw, R - 1 - k);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int d = lane + 1 + 32 * q;
-        if (d <= rows) win[(k + d) & 127] = fma(-ck[d], zk, win[(k + d) & 127]);
-      }
-      if (lane == 0) {
-        w[k] = zk;
-        if (k + bw + 1 < R) win[(k + bw + 1) & 127] = vring[k % D];
-      }
-      __syncwarp();
-    }
-    cp_async_wait<0>();
-    __syncwarp();
-    for (int i = hi + lane; i < R; i += 32) v[i] = win[i & 127];
-  }
-
-  // Backward substitution by one warp over the rows [lo, R): x_k =
-  // (w_k - sum_d l_{k+d,k} x_{k+d}) / l_kk for k in [lo, hi), into v[k];
-  // the rows [hi, R) hold known values of x in v (the separator that
-  // follows a partition) and only contribute.  Group c of the ring copies
-  // row c of L (l_{c,c-d} at column c-d, offset d; offset 0 = 1 / l_cc) and
-  // w[c - bw - 1].
-  template <typename T>
-  __device__ void band_bwd_range(T* v, T* w, int lo, int hi, int R, int lane) {
-    const int bw = this->bw, ldl = bw + 1;
-    const T* L = reinterpret_cast<const T*>(Lb);
-    T* win = reinterpret_cast<T*>(bwin);
-    T* ring = win + 128;
-    T* vring = ring + kBandRing * 128;
-    constexpr int D = kBandRing;
-    __threadfence_block();  // w (plain stores) before the copies read it
-    __syncwarp();
-    auto issue_bwd = [&](int c) {
-      T* rc = ring + ((c % D + D) % D) * 128;
-      const int rows = min(bw, c - lo);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int d = lane + 32 * q;
-        const bool ok = c >= lo && d <= rows;
-        cp_async_elem(rc + d, L + (ok ? size_t(c - d) * ldl + d : 0), ok);
-      }
-      if (lane == 0) {
-        const bool ok = c - bw - 1 >= lo;
-        cp_async_elem(vring + (c % D + D) % D, w + (ok ? c - bw - 1 : 0), ok);
-      }
-      cp_async_commit();
-    };
-    for (int i = lane; i <= min(bw, R - 1 - lo); i += 32) {
-      const int r = R - 1 - i;
-      win[r & 127] = r >= hi ? v[r] : w[r];
-    }
-    for (int c = R - 1; c > R - D; --c) issue_bwd(c);
-    for (int k = R - 1; k >= lo; --k) {
-      issue_bwd(k - D + 1);
-      cp_async_wait<D - 1>();
-      __syncwarp();
-      const T* rk = ring + ((k % D + D) % D) * 128;
-      const T xk = k >= hi ? win[k & 127] : win[k & 127] * rk[0];
-      const int rows = min(bw, k - lo);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int d = lane + 1 + 32 * q;
-        if (d <= rows && k - d < hi) win[(k - d) & 127] = fma(-rk[d], xk, win[(k - d) & 127]);
-      }
-      if (lane == 0) {
-        if (k < hi) v[k] = xk;
-        if (k - bw - 1 >= lo) win[(k - bw - 1) & 127] = vring[(k % D + D) % D];
-      }
-      __syncwarp();
-    }
-    cp_async_wait<0>();
   }
 
   template <typename T>
