@@ -92,7 +92,7 @@ __host__ __device__ inline size_t band_grid_smem_need(int bw) {
   const size_t spike = (size_t(bw) + 1) * bw * e + 256 * e;
   const size_t prod = size_t(bw) * bw * e + 32 * 4 * ((size_t(bw) + 3) / 4) * e;
   const size_t chain = (2 * (size_t(bw) * sep_pitch(bw) + 4) + 3 * 128 + 256 + 2 * 16) * e;
-  const size_t solve = (128 + kBandRing * 128 + kBandRing) * e + 512 * e;
+  const size_t solve = (kBandSolveElems + 512) * e;
   if (spike > need) need = spike;
   if (prod > need) need = prod;
   if (chain > need) need = chain;
@@ -703,7 +703,7 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
             warp = lt >> 5;
   constexpr int kNW = kGridBT / 32;
   // Scratch after the blocked band solves' window and staging.
-  T* scr = reinterpret_cast<T*>(s.bwin) + (128 + kBandRing * 128 + kBandRing);
+  T* scr = reinterpret_cast<T*>(s.bwin) + kBandSolveElems;
   QTQP_TIC();
   // Forward per interior; the spike term W_L^T y of interior k for
   // separator k - 1.

@@ -97,7 +97,10 @@ __host__ __device__ inline BandLayout plan_band_layout(int n, int m, int bw, int
 // kBandWinMaxBw use it (the (bw+2)^2 window, the per-thread Gram columns and
 // the 128-slot solve window must fit).
 constexpr int kBandWinMaxBw = 126;
-constexpr int kBandRing = 32;  // factor columns / rows in flight in the band solves
+// Shared-memory elements reserved for the blocked band solves: 256 window
+// slots, two staged blocks of factor entries (forward: 2 x 8 x (bw + 1);
+// backward: 2 x (bw + 8) x 8, bw <= 126) and the block's 8 values.
+constexpr int kBandSolveElems = 256 + 2 * (126 + 8) * 8 + 16;
 constexpr int kBandPanel = 8;  // columns per panel of the blocked band Cholesky
 // Shared memory of the blocked band Cholesky (band_chol_panel_range): the
 // circular (bw + kBandPanel)^2 window, the panel rows, the publish slots
@@ -111,7 +114,7 @@ __host__ __device__ inline size_t band_win_bytes(int bw, int nt) {
   const size_t b2 = (size_t(bw) + 2) * (size_t(bw) + 2) * sizeof(double);
   const size_t pairs = size_t(bw) * (size_t(bw) + 1) / 2 * sizeof(uint32_t);
   const size_t cols = size_t(nt) * (size_t(bw) + 1) * sizeof(double);
-  const size_t solve = (128 + kBandRing * 128 + kBandRing) * sizeof(double);
+  const size_t solve = size_t(kBandSolveElems) * sizeof(double);
   size_t e = b2 + pairs;
   if (bw + kBandPanel <= nt && band_panel_bytes(bw) > e) e = band_panel_bytes(bw);
   if (cols > e) e = cols;
