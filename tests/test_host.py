@@ -154,3 +154,21 @@ def test_stats_record_conversion_and_log_line(capsys):
   qb._log_iteration(d)
   line = capsys.readouterr().out
   assert line.startswith("|    0 |") and " *, 2, 2 |" in line
+
+
+def test_storage_routing_of_banded_problems():
+  """A banded QP solved on its own from n >= BAND_GRID_N goes to the whole
+  GPU (partitioned band factorisation); in a batch it stays one per block;
+  short horizons stay banded; bands too wide for the partitioned form fall
+  back to the one-block path."""
+  from qtqp_b200 import band
+  a, b, c, z, p = problems.mpc_feasible(20)   # n = 1200, half-bandwidth 99
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert q.n >= qb.BAND_GRID_N
+  assert q.storage_format(single=True) == "band_grid"
+  assert q.storage_format() == "band"
+  a, b, c, z, p = problems.mpc_feasible(10)   # n = 600 < BAND_GRID_N
+  assert qb.QTQP(a=a, b=b, c=c, z=z, p=p).storage_format(single=True) == "band"
+  assert band.grid_supported(99, 30000)
+  assert not band.grid_supported(band.GRID_MAX_BW + 1, 30000)
+  assert not band.grid_supported(99, 150)    # fewer columns than two bands
