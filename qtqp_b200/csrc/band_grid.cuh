@@ -737,17 +737,22 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
   };
   int levels = 0;
   while ((1 << levels) <= N) ++levels;
+  // Level 0: z_j = Di_j t_j for the separators eliminated first.  Every
+  // separator eliminated at level l + 1 is a survivor of level l, so its
+  // block forms z right after updating t (one grid barrier per level).
+  auto form_z = [&](int kk) {  // t (shared) -> z_kk
+    stage_async(sm.Mt, ldm, sep_block<T>(s, kk, kSbI), bw, false);
+    stage_wait();
+    const T z = smem_matvec(sm.Mt, ldm, bw, t, false, red);
+    if (lt < bw) sep_vec<T>(s, kk, kSvZ)[lt] = z;
+  };
+  if (N >= 1 && 2 * k + 1 <= N) {
+    load_t(0, 2 * k);
+    form_z(2 * k);
+  }
+  s.sync();
   for (int l = 0; l < levels; ++l) {
     const int h = 1 << l;
-    const int j = h * (2 * k + 1);
-    if (j <= N) {  // z_j = Di_j t_j
-      load_t(l, j - 1);
-      stage_async(sm.Mt, ldm, sep_block<T>(s, j - 1, kSbI), bw, false);
-      stage_wait();
-      const T z = smem_matvec(sm.Mt, ldm, bw, t, false, red);
-      if (lt < bw) sep_vec<T>(s, j - 1, kSvZ)[lt] = z;
-    }
-    s.sync();
     const int jp = 2 * h * (k + 1);
     if (jp <= N) {  // t_j' -= Cr z (left neighbour) + Cl^T z (right neighbour)
       load_t(l, jp - 1);
@@ -763,7 +768,14 @@ __device__ void bandp_solve(S& s, T* v, T* w) {
         stage_wait();
         acc += smem_matvec(sm.Mt, ldm, bw, xb, true, red);
       }
-      if (lt < bw) sep_vec<T>(s, jp - 1, kSvT)[lt] = t[lt] - acc;
+      const T tv = lt < bw ? t[lt] - acc : T(0);
+      if ((jp & (4 * h - 1)) == 2 * h) {  // eliminated at level l + 1
+        __syncthreads();                    // every thread has read t
+        if (lt < bw) t[lt] = tv;
+        form_z(jp - 1);                     // stage_wait orders t before the product
+      } else if (lt < bw) {
+        sep_vec<T>(s, jp - 1, kSvT)[lt] = tv;
+      }
     }
     s.sync();
   }
