@@ -596,7 +596,7 @@ def run_mpc(args):
   nnz = int(hb.inst["nnz_a"][0])
   n_, m_ = int(hb.inst["n"][0]), int(hb.inst["m"][0])
   iters = int(res["iterations"])
-  # Algorithmic bytes per IPM iteration: the survey's SpMV bytes of A x (CSR:
+  # Algorithmic bytes per IPM iteration: the SpMV bytes of A x in CSR (
   # 12 nnz + 4 (rows + 1) + 8 (cols + rows)), twice (A x and A^T y), plus the
   # band factor written and read (8 n (bw + 1) each).
   bw = int(hb.inst["bw"][0])

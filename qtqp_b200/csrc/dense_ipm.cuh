@@ -1480,7 +1480,7 @@ struct Ipm {
         }
       }
       reduce<0, 1>(dummy, v);
-      // The plain test judges the projected point: clipped duals and slacks
+      // The plain test evaluates the projected point: clipped duals and slacks
       // show up in its residuals.
       if (termination(1.0, nb, nc, nullptr, false) == QTQP_STATUS_SOLVED) return true;
       if (!(v[0] > 0.0)) return false;  // the set is stable yet not acceptable

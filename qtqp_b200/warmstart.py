@@ -9,7 +9,7 @@ whether the row is active.  The prediction gives a starting point and an
 active set; the device solver then solves the KKT system on that set (with
 at most `warm_corrections` primal-dual active-set corrections) and keeps the
 result only if the plain termination test passes -- otherwise the plain
-method runs, so it is both the fallback and the judge.
+method runs, so it is both the fallback and the arbiter.
 
 Training and inference run on the GPU through the library's hand-written
 kernels (qtqp_mlp_*: tiled FP32 GEMM with fused bias/ReLU, ReLU backward,
