@@ -2488,7 +2488,8 @@ struct Ipm {
           if (c < pw) {
             T t = win[(k0 + c) & 255];
 #pragma unroll
-            for (int c2 = 0; c2 < c; ++c2) t = fma(-pc[c2 * ldl + (c - c2)], zl[c2], t);
+            for (int c2 = 0; c2 < c; ++c2)
+              if (c - c2 <= bw) t = fma(-pc[c2 * ldl + (c - c2)], zl[c2], t);
             zl[c] = t * pc[c * ldl];
             zz[c] = zl[c];
             w[k0 + c] = zl[c];

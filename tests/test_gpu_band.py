@@ -81,3 +81,19 @@ def test_band_lp_without_p():
   ref = orc.solve(a, b, c, z, None, backend="superlu")
   assert sol.status.value == ref.status
   kkt_checks.assert_status_certificate(sol, a, b, c, sp.csc_matrix(p.shape), z)
+
+
+@pytest.mark.parametrize("nx,nu,horizon", [(2, 1, 60), (4, 2, 40), (1, 1, 120)])
+def test_band_narrow_bands(nx, nu, horizon):
+  """Half-bandwidths 4, 9 and 2: bands narrower than the band kernels'
+  8-column panels and solve blocks."""
+  a, b, c, z, p = problems.mpc_feasible(horizon, nx=nx, nu=nu, seed=11)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert q.storage_format() == "band"
+  ref = orc.solve(a, b, c, z, p, backend="superlu")
+  for precision in ("fp64", "mixed"):
+    sol = qb.solve_batch([q], storage="band", precision=precision)[0]
+    assert sol.status.value == ref.status
+    kkt_checks.assert_status_certificate(sol, a, b, c, p, z)
+    if ref.status == "solved":
+      assert kkt_checks.objective_rel_err(sol.x, ref.x, c, p) <= OBJ_TOL

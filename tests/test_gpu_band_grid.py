@@ -101,3 +101,17 @@ def test_grid_full_size_mpc():
   assert sol.status.value == ref.status == "solved"
   kkt_checks.assert_solved(sol, a, b, c, p, z)
   assert kkt_checks.objective_rel_err(sol.x, ref.x, c, p) <= OBJ_TOL
+
+
+def test_grid_tiny_band_short_interiors():
+  """Half-bandwidth 2 with the default 128 partitions: interiors of about 7
+  columns, shorter than one 8-column panel."""
+  a, b, c, z, p = problems.mpc_feasible(600, nx=1, nu=1, seed=13)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert band.gram_bandwidth(q.a, q.p) == 2
+  ref = orc.solve(a, b, c, z, p, backend="superlu")
+  res, x, y, s, parts = _grid_solve(q)
+  assert parts == 128
+  assert int(res["status"]) == 0 and ref.status == "solved"
+  _assert_feasible(x, y, s, a, b, c, p)
+  assert kkt_checks.objective_rel_err(x, ref.x, c, p) <= OBJ_TOL
