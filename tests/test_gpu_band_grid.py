@@ -115,3 +115,18 @@ def test_grid_tiny_band_short_interiors():
   assert int(res["status"]) == 0 and ref.status == "solved"
   _assert_feasible(x, y, s, a, b, c, p)
   assert kkt_checks.objective_rel_err(x, ref.x, c, p) <= OBJ_TOL
+
+
+def test_grid_wide_band():
+  """nx=40, nu=36: half-bandwidth 115, near the widest band whose separator
+  blocks fit in shared memory."""
+  a, b, c, z, p = problems.mpc_feasible(20, nx=40, nu=36, seed=17)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert band.gram_bandwidth(q.a, q.p) == 115
+  assert q.storage_format(single=True) == "band_grid"
+  ref = orc.solve(a, b, c, z, p, backend="superlu")
+  sol = qb.solve_batch([q], storage="band_grid")[0]
+  assert sol.status.value == ref.status
+  kkt_checks.assert_status_certificate(sol, a, b, c, p, z)
+  if ref.status == "solved":
+    assert kkt_checks.objective_rel_err(sol.x, ref.x, c, p) <= OBJ_TOL
