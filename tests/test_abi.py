@@ -117,3 +117,27 @@ def test_band_grid_partition_limits(lib):
   wide = _band_inst(30000, 127)
   assert lib.qtqp_band_grid_workspace_bytes(wide.ctypes.data, 4) == 0
   assert b"too wide" in lib.qtqp_last_error()
+
+
+def test_band_grid_solve_rejects_bad_arguments(lib):
+  """Argument errors of the whole-GPU banded entry point come back as
+  QTQP_ERR_BAD_ARG with a message, before any device work."""
+  inst = _band_inst(3000, 99)
+  opts = batch.SolveOptions().to_c()
+  ws_bytes = lib.qtqp_band_grid_workspace_bytes(inst.ctypes.data, 8)
+  fake = 1 << 20  # a non-null device-looking address, never dereferenced
+  def call(parts=8, pools=fake, ws=fake, nbytes=ws_bytes, o=ctypes.byref(opts)):
+    return lib.qtqp_band_grid_solve(inst.ctypes.data, parts, pools, pools, pools, pools, pools,
+                                    pools, pools, pools, None, ws, nbytes, o, None)
+  assert call(parts=0) == _lib.QTQP_ERR_BAD_ARG
+  assert b"parts must be" in lib.qtqp_last_error()
+  assert call(pools=None) == _lib.QTQP_ERR_BAD_ARG
+  assert b"null argument" in lib.qtqp_last_error()
+  assert call(nbytes=ws_bytes - 1) == _lib.QTQP_ERR_BAD_ARG
+  assert b"workspace smaller" in lib.qtqp_last_error()
+  assert call(ws=fake + 8) == _lib.QTQP_ERR_BAD_ARG
+  assert b"256-byte aligned" in lib.qtqp_last_error()
+  bad = batch.SolveOptions().to_c()
+  bad.max_iter = 0
+  assert call(o=ctypes.byref(bad)) == _lib.QTQP_ERR_BAD_ARG
+  assert b"invalid options" in lib.qtqp_last_error()
