@@ -1,9 +1,10 @@
 """The JSON line contract of bench.py's reference arm (CPU only).
 
 `bench.py --impl reference` times the oracle port of the reference algorithm
-on the host cores; it needs no GPU, so its line is checked here: one JSON
-object with the metric, unit, timing, config, cpu_baseline and e2e keys, and
-silence (exit 0, no line) on ranks other than 0.
+on the host cores; it needs no GPU, so its line is checked here for each
+workload (at reduced sizes): one JSON object with the metric, unit, timing,
+config, cpu_baseline and e2e keys, and silence (exit 0, no line) on ranks
+other than 0.
 """
 
 import json
@@ -23,9 +24,18 @@ def _run_bench(extra_env=None, *args):
                         cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
 
 
-def test_reference_arm_line():
-  proc = _run_bench({"RANK": "0", "WORLD_SIZE": "1"}, "--impl", "reference", "--steps", "1",
-                    "--warmup", "0")
+WORKLOADS = {
+    "batch_small": [],
+    "dense_large": ["--workload", "dense_large", "--large-n", "64"],
+    "mpc": ["--workload", "mpc", "--mpc-horizon", "20"],
+    "parametric": ["--workload", "parametric", "--train", "64", "--count", "16"],
+}
+
+
+@pytest.mark.parametrize("workload", sorted(WORKLOADS))
+def test_reference_arm_line(workload):
+  proc = _run_bench({"RANK": "0", "WORLD_SIZE": "1"}, *WORKLOADS[workload], "--impl",
+                    "reference", "--steps", "1", "--warmup", "1")
   assert proc.returncode == 0, proc.stderr[-2000:]
   lines = [l for l in proc.stdout.splitlines() if l.startswith("{")]
   assert len(lines) == 1, proc.stdout
@@ -36,7 +46,7 @@ def test_reference_arm_line():
     assert key in rec, key
   assert rec["impl"] == "reference"
   assert rec["unit"] == "QPs/s" and rec["higher_is_better"] is True
-  assert rec["steps"] == 1 and rec["warmup"] == 0 and rec["n_gpus"] == 1
+  assert rec["steps"] == 1 and rec["warmup"] == 1 and rec["n_gpus"] == 1
   assert rec["value"] > 0 and rec["ms_per_step"] > 0
   assert rec["vs_baseline"] is None
   assert "workload" in rec["config"]
@@ -48,9 +58,9 @@ def test_reference_arm_line():
   assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
 
 
-@pytest.mark.parametrize("rank", ["1", "3"])
-def test_reference_arm_other_ranks_are_silent(rank):
-  proc = _run_bench({"RANK": rank, "WORLD_SIZE": "4"}, "--impl", "reference", "--steps", "1",
-                    "--warmup", "0")
+@pytest.mark.parametrize("workload", sorted(WORKLOADS))
+def test_reference_arm_other_ranks_are_silent(workload):
+  proc = _run_bench({"RANK": "1", "WORLD_SIZE": "4"}, *WORKLOADS[workload], "--impl",
+                    "reference", "--steps", "1", "--warmup", "0")
   assert proc.returncode == 0, proc.stderr[-2000:]
   assert not [l for l in proc.stdout.splitlines() if l.startswith("{")]
