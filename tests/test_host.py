@@ -136,6 +136,74 @@ def test_direct_kkt_solver_host_driver():
   assert (kkt._kkt - sp.triu(kkt._kkt)).nnz == 0
 
 
+class _ScaledGram(_CpuGram):
+  """Returns `scale` times the exact regularised solve: refinement contracts
+  by |1 - scale| per step (scale in (0, 2)) or grows (scale outside)."""
+
+  def __init__(self, scale):
+    self.scale = scale
+    self.freed = 0
+
+  def solve(self, rhs):
+    return self.scale * super().solve(rhs)
+
+  def free(self):
+    self.freed += 1
+
+
+class _NanGram(_CpuGram):
+
+  def solve(self, rhs):
+    return np.full_like(rhs, np.nan)
+
+
+def _kkt_case(solver, steps, seed=7):
+  rng = np.random.default_rng(seed)
+  m, n, z = 30, 20, 4
+  a, b, c, _, p = problems.feasible(m, n, z, rng)
+  s, y = rng.uniform(0.5, 1.5, size=m), rng.uniform(0.5, 1.5, size=m)
+  s[:z] = 0.0
+  kkt = direct.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
+                               max_iterative_refinement_steps=steps, atol=1e-12, rtol=1e-12,
+                               solver=solver)
+  kkt.update(mu=0.3, s=s, y=y)
+  return kkt, np.concatenate([c, b])
+
+
+def test_ir_more_steps_never_worse():
+  """More refinement steps give a residual no larger (tests/test_qtqp.py:1977-1999)."""
+  finals = []
+  for steps in (1, 2, 5, 50):
+    kkt, rhs = _kkt_case(_ScaledGram(0.5), steps)
+    _, st = kkt.solve(rhs=rhs, warm_start=np.zeros(rhs.size))
+    assert st["solves"] <= steps and st["status"] != "stalled"
+    finals.append(st["final_residual_norm"])
+  assert all(f1 >= f2 for f1, f2 in zip(finals, finals[1:]))
+  assert finals[-1] < 1e-10 * max(1.0, np.abs(rhs).max())
+
+
+def test_ir_stall_rule_stops_a_growing_residual():
+  """A step that does not reduce the residual ends refinement as "stalled"
+  (direct.py:274-283) and returns the last iterate."""
+  kkt, rhs = _kkt_case(_ScaledGram(2.5), 20)
+  _, st = kkt.solve(rhs=rhs, warm_start=np.zeros(rhs.size))
+  assert st["status"] == "stalled" and not st["converged"] and st["solves"] == 1
+
+
+def test_ir_nan_raises_value_error():
+  """NaNs from the backend raise the reference's ValueError (direct.py:293-294)."""
+  kkt, rhs = _kkt_case(_NanGram(), 3)
+  with pytest.raises(ValueError, match="Linear solver returned NaNs."):
+    kkt.solve(rhs=rhs, warm_start=np.zeros(rhs.size))
+
+
+def test_free_reaches_the_backend():
+  backend = _ScaledGram(1.0)
+  kkt, _ = _kkt_case(backend, 2)
+  kkt.free()
+  assert backend.freed == 1
+
+
 def test_stats_record_conversion_and_log_line(capsys):
   rec = np.zeros(64)
   rec[:22] = np.arange(22, dtype=float)
