@@ -13,6 +13,9 @@ known answers (README example x=[0.3,-0.7], the minimal QP x=1).
 
 Each function cites the reference lines it follows (paths relative to the
 reference project root).  All arithmetic is FP64, as in the reference.
+``warm_try`` restates the device solver's learned-warm-start attempt, which has
+no reference counterpart, on the reference's own KKT refinement and
+termination test; ``tests/test_oracle_warm.py`` checks it.
 """
 
 from __future__ import annotations
@@ -508,3 +511,99 @@ def _termination(a, p, b, c, d, e, x, y, tau, s, nb, nc, z, atol, rtol,
              "norm_x": nx, "norm_y": ny, "status": status, "prelrhs": prel,
              "drelrhs": drel})
   return status
+
+
+# ---------------------------------------------------------------------------
+# Learned warm start: the reduced KKT attempt (no reference counterpart).
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class WarmResult:
+  accepted: bool
+  rounds: int        # reduced solves made (1 + corrections used)
+  x: np.ndarray      # the last projected point, original scaling
+  y: np.ndarray
+  s: np.ndarray
+  solves: int        # refinement solves over all rounds
+
+
+def warm_try(a, b, c, z, p, wx, wy, active, *, corrections=0, atol=1e-7, rtol=1e-8,
+             atol_infeas=1e-8, rtol_infeas=1e-9, min_static_regularization=1e-8,
+             max_iterative_refinement_steps=20, linear_solver_atol=1e-12,
+             linear_solver_rtol=1e-12, equilibrate=True, backend="superlu") -> WarmResult:
+  """The warm-start attempt of the device solver, restated on the CPU.
+
+  A predicted point (wx, wy; original scaling) and active-row mask decide
+  which inequality rows are held tight.  Each round solves the KKT system of
+  the equality QP on that set with the reference's regularised factorisation
+  and FP64 refinement (direct.py:183-307): true diagonal [diag(P); 0 on tight
+  rows, -1e10 on free rows], regularised [max(diag(P), min_reg); -max(min_reg,
+  1e-10) on tight rows, -1e10 on free rows], right-hand side -[c; b], warm
+  started from the current point.  Then s = b - A x, the point is projected
+  onto the cone (y = max(y, 0) on tight rows, y = 0 on free rows, s =
+  max(s, 0) on inequality rows, s = 0 on equality rows), and it is accepted
+  when the reference's termination test (__init__.py:888-1008) reports
+  SOLVED at tau = 1.  Otherwise, while corrections remain, tight rows whose
+  dual came out negative leave the set, free rows whose slack came out
+  negative enter it, and the next round starts; a round that changes no row
+  ends the attempt.  Problems with rows the presolve would drop (b >= 1e20)
+  are not handled.
+  """
+  a = sp.csc_matrix(a, dtype=np.float64)
+  m, n = a.shape
+  b = np.array(b, dtype=np.float64)
+  c = np.array(c, dtype=np.float64)
+  p = sp.csc_matrix((n, n)) if p is None else sp.csc_matrix(p, dtype=np.float64)
+  if np.any(b[z:] >= 1e20):
+    raise ValueError("warm_try: rows that the presolve drops are not handled")
+  if equilibrate:
+    a_eq, p_eq, b_eq, c_eq, d, e = ruiz(a, p, b, c)
+  else:
+    a_eq, p_eq, b_eq, c_eq = a, p, b, c
+    d, e = np.ones(m), np.ones(n)
+  q = np.concatenate([c_eq, b_eq])
+  nb, nc = np.linalg.norm(b, np.inf), np.linalg.norm(c, np.inf)
+  be = DenseGramKkt(a_eq, p_eq) if backend == "dense" else SuperLUKkt(a_eq, p_eq)
+  kkt = KktIR(be, p_eq.diagonal(), n, m, z, min_static_regularization,
+              max_iterative_refinement_steps, linear_solver_atol, linear_solver_rtol)
+  x = np.asarray(wx, dtype=np.float64) / e
+  y = np.asarray(wy, dtype=np.float64) / d
+  s = np.zeros(m)
+  tight = np.asarray(active, dtype=bool).copy()
+  tight[:z] = True
+  ineq = np.arange(m) >= z
+  dmin, big = max(min_static_regularization, 1e-10), 1e10
+  pdiag = p_eq.diagonal()
+  true = np.empty(n + m)
+  reg = np.empty(n + m)
+  true[:n] = pdiag
+  reg[:n] = np.maximum(pdiag, min_static_regularization)
+  rounds = solves = 0
+  for _ in range(1 + max(0, min(corrections, 64))):
+    true[n:] = np.where(tight, 0.0, -big)
+    reg[n:] = np.where(tight, -dmin, -big)
+    be.update_diag(reg)
+    try:
+      be.factorize()
+    except (np.linalg.LinAlgError, RuntimeError):
+      break
+    kkt.corr = reg - true
+    try:
+      sol, st = kkt.solve(-q, np.concatenate([x, y]))
+    except ValueError:
+      break
+    rounds += 1
+    solves += st["solves"]
+    x, ys = sol[:n], sol[n:]
+    sk = b_eq - a_eq @ x
+    leave = tight & ineq & (ys < 0.0)
+    enter = ~tight & ineq & (sk < 0.0)
+    y = np.where(ineq, np.where(tight, np.maximum(ys, 0.0), 0.0), ys)
+    s = np.where(ineq, np.maximum(sk, 0.0), 0.0)
+    status = _termination(a, p, b, c, d, e, x, y, 1.0, s, nb, nc, z, atol, rtol,
+                          atol_infeas, rtol_infeas, {})
+    if status == STATUS_SOLVED:
+      return WarmResult(True, rounds, e * x, d * y, s / d, solves)
+    if not (leave.any() or enter.any()):
+      break
+    tight = (tight & ~leave) | enter
+  return WarmResult(False, rounds, e * x, d * y, s / d, solves)
