@@ -15,7 +15,9 @@ Each function cites the reference lines it follows (paths relative to the
 reference project root).  All arithmetic is FP64, as in the reference.
 ``warm_try`` restates the device solver's learned-warm-start attempt, which has
 no reference counterpart, on the reference's own KKT refinement and
-termination test; ``tests/test_oracle_warm.py`` checks it.
+termination test; ``solve(init=...)`` starts the interior-point method from a
+given point instead of the reference's cold start (also no counterpart);
+``tests/test_oracle_warm.py`` checks both.
 """
 
 from __future__ import annotations
@@ -331,12 +333,15 @@ def solve(a, b, c, z, p=None, *, atol=1e-7, rtol=1e-8, atol_infeas=1e-8,
           rtol_infeas=1e-9, max_iter=100, step_size_scale=0.99,
           min_static_regularization=1e-8, max_iterative_refinement_steps=20,
           linear_solver_atol=1e-12, linear_solver_rtol=1e-12,
-          equilibrate=True, backend="dense", tau_mode="auto") -> OracleResult:
+          equilibrate=True, backend="dense", tau_mode="auto", init=None) -> OracleResult:
   """Solves min 1/2 x'Px + c'x s.t. Ax + s = b, s[:z] = 0, s[z:] >= 0.
 
   backend: "dense" (Gram/Cholesky, solvers_dense.py) or "superlu"
   (solvers_sparse.py:96-121).  tau_mode "linearized" forces the fallback
-  (the reference's test_linearized_tau_always_converges patch).
+  (the reference's test_linearized_tau_always_converges patch).  init: an
+  optional starting point (x, y, s) in the original scaling that replaces
+  _init_variables (no reference counterpart: it restates an interior-point
+  method warm-started from a predicted point; s[z:] and y[z:] must be > 0).
   """
   a = sp.csc_matrix(a, dtype=np.float64)
   m_full, n = a.shape
@@ -372,6 +377,14 @@ def solve(a, b, c, z, p=None, *, atol=1e-7, rtol=1e-8, atol_infeas=1e-8,
   s = np.zeros(m)
   y[z:] = 1.0
   s[z:] = 1.0
+  if init is not None:
+    if drop.any():
+      raise ValueError("init: problems with rows that the presolve drops are not handled")
+    x, y, s = (np.array(v, dtype=np.float64) for v in init)
+    if x.shape != (n,) or y.shape != (m,) or s.shape != (m,):
+      raise ValueError("init: x, y, s must have the problem's shapes")
+    if np.any(y[z:] <= 0.0) or np.any(s[z:] <= 0.0):
+      raise ValueError("init: y and s must be positive on the inequality rows")
   x, y, s = x / e, y / d, s * d
   tau = 1.0
   kq = np.zeros(n + m)

@@ -73,3 +73,30 @@ def test_zero_corrections_means_one_round():
   r = orc.warm_try(*qp, np.zeros_like(plain.x), np.zeros_like(plain.y),
                    np.zeros_like(act), corrections=0)
   assert r.rounds == 1
+
+
+@pytest.mark.parametrize("seed", [3, 11])
+def test_ipm_started_from_the_solution_keeps_status_and_is_shorter(seed):
+  """The oracle's interior-point method started near the plain solution (y and
+  s shifted into the interior by 0.1) ends with the same status and
+  objective in fewer iterations than from the cold start."""
+  qp, plain, _ = _case(seed)
+  a, b, c, z, p = qp
+  y0, s0 = plain.y.copy(), plain.s.copy()
+  y0[z:] = np.maximum(y0[z:], 0.0) + 0.1
+  s0[z:] = np.maximum(s0[z:], 0.0) + 0.1
+  s0[:z] = 0.0
+  warm = orc.solve(a, b, c, z, p, backend="superlu", init=(plain.x, y0, s0))
+  assert warm.status == plain.status
+  assert len(warm.stats) < len(plain.stats)
+  obj = lambda x: c @ x + 0.5 * x @ (p @ x)
+  assert abs(obj(warm.x) - obj(plain.x)) <= 1e-6 * max(1.0, abs(obj(plain.x)))
+
+
+def test_ipm_start_is_validated():
+  qp, plain, _ = _case(3)
+  a, b, c, z, p = qp
+  with pytest.raises(ValueError, match="positive"):
+    orc.solve(a, b, c, z, p, init=(plain.x, np.zeros_like(plain.y), plain.s + 1.0))
+  with pytest.raises(ValueError, match="shapes"):
+    orc.solve(a, b, c, z, p, init=(plain.x[:-1], plain.y + 1.0, plain.s + 1.0))
