@@ -303,19 +303,24 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     opts.validate()
   else:
     opts, verbose = _opts, _verbose
-  _lib.require_device()
-  records = bool(verbose or opts.collect_stats)
-  # Dense and banded problems go to their own device batches; each large
-  # problem gets the whole GPU in turn.
+  # Arguments are checked before any device work.  Dense and banded problems
+  # go to their own device batches; each large problem gets the whole GPU in
+  # turn.
   kinds = [q.storage_format() if storage == "auto" else storage for q in problems]
   if any(k not in ("dense", "band", "large", "band_grid") for k in kinds):
     raise ValueError("storage must be 'auto', 'dense', 'band', 'large' or 'band_grid', "
                      f"got {storage!r}")
+  if warm_start is not None:
+    if any(k != "band" for k in kinds):
+      raise ValueError("warm_start needs every problem on the banded path")
+    model, _ = warm_start
+    if any((q.n, q.m) != (model.n, model.m) for q in problems):
+      raise ValueError("warm_start: every problem must have the model's (n, m)")
+  _lib.require_device()
+  records = bool(verbose or opts.collect_stats)
   per = {}  # kind -> (indices, results, x, y, s, stats, inst)
   where = {}
   t_launch = 0.0
-  if warm_start is not None and any(k != "band" for k in kinds):
-    raise ValueError("warm_start needs every problem on the banded path")
   for i in [i for i, k in enumerate(kinds) if k == "large"]:
     from . import large as _large  # pylint: disable=g-import-not-at-top
     dl = _large.DeviceLarge(problems[i].dense_problem(), opts, records=records)
@@ -349,8 +354,6 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     t_launch = timeit.default_timer() - start
     if warm_start is not None:
       model, thetas = warm_start
-      if any((q.n, q.m) != (model.n, model.m) for q in problems):
-        raise ValueError("warm_start: every problem must have the model's (n, m)")
       db.launch(warm=model.predict_device(np.asarray(thetas)))
     else:
       db.launch()

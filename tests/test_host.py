@@ -240,3 +240,21 @@ def test_storage_routing_of_banded_problems():
   assert band.grid_supported(99, 30000)
   assert not band.grid_supported(band.GRID_MAX_BW + 1, 30000)
   assert not band.grid_supported(99, 150)    # fewer columns than two bands
+
+
+def test_solve_batch_checks_arguments_before_device_work():
+  """solve_batch rejects a bad storage name and warm starts that do not fit
+  before it touches a GPU (so these errors are the same with or without one)."""
+  import types
+  a, b, c, z, p = problems.feasible(12, 8, 2, 3)
+  dense_q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  with pytest.raises(ValueError, match="storage must be"):
+    qb.solve_batch([dense_q], storage="sparse")
+  model = types.SimpleNamespace(n=dense_q.n, m=dense_q.m)
+  with pytest.raises(ValueError, match="banded path"):
+    qb.solve_batch([dense_q], storage="dense", warm_start=(model, np.zeros((1, 32))))
+  a, b, c, z, p = problems.mpc_feasible(4)
+  band_q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  wrong = types.SimpleNamespace(n=band_q.n + 1, m=band_q.m)
+  with pytest.raises(ValueError, match="model's"):
+    qb.solve_batch([band_q], storage="band", warm_start=(wrong, np.zeros((1, 32))))
