@@ -40,7 +40,7 @@ HBM_FALLBACK_GBS = 6650.0  # only if MEASURED_PEAKS.json is absent
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), nominal; for context only
 # DRAM bytes (read + write) of one batch solve (its 8 group launches, mixed
 # precision) on this workload, from an ncu capture of
-# dram__bytes_read.sum + dram__bytes_write.sum (profiles/dense_batch_kernel_config1.md).
+# dram__bytes_read.sum + dram__bytes_write.sum (profiles/dense_batch_kernel_small_dense_batch.md).
 NCU_TRAFFIC_BYTES = 171.6e6
 
 
@@ -74,7 +74,7 @@ def _args():
 
 def _instances(rank: int, count: int):
   from qtqp_b200 import problems
-  return [problems.config1_instance(rank * COUNT + i) for i in range(count)]
+  return [problems.small_dense_instance(rank * COUNT + i) for i in range(count)]
 
 
 # ---------------------------------------------------------------------------
@@ -86,7 +86,7 @@ def _oracle_chunk(ids):
   from qtqp_b200 import problems
   solved = 0
   for i in ids:
-    a, b, c, z, p = problems.config1_instance(i)
+    a, b, c, z, p = problems.small_dense_instance(i)
     if orc.solve(a, b, c, z, p, backend="dense").status == orc.STATUS_SOLVED:
       solved += 1
   return solved
@@ -387,10 +387,10 @@ def _param_oracle_chunk(spec):
   from qtqp_b200 import problems
   count, ids = spec
   if count not in _PARAM_FAMILY:
-    _PARAM_FAMILY[count] = problems.config4_family(count=count)
+    _PARAM_FAMILY[count] = problems.parametric_mpc_family(count=count)
   fam = _PARAM_FAMILY[count]
   for i in ids:
-    a, b, c, z, p = problems.config4_instance(fam, i)
+    a, b, c, z, p = problems.parametric_mpc_instance(fam, i)
     orc.solve(a, b, c, z, p, backend="superlu")
   return len(ids)
 
@@ -421,7 +421,7 @@ def run_dense_large(args):
   local = int(os.environ.get("LOCAL_RANK", "0"))
   from qtqp_b200 import problems
   nl = args.large_n
-  a, b, c, z, p = problems.config2(seed=1002 + rank, n=nl, m=2 * nl, z=nl // 4,
+  a, b, c, z, p = problems.large_dense(seed=1002 + rank, n=nl, m=2 * nl, z=nl // 4,
                                    rank=min(256, nl // 4))
   m, n = a.shape
   flops = m * n * (n + 1) + n ** 3 / 3.0  # one factorisation (Gram + Cholesky)
@@ -673,9 +673,9 @@ def run_parametric(args):
     return
   test_count = args.count if args.count != COUNT else 512
   from qtqp_b200 import problems
-  fam = problems.config4_family(count=args.train + test_count)
+  fam = problems.parametric_mpc_family(count=args.train + test_count)
   thetas = fam[-1]
-  insts = [problems.config4_instance(fam, i) for i in range(args.train + test_count)]
+  insts = [problems.parametric_mpc_instance(fam, i) for i in range(args.train + test_count)]
   if args.impl == "reference":
     # One held-out instance per host core per step, each core a spawned
     # process with one BLAS thread; instances cycle through the held-out set.

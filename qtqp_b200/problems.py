@@ -6,8 +6,9 @@ parametric family) and the three certificate families used by the tests
 (feasible, primal infeasible, dual infeasible).  Every generator takes a seed
 and returns (a: csc, b, c, z, p: csc).
 
-Seeds: configuration k uses ``default_rng(1000 + k)``; instance i of a batch
-uses ``default_rng([1000 + k, i])``.
+Seeds: the single sparse QP uses ``default_rng(1000)``, the small dense batch
+1001, the large dense QP 1002, the MPC QP 1003 and the parametric family 1004;
+instance i of a batch uses ``default_rng([base, i])``.
 """
 
 from __future__ import annotations
@@ -38,24 +39,24 @@ def _feasible_pair(rng, a, p, z):
 # ---------------------------------------------------------------------------
 # Benchmark configurations.
 # ---------------------------------------------------------------------------
-CFG0_M_DENSITY = 0.10  # density of M in P = M M^T + 1e-2 I (not fixed upstream)
+SPARSE_QP_M_DENSITY = 0.10  # density of M in P = M M^T + 1e-2 I (not fixed upstream)
 
 
-def config0(seed: int = 1000):
+def sparse_qp_n200(seed: int = 1000):
   """Single sparse QP: n=200, m=300, z=50; A = 5% Bernoulli mask x N(0,1);
   P = M M^T + 1e-2 I with M 200x20 sparse N(0,1) (10% dense)."""
   rng = np.random.default_rng(seed)
   n, m, z = 200, 300, 50
   mask = rng.random((m, n)) < 0.05
   a = sp.csc_matrix(np.where(mask, rng.normal(size=(m, n)), 0.0))
-  mm = sp.random(n, 20, density=CFG0_M_DENSITY, format="csc", rng=rng,
+  mm = sp.random(n, 20, density=SPARSE_QP_M_DENSITY, format="csc", rng=rng,
                  data_rvs=lambda k: rng.normal(size=k))
   p = sp.csc_matrix(mm @ mm.T + 1e-2 * sp.eye(n))
   b, c = _feasible_pair(rng, a, p, z)
   return a, b, c, z, p
 
 
-def config1_instance(i: int, base: int = 1001):
+def small_dense_instance(i: int, base: int = 1001):
   """One of the uneven small dense QPs: n ~ U{8..64}, m = 2n, z = n // 4,
   A ~ N(0,1) dense, P = L L^T + 1e-3 I with L n x n//2 ~ N(0,1)."""
   rng = np.random.default_rng([base, i])
@@ -69,11 +70,11 @@ def config1_instance(i: int, base: int = 1001):
   return sp.csc_matrix(a_d), b, c, z, sp.csc_matrix(p_d)
 
 
-def config1(count: int = 4096):
-  return [config1_instance(i) for i in range(count)]
+def small_dense_batch(count: int = 4096):
+  return [small_dense_instance(i) for i in range(count)]
 
 
-def config2(seed: int = 1002, n: int = 4096, m: int = 8192, z: int = 1024, rank: int = 256):
+def large_dense(seed: int = 1002, n: int = 4096, m: int = 8192, z: int = 1024, rank: int = 256):
   """Large dense QP: A ~ N(0, 1/n); P = U diag(d) U^T + 1e-4 I with U n x rank
   ~ N(0,1), d ~ U(0.1, 10).  Returns dense arrays (a, b, c, z, p)."""
   rng = np.random.default_rng(seed)
@@ -152,14 +153,14 @@ def mpc_feasible(horizon: int, seed: int = 1003, active_frac: float = 0.1,
   return a, b, c, z, p
 
 
-def config3():
+def mpc_t500():
   return mpc_feasible(500)
 
 
-CFG4_NX = 40  # initial-state rows of b carry the parameter
+PARAMETRIC_NX = 40  # initial-state rows of b carry the parameter
 
 
-def config4_family(count: int = 20000, horizon: int = 50, dim: int = 32, seed: int = 1004):
+def parametric_mpc_family(count: int = 20000, horizon: int = 50, dim: int = 32, seed: int = 1004):
   """Parametric family: fixed (A, P) of the T=50 MPC QP; (b, c) = (b_bar,
   c_bar) + W theta, theta ~ N(0, I_dim), W with N(0, 0.1^2) entries (std 0.1).
 
@@ -175,14 +176,14 @@ def config4_family(count: int = 20000, horizon: int = 50, dim: int = 32, seed: i
   rng = np.random.default_rng(seed)
   mtot, n = a.shape
   w = np.zeros((mtot + n, dim))
-  w[:CFG4_NX] = rng.normal(scale=0.1, size=(CFG4_NX, dim))
+  w[:PARAMETRIC_NX] = rng.normal(scale=0.1, size=(PARAMETRIC_NX, dim))
   w[mtot:] = rng.normal(scale=0.1, size=(n, dim))
   thetas = np.random.default_rng([seed, 2]).normal(size=(count, dim))
   return a, z, p, b_bar, c_bar, w, thetas
 
 
-def config4_instance(family, i: int):
-  """(a, b, c, z, p) of instance i of a family from config4_family."""
+def parametric_mpc_instance(family, i: int):
+  """(a, b, c, z, p) of instance i of a family from parametric_mpc_family."""
   a, z, p, b_bar, c_bar, w, thetas = family
   d = w @ thetas[i]
   m = a.shape[0]

@@ -83,10 +83,10 @@ def _cases(tests):
       [[3.0, -1.0], [-1.0, 2.0]])
   add("minimal", [[-1.0], [1.0]], [0.0, 2.0], [-1.0], 0, [[1.0]])
   out = list(cases)
-  a, b, c, z, p = problems.config0()
+  a, b, c, z, p = problems.sparse_qp_n200()
   out.append(("config0", a, b, c, z, p))
   for i in range(6):
-    a, b, c, z, p = problems.config1_instance(i)
+    a, b, c, z, p = problems.small_dense_instance(i)
     out.append((f"config1_i{i}", a, b, c, z, p))
   return out
 

@@ -44,7 +44,7 @@ def test_version_and_last_error(lib):
 
 
 def test_plan_orders_by_cost_and_sizes_workspace(lib):
-  probs = [batch.DenseProblem(*_dense(problems.config1_instance(i))) for i in range(50)]
+  probs = [batch.DenseProblem(*_dense(problems.small_dense_instance(i))) for i in range(50)]
   hb = batch.HostBatch(probs, batch.SolveOptions())
   ns = hb.inst["n"][hb.order[:hb.count]]
   costs = hb.inst["m"][hb.order] * ns.astype(float) ** 2 + ns.astype(float) ** 3 / 3

@@ -48,10 +48,10 @@ def test_band_and_dense_paths_agree():
 
 def test_band_batch_of_parametric_instances():
   """The parametric family: same A, P; (b, c) perturbed per instance."""
-  fam = problems.config4_family(count=24, horizon=8)
+  fam = problems.parametric_mpc_family(count=24, horizon=8)
   qps, refs = [], []
   for i in range(24):
-    a, b, c, z, p = problems.config4_instance(fam, i)
+    a, b, c, z, p = problems.parametric_mpc_instance(fam, i)
     qps.append(qb.QTQP(a=a, b=b, c=c, z=z, p=p))
     refs.append(orc.solve(a, b, c, z, p, backend="superlu"))
   sols = qb.solve_batch(qps, storage="band")

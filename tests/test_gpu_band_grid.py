@@ -93,7 +93,7 @@ def test_grid_infeasible_mpc():
 
 def test_grid_full_size_mpc():
   """The T=500 MPC QP (n=30000, m=80000) through QTQP.solve."""
-  a, b, c, z, p = problems.config3()
+  a, b, c, z, p = problems.mpc_t500()
   q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
   assert q.storage_format(single=True) == "band_grid"
   sol = q.solve(verbose=False)

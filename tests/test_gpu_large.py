@@ -21,8 +21,8 @@ pytestmark = pytest.mark.gpu
 OBJ_TOL = 1e-6
 
 
-def _cfg2_like(n, m, z, rank, seed=1002):
-  a, b, c, z, p = problems.config2(seed=seed, n=n, m=m, z=z, rank=rank)
+def _large_dense_like(n, m, z, rank, seed=1002):
+  a, b, c, z, p = problems.large_dense(seed=seed, n=n, m=m, z=z, rank=rank)
   return a, b, c, z, p
 
 
@@ -35,7 +35,7 @@ def _solve(a, b, c, z, p, precision, **kw):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_large_matches_oracle(shape, precision):
   n, m, z, rank = shape
-  a, b, c, z, p = _cfg2_like(n, m, z, rank)
+  a, b, c, z, p = _large_dense_like(n, m, z, rank)
   sol = _solve(a, b, c, z, p, precision)
   ref = orc.solve(sp.csc_matrix(a), b, c, z, sp.csc_matrix(p), backend="dense")
   assert sol.status.value == ref.status
@@ -58,7 +58,7 @@ def test_large_certificates(precision):
 
 
 def test_large_and_block_paths_agree():
-  a, b, c, z, p = _cfg2_like(200, 400, 50, 16, seed=7)
+  a, b, c, z, p = _large_dense_like(200, 400, 50, 16, seed=7)
   q = qb.QTQP(a=sp.csc_matrix(a), b=b, c=c, z=z, p=sp.csc_matrix(p))
   s_large = qb.solve_batch([q], storage="large")[0]
   s_dense = qb.solve_batch([q], storage="dense")[0]
@@ -76,7 +76,7 @@ def test_large_lp_without_p():
 
 
 def test_single_qp_solve_routes_to_the_large_path():
-  a, b, c, z, p = _cfg2_like(320, 640, 64, 16, seed=3)
+  a, b, c, z, p = _large_dense_like(320, 640, 64, 16, seed=3)
   q = qb.QTQP(a=sp.csc_matrix(a), b=b, c=c, z=z, p=sp.csc_matrix(p))
   assert q.storage_format(single=True) == "large"
   sol = q.solve(verbose=False)

@@ -78,9 +78,9 @@ def test_decode_matches_oracle():
 
 
 def _family(count, horizon=8):
-  fam = problems.config4_family(count=count, horizon=horizon)
+  fam = problems.parametric_mpc_family(count=count, horizon=horizon)
   qps = [qb.QTQP(a=a, b=b, c=c, z=z, p=p) for a, b, c, z, p in
-         (problems.config4_instance(fam, i) for i in range(count))]
+         (problems.parametric_mpc_instance(fam, i) for i in range(count))]
   return fam[-1], qps
 
 

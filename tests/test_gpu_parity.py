@@ -65,11 +65,11 @@ def test_fp64_trajectory_follows_reference():
     np.testing.assert_allclose(got, ref[key][:k], rtol=1e-5, atol=1e-10, err_msg=key)
 
 
-def test_batch_matches_oracle_config1():
+def test_batch_matches_oracle_small_dense():
   """64 uneven dense QPs of the batched workload in one launch vs the oracle."""
   qps, refs = [], []
   for i in range(64):
-    a, b, c, z, p = problems.config1_instance(i)
+    a, b, c, z, p = problems.small_dense_instance(i)
     qps.append(qb.QTQP(a=a, b=b, c=c, z=z, p=p))
     refs.append(orc.solve(a, b, c, z, p, backend="dense"))
   for precision in ("fp64", "mixed"):

@@ -63,7 +63,7 @@ def test_presolve_drops_and_restores_rows():
 
 
 def test_dense_problem_packing():
-  a, b, c, z, p = problems.config1_instance(3)
+  a, b, c, z, p = problems.small_dense_instance(3)
   q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
   dp = q.dense_problem()
   np.testing.assert_array_equal(dp.a, a.toarray())

@@ -26,7 +26,7 @@ def _dense(prob):
 
 def _mixed_batch():
   """Small on-chip QPs plus two QPs whose A and P live in the scratch."""
-  probs = [_dense(problems.config1_instance(i)) for i in range(24)]
+  probs = [_dense(problems.small_dense_instance(i)) for i in range(24)]
   probs += [_dense(problems.feasible(220, 130, 12, s)) for s in (5, 6)]
   return batch.HostBatch(probs, batch.SolveOptions())
 
