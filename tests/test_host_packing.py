@@ -1,7 +1,8 @@
-"""Host packing of the banded batch (CPU only): every instance's A (CSR and
-CSC), P, b and c can be read back exactly from the int32/double pools at the
+"""Host packing of the batches (CPU only).  Banded batch: every instance's A
+(CSR and CSC), P, b and c read back exactly from the int32/double pools at the
 offsets in its descriptor; problems built from the same A and P objects share
 one packed copy; the plan orders every instance once and sizes a workspace.
+Dense batch: A, P, b and c read back exactly from the row-major pools.
 """
 
 import numpy as np
@@ -67,3 +68,27 @@ def test_plan_orders_each_instance_once():
   assert hb.workspace_bytes > 0
   assert hb.n_total == sum(int(d["n"]) for d in hb.inst)
   assert hb.m_total == sum(int(d["m"]) for d in hb.inst)
+
+
+def test_dense_pools_read_back_every_instance():
+  """The dense batch's pools (A m x n and P n x n row-major per instance; an
+  LP or an all-zero P packs no P) read back exactly at each descriptor's
+  offsets."""
+  from qtqp_b200 import batch
+  probs = []
+  for i in range(5):
+    a, b, c, z, p = problems.small_dense_instance(i)
+    probs.append(batch.DenseProblem(a.toarray(), b, c, z, p.toarray() if i != 2 else None))
+  hb = batch.HostBatch(probs, SolveOptions())
+  for i, pr in enumerate(probs):
+    d = hb.inst[i]
+    m, n = pr.a.shape
+    a0, p0 = int(d["a_off"]), int(d["p_off"])
+    np.testing.assert_array_equal(hb.a_pool[a0:a0 + m * n].reshape(m, n), pr.a)
+    assert int(d["has_p"]) == (pr.p is not None)
+    if pr.p is not None:
+      np.testing.assert_array_equal(hb.p_pool[p0:p0 + n * n].reshape(n, n), pr.p)
+    m0, n0 = int(d["m_off"]), int(d["n_off"])
+    np.testing.assert_array_equal(hb.b_pool[m0:m0 + m], pr.b)
+    np.testing.assert_array_equal(hb.c_pool[n0:n0 + n], pr.c)
+  assert hb.p_pool.size == sum(p.a.shape[1] ** 2 for p in probs if p.p is not None)
