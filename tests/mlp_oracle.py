@@ -1,4 +1,5 @@
-"""Numpy oracle of the warm-start MLP (theta -> 256 -> 256 -> out, ReLU, MSE).
+"""Numpy oracle of the warm-start MLP (theta -> 256 -> 256 -> out, ReLU, MSE;
+optionally a hinge term on the sign of the inequality outputs).
 
 Test infrastructure: forward and hand-derived backward in FP64, checked by
 finite differences (tests/test_mlp_oracle.py) and used as the reference for
@@ -25,9 +26,34 @@ def loss(params, x, t):
 
 def gradients(params, x, t):
   """Gradients of mean((y - t)^2) w.r.t. (w1, b1, w2, b2, w3, b3)."""
-  _, _, w2, _, w3, _ = params
-  a1, h1, a2, h2, y = forward(params, x)
+  fw = forward(params, x)
+  y = fw[-1]
+  return _backward(params, x, fw, 2.0 * (y - t) / y.size)
+
+
+def hinge_loss(params, x, t, cols, zero, sign, weight, margin=0.5):
+  """mean((y - t)^2) + weight * mean over (batch, cols) of
+  relu(margin - sign * (y[:, cols] - zero)): the MSE plus a hinge that pushes
+  each inequality output to the side of its decision point (`zero`, the
+  standardised value of y - s = 0) given by the target's sign (+1 / -1)."""
+  y = forward(params, x)[-1]
+  h = np.maximum(margin - sign * (y[:, cols] - zero), 0.0)
+  return float(np.mean((y - t) ** 2) + weight * h.mean())
+
+
+def hinge_gradients(params, x, t, cols, zero, sign, weight, margin=0.5):
+  """Gradients of hinge_loss w.r.t. (w1, b1, w2, b2, w3, b3)."""
+  fw = forward(params, x)
+  y = fw[-1]
   dy = 2.0 * (y - t) / y.size
+  active = (margin - sign * (y[:, cols] - zero)) > 0.0
+  dy[:, cols] += -weight * sign * active / (y.shape[0] * len(cols))
+  return _backward(params, x, fw, dy)
+
+
+def _backward(params, x, fw, dy):
+  _, _, w2, _, w3, _ = params
+  a1, h1, a2, h2, _ = fw
   g3 = h2.T @ dy
   gb3 = dy.sum(axis=0)
   dh2 = (dy @ w3.T) * (a2 > 0)

@@ -32,6 +32,38 @@ def test_backward_matches_finite_differences():
       np.testing.assert_allclose(gflat[idx], (lp - lm) / (2 * h), rtol=1e-5, atol=1e-8)
 
 
+def test_hinge_backward_matches_finite_differences():
+  """The MSE + hinge gradient (the training change that raises warm-start
+  acceptance) against central differences, away from the hinge's kink."""
+  rng = np.random.default_rng(1)
+  params = _params(rng)
+  x = rng.normal(size=(7, 4))
+  t = rng.normal(size=(7, 5))
+  cols = np.array([2, 3, 4])
+  zero = rng.normal(size=3) * 0.2
+  sign = np.where(t[:, cols] > zero, 1.0, -1.0)
+  args = (x, t, cols, zero, sign, 0.7)
+  y = mlp_oracle.forward(params, x)[-1]
+  kink = np.abs(0.5 - sign * (y[:, cols] - zero))
+  assert kink.min() > 1e-3 and np.any(0.5 - sign * (y[:, cols] - zero) > 0)
+  grads = mlp_oracle.hinge_gradients(params, *args)
+  h = 1e-7
+  for p, g in zip(params, grads):
+    flat, gflat = p.reshape(-1), g.reshape(-1)
+    for idx in range(flat.size):
+      old = flat[idx]
+      flat[idx] = old + h
+      lp = mlp_oracle.hinge_loss(params, *args)
+      flat[idx] = old - h
+      lm = mlp_oracle.hinge_loss(params, *args)
+      flat[idx] = old
+      np.testing.assert_allclose(gflat[idx], (lp - lm) / (2 * h), rtol=1e-5, atol=1e-7)
+  # With zero weight it is the plain MSE gradient.
+  plain = mlp_oracle.gradients(params, x, t)
+  for g0, g1 in zip(plain, mlp_oracle.hinge_gradients(params, x, t, cols, zero, sign, 0.0)):
+    np.testing.assert_array_equal(g0, g1)
+
+
 def test_adam_first_step_moves_by_lr():
   p = np.array([1.0, -2.0, 3.0])
   g = np.array([0.5, -0.1, 0.0])
