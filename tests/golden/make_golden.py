@@ -84,10 +84,10 @@ def _cases(tests):
   add("minimal", [[-1.0], [1.0]], [0.0, 2.0], [-1.0], 0, [[1.0]])
   out = list(cases)
   a, b, c, z, p = problems.sparse_qp_n200()
-  out.append(("config0", a, b, c, z, p))
+  out.append(("sparse_qp_n200", a, b, c, z, p))
   for i in range(6):
     a, b, c, z, p = problems.small_dense_instance(i)
-    out.append((f"config1_i{i}", a, b, c, z, p))
+    out.append((f"small_dense_i{i}", a, b, c, z, p))
   return out
 
 
@@ -103,7 +103,7 @@ def make_e2e(qtqp, tests):
     out[name + "/z"] = np.array(z)
     for backend in ("SCIPY", "SCIPY_DENSE"):
       for eq in (True, False):
-        if not eq and (backend == "SCIPY" or name.startswith("config")):
+        if not eq and (backend == "SCIPY" or name.startswith(("sparse_qp_n200", "small_dense_i"))):
           continue
         tag = f"{name}/{backend}/{'eq' if eq else 'noeq'}"
         sol = qtqp.QTQP(a=a, b=b, c=c, z=z, p=p).solve(
