@@ -167,8 +167,9 @@ int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst,
  * library until the process exits).  Plans needing more scratch than
  * qtqp_dense_batch_noalloc_max_workspace() are rejected with
  * QTQP_ERR_BAD_ARG.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call uses the same array, so calls whose work overlaps on
+ * address (cudaGetSymbolAddress), and so does the first call after the
+ * device's context was replaced (cudaDeviceReset); make those calls before
+ * any stream capture.  Every call uses the same array, so calls whose work overlaps on
  * the GPU (e.g. on two streams) race and must not be issued; groups run in
  * sequence on `stream`.  Arguments and results as qtqp_dense_batch_solve. */
 size_t qtqp_dense_batch_noalloc_max_workspace(void);
@@ -350,6 +351,19 @@ int qtqp_kkt_dense_solve(int32_t n, int32_t m, const double* d_rhs,
 /* __matmul__ (solvers_dense.py:118-128): out = K_reg x. */
 int qtqp_kkt_dense_matvec(int32_t n, int32_t m, const double* d_x,
                           double* d_out, void* d_ws, void* stream);
+
+/* Ruiz equilibration of one dense QP on the device, the first phase of the
+ * device IPM on its own: replaces QTQP._equilibrate
+ * (src/qtqp/__init__.py:616-663; 10 sweeps, scales clipped to [1e-3, 1e3],
+ * a_ij scaled by d_i * e_j).  Inputs: A (m x n) and P (n x n, or NULL for
+ * P = 0), b (m), c (n), row-major.  Outputs: d (m), e (n), the equilibrated
+ * A (m x n) and P (n x n).  d_ws: qtqp_kkt_dense_workspace_bytes(n, m)
+ * bytes (overwritten). */
+int qtqp_dense_equilibrate(int32_t n, int32_t m, const double* d_a,
+                           const double* d_p, const double* d_b,
+                           const double* d_c, void* d_ws, double* d_d,
+                           double* d_e, double* d_a_eq, double* d_p_eq,
+                           void* stream);
 
 #ifdef __cplusplus
 }

@@ -28,15 +28,20 @@ struct ForkStreams {
   cudaEvent_t fork = nullptr;
   bool ready = false;
 };
-static std::mutex g_fork_mu;
+static std::mutex g_fork_mu[64];
 static ForkStreams g_fork[64];
 
-static int fork_streams(ForkStreams** out) {
+// The side streams of the current device.  The caller holds `lk`, the
+// device's fork lock, from the fork record until the last join has been
+// enqueued: the fork/join events are shared by every call on the device, and
+// a second host thread re-recording them in between would make this call's
+// groups wait on the other call's stream instead of this one's.
+static int fork_streams(ForkStreams** out, std::unique_lock<std::mutex>& lk) {
   int dev = 0;
   int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   if (rc) return rc;
   if (dev < 0 || dev >= 64) return fail(QTQP_ERR_BAD_ARG, "device index out of range");
-  std::lock_guard<std::mutex> lk(g_fork_mu);
+  lk = std::unique_lock<std::mutex>(g_fork_mu[dev]);
   ForkStreams& f = g_fork[dev];
   if (!f.ready) {
     for (int g = 0; g < QTQP_MAX_GROUPS; ++g) {
@@ -206,8 +211,9 @@ extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const i
   base.opt = *opt;
   const int ng = plan->num_groups;
   ForkStreams* fk = nullptr;
+  std::unique_lock<std::mutex> fork_lock;  // held until every join is enqueued
   if (ng > 1) {
-    rc = fork_streams(&fk);
+    rc = fork_streams(&fk, fork_lock);
     if (rc) return rc;
     rc = cuda_check(cudaEventRecord(fk->fork, st), "cudaEventRecord");
     if (rc) return rc;
@@ -258,21 +264,57 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 
 static std::mutex g_static_mu;
 static void* g_static_ptr[64];
+static unsigned long long g_static_ctx[64];  // context the cached address belongs to
+
+// Unique id of the calling thread's current CUDA context (the driver's
+// cuCtxGetCurrent + cuCtxGetId, reached through the runtime so that the
+// library needs no link against the driver library); 0 if unavailable.
+static unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(p);
+  });
+  if (get_current == nullptr || get_id == nullptr) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 // Device address of g_static_scratch on the current device.  The symbol's
-// name is only a host-side handle, so the address is looked up once per
-// device (with that device current) and cached.
+// name is only a host-side handle, so the address is looked up with that
+// device current and cached per device.  The cache remembers the context it
+// was taken in: after a cudaDeviceReset the device's next context gets a new
+// id and the address is looked up again instead of pointing into the
+// destroyed context.
 static int static_scratch(void** out) {
   int dev = 0;
   int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   if (rc) return rc;
   if (dev < 0 || dev >= 64) return fail(QTQP_ERR_BAD_ARG, "device index out of range");
+  // Before the runtime's first call on this device there is no current
+  // context (id 0): the lookup then runs, initialises the context, and the
+  // id is read afterwards.
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lk(g_static_mu);
-  if (g_static_ptr[dev] == nullptr) {
+  if (g_static_ptr[dev] == nullptr || ctx == 0 || g_static_ctx[dev] != ctx) {
     void* p = nullptr;
     rc = cuda_check(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress");
     if (rc) return rc;
     g_static_ptr[dev] = p;
+    g_static_ctx[dev] = current_context_id();
   }
   *out = g_static_ptr[dev];
   return QTQP_OK;

@@ -147,13 +147,11 @@ extern "C" int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t h
   if (rc) return rc;
   rc = make_map_f32(&ml, reinterpret_cast<const float*>(ws + L.xlo_off), L.npad, L.mpad, L.mpad);
   if (rc) return rc;
-  static std::once_flag attr;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(attr, [] {
-    attr_err = cudaFuncSetAttribute(large_solve_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLargeSmem));
-  });
-  rc = cuda_check(attr_err, "cudaFuncSetAttribute(large_solve_kernel)");
+  // Set on every call: the attribute belongs to the current device.
+  rc = cuda_check(cudaFuncSetAttribute(large_solve_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(kLargeSmem)),
+                  "cudaFuncSetAttribute(large_solve_kernel)");
   if (rc) return rc;
   int dev = 0, sms = 0, per_sm = 0, coop = 0;
   cudaGetDevice(&dev);

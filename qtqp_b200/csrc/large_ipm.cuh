@@ -6,11 +6,13 @@
 //   Gram      G = P_off + diag(Rx) + A^T diag(1/Ry) A  (solvers_dense.py:99-116)
 //             FP32 factor: X = (diag(1/sqrt(Ry)) A)^T split into TF32 hi + lo,
 //             lower 128 x 128 tiles of X X^T on tcgen05 (three TF32 products,
-//             FP32 accumulation in TMEM).  FP64 factor: 64 x 64 SIMT tiles.
+//             FP32 accumulation in TMEM).  FP64 factor: lower 128 x 128 tiles
+//             on the FP64 tensor cores (DMMA, mma.sync m8n8k4).
 //   Cholesky  right-looking with 128-wide panels: the diagonal block by one
 //             CTA in shared memory, the panel by row-wise substitution (one
-//             warp per row), the trailing update in 64 x 64 SIMT tiles; then
-//             the inverse of every diagonal block.
+//             warp per row), the trailing update in 128 x 128 tiles (DMMA in
+//             FP64, 8 x 8 register tiles in FP32); then the inverse of every
+//             diagonal block.
 //   Solves    block forward / backward substitution with the inverted
 //             diagonal blocks, one grid barrier per 128-block step.
 //
@@ -137,6 +139,7 @@ __device__ void large_gram_tc(S& s) {
         const int st = int(g % kTcStages);
         const uint32_t use = g / kTcStages;
         if (use > 0 && !tc::mbar_wait(&empty[st], (use - 1) & 1)) {
+          s.tc_load--;  // stage g was not issued
           atomicExch(failed, 1);
           break;
         }
@@ -153,6 +156,7 @@ __device__ void large_gram_tc(S& s) {
         const int st = int(g % kTcStages);
         const uint32_t use = g / kTcStages;
         if (!tc::mbar_wait(&full[st], use & 1)) {
+          s.tc_mma--;  // stage g was not consumed
           atomicExch(failed, 1);
           break;
         }
@@ -178,8 +182,21 @@ __device__ void large_gram_tc(S& s) {
     if (!tc::mbar_wait(done, s.tc_tiles & 1)) atomicExch(failed, 1);
     s.tc_tiles++;
     tc::fence_after_sync();
+    if (warp == 1 && lane == 0) failed[1] = int(s.tc_mma);  // stages consumed so far
     __syncthreads();
-    if (*failed == 0) {
+    if (*failed != 0) {
+      // A bounded wait gave up: stop issuing tiles.  Before the CTA moves on,
+      // the producer waits (again bounded) for the stages it issued that the
+      // MMA issuer never consumed, so that no bulk copy still targets the
+      // ring when the arena is reused.
+      if (warp == 0 && lane == 0) {
+        for (uint32_t g = uint32_t(failed[1]); g < s.tc_load; ++g)
+          if (!tc::mbar_wait(&full[g % kTcStages], (g / kTcStages) & 1)) break;
+      }
+      __syncthreads();
+      break;
+    }
+    {
       const int q = warp & 3, half = warp >> 2;
       const int row = ti * kLB + q * 32 + lane;
       float* grow = s.g32l + size_t(row) * npad + size_t(tj) * kLB + half * 64;

@@ -186,13 +186,11 @@ int launch_gram_tf32(int n, int k, const float* hi, const float* lo, int ld, flo
   if (rc) return rc;
   rc = make_map_f32(&ml, split ? lo : hi, n, k, ld);
   if (rc) return rc;
-  static std::once_flag attr;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(attr, [] {
-    attr_err = cudaFuncSetAttribute(gram_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(kGramSmem));
-  });
-  rc = cuda_check(attr_err, "cudaFuncSetAttribute(gram_tf32_kernel)");
+  // Set on every call: the attribute belongs to the current device.
+  rc = cuda_check(cudaFuncSetAttribute(gram_tf32_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(kGramSmem)),
+                  "cudaFuncSetAttribute(gram_tf32_kernel)");
   if (rc) return rc;
   const int nt = n / kGramTile;
   gram_tf32_kernel<<<nt * (nt + 1) / 2, 128, kGramSmem, st>>>(mh, ml, k / kGramBK, split, c, ldc,

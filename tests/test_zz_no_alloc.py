@@ -6,7 +6,12 @@ loop that must not touch the allocator once started): its scratch is a fixed
 array inside the library instead of a caller-provided workspace.  These tests
 call it through the C-ABI twice in a row and require the same results as the
 workspace entry point, and check that a plan larger than the fixed array is
-refused before anything is launched.  This file is collected last on purpose.
+refused before anything is launched.
+
+The file name sorts last, so pytest collects it after every other test file:
+a run that stops at the first failure (-x) has then already run all the other
+tests when one of these fails.  The tests also pass on their own in a fresh
+process (the entry point looks the array's address up on its first call).
 """
 
 import numpy as np
