@@ -47,11 +47,25 @@ class LinearSolver(enum.Enum):
 
   AUTO resolves to CUDA.  CUDA runs the device-resident loop whose KKT layer is
   the CudaDenseSolver algorithm; the class is also usable on its own as a
-  plugin for the reference's DirectKktSolver.
+  plugin for the reference's DirectKktSolver.  The reference's other members
+  name CPU / vendor library backends this build does not ship: solving with
+  one raises ImportError, as the reference does when a backend's library is
+  not installed.
   """
 
   AUTO = "auto"
   CUDA = direct.CudaDenseSolver
+  ACCELERATE = direct.AccelerateSolver
+  SCIPY = direct.ScipySolver
+  SCIPY_DENSE = direct.ScipyDenseSolver
+  CUPY_DENSE = direct.CupyDenseSolver
+  UMFPACK = direct.UmfpackSolver
+  PARDISO = direct.MklPardisoSolver
+  QDLDL = direct.QdldlSolver
+  CHOLMOD = direct.CholModSolver
+  CUDSS = direct.CuDssSolver
+  EIGEN = direct.EigenSolver
+  MUMPS = direct.MumpsSolver
 
 
 class SolutionStatus(enum.Enum):
@@ -225,8 +239,10 @@ class QTQP:
         linear_solver_atol=linear_solver_atol, linear_solver_rtol=linear_solver_rtol,
         equilibrate=equilibrate, collect_stats=collect_stats, precision=precision)
     opts.validate()
-    if linear_solver not in (LinearSolver.AUTO, LinearSolver.CUDA):
+    if not isinstance(linear_solver, LinearSolver):
       raise ValueError(f"unsupported linear_solver {linear_solver}")
+    if linear_solver not in (LinearSolver.AUTO, LinearSolver.CUDA):
+      linear_solver.value()  # raises ImportError: the backend is not shipped
     _lib.require_device()
     start = timeit.default_timer()
     if verbose:
@@ -313,9 +329,12 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   if warm_start is not None:
     if any(k != "band" for k in kinds):
       raise ValueError("warm_start needs every problem on the banded path")
-    model, _ = warm_start
+    model, thetas = warm_start
     if any((q.n, q.m) != (model.n, model.m) for q in problems):
       raise ValueError("warm_start: every problem must have the model's (n, m)")
+    if np.asarray(thetas).shape[0] != len(problems):
+      raise ValueError(f"warm_start: {np.asarray(thetas).shape[0]} parameter vectors for "
+                       f"{len(problems)} problems")
   _lib.require_device()
   records = bool(verbose or opts.collect_stats)
   per = {}  # kind -> (indices, results, x, y, s, stats, inst)

@@ -5,16 +5,20 @@
 solve / __matmul__ / format / free.  ``CudaDenseSolver`` implements it on the
 GPU through the C-ABI (Gram/Schur reduction + Cholesky, the algorithm of
 src/qtqp/solvers_dense.py:25-145), so it can be plugged into the reference's
-own ``DirectKktSolver``.  ``DirectKktSolver`` here is the host-side refinement
-driver with the reference's semantics (direct.py:112-311), used to exercise a
-plugin in isolation.
+own ``DirectKktSolver`` (direct.py:112-311), which drives the FP64 iterative
+refinement around it.
+
+The reference's other backends (SuperLU, PARDISO, CHOLMOD, cuDSS, ... in
+src/qtqp/solvers_*.py) wrap CPU or vendor libraries that this build does not
+ship; their enum names exist for drop-in use and raise ImportError when
+instantiated, which is what the reference raises for a backend whose library
+is not installed.
 """
 
 from __future__ import annotations
 
 import ctypes
-import logging
-from typing import Any, Literal
+from typing import Literal
 
 import numpy as np
 import scipy.sparse as sp
@@ -153,72 +157,24 @@ class CudaDenseSolver(LinearSolver):
     self._a_dev = self._p_dev = None
 
 
-class DirectKktSolver:
-  """Regularised KKT solve with FP64 iterative refinement (direct.py:112-311).
+def _unavailable(name: str, ref: str) -> type:
+  """A backend class of the reference that this build does not ship."""
 
-      [ P + mu I        A^T      ] [x]   [ rhs_x ]
-      [     A      -(D + mu I)   ] [y] = [-rhs_y ]
-  """
+  def __init__(self, *args, **kwargs):
+    raise ImportError(f"{name} ({ref}) is not part of the B200 build: use "
+                      "LinearSolver.CUDA (or AUTO)")
 
-  def __init__(self, *, a, p, z, min_static_regularization,
-               max_iterative_refinement_steps, atol, rtol, solver: LinearSolver):
-    self.m, self.n = a.shape
-    self.z = z
-    self._p_diags = p.diagonal()
-    self.min_static_regularization = min_static_regularization
-    self.max_iterative_refinement_steps = max_iterative_refinement_steps
-    self._atol, self._rtol = atol, rtol
-    self._solver = solver
-    solver.set_dims(n=self.n, m=self.m, z=self.z)
-    self._kkt = sp.bmat(
-        [[sp.triu(p, format="csc") + sp.eye(self.n, format="csc"), a.T],
-         [None, sp.eye(self.m, format="csc")]],
-        format=solver.format(), dtype=np.float64)
-    solver.set_kkt(self._kkt)
-    nm = self.n + self.m
-    self._true = np.empty(nm)
-    self._reg = np.empty(nm)
-    self._rhs = np.empty(nm)
-    self._corr = np.zeros(nm)
+  return type(name, (LinearSolver,), {"__init__": __init__, "__doc__": f"Not shipped: {ref}."})
 
-  def update(self, mu: float, s: np.ndarray, y: np.ndarray) -> None:
-    n, z = self.n, self.z
-    self._true[:n] = self._p_diags
-    self._true[:n] += mu
-    self._true[n:n + z] = mu
-    self._true[n + z:] = s[z:] / y[z:] + mu
-    np.maximum(self._true, self.min_static_regularization, out=self._reg)
-    self._true[n:] *= -1.0
-    self._reg[n:] *= -1.0
-    self._solver.update_diag(self._reg)
-    self._solver.factorize()
-    np.subtract(self._reg, self._true, out=self._corr)
 
-  def solve(self, rhs: np.ndarray, warm_start: np.ndarray) -> tuple[np.ndarray, dict[str, Any]]:
-    np.copyto(self._rhs, rhs)
-    self._rhs[self.n:] *= -1.0
-    rhs_norm = np.linalg.norm(self._rhs, np.inf)
-    tol = self._atol + self._rtol * rhs_norm
-    sol = warm_start.copy()
-    res = self._rhs - self._solver @ sol + self._corr * sol
-    res_norm = np.linalg.norm(res, np.inf)
-    status, solves = "non-converged", 0
-    for solves in range(1, self.max_iterative_refinement_steps + 1):
-      prev = res_norm
-      sol += self._solver.solve(res)
-      res = self._rhs - self._solver @ sol + self._corr * sol
-      res_norm = np.linalg.norm(res, np.inf)
-      if res_norm < tol:
-        status = "converged"
-        break
-      if res_norm >= prev:
-        logging.debug("IR stalled at step %d (%e -> %e)", solves, prev, res_norm)
-        status = "stalled"
-        break
-    if np.any(np.isnan(sol)):
-      raise ValueError("Linear solver returned NaNs.")
-    return sol, {"solves": solves, "final_residual_norm": res_norm, "rhs_norm": rhs_norm,
-                 "tolerance": tol, "converged": status == "converged", "status": status}
-
-  def free(self) -> None:
-    self._solver.free()
+AccelerateSolver = _unavailable("AccelerateSolver", "solvers_sparse.py, Apple Accelerate")
+ScipySolver = _unavailable("ScipySolver", "solvers_sparse.py, SciPy SuperLU")
+ScipyDenseSolver = _unavailable("ScipyDenseSolver", "solvers_dense.py, LAPACK potrf")
+CupyDenseSolver = _unavailable("CupyDenseSolver", "solvers_gpu.py, CuPy")
+UmfpackSolver = _unavailable("UmfpackSolver", "solvers_sparse.py, UMFPACK")
+MklPardisoSolver = _unavailable("MklPardisoSolver", "solvers_sparse.py, MKL PARDISO")
+QdldlSolver = _unavailable("QdldlSolver", "solvers_sparse.py, QDLDL")
+CholModSolver = _unavailable("CholModSolver", "solvers_sparse.py, CHOLMOD")
+CuDssSolver = _unavailable("CuDssSolver", "solvers_gpu.py, cuDSS")
+EigenSolver = _unavailable("EigenSolver", "solvers_sparse.py, Eigen")
+MumpsSolver = _unavailable("MumpsSolver", "solvers_sparse.py, MUMPS")

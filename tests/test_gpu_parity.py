@@ -14,7 +14,7 @@ import scipy.sparse as sp
 import qtqp_b200 as qb
 from oracle import qtqp_oracle as orc
 from qtqp_b200 import problems
-from tests import golden_io, kkt_checks
+from tests import golden_io, kkt_checks, kkt_driver
 
 pytestmark = pytest.mark.gpu
 
@@ -165,7 +165,7 @@ def test_plugin_backend_residual():
     s[:z] = 0.0
     d = np.concatenate([np.zeros(z), s[z:] / y[z:]])
     for precision in ("fp64", "mixed"):
-      kkt = direct.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
+      kkt = kkt_driver.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
                                    max_iterative_refinement_steps=30, atol=1e-12,
                                    rtol=1e-12, solver=direct.CudaDenseSolver(precision))
       kkt.update(mu=mu, s=s, y=y)
@@ -184,7 +184,7 @@ def test_plugin_matvec_matches_full_kkt():
   mu = rng.uniform()
   s, y = rng.uniform(size=m), rng.uniform(size=m)
   s[:z] = 0.0
-  kkt = direct.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
+  kkt = kkt_driver.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
                                max_iterative_refinement_steps=2, atol=1e-12, rtol=1e-12,
                                solver=direct.CudaDenseSolver())
   kkt.update(mu=mu, s=s, y=y)

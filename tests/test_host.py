@@ -10,6 +10,7 @@ import scipy.sparse as sp
 import qtqp_b200 as qb
 from oracle import qtqp_oracle as orc
 from qtqp_b200 import batch, direct, problems
+from tests import kkt_driver
 
 
 def test_enum_surface():
@@ -124,7 +125,7 @@ def test_direct_kkt_solver_host_driver():
   s, y = rng.uniform(size=m), rng.uniform(size=m)
   s[:z] = 0.0
   d = np.concatenate([np.zeros(z), s[z:] / y[z:]])
-  kkt = direct.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
+  kkt = kkt_driver.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
                                max_iterative_refinement_steps=10, atol=1e-12, rtol=1e-12,
                                solver=_CpuGram())
   kkt.update(mu=mu, s=s, y=y)
@@ -163,7 +164,7 @@ def _kkt_case(solver, steps, seed=7):
   a, b, c, _, p = problems.feasible(m, n, z, rng)
   s, y = rng.uniform(0.5, 1.5, size=m), rng.uniform(0.5, 1.5, size=m)
   s[:z] = 0.0
-  kkt = direct.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
+  kkt = kkt_driver.DirectKktSolver(a=a, p=p, z=z, min_static_regularization=1e-8,
                                max_iterative_refinement_steps=steps, atol=1e-12, rtol=1e-12,
                                solver=solver)
   kkt.update(mu=0.3, s=s, y=y)
