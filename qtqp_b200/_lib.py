@@ -44,6 +44,7 @@ EXPORTS = (
     "qtqp_kkt_dense_factorize",
     "qtqp_kkt_dense_solve",
     "qtqp_kkt_dense_matvec",
+    "qtqp_dense_equilibrate",
     "qtqp_mlp_gemm",
     "qtqp_mlp_relu_grad",
     "qtqp_mlp_colsum",
@@ -204,6 +205,7 @@ def load() -> ctypes.CDLL:
     lib.qtqp_kkt_dense_factorize.argtypes = [i32, i32, vp, i32, vp, vp, vp]
     lib.qtqp_kkt_dense_solve.argtypes = [i32, i32, vp, vp, vp, vp]
     lib.qtqp_kkt_dense_matvec.argtypes = [i32, i32, vp, vp, vp, vp]
+    lib.qtqp_dense_equilibrate.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     for name in EXPORTS:  # every declared entry point must resolve
       getattr(lib, name)
     _lib = lib

@@ -68,6 +68,43 @@ __global__ void __launch_bounds__(kPluginThreads)
   s.kkt_matvec(x, out);
 }
 
+// Ruiz equilibration alone (the device IPM's load_and_equilibrate phase, the
+// algorithm of src/qtqp/__init__.py:616-663) with its outputs written back:
+// d (m), e (n), the equilibrated A (m x n) and P (n x n, diagonal included),
+// all row-major.
+__global__ void __launch_bounds__(kPluginThreads)
+    plugin_equilibrate_kernel(int n, int m, const double* a, const double* p, const double* b,
+                              const double* c, char* ws, double* d_out, double* e_out,
+                              double* a_eq, double* p_eq) {
+  __shared__ double red[2 * (kPluginThreads / 32) * kRedMax];
+  DenseIpm<kPluginThreads> s;
+  plugin_bind(s, n, m, ws, red);
+  s.has_p = p != nullptr;
+  s.A0 = a;
+  s.P0 = p;
+  s.b0 = b;
+  s.c0 = c;
+  double nb, nc;
+  s.load_and_equilibrate(true, nb, nc);
+  const double* de = s.vec(kDE);
+  const double* pi = s.vec(kPI);
+  for (int k = threadIdx.x; k < n + m; k += kPluginThreads) {
+    if (k < n) {
+      e_out[k] = de[k];
+    } else {
+      d_out[k - n] = de[k];
+    }
+  }
+  for (int idx = threadIdx.x; idx < m * n; idx += kPluginThreads) {
+    const int i = idx / n, j = idx - i * n;
+    a_eq[idx] = s.A[i * s.lda + j];
+  }
+  for (int idx = threadIdx.x; idx < n * n; idx += kPluginThreads) {
+    const int i = idx / n, j = idx - i * n;
+    p_eq[idx] = (i == j) ? pi[i] : s.P[i * s.ldp + j];
+  }
+}
+
 static int plugin_args(int n, int m, const void* ws) {
   if (n < 1 || m < 1) return fail(QTQP_ERR_BAD_ARG, "dense KKT: need n >= 1 and m >= 1");
   if (ws == nullptr) return fail(QTQP_ERR_BAD_ARG, "dense KKT: null workspace");
@@ -127,4 +164,18 @@ extern "C" int qtqp_kkt_dense_matvec(int32_t n, int32_t m, const double* d_x, do
   plugin_matvec_kernel<<<1, kPluginThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       n, m, d_x, d_out, static_cast<char*>(d_ws));
   return cuda_check(cudaGetLastError(), "plugin_matvec_kernel launch");
+}
+
+extern "C" int qtqp_dense_equilibrate(int32_t n, int32_t m, const double* d_a, const double* d_p,
+                                      const double* d_b, const double* d_c, void* d_ws,
+                                      double* d_d, double* d_e, double* d_a_eq, double* d_p_eq,
+                                      void* stream) {
+  int rc = plugin_args(n, m, d_ws);
+  if (rc) return rc;
+  if (d_a == nullptr || d_b == nullptr || d_c == nullptr || d_d == nullptr || d_e == nullptr ||
+      d_a_eq == nullptr || d_p_eq == nullptr)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_equilibrate: null argument");
+  plugin_equilibrate_kernel<<<1, kPluginThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, m, d_a, d_p, d_b, d_c, static_cast<char*>(d_ws), d_d, d_e, d_a_eq, d_p_eq);
+  return cuda_check(cudaGetLastError(), "plugin_equilibrate_kernel launch");
 }

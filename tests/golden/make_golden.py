@@ -1,15 +1,26 @@
 """Generates the golden fixtures from the reference solver itself.
 
-Run in a container that has the reference checkout (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run where a checkout of the reference (google-deepmind/qtqp v0.0.5) is
+readable, naming its root in the REFERENCE_ROOT environment variable:
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py [e2e] [units]
+        [configs] [plugin]
 
-It imports the reference package (google-deepmind/qtqp v0.0.5, pure Python)
-and its test-suite generators, solves a fixed list of seeded problems with the
-reference's SCIPY (SuperLU) and SCIPY_DENSE backends, and records inputs and
-outputs in tests/golden/*.npz.  The tests never import the reference: they
-read these files.
+(no names: all four files).  It imports the reference package (pure Python)
+under the name ``qtqp_ref`` -- this repository's own package is ``qtqp`` --
+together with its test-suite generators, solves a fixed list of seeded problems
+with the reference's SCIPY (SuperLU) and SCIPY_DENSE backends, and records
+inputs and outputs in tests/golden/*.npz:
+
+  reference_e2e.npz      end-to-end cases (test-suite generators, README, ...)
+  reference_units.npz    known answers of hot-path pieces (Ruiz, tau, sigma, ...)
+  reference_configs.npz  the benchmark configurations at their stated sizes:
+                         the large dense QP (n=4096, m=8192) and 32 held-out
+                         instances of the T=50 parametric family
+  reference_plugin.npz   the reference's DirectKktSolver (its IR driver) with
+                         its dense and SuperLU backends on seeded KKT systems
+
+The tests never import the reference: they read these files.
 """
 
 from __future__ import annotations
@@ -24,17 +35,27 @@ import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
 
 
 def _load_reference():
-  sys.path.insert(0, os.path.join(REFERENCE_ROOT, "src"))
-  import qtqp  # the reference package
+  """(qtqp_ref, its tests module).  The reference's modules import each other
+  relatively, so the package loads under another name; its test module's
+  `import qtqp` is pointed at it."""
+  root = os.environ.get("REFERENCE_ROOT")
+  if not root:
+    raise SystemExit("set REFERENCE_ROOT to the root of a google-deepmind/qtqp v0.0.5 checkout")
+  pkg = os.path.join(root, "src", "qtqp")
   spec = importlib.util.spec_from_file_location(
-      "ref_tests", os.path.join(REFERENCE_ROOT, "tests", "test_qtqp.py"))
+      "qtqp_ref", os.path.join(pkg, "__init__.py"), submodule_search_locations=[pkg])
+  qtqp_ref = importlib.util.module_from_spec(spec)
+  sys.modules["qtqp_ref"] = qtqp_ref
+  spec.loader.exec_module(qtqp_ref)
+  sys.modules["qtqp"] = qtqp_ref
+  spec = importlib.util.spec_from_file_location(
+      "ref_tests", os.path.join(root, "tests", "test_qtqp.py"))
   tests = importlib.util.module_from_spec(spec)
   spec.loader.exec_module(tests)
-  return qtqp, tests
+  return qtqp_ref, tests
 
 
 def _put_csc(out, prefix, mat):
@@ -183,12 +204,94 @@ def make_units(qtqp, tests):
   return out
 
 
+def _objective(a, b, c, p, x):
+  return float(c @ x + 0.5 * x @ (p @ x))
+
+
+PARAM_TEST_FIRST = 16384  # held-out split of the 20000-instance family
+PARAM_CASES = 32
+
+
+def make_configs(qtqp):
+  """The large dense QP and held-out parametric instances at full size:
+  status, iterations, objective (and x for the large QP)."""
+  sys.path.insert(0, REPO)
+  from qtqp_b200 import problems
+  out = {}
+  a, b, c, z, p = problems.large_dense()
+  a, p = sp.csc_matrix(a), sp.csc_matrix(p)
+  sol = qtqp.QTQP(a=a, b=b, c=c, z=z, p=p).solve(
+      linear_solver=qtqp.LinearSolver.SCIPY_DENSE, verbose=False, collect_stats=True)
+  out["large_dense/status"] = np.array(sol.status.value)
+  out["large_dense/iters"] = np.array(len(sol.stats))
+  out["large_dense/objective"] = np.array(_objective(a, b, c, p, sol.x))
+  out["large_dense/x"] = sol.x
+  out["large_dense/mu"] = np.array([st["mu"] for st in sol.stats])
+  fam = problems.parametric_mpc_family()
+  idx = np.arange(PARAM_TEST_FIRST, PARAM_TEST_FIRST + PARAM_CASES)
+  status, iters, obj = [], [], []
+  for i in idx:
+    a, b, c, z, p = problems.parametric_mpc_instance(fam, int(i))
+    a, p = sp.csc_matrix(a), sp.csc_matrix(p)
+    sol = qtqp.QTQP(a=a, b=b, c=c, z=z, p=p).solve(
+        linear_solver=qtqp.LinearSolver.SCIPY, verbose=False, collect_stats=True)
+    status.append(sol.status.value)
+    iters.append(len(sol.stats))
+    obj.append(_objective(a, b, c, p, sol.x) if sol.status.value == "solved" else np.nan)
+  out["parametric/index"] = idx
+  out["parametric/status"] = np.array(status)
+  out["parametric/iters"] = np.array(iters)
+  out["parametric/objective"] = np.array(obj)
+  return out
+
+
+def make_plugin(qtqp, tests):
+  """The reference's DirectKktSolver driving its dense (SCIPY_DENSE) and
+  SuperLU (SCIPY) backends on seeded regularised KKT systems: the solution,
+  the refinement statistics, and the inputs that produced them."""
+  out = {}
+  rng = np.random.default_rng(3142)
+  for k in range(4):
+    m, n, z = (150, 100, 10) if k < 3 else (40, 25, 5)
+    a, b, c, p = tests._gen_feasible(m, n, z, int(rng.integers(1 << 30)))
+    mu = float(rng.uniform(1e-6, 1.0))
+    s = rng.uniform(size=m)
+    y = rng.uniform(size=m)
+    s[:z] = 0.0
+    rhs = rng.normal(size=n + m)
+    pre = f"plugin{k}/"
+    _put_csc(out, pre + "a", a)
+    _put_csc(out, pre + "p", p)
+    out[pre + "z"], out[pre + "mu"] = np.array(z), np.array(mu)
+    out[pre + "s"], out[pre + "y"], out[pre + "rhs"] = s, y, rhs
+    for backend, cls in (("dense", qtqp.direct.ScipyDenseSolver),
+                         ("superlu", qtqp.direct.ScipySolver)):
+      kkt = qtqp.direct.DirectKktSolver(
+          a=a, p=p, z=z, min_static_regularization=1e-8, max_iterative_refinement_steps=20,
+          atol=1e-12, rtol=1e-12, solver=cls())
+      kkt.update(mu=mu, s=s, y=y)
+      sol, st = kkt.solve(rhs=rhs, warm_start=np.zeros(n + m))
+      kkt.free()
+      out[pre + backend + "/sol"] = sol
+      out[pre + backend + "/solves"] = np.array(st["solves"])
+      out[pre + backend + "/final_residual_norm"] = np.array(st["final_residual_norm"])
+      out[pre + backend + "/status"] = np.array(st["status"])
+  return out
+
+
 def main():
   warnings.simplefilter("ignore")
+  which = set(sys.argv[1:]) or {"e2e", "units", "configs", "plugin"}
   qtqp, tests = _load_reference()
-  np.savez_compressed(os.path.join(HERE, "reference_e2e.npz"), **make_e2e(qtqp, tests))
-  np.savez_compressed(os.path.join(HERE, "reference_units.npz"), **make_units(qtqp, tests))
-  print("wrote", os.listdir(HERE))
+  if "e2e" in which:
+    np.savez_compressed(os.path.join(HERE, "reference_e2e.npz"), **make_e2e(qtqp, tests))
+  if "units" in which:
+    np.savez_compressed(os.path.join(HERE, "reference_units.npz"), **make_units(qtqp, tests))
+  if "configs" in which:
+    np.savez_compressed(os.path.join(HERE, "reference_configs.npz"), **make_configs(qtqp))
+  if "plugin" in which:
+    np.savez_compressed(os.path.join(HERE, "reference_plugin.npz"), **make_plugin(qtqp, tests))
+  print("wrote", sorted(which))
 
 
 if __name__ == "__main__":
