@@ -38,10 +38,10 @@ CPU_SAMPLE = 1024          # instances in the CPU-baseline sample
 REF_SAMPLE = 1024          # instances per step of the reference arm
 HBM_FALLBACK_GBS = 6650.0  # only if MEASURED_PEAKS.json is absent
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), nominal; for context only
-# DRAM bytes (read + write) of one batch solve (its 8 group launches, mixed
-# precision) on this workload, from an ncu capture of
-# dram__bytes_read.sum + dram__bytes_write.sum (profiles/dense_batch_kernel_small_dense_batch.md).
-NCU_TRAFFIC_BYTES = 171.6e6
+# DRAM bytes (read + write) of one batch solve of this workload (all its group
+# launches), per precision form, from one ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum; None where no capture exists.
+NCU_TRAFFIC_BYTES = {"fp64": None, "mixed": 171.6e6}
 
 
 def _args():
@@ -116,8 +116,8 @@ def run_reference(args) -> None:
     for _ in range(args.warmup):
       _time_oracle(pool, cores, list(range(REF_SAMPLE)))
     times, solved = [], 0
-    for k in range(args.steps):
-      ids = list(range(k * REF_SAMPLE, (k + 1) * REF_SAMPLE))
+    for _ in range(args.steps):
+      ids = list(range(REF_SAMPLE))  # the first instances of the workload, every step
       t, s = _time_oracle(pool, cores, ids)
       times.append(t)
       solved += s
@@ -131,7 +131,8 @@ def run_reference(args) -> None:
       "config": {"workload": WORKLOAD, "sample_per_step": REF_SAMPLE,
                  "backend": "dense Gram/Cholesky (SCIPY_DENSE algorithm)"},
       "cpu_baseline": {"value": value, "unit": "QPs/s", "cores": cores, "kind": "port",
-                       "sample": f"{REF_SAMPLE} instances per step, {args.steps} steps"},
+                       "sample": f"the first {REF_SAMPLE} of the workload's {COUNT} instances "
+                                 f"(generated and solved) every step, {args.steps} steps"},
       "e2e": {"value": value, "unit": "QPs/s", "h2d_bytes_per_step": 0,
               "d2h_bytes_per_step": 0},
   }
@@ -225,10 +226,9 @@ def run_ours(args) -> None:
 
   insts = _instances(rank, args.count)
   qps = [qb.QTQP(a=a, b=b, c=c, z=z, p=p) for a, b, c, z, p in insts]
-  probs = [q.dense_problem() for q in qps]
 
   def prepare(precision):
-    hb = batch.HostBatch(probs, batch.SolveOptions(precision=precision))
+    hb = batch.HostBatch(qps, batch.SolveOptions(precision=precision), pinned=True)
     db = batch.DeviceBatch(hb, device=dev)
     db.upload(stream)
     torch.cuda.synchronize(dev)
@@ -288,32 +288,60 @@ def run_ours(args) -> None:
   fp64_value = forms["fp64"]["solved"] * world * args.steps / forms["fp64"]["time"]
   same_status = bool(np.array_equal(forms["fp64"]["res"]["status"], res["status"]))
 
-  # End to end through the C-ABI with host buffers: H2D inputs, solve, D2H outputs.
-  h_out = [torch.empty_like(t, device="cpu").pin_memory() for t in (db.x, db.y, db.s,
-                                                                   db.results)]
+  def ev_pair():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+  # End to end through the public API: a list of CSC QTQP objects in, a list
+  # of Solutions out (packing, planning, H2D copies, the solve, D2H copies,
+  # unpacking), timed with CUDA events recorded before the call and after it
+  # returns (the call synchronises).
   for _ in range(args.warmup):
-    db.upload(stream)
-    db.launch(stream)
+    qb.solve_batch(qps, precision=args.precision)
   barrier()
-  e_total = 0.0
+  e_total, e2e_solved = 0.0, 0
   for _ in range(args.steps):
     flush.fill_(1)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    e0, e1 = ev_pair()
     e0.record(stream)
-    db.upload(stream)
-    db.launch(stream)
-    with torch.cuda.stream(stream):
-      for dst, src in zip(h_out, (db.x, db.y, db.s, db.results)):
-        dst.copy_(src, non_blocking=True)
+    sols = qb.solve_batch(qps, precision=args.precision)
     e1.record(stream)
     e1.synchronize()
     e_total += e0.elapsed_time(e1) * 1e-3
+    e2e_solved = sum(1 for x in sols if x.status == qb.SolutionStatus.SOLVED)
   barrier()
   e_total = max_over_ranks(e_total)
-  e2e_value = solved_total * args.steps / e_total
+  e2e_value = e2e_solved * world * args.steps / e_total
   h2d = hb.input_bytes
-  d2h = sum(int(t.numel() * t.element_size()) for t in h_out)
+  d2h = db.output_bytes
+
+  # The same through the C-ABI from already packed pinned pools (upload,
+  # launch, download), and the two copies timed on their own.
+  for _ in range(args.warmup):
+    db.upload(stream)
+    db.launch(stream)
+    db.download(stream)
+  barrier()
+  d_total = h2d_t = d2h_t = 0.0
+  for _ in range(args.steps):
+    flush.fill_(1)
+    e0, e1 = ev_pair()
+    c0, c1 = ev_pair()
+    c2, c3 = ev_pair()
+    e0.record(stream)
+    c0.record(stream)
+    db.upload(stream)
+    c1.record(stream)
+    db.launch(stream)
+    c2.record(stream)
+    db.download(stream)
+    c3.record(stream)
+    e1.record(stream)
+    e1.synchronize()
+    d_total += e0.elapsed_time(e1) * 1e-3
+    h2d_t += c0.elapsed_time(c1) * 1e-3
+    d2h_t += c2.elapsed_time(c3) * 1e-3
+  barrier()
+  d_total = max_over_ranks(d_total)
 
   # Roofline of the dominant kernel (the batch kernel is the only one).
   iters = res["iterations"].astype(np.float64)
@@ -329,7 +357,10 @@ def run_ours(args) -> None:
   roofline = {
       "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
       "frac": achieved / peak, "peak_source": peak_kind,
-      "traffic": NCU_TRAFFIC_BYTES,
+      "traffic": NCU_TRAFFIC_BYTES.get(args.precision),
+      "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum over one batch "
+                         f"solve, {args.precision} form") if NCU_TRAFFIC_BYTES.get(
+                             args.precision) else "no capture of this form",
       "kernel": "dense_batch_kernel",
       "algorithmic_bytes_per_launch": alg_bytes,
       "kkt_factor_flops_per_launch": factor_flops,
@@ -357,7 +388,14 @@ def run_ours(args) -> None:
         "factorizations": {"fp32": int(res["fp32_factorizations"].sum()),
                            "fp64": int(res["fp64_factorizations"].sum())},
         "e2e": {"value": e2e_value, "unit": "QPs/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h,
+                "path": "qtqp.solve_batch(list of CSC QTQP) -> list of Solution",
+                "ms_per_step": 1e3 * e_total / args.steps},
+        "e2e_device_api": {"value": solved_total * args.steps / d_total, "unit": "QPs/s",
+                           "path": "C-ABI from packed pinned pools: H2D, solve, D2H",
+                           "ms_per_step": 1e3 * d_total / args.steps,
+                           "h2d_ms": 1e3 * h2d_t / args.steps,
+                           "d2h_ms": 1e3 * d2h_t / args.steps},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": chosen["clocks"],

@@ -62,14 +62,19 @@ typedef struct {
                             counterpart): primal-dual active-set corrections
                             after the first reduced KKT solve; 0 = exactly
                             one reduced solve                                */
+  double warm_shift;     /* learned warm start only: > 0 starts the IPM of an
+                            instance whose prediction was not accepted from
+                            that prediction, y and s on the inequality rows
+                            shifted by warm_shift; 0 = the cold start         */
 } qtqp_options;
 
 /* One QP of a batch.  Offsets are element offsets into the caller's pools. */
 typedef struct {
   int32_t n, m, z;  /* variables, constraints (after presolve), equalities */
   int32_t has_p;    /* nnz(P) > 0 (the reference's p.nnz > 0 tests)       */
-  int64_t a_off;    /* A: m x n row-major FP64 in a_pool                   */
-  int64_t p_off;    /* P: n x n row-major FP64 (symmetric) in p_pool       */
+  int64_t a_off;    /* A: m x n column-major FP64 in a_pool (the value
+                       order of a CSC matrix that stores every entry)     */
+  int64_t p_off;    /* P: n x n column-major FP64 (symmetric) in p_pool    */
   int64_t n_off;    /* c in c_pool, x in x_pool: n doubles each            */
   int64_t m_off;    /* b in b_pool, y / s in y_pool / s_pool: m doubles    */
   int64_t ws_off;   /* byte offset of this instance's global workspace     */
@@ -125,6 +130,14 @@ int qtqp_version(void);
 /* Number of SMs of the current device (0 when no device is visible). */
 int qtqp_device_sm_count(void);
 
+/* Host-only helper (no device work, no CUDA call): copies `count` host
+ * blocks, h_src[i] (an address) of h_bytes[i] bytes, to h_dst + h_dst_off[i],
+ * on `threads` host threads (0: up to 8).  Packs the batch pools below from
+ * the thousands of per-QP arrays a batch arrives as (the reference packs
+ * nothing: its solver handles one QP at a time, src/qtqp/__init__.py:183-246). */
+int qtqp_host_gather(int32_t count, const uint64_t* h_src, const int64_t* h_bytes,
+                     const int64_t* h_dst_off, void* h_dst, int32_t threads);
+
 /* ---- batched dense device-resident IPM ---------------------------------- *
  * Replaces QTQP._solve_impl (src/qtqp/__init__.py:351-614) with its KKT layer
  * (src/qtqp/direct.py:112-311) and the dense Gram/Cholesky backend
@@ -157,6 +170,26 @@ int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst,
                            qtqp_iter_stats* d_stats, void* d_workspace,
                            size_t workspace_bytes, const qtqp_options* opt,
                            void* stream);
+
+/* qtqp_dense_batch_solve started from given points instead of the cold
+ * start of _init_variables (src/qtqp/__init__.py:299-307; the reference has
+ * no warm start -- its re-solve, tests/test_qtqp.py:1578-1598, starts cold
+ * every time): d_x0_pool / d_y0_pool / d_s0_pool hold one point per
+ * instance laid out like the x / y / s pools, in the original scaling, with
+ * y and s positive on the inequality rows (s zero on the equality rows).
+ * An earlier solution of the same or a nearby QP, moved into the interior,
+ * is the typical start. */
+int qtqp_dense_batch_solve_from(const qtqp_dense_instance* d_inst,
+                                const int32_t* d_order,
+                                const qtqp_batch_plan* plan,
+                                const double* d_a_pool, const double* d_p_pool,
+                                const double* d_b_pool, const double* d_c_pool,
+                                double* d_x_pool, double* d_y_pool,
+                                double* d_s_pool, qtqp_result* d_results,
+                                qtqp_iter_stats* d_stats, void* d_workspace,
+                                size_t workspace_bytes, const qtqp_options* opt,
+                                const double* d_x0_pool, const double* d_y0_pool,
+                                const double* d_s0_pool, void* stream);
 
 /* Allocation-free variant of qtqp_dense_batch_solve.  It has no counterpart
  * in the reference (whose solver is pure Python).  It exists for callers that

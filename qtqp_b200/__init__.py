@@ -228,9 +228,12 @@ class QTQP:
             linear_solver_rtol: float = 1e-12,
             linear_solver: LinearSolver = LinearSolver.AUTO, verbose: bool = True,
             equilibrate: bool = True, collect_stats: bool = False,
-            precision: str = "fp64") -> Solution:
+            precision: str = "fp64", initial=None) -> Solution:
     """Solves the QP on the GPU (same keyword arguments as the reference,
-    __init__.py:309-326, plus ``precision``: 'fp64' or 'mixed')."""
+    __init__.py:309-326, plus ``precision``: 'fp64' or 'mixed', and
+    ``initial``: a starting point -- e.g. the Solution of an earlier solve of
+    this or a nearby QP -- for QPs on the dense path; no reference
+    counterpart, whose re-solve always starts cold)."""
     opts = _batch.SolveOptions(
         atol=atol, rtol=rtol, atol_infeas=atol_infeas, rtol_infeas=rtol_infeas,
         max_iter=max_iter, step_size_scale=step_size_scale,
@@ -248,8 +251,11 @@ class QTQP:
     if verbose:
       print(f"| QTQP v{__version__}: m={self.m}, n={self.n}, z={self.z}, "
             f"nnz(A)={self.a.nnz}, nnz(P)={self.p.nnz}, linear_solver=CUDA")
-    out = solve_batch([self], storage=self.storage_format(single=True), _opts=opts,
-                      _verbose=verbose, _start=start)[0]
+    storage = self.storage_format(single=True)
+    if initial is not None and storage != "dense":
+      storage = "dense" if self.n < LARGE_N else storage
+    out = solve_batch([self], storage=storage, _opts=opts, _verbose=verbose, _start=start,
+                      initial=None if initial is None else [initial])[0]
     return out
 
 
@@ -298,18 +304,23 @@ def _log_iteration(st: Dict[str, Any]) -> None:
 
 
 def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: str = "auto",
-                warm_start=None, _opts=None,
+                warm_start=None, initial=None, initial_shift: float = 0.1, _opts=None,
                 _verbose: bool = False, _start: float | None = None,
                 **solve_kwargs) -> List[Solution]:
   """Solves independent QPs in one persistent GPU launch.
 
   Accepts the keyword arguments of QTQP.solve (verbose defaults to False)
-  plus warm_corrections.  storage: 'auto' (per problem: banded when the Gram
-  matrix is narrow-banded, else dense), 'dense' or 'band'.  warm_start:
-  (WarmStartMLP, thetas) for instances of a parametric family, all on the
-  banded path -- each instance first solves the KKT system on the predicted
-  active set and keeps that point only if the plain termination test passes,
-  else the plain method runs.  Returns one Solution per problem, in order.
+  plus warm_corrections and warm_shift.  storage: 'auto' (per problem:
+  banded when the Gram matrix is narrow-banded, else dense), 'dense' or
+  'band'.  warm_start: (WarmStartMLP, thetas) for instances of a parametric
+  family, all on the banded path -- each instance first solves the KKT system
+  on the predicted active set and keeps that point only if the plain
+  termination test passes, else the plain method runs (from the prediction
+  when warm_shift > 0).  initial: one starting point per problem (a Solution,
+  an (x, y, s) triple, or None for the cold start), e.g. the solutions of an
+  earlier call on the same or nearby QPs; its inequality rows are moved
+  initial_shift inside the cone (dense storage only).  Returns one Solution
+  per problem, in order.
   """
   start = timeit.default_timer() if _start is None else _start
   if _opts is None:
@@ -326,6 +337,11 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   if any(k not in ("dense", "band", "large", "band_grid") for k in kinds):
     raise ValueError("storage must be 'auto', 'dense', 'band', 'large' or 'band_grid', "
                      f"got {storage!r}")
+  if initial is not None:
+    if len(initial) != len(problems):
+      raise ValueError(f"initial: {len(initial)} points for {len(problems)} problems")
+    if any(k != "dense" for k, pt in zip(kinds, initial) if pt is not None):
+      raise ValueError("initial points are supported for dense storage only")
   if warm_start is not None:
     if any(k != "band" for k in kinds):
       raise ValueError("warm_start needs every problem on the banded path")
@@ -363,7 +379,7 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     if not idx:
       continue
     if kind == "dense":
-      hb = _batch.HostBatch([problems[i].dense_problem() for i in idx], opts)
+      hb = _batch.HostBatch([problems[i] for i in idx], opts, pinned=True)
       db = _batch.DeviceBatch(hb, records=records)
     else:
       from . import band as _band  # pylint: disable=g-import-not-at-top
@@ -374,43 +390,79 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     if warm_start is not None:
       model, thetas = warm_start
       db.launch(warm=model.predict_device(np.asarray(thetas)))
+    elif kind == "dense" and initial is not None:
+      import torch  # pylint: disable=g-import-not-at-top
+      pools = _batch.start_points(hb, [problems[i] for i in idx], [initial[i] for i in idx],
+                                  initial_shift)
+      db.launch(start=[torch.from_numpy(v).to(db.device) for v in pools])
     else:
       db.launch()
     per[kind] = (idx, *db.fetch(), hb.inst)
+  # Errors first, in problem order (every error code of every batch at once).
+  errs = [(i, int(r["error"])) for i, (r, *_) in where.items() if int(r["error"])]
+  for kind, (idx, res, *_rest) in per.items():
+    bad = np.nonzero(res["error"])[0]
+    errs += [(idx[j], int(res["error"][j])) for j in bad]
+  if errs:
+    _raise_device_error(min(errs)[1])
+  out: List[Solution | None] = [None] * len(problems)
   for kind, (idx, res, xp, yp, sp_, st, inst) in per.items():
+    ns = inst["n"].tolist()
+    ms = inst["m"].tolist()
+    n_off = inst["n_off"].tolist()
+    m_off = inst["m_off"].tolist()
+    codes = res["status"].tolist()
+    iters = res["iterations"].tolist()
     for j, i in enumerate(idx):
-      where[i] = (res[j], xp, yp, sp_, None if st is None else st[j], inst[j])
-  out = []
-  for i, q in enumerate(problems):
-    r, x_pool, y_pool, s_pool, recs, d = where[i]
-    if int(r["error"]) == _lib.QTQP_ERR_NOT_SPD:
-      raise np.linalg.LinAlgError("Cholesky failed: the KKT Gram matrix is not positive definite")
-    if int(r["error"]) == _lib.QTQP_ERR_NAN:
-      raise ValueError("Linear solver returned NaNs.")
-    if int(r["error"]) == _lib.QTQP_ERR_TIMEOUT:
-      raise RuntimeError("qtqp_b200: a grid barrier of a whole-GPU solve timed out")
+      n0, m0, mj = n_off[j], m_off[j], ms[j]
+      out[i] = _make_solution(problems[i], xp[n0:n0 + ns[j]], yp[m0:m0 + mj],
+                              sp_[m0:m0 + mj], codes[j], iters[j],
+                              None if st is None else st[j], opts, verbose, t_launch)
+  for i, (r, x_pool, y_pool, s_pool, recs, d) in where.items():
+    q = problems[i]
     n0, m0 = int(d["n_off"]), int(d["m_off"])
-    x = x_pool[n0:n0 + q.n].copy()
-    y = y_pool[m0:m0 + q.m].copy()
-    s = s_pool[m0:m0 + q.m].copy()
-    status = _STATUS_FROM_CODE[int(r["status"])]
+    out[i] = _make_solution(q, x_pool[n0:n0 + q.n].copy(), y_pool[m0:m0 + q.m].copy(),
+                            s_pool[m0:m0 + q.m].copy(), int(r["status"]),
+                            int(r["iterations"]), recs, opts, verbose, t_launch)
+  return out
+
+
+def _raise_device_error(code: int) -> None:
+  """The reference's exception for a failed solve (direct.py:293-294 for NaNs;
+  a failed Cholesky raises numpy's LinAlgError as the dense backend does)."""
+  if code == _lib.QTQP_ERR_NOT_SPD:
+    raise np.linalg.LinAlgError("Cholesky failed: the KKT Gram matrix is not positive definite")
+  if code == _lib.QTQP_ERR_NAN:
+    raise ValueError("Linear solver returned NaNs.")
+  if code == _lib.QTQP_ERR_TIMEOUT:
+    raise RuntimeError("qtqp_b200: a grid barrier of a whole-GPU solve timed out")
+  raise RuntimeError(f"qtqp_b200: device error {code}")
+
+
+_STATUS_LIST = [_STATUS_FROM_CODE[k] for k in range(6)]
+
+
+def _make_solution(q, x, y, s, code, iters, recs, opts, verbose, t_launch) -> Solution:
+  """One Solution from the device outputs of one QP (x, y, s already owned by
+  the caller): presolve rows restored (__init__.py:272-297), the per-iteration
+  records turned into the reference's dictionaries, the verbose table."""
+  status = _STATUS_LIST[code]
+  if q._presolve_state is not None:  # pylint: disable=protected-access
     if status == SolutionStatus.INFEASIBLE:
       y, s = q._postsolve(y, s)
     elif status == SolutionStatus.UNBOUNDED:
       y, s = q._postsolve(y, s, y_dropped=np.nan)
     else:
       y, s = q._postsolve(y, s, s_dropped=q._dropped_slack(x))
-    st_list: List[Dict[str, Any]] = []
-    iters = int(r["iterations"])
-    if recs is not None:
-      st_list = [_record_to_dict(recs[k], opts.collect_stats, t_launch) for k in range(iters)]
-    if verbose:
-      print(f"{_SEPARA}\n{_HEADER}\n{_SEPARA}")
-      for st in st_list:
-        _log_iteration(st)
-      print(f"{_SEPARA}\n| {_FOOTER.get(status, 'Failed to converge')}")
-    out.append(Solution(x, y, s, st_list if opts.collect_stats else [], status))
-  return out
+  st_list: List[Dict[str, Any]] = []
+  if recs is not None:
+    st_list = [_record_to_dict(recs[k], opts.collect_stats, t_launch) for k in range(iters)]
+  if verbose:
+    print(f"{_SEPARA}\n{_HEADER}\n{_SEPARA}")
+    for st in st_list:
+      _log_iteration(st)
+    print(f"{_SEPARA}\n| {_FOOTER.get(status, 'Failed to converge')}")
+  return Solution(x, y, s, st_list if opts.collect_stats else [], status)
 
 
 __all__ = ["QTQP", "Solution", "SolutionStatus", "LinearSolver", "solve_batch", "direct",

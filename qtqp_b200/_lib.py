@@ -33,8 +33,10 @@ EXPORTS = (
     "qtqp_last_error",
     "qtqp_version",
     "qtqp_device_sm_count",
+    "qtqp_host_gather",
     "qtqp_dense_batch_plan",
     "qtqp_dense_batch_solve",
+    "qtqp_dense_batch_solve_from",
     "qtqp_dense_batch_noalloc_max_workspace",
     "qtqp_dense_batch_solve_noalloc",
     "qtqp_band_batch_plan",
@@ -78,6 +80,7 @@ class Options(ctypes.Structure):
       ("collect_stats", ctypes.c_int32),
       ("tau_mode", ctypes.c_int32),
       ("warm_corrections", ctypes.c_int32),
+      ("warm_shift", ctypes.c_double),
   ]
 
 
@@ -164,11 +167,16 @@ def load() -> ctypes.CDLL:
     lib.qtqp_last_error.restype = ctypes.c_char_p
     lib.qtqp_version.restype = ctypes.c_int
     lib.qtqp_device_sm_count.restype = ctypes.c_int
+    lib.qtqp_host_gather.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
     lib.qtqp_dense_batch_plan.argtypes = [vp, i32, ctypes.POINTER(Options), vp, i32, i32,
                                           ctypes.POINTER(BatchPlan)]
     lib.qtqp_dense_batch_solve.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp, vp,
                                            vp, vp, vp, vp, vp, vp, sz,
                                            ctypes.POINTER(Options), vp]
+    lib.qtqp_dense_batch_solve_from.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp,
+                                                vp, vp, vp, vp, vp, vp, vp, sz,
+                                                ctypes.POINTER(Options), vp, vp, vp, vp]
     lib.qtqp_dense_batch_noalloc_max_workspace.restype = sz
     lib.qtqp_dense_batch_noalloc_max_workspace.argtypes = []
     lib.qtqp_dense_batch_solve_noalloc.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp,

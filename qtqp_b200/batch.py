@@ -1,8 +1,10 @@
 """Device-resident batched solve of dense QPs through the C-ABI.
 
-A batch is packed once into flat pools (row-major A and P per instance, b, c),
-planned by the library (processing order, launch shape, workspace), copied to
-the device, and solved by one persistent launch of
+A batch is packed once into flat pools (column-major A and P per instance --
+the value order of a CSC matrix that stores every entry, so a dense QP given
+in CSC form packs without conversion -- then b and c), planned by the library
+(processing order, launch shape, workspace), copied to the device, and solved
+by one persistent launch of
 ``qtqp_dense_batch_solve``: one thread block runs one QP's whole interior-point
 method (the device counterpart of ``QTQP._solve_impl``,
 src/qtqp/__init__.py:351-614 of the reference).
@@ -15,6 +17,7 @@ import dataclasses
 from typing import Sequence
 
 import numpy as np
+import scipy.sparse as sp
 
 from . import _lib
 
@@ -39,6 +42,7 @@ class SolveOptions:
   precision: str = "fp64"  # "fp64" or "mixed"
   tau_mode: int = 0
   warm_corrections: int = 0  # learned warm start: active-set corrections
+  warm_shift: float = 0.0  # learned warm start: > 0 starts a rejected instance's IPM there
 
   def validate(self) -> None:
     """The reference's argument checks (__init__.py:403-412)."""
@@ -53,6 +57,7 @@ class SolveOptions:
     assert self.linear_solver_atol >= 0
     assert self.linear_solver_rtol >= 0
     assert 0 <= self.warm_corrections <= 64
+    assert self.warm_shift >= 0
     if self.precision not in ("fp64", "mixed"):
       raise ValueError(f"precision must be 'fp64' or 'mixed', got {self.precision!r}")
 
@@ -63,7 +68,8 @@ class SolveOptions:
         self.linear_solver_atol, self.linear_solver_rtol, int(self.max_iter),
         int(self.max_iterative_refinement_steps), int(bool(self.equilibrate)),
         _lib.PREC_FP64 if self.precision == "fp64" else _lib.PREC_MIXED,
-        int(bool(self.collect_stats)), int(self.tau_mode), int(self.warm_corrections))
+        int(bool(self.collect_stats)), int(self.tau_mode), int(self.warm_corrections),
+        float(self.warm_shift))
 
 
 @dataclasses.dataclass
@@ -77,41 +83,115 @@ class DenseProblem:
   p: np.ndarray | None = None
 
 
-class HostBatch:
-  """Packed host pools of a batch (pinned when torch is available)."""
+class _Pack:
+  """Column-major FP64 values of one QP's A and P (P: None when it is zero)
+  and their host addresses, ready for the gather into the batch pools."""
 
-  def __init__(self, problems: Sequence[DenseProblem], opts: SolveOptions,
-               block_threads: int = 0, smem_bytes: int = 0):
+  __slots__ = ("src_a", "src_p", "n", "m", "z", "a_vals", "p_vals", "a_ptr", "p_ptr")
+
+  def __init__(self, src_a, src_p, n, m, z, a_vals, p_vals):
+    self.src_a, self.src_p = src_a, src_p
+    self.n, self.m, self.z = n, m, z
+    self.a_vals = a_vals
+    self.p_vals = p_vals
+    self.a_ptr = a_vals.ctypes.data
+    self.p_ptr = 0 if p_vals is None else p_vals.ctypes.data
+
+
+def _colmajor_values(mat, rows: int, cols: int) -> tuple[np.ndarray, bool]:
+  """(values, zero_copy): the column-major dense values of a sparse or dense
+  matrix.  A CSC matrix that stores every entry in canonical order already
+  holds them in its data array (zero copy); anything else is densified."""
+  if sp.issparse(mat):
+    if (mat.format == "csc" and mat.nnz == rows * cols and mat.dtype == np.float64 and
+        mat.has_canonical_format and mat.data.flags.c_contiguous):
+      return mat.data, True
+    return np.asarray(mat.toarray(order="F"), dtype=np.float64).ravel(order="F"), False
+  return np.asarray(mat, dtype=np.float64).ravel(order="F"), False
+
+
+def _pack_of(pr) -> _Pack:
+  """The pack of a QTQP (cached on it while its A and P objects stay the same
+  and their values can be read in place) or of a DenseProblem."""
+  if isinstance(pr, DenseProblem):
+    m, n = pr.a.shape
+    a_vals, _ = _colmajor_values(pr.a, m, n)
+    has_p = pr.p is not None and bool(np.any(pr.p != 0))
+    p_vals = _colmajor_values(pr.p, n, n)[0] if has_p else None
+    return _Pack(None, None, n, m, pr.z, a_vals, p_vals)
+  pk = getattr(pr, "_dense_pack", None)
+  if pk is not None and pk.src_a is pr.a and pk.src_p is pr.p:
+    return pk
+  n, m = pr.n, pr.m
+  a_vals, a_view = _colmajor_values(pr.a, m, n)
+  p_vals, p_view = None, True
+  if pr.p.nnz and np.any(pr.p.data != 0):  # the device needs P when it is non-zero
+    p_vals, p_view = _colmajor_values(pr.p, n, n)
+  pk = _Pack(pr.a, pr.p, n, m, pr.z, a_vals, p_vals)
+  if a_view and p_view:  # values read in place: valid while the matrices are
+    pr._dense_pack = pk  # pylint: disable=protected-access
+  return pk
+
+
+def _gather(lib, pool: np.ndarray, ptrs, nbytes, offs) -> None:
+  ptrs = np.ascontiguousarray(ptrs, dtype=np.uint64)
+  nbytes = np.ascontiguousarray(nbytes, dtype=np.int64)
+  offs = np.ascontiguousarray(offs, dtype=np.int64)
+  if ptrs.size:
+    _lib.check(lib.qtqp_host_gather(int(ptrs.size), ptrs.ctypes.data, nbytes.ctypes.data,
+                                    offs.ctypes.data, pool.ctypes.data, 0))
+
+
+class HostBatch:
+  """Packed host pools of a batch: A and P column-major per instance, b, c.
+
+  problems: QTQP objects (their CSC values are gathered in place when every
+  entry is stored) or DenseProblems.  pinned=True allocates the pools in
+  pinned host memory (torch), so that they are copied to the device
+  asynchronously without a staging copy.
+  """
+
+  def __init__(self, problems: Sequence, opts: SolveOptions, block_threads: int = 0,
+               smem_bytes: int = 0, pinned: bool = False):
     lib = _lib.load()
     count = len(problems)
     self.count = count
+    packs = [_pack_of(pr) for pr in problems]
+    ns = np.fromiter((pk.n for pk in packs), np.int64, count)
+    ms = np.fromiter((pk.m for pk in packs), np.int64, count)
+    has_p = np.fromiter((pk.p_ptr != 0 for pk in packs), np.bool_, count)
     inst = np.zeros(count, dtype=_lib.INSTANCE_DTYPE)
-    a_off = p_off = n_off = m_off = 0
-    for i, pr in enumerate(problems):
-      m, n = pr.a.shape
-      inst[i]["n"], inst[i]["m"], inst[i]["z"] = n, m, pr.z
-      inst[i]["has_p"] = int(pr.p is not None and np.any(pr.p != 0))
-      inst[i]["a_off"], inst[i]["p_off"] = a_off, p_off
-      inst[i]["n_off"], inst[i]["m_off"] = n_off, m_off
-      inst[i]["st_off"] = i * opts.max_iter
-      a_off += m * n
-      p_off += n * n if inst[i]["has_p"] else 0
-      n_off += n
-      m_off += m
-    self.a_pool = np.empty(max(a_off, 1))
-    self.p_pool = np.zeros(max(p_off, 1))
-    self.b_pool = np.empty(max(m_off, 1))
-    self.c_pool = np.empty(max(n_off, 1))
-    for i, pr in enumerate(problems):
-      d = inst[i]
-      m, n = int(d["m"]), int(d["n"])
-      self.a_pool[d["a_off"]:d["a_off"] + m * n] = np.ascontiguousarray(pr.a, np.float64).ravel()
-      if d["has_p"]:
-        self.p_pool[d["p_off"]:d["p_off"] + n * n] = np.ascontiguousarray(
-            pr.p, np.float64).ravel()
-      self.b_pool[d["m_off"]:d["m_off"] + m] = pr.b
-      self.c_pool[d["n_off"]:d["n_off"] + n] = pr.c
-    self.n_total, self.m_total = n_off, m_off
+    inst["n"], inst["m"] = ns, ms
+    inst["z"] = np.fromiter((pk.z for pk in packs), np.int64, count)
+    inst["has_p"] = has_p
+    a_sz, p_sz = ms * ns, np.where(has_p, ns * ns, 0)
+    inst["a_off"] = np.cumsum(a_sz) - a_sz
+    inst["p_off"] = np.cumsum(p_sz) - p_sz
+    inst["n_off"] = np.cumsum(ns) - ns
+    inst["m_off"] = np.cumsum(ms) - ms
+    inst["st_off"] = np.arange(count, dtype=np.int64) * opts.max_iter
+    a_total, p_total = int(a_sz.sum()), int(p_sz.sum())
+    self.n_total, self.m_total = int(ns.sum()), int(ms.sum())
+    self.pinned = pinned
+    self.h_pools = None
+    sizes = (max(a_total, 1), max(p_total, 1), max(self.m_total, 1), max(self.n_total, 1))
+    if pinned:
+      import torch  # pylint: disable=g-import-not-at-top
+      self.h_pools = [torch.empty(k, dtype=torch.float64, pin_memory=True) for k in sizes]
+      self.a_pool, self.p_pool, self.b_pool, self.c_pool = (t.numpy() for t in self.h_pools)
+    else:
+      self.a_pool, self.p_pool, self.b_pool, self.c_pool = (np.empty(k) for k in sizes)
+    if p_total == 0:
+      self.p_pool[:] = 0.0
+    _gather(lib, self.a_pool, [pk.a_ptr for pk in packs], 8 * a_sz, 8 * inst["a_off"])
+    sel = np.nonzero(has_p)[0]
+    _gather(lib, self.p_pool, [packs[i].p_ptr for i in sel], 8 * p_sz[sel],
+            8 * inst["p_off"][sel])
+    if count:
+      np.concatenate([np.asarray(pr.b, dtype=np.float64) for pr in problems],
+                     out=self.b_pool[:self.m_total])
+      np.concatenate([np.asarray(pr.c, dtype=np.float64) for pr in problems],
+                     out=self.c_pool[:self.n_total])
     order = np.zeros(max(count, 1), dtype=np.int32)
     plan = _lib.BatchPlan()
     copts = opts.to_c()
@@ -159,9 +239,13 @@ class DeviceBatch:
       self.stats = torch.empty(max(hb.count, 1) * hb.opts.max_iter * _lib.STATS_DOUBLES, **f64)
     self.workspace = torch.empty(hb.workspace_bytes, **u8)
     self._copts = hb.opts.to_c()
-    # Pinned staging copies of the inputs for end-to-end (host->device) use.
-    self.h_pools = [torch.from_numpy(x).pin_memory() for x in
-                    (hb.a_pool, hb.p_pool, hb.b_pool, hb.c_pool)]
+    # Pinned staging copies of the inputs for asynchronous host->device copies.
+    if hb.pinned:
+      self.h_pools = hb.h_pools
+    else:
+      self.h_pools = [torch.from_numpy(x).pin_memory() for x in
+                      (hb.a_pool, hb.p_pool, hb.b_pool, hb.c_pool)]
+    self._h_out = None
 
   def upload(self, stream=None) -> None:
     torch = self.torch
@@ -169,19 +253,27 @@ class DeviceBatch:
       for dst, src in zip((self.a, self.p, self.b, self.c), self.h_pools):
         dst.copy_(src, non_blocking=True)
 
-  def launch(self, stream=None) -> None:
-    """Enqueues the persistent batch solve on `stream` (no synchronisation)."""
+  def launch(self, stream=None, start=None) -> None:
+    """Enqueues the persistent batch solve on `stream` (no synchronisation).
+    start: optional device tensors (x0, y0, s0) laid out like x / y / s,
+    starting points that replace the cold start (see start_points)."""
     torch = self.torch
     lib = _lib.load()
     st = stream or torch.cuda.current_stream(self.device)
     hb = self.hb
-    _lib.check(lib.qtqp_dense_batch_solve(
-        self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan),
-        self.a.data_ptr(), self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
-        self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
-        self.stats.data_ptr() if self.stats is not None else None,
-        self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts),
-        _lib.stream_handle(st)))
+    args = (self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan),
+            self.a.data_ptr(), self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
+            self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(), self.results.data_ptr(),
+            self.stats.data_ptr() if self.stats is not None else None,
+            self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts))
+    if start is None:
+      _lib.check(lib.qtqp_dense_batch_solve(*args, _lib.stream_handle(st)))
+    else:
+      x0, y0, s0 = start
+      if (x0.numel() < hb.n_total or y0.numel() < hb.m_total or s0.numel() < hb.m_total):
+        raise ValueError("start: pools smaller than the batch's x / y / s")
+      _lib.check(lib.qtqp_dense_batch_solve_from(*args, x0.data_ptr(), y0.data_ptr(),
+                                                 s0.data_ptr(), _lib.stream_handle(st)))
 
   def launch_noalloc(self, stream=None) -> None:
     """Enqueues the allocation-free variant: same solve, but its scratch is the
@@ -198,12 +290,70 @@ class DeviceBatch:
         self.stats.data_ptr() if self.stats is not None else None, ctypes.byref(self._copts),
         _lib.stream_handle(st)))
 
+  def download(self, stream=None) -> None:
+    """Enqueues the device->host copies of the outputs into pinned buffers."""
+    torch = self.torch
+    if self._h_out is None:
+      self._h_out = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                     for t in (self.results, self.x, self.y, self.s)]
+    with torch.cuda.stream(stream or torch.cuda.current_stream(self.device)):
+      for dst, src in zip(self._h_out, (self.results, self.x, self.y, self.s)):
+        dst.copy_(src, non_blocking=True)
+
+  @property
+  def output_bytes(self) -> int:
+    return sum(int(t.numel() * t.element_size()) for t in (self.results, self.x, self.y, self.s))
+
   def fetch(self):
-    """Synchronises and returns (results, x, y, s, stats) as numpy arrays."""
+    """Copies the outputs back, synchronises, and returns (results, x, y, s,
+    stats) as numpy arrays owned by the caller."""
+    self.download()
     self.torch.cuda.synchronize(self.device)
-    res = self.results.cpu().numpy().view(_lib.RESULT_DTYPE)[: self.hb.count]
+    res_b, x, y, s = (t.numpy() for t in self._h_out)
+    res = res_b.view(_lib.RESULT_DTYPE)[: self.hb.count].copy()
     stats = None
     if self.stats is not None:
       stats = self.stats.cpu().numpy().reshape(self.hb.count, self.hb.opts.max_iter,
                                                 _lib.STATS_DOUBLES)
-    return (res, self.x.cpu().numpy(), self.y.cpu().numpy(), self.s.cpu().numpy(), stats)
+    return (res, x.copy(), y.copy(), s.copy(), stats)
+
+
+def start_points(hb: HostBatch, problems: Sequence, points: Sequence, shift: float = 0.1):
+  """Host pools (x0, y0, s0) of starting points for DeviceBatch.launch.
+
+  points[j]: a Solution (or an (x, y, s) triple) of problems[j] -- typically
+  an earlier solve of the same or a nearby QP -- or None for the cold start
+  (x = 0, y = s = 1 on the inequality rows).  y and s of a solution sit on the
+  cone's boundary, so their inequality rows are moved inside: max(., 0) +
+  shift.  Points of a QP whose presolve dropped rows may be given with all
+  rows (as Solutions are); the dropped rows are left out.  A point with
+  non-finite entries (a certificate) falls back to the cold start.
+  """
+  if shift <= 0:
+    raise ValueError("shift must be positive: the method starts inside the cone")
+  x0 = np.zeros(max(hb.n_total, 1))
+  y0 = np.zeros(max(hb.m_total, 1))
+  s0 = np.zeros(max(hb.m_total, 1))
+  for j, (q, pt) in enumerate(zip(problems, points)):
+    d = hb.inst[j]
+    n0, m0, n, m, z = (int(d[k]) for k in ("n_off", "m_off", "n", "m", "z"))
+    y0[m0 + z:m0 + m] = 1.0
+    s0[m0 + z:m0 + m] = 1.0
+    if pt is None:
+      continue
+    x, y, sl = (pt.x, pt.y, pt.s) if hasattr(pt, "x") else pt
+    x, y, sl = (np.asarray(v, dtype=np.float64) for v in (x, y, sl))
+    keep = getattr(getattr(q, "_presolve_state", None), "keep", None)
+    if keep is not None and y.shape[0] == keep.shape[0]:
+      y, sl = y[keep], sl[keep]
+    if x.shape != (n,) or y.shape != (m,) or sl.shape != (m,):
+      raise ValueError(f"initial point {j}: shapes {x.shape}, {y.shape}, {sl.shape} do not "
+                       f"match the problem's n={n}, m={m}")
+    if not (np.all(np.isfinite(x)) and np.all(np.isfinite(y[:z])) and
+            np.all(np.isfinite(y[z:])) and np.all(np.isfinite(sl[z:]))):
+      continue
+    x0[n0:n0 + n] = x
+    y0[m0:m0 + z] = y[:z]
+    y0[m0 + z:m0 + m] = np.maximum(y[z:], 0.0) + shift
+    s0[m0 + z:m0 + m] = np.maximum(sl[z:], 0.0) + shift
+  return x0, y0, s0

@@ -171,14 +171,14 @@ extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
   return QTQP_OK;
 }
 
-extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d_order,
-                                      const qtqp_batch_plan* plan, const double* d_a_pool,
-                                      const double* d_p_pool, const double* d_b_pool,
-                                      const double* d_c_pool, double* d_x_pool, double* d_y_pool,
-                                      double* d_s_pool, qtqp_result* d_results,
-                                      qtqp_iter_stats* d_stats, void* d_workspace,
-                                      size_t workspace_bytes, const qtqp_options* opt,
-                                      void* stream) {
+static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d_order,
+                             const qtqp_batch_plan* plan, const double* d_a_pool,
+                             const double* d_p_pool, const double* d_b_pool,
+                             const double* d_c_pool, double* d_x_pool, double* d_y_pool,
+                             double* d_s_pool, qtqp_result* d_results, qtqp_iter_stats* d_stats,
+                             void* d_workspace, size_t workspace_bytes, const qtqp_options* opt,
+                             const double* d_x0_pool, const double* d_y0_pool,
+                             const double* d_s0_pool, void* stream) {
   if (plan == nullptr || opt == nullptr)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve: null plan/options");
   if (plan->num_groups == 0) return QTQP_OK;
@@ -209,6 +209,9 @@ extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const i
   base.stats = d_stats;
   base.ws = static_cast<char*>(d_workspace);
   base.opt = *opt;
+  base.x0_pool = d_x0_pool;
+  base.y0_pool = d_y0_pool;
+  base.s0_pool = d_s0_pool;
   const int ng = plan->num_groups;
   ForkStreams* fk = nullptr;
   std::unique_lock<std::mutex> fork_lock;  // held until every join is enqueued
@@ -245,6 +248,33 @@ extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const i
     }
   }
   return QTQP_OK;
+}
+
+extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d_order,
+                                      const qtqp_batch_plan* plan, const double* d_a_pool,
+                                      const double* d_p_pool, const double* d_b_pool,
+                                      const double* d_c_pool, double* d_x_pool, double* d_y_pool,
+                                      double* d_s_pool, qtqp_result* d_results,
+                                      qtqp_iter_stats* d_stats, void* d_workspace,
+                                      size_t workspace_bytes, const qtqp_options* opt,
+                                      void* stream) {
+  return dense_batch_solve(d_inst, d_order, plan, d_a_pool, d_p_pool, d_b_pool, d_c_pool,
+                           d_x_pool, d_y_pool, d_s_pool, d_results, d_stats, d_workspace,
+                           workspace_bytes, opt, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" int qtqp_dense_batch_solve_from(
+    const qtqp_dense_instance* d_inst, const int32_t* d_order, const qtqp_batch_plan* plan,
+    const double* d_a_pool, const double* d_p_pool, const double* d_b_pool,
+    const double* d_c_pool, double* d_x_pool, double* d_y_pool, double* d_s_pool,
+    qtqp_result* d_results, qtqp_iter_stats* d_stats, void* d_workspace,
+    size_t workspace_bytes, const qtqp_options* opt, const double* d_x0_pool,
+    const double* d_y0_pool, const double* d_s0_pool, void* stream) {
+  if (d_x0_pool == nullptr || d_y0_pool == nullptr || d_s0_pool == nullptr)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_from: null starting point pool");
+  return dense_batch_solve(d_inst, d_order, plan, d_a_pool, d_p_pool, d_b_pool, d_c_pool,
+                           d_x_pool, d_y_pool, d_s_pool, d_results, d_stats, d_workspace,
+                           workspace_bytes, opt, d_x0_pool, d_y0_pool, d_s0_pool, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -368,6 +398,7 @@ extern "C" int qtqp_dense_batch_solve_noalloc(
   base.stats = d_stats;
   base.ws = static_cast<char*>(ws);
   base.opt = *opt;
+  base.x0_pool = base.y0_pool = base.s0_pool = nullptr;
   // Groups run one after another on the caller's stream (no side streams).
   for (int g = 0; g < plan->num_groups; ++g) {
     const qtqp_launch_group& G = plan->groups[g];

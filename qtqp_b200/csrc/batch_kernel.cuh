@@ -30,6 +30,9 @@ struct BatchParams {
   int* counter;
   qtqp_options opt;
   size_t smem_cap;
+  const double* x0_pool;  // starting points laid out like x / y / s (or null)
+  const double* y0_pool;
+  const double* s0_pool;
 };
 
 template <int NT>
@@ -46,8 +49,15 @@ inline size_t red_bytes_rt(int nt) {
   }
 }
 
+// Resident blocks per SM the compiler must allow for (it caps the registers
+// per thread at 64K / (NT * min blocks)); 1 leaves the register count free.
+#ifndef QTQP_BATCH_MIN_BLOCKS
+#define QTQP_BATCH_MIN_BLOCKS(NT) 1
+#endif
+
 template <int NT>
-__global__ void __launch_bounds__(NT) dense_batch_kernel(const BatchParams p) {
+__global__ void __launch_bounds__(NT, QTQP_BATCH_MIN_BLOCKS(NT))
+    dense_batch_kernel(const BatchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ qtqp_options sopt;
   __shared__ int next_idx;
@@ -65,13 +75,20 @@ __global__ void __launch_bounds__(NT) dense_batch_kernel(const BatchParams p) {
     s.has_p = d.has_p != 0;
     s.A0 = p.a_pool + d.a_off;
     s.P0 = p.p_pool + d.p_off;
+    s.colmajor = true;  // batch pools hold A and P column-major
     s.b0 = p.b_pool + d.m_off;
     s.c0 = p.c_pool + d.n_off;
     s.red = red;
     s.phase = 0;
     s.o = &sopt;
     double* st = p.stats ? reinterpret_cast<double*>(p.stats + d.st_off) : nullptr;
-    s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off);
+    if (p.x0_pool != nullptr) {
+      s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off,
+              nullptr, nullptr, nullptr, p.x0_pool + d.n_off, p.y0_pool + d.m_off,
+              p.s0_pool + d.m_off);
+    } else {
+      s.solve(p.results + id, st, p.x_pool + d.n_off, p.y_pool + d.m_off, p.s_pool + d.m_off);
+    }
     __syncthreads();
     if (threadIdx.x == 0) next_idx = atomicAdd(p.counter, 1) + int(gridDim.x);
     __syncthreads();

@@ -49,9 +49,14 @@ enum VecId : int {
 __host__ __device__ inline int odd_ld(int n) { return (n & 1) ? n : n + 1; }
 __host__ __device__ inline size_t round16(size_t b) { return (b + 15) & ~size_t(15); }
 
+// Panel buffer of the tile Cholesky (tile_cholesky): two panels of (n+3)/4
+// tiles of 4 x 4, each tile padded to 17 elements so that lanes reading
+// different tiles hit different banks.
+__host__ __device__ inline size_t panel_buf_elems(int n) { return size_t(34) * ((n + 3) >> 2); }
+
 struct InstLayout {
   int lda, ldp, ldg, np;  // leading dims (doubles) and padded vector length
-  size_t a_bytes, p_bytes, g_bytes, v_bytes;
+  size_t a_bytes, p_bytes, g_bytes, v_bytes;  // v_bytes: vectors + panel buffer
   int ap_smem, gv_smem;   // 1 when that region lives in shared memory
   size_t smem_bytes, global_bytes;
 };
@@ -67,7 +72,7 @@ __host__ __device__ inline InstLayout plan_layout(int n, int m, size_t smem_cap)
   L.a_bytes = round16(size_t(m) * L.lda * 8);
   L.p_bytes = round16(size_t(n) * L.ldp * 8);
   L.g_bytes = round16(size_t(n) * L.ldg * 8);
-  L.v_bytes = round16(size_t(kNumVec) * L.np * 8);
+  L.v_bytes = round16((size_t(kNumVec) * L.np + panel_buf_elems(n)) * 8);
   const size_t gv = L.g_bytes + L.v_bytes, ap = L.a_bytes + L.p_bytes;
   L.gv_smem = gv <= smem_cap;
   L.ap_smem = L.gv_smem && (gv + ap <= smem_cap);
@@ -159,6 +164,11 @@ struct IrOutcome {
   (void)tid; (void)n; (void)m; (void)z; (void)N; (void)lda; (void)ldp; (void)ldg; \
   (void)A; (void)P; (void)G; (void)has_p
 
+// Independent partial sums per lane of a block's row dots (rowdot).
+#ifndef QTQP_ROWDOT_UNROLL
+#define QTQP_ROWDOT_UNROLL 4
+#endif
+
 // Storage formats of A, P and the KKT factor.
 enum MatFormat : int {
   kFmtDense = 0,  // dense A (m x n), dense P, dense Gram G / Cholesky factor
@@ -187,9 +197,11 @@ struct Ipm {
   int tid;
   int n, m, z, N;
   bool has_p;
-  // Original (presolved, unequilibrated) data in global memory.
+  // Original (presolved, unequilibrated) data in global memory: row-major,
+  // or column-major (the value order of a dense CSC matrix) when colmajor.
   const double* A0;
   const double* P0;
+  bool colmajor = false;
   const double* b0;
   const double* c0;
   // Working data.
@@ -197,6 +209,7 @@ struct Ipm {
   double* P;  // n x ldp equilibrated P with a zero diagonal (P_off)
   double* G;  // n x ldg Gram matrix / Cholesky factor (FP64, or FP32 alias)
   double* V;  // kNumVec vectors of np doubles
+  double* PB;  // panel buffer of tile_cholesky (panel_buf_elems(n) elements)
   int lda, ldp, ldg, np;
   double* red;
   int phase;
@@ -289,7 +302,8 @@ struct Ipm {
   // s * (32/S) + g) so that neighbouring lanes work on neighbouring outputs;
   // their partial sums are combined with xor shuffles, and lane s == 0 calls
   // epi(k, sum).  NACC independent sums per output.  No barrier inside.
-  template <int NACC, bool MAXOP = false, int FORCE_S = 0, typename Body, typename Epi>
+  template <int NACC, bool MAXOP = false, int FORCE_S = 0, typename AccT = double,
+            typename Body, typename Epi>
   __device__ __forceinline__ void rowdot(int K, int len, Body body, Epi epi) const {
     const int S = FORCE_S > 0 ? FORCE_S : lanes_for(K);
     const int per_warp = 32 / S;
@@ -299,40 +313,37 @@ struct Ipm {
     const int per_pass = (NT / 32) * per_warp;
     for (int k0 = 0; k0 < K; k0 += per_pass) {
       const int k = k0 + warp * per_warp + g;
-      double acc[NACC];
+      AccT acc[NACC];
 #pragma unroll
-      for (int a = 0; a < NACC; ++a) acc[a] = 0.0;
+      for (int a = 0; a < NACC; ++a) acc[a] = AccT(0);
       if (k < K) {
-        if constexpr (NT > 1024) {
-          // Grid mode streams A and P from HBM: U independent partial sums
-          // keep U loads in flight per lane.
-          constexpr int U = 8;
-          double part[U][NACC];
+        // U independent partial sums per lane keep U loads (and U FMA
+        // chains) in flight: grid mode streams A and P from HBM; a block's
+        // loads come from shared memory or L2.
+        constexpr int U = NT > 1024 ? 8 : QTQP_ROWDOT_UNROLL;
+        AccT part[U][NACC];
 #pragma unroll
-          for (int u = 0; u < U; ++u)
+        for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int a = 0; a < NACC; ++a) part[u][a] = 0.0;
-          int i = s;
-          for (; i + (U - 1) * S < len; i += U * S) {
+          for (int a = 0; a < NACC; ++a) part[u][a] = AccT(0);
+        int i = s;
+        for (; i + (U - 1) * S < len; i += U * S) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) body(k, i + u * S, part[u]);
-          }
-          for (; i < len; i += S) body(k, i, part[0]);
+          for (int u = 0; u < U; ++u) body(k, i + u * S, part[u]);
+        }
+        for (; i < len; i += S) body(k, i, part[0]);
 #pragma unroll
-          for (int a = 0; a < NACC; ++a) {
-            double t = part[0][a];
+        for (int a = 0; a < NACC; ++a) {
+          AccT t = part[0][a];
 #pragma unroll
-            for (int u = 1; u < U; ++u) t = MAXOP ? fmax(t, part[u][a]) : t + part[u][a];
-            acc[a] = t;
-          }
-        } else {
-          for (int i = s; i < len; i += S) body(k, i, acc);
+          for (int u = 1; u < U; ++u) t = MAXOP ? fmax(t, part[u][a]) : t + part[u][a];
+          acc[a] = t;
         }
       }
       for (int off = 16; off >= per_warp; off >>= 1) {
 #pragma unroll
         for (int a = 0; a < NACC; ++a) {
-          const double o = __shfl_xor_sync(0xffffffffu, acc[a], off);
+          const AccT o = __shfl_xor_sync(0xffffffffu, acc[a], off);
           acc[a] = MAXOP ? fmax(acc[a], o) : acc[a] + o;
         }
       }
@@ -360,6 +371,7 @@ struct Ipm {
     char* gv = L.gv_smem ? smem : gmem;
     G = reinterpret_cast<double*>(gv);
     V = reinterpret_cast<double*>(gv + L.g_bytes);
+    PB = V + size_t(kNumVec) * np;
     char* ap = L.ap_smem ? smem + L.g_bytes + L.v_bytes
                          : gmem + (L.gv_smem ? 0 : L.g_bytes + L.v_bytes);
     A = reinterpret_cast<double*>(ap);
@@ -381,10 +393,17 @@ struct Ipm {
     double* sc = vec(kTMP);  // per-sweep [e_i; d_i]
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    for (int i = warp; i < m; i += NW)
-      for (int j = lane; j < n; j += 32) A[i * lda + j] = A0[size_t(i) * n + j];
-    for (int i = warp; i < n; i += NW)
-      for (int j = lane; j < n; j += 32) P[i * ldp + j] = has_p ? P0[size_t(i) * n + j] : 0.0;
+    if (colmajor) {  // coalesced column reads; odd lda/ldp keep the stores conflict-free
+      for (int j = warp; j < n; j += NW)
+        for (int i = lane; i < m; i += 32) A[i * lda + j] = A0[size_t(j) * m + i];
+      for (int j = warp; j < n; j += NW)
+        for (int i = lane; i < n; i += 32) P[i * ldp + j] = has_p ? P0[size_t(j) * n + i] : 0.0;
+    } else {
+      for (int i = warp; i < m; i += NW)
+        for (int j = lane; j < n; j += 32) A[i * lda + j] = A0[size_t(i) * n + j];
+      for (int i = warp; i < n; i += NW)
+        for (int j = lane; j < n; j += 32) P[i * ldp + j] = has_p ? P0[size_t(i) * n + j] : 0.0;
+    }
     for (int k = tid; k < N; k += NT) de[k] = 1.0;
     sync();
     if (equilibrate) {
@@ -587,64 +606,139 @@ struct Ipm {
       if (mine && bi == bj && i0 + a < n) acc[a][a] = T(double(acc[a][a]) + jit);
     QTQP_TOC(kPhGram);
     QTQP_RETIC();
-    // Broadcast buffers: column k (as left by step k-1) at [0, n).
-    T* buf0 = reinterpret_cast<T*>(vec(kW));
-    T* buf1 = reinterpret_cast<T*>(vec(kTMP));
-    auto publish = [&](int k, T* buf) {
-      if (!mine || bj != (k >> 2)) return;
-      const int c = k & 3;
+    const int info = tile_cholesky<T>(acc, mine, bi, bj, g);
+    QTQP_TOC(kPhChol);
+    return info;
+  }
+
+  // Right-looking Cholesky of the register tiles of factorize_regs in 4-column
+  // panels, one barrier per panel.  Panel k's off-diagonal tiles L_{i,k} =
+  // G_{i,k} L_kk^{-T} are published in the double-buffered panel buffer PB;
+  // every tile right of panel k is then updated by the rank-4 product
+  // L_{i,k} L_{j,k}^T.  The 4 x 4 diagonal factor L_kk is formed by every
+  // thread from the diagonal tile, which its owner publishes in g (its own,
+  // not yet written, region of the factor) one panel ahead, before its last
+  // update; each thread applies that update itself in the owner's order, so
+  // all copies agree to the bit, and a non-positive pivot stops every thread
+  // at the same column.  The diagonal of the result keeps 1 / l_jj, and every 32 x 32
+  // diagonal block of L is inverted in place afterwards (see chol_solve).
+  // Returns 0 or the 1-based index of the first non-positive pivot.
+  template <typename T>
+  __device__ int tile_cholesky(T (&acc)[4][4], bool mine, int bi, int bj, T* g) {
+    QTQP_LOCALS;
+    const int nb = (n + 3) >> 2;
+    const int i0 = bi * 4, j0 = bj * 4;
+    // Lower entries of a diagonal tile into g (its own region).
+    auto put_diag = [&](int t) {
+      if (!mine || bi != t || bj != t) return;
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = i0 + a;
-        if (i >= k && i < n) {
-          T v = acc[a][0];  // acc[a][c] without a run-time register index
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 1; b < 4; ++b)
-            if (b == c) v = acc[a][b];
-          buf[i] = v;
-        }
-      }
+        for (int b = 0; b < 4; ++b)
+          if (b <= a && i0 + a < n) g[(i0 + a) * ldg + j0 + b] = acc[a][b];
     };
-    publish(0, buf0);
-    sync();
-    int info = 0;
-    for (int k = 0; k < n; ++k) {
-      T* buf = (k & 1) ? buf1 : buf0;
-      const T d = buf[k];
-      if (!(d > T(0))) {
-        info = k + 1;
-        break;
-      }
-      // Every thread derives the pivot scalars itself (no divide on the
-      // critical path): 1/sqrt(d), 1/d = (1/sqrt(d))^2.
-      const T il = rsqrt(d);
-      if (mine && j0 + 3 > k) {
-        const T inv_d = il * il;
-        T ci[4], cj[4];
+    // Panel t's tiles (L values; exactly zero in rows and columns beyond n)
+    // live in pb[t & 1] at 17 elements per tile.
+    T* const pb0 = reinterpret_cast<T*>(PB);
+    const int pstride = 17 * nb;
+    auto get_rows = [&](int r0, int t, T (&l)[4][4]) {
+      const T* src = pb0 + (t & 1) * pstride + (r0 >> 2) * 17;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          ci[a] = (i0 + a < n && i0 + a > k) ? buf[i0 + a] : T(0);
-          cj[a] = (j0 + a < n && j0 + a > k) ? buf[j0 + a] * inv_d : T(0);
-        }
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) l[a][c] = src[a * 4 + c];
+    };
+    // The factor of diagonal tile t: D (as published, one update short when
+    // t > 0) minus the rows of panel t-1, then the 4 x 4 Cholesky.  ld keeps
+    // 1 / l on its diagonal.  Returns 0 or the failing 1-based column.
+    auto diag_factor = [&](int t, T (&ld)[4][4]) -> int {
+      T d[4][4];
+      const int r0 = t * 4;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          d[a][b] = (b <= a && r0 + a < n) ? g[(r0 + a) * ldg + r0 + b] : T(0);
+      if (t > 0) {
+        T l[4][4];
+        get_rows(r0, t - 1, l);
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = fma(-ci[a], cj[b], acc[a][b]);
+          for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) d[a][b] = fma(-l[a][c], l[b][c], d[a][b]);
       }
-      if (mine && bj == (k >> 2)) {  // finish column k; the diagonal keeps 1/l_kk
-        const int c = k & 3;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int i = i0 + a;
+      for (int c = 0; c < 4; ++c) {
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            if (b != c) continue;
-            if (i == k) acc[a][b] = il;
-            else if (i > k) acc[a][b] *= il;
-          }
+        for (int a = 0; a < 4; ++a) ld[a][c] = T(0);
+        if (r0 + c >= n) continue;
+        const T piv = d[c][c];
+        if (!(piv > T(0))) return r0 + c + 1;
+        const T il = rsqrt(piv);
+        ld[c][c] = il;
+#pragma unroll
+        for (int a = c + 1; a < 4; ++a) ld[a][c] = d[a][c] * il;
+#pragma unroll
+        for (int a = c + 1; a < 4; ++a)
+#pragma unroll
+          for (int b = c + 1; b <= a; ++b) d[a][b] = fma(-ld[a][c], ld[b][c], d[a][b]);
+      }
+      return 0;
+    };
+    // This thread's tile of panel t (already updated by panels < t) becomes
+    // L_{i,t} = tile L_tt^{-T}; the diagonal tile becomes L_tt itself.
+    auto finish_panel = [&](int t, const T (&ld)[4][4]) {
+      if (bi == t) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[a][c] = ld[a][c];
+        return;
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          T x = acc[a][c];
+#pragma unroll
+          for (int q = 0; q < c; ++q) x = fma(-acc[a][q], ld[c][q], x);
+          acc[a][c] = x * ld[c][c];  // ld[c][c] = 1 / l_cc (0 beyond n)
         }
       }
-      if (k + 1 < n) publish(k + 1, (k & 1) ? buf0 : buf1);
+      T* dst = pb0 + (t & 1) * pstride + bi * 17;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dst[a * 4 + c] = acc[a][c];
+    };
+    put_diag(0);
+    put_diag(1);
+    sync();
+    int info = 0;
+    {
+      T ld[4][4];
+      info = diag_factor(0, ld);
+      if (info == 0 && mine && bj == 0) finish_panel(0, ld);
+    }
+    sync();
+    for (int kb = 0; info == 0 && kb + 1 < nb; ++kb) {
+      if (mine && bj > kb) {  // rank-4 update with panel kb
+        T li[4][4], lj[4][4];
+        get_rows(i0, kb, li);
+        get_rows(j0, kb, lj);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b] = fma(-li[a][c], lj[b][c], acc[a][b]);
+      }
+      T ld[4][4];
+      info = diag_factor(kb + 1, ld);
+      if (info == 0 && mine && bj == kb + 1) finish_panel(kb + 1, ld);
+      if (kb + 2 < nb) put_diag(kb + 2);
       sync();
     }
     if (info == 0 && mine) {
@@ -658,7 +752,6 @@ struct Ipm {
     }
     sync();
     if (info == 0) invert_diag_blocks<T>(g);
-    QTQP_TOC(kPhChol);
     return info;
   }
 
@@ -816,6 +909,8 @@ struct Ipm {
   // Solves L L^T v = v in place with the block-inverted factor: forward
   // z_b = X_bb (v_b - sum_{c<b} L_bc z_c), backward x_b = X_bb^T (z_b -
   // sum_{c>b} L_cb^T x_c), two barriers per 32-block; w is n scratch entries.
+  // Each phase is a set of row dots (rowdot: several lanes per row, partial
+  // sums combined by shuffles), so no thread walks a 32-long chain alone.
   template <typename T>
   QTQP_PHASE void chol_solve(const T* g, T* v, T* w) {
     if constexpr (FMT == kFmtLarge) {
@@ -826,37 +921,39 @@ struct Ipm {
     const int nblk = (n + 31) >> 5;
     for (int blk = 0; blk < nblk; ++blk) {
       const int kb = blk * 32, bs = min(32, n - kb);
-      for (int r = tid; r < bs; r += NT) {
-        const T* row = g + (kb + r) * ldg + kb;
-        T acc = T(0);
-        for (int k = 0; k <= r; ++k) acc = fma(row[k], v[kb + k], acc);
-        w[kb + r] = acc;
-      }
+      const T* gb = g + kb * ldg + kb;
+      rowdot<1, false, 0, T>(bs, bs,
+                [&](int r, int k, T* acc) {
+                  if (k <= r) acc[0] = fma(gb[r * ldg + k], v[kb + k], acc[0]);
+                },
+                [&](int r, T* acc) { w[kb + r] = acc[0]; });
       sync();
       if (kb + bs < n) {
-        for (int i = kb + bs + tid; i < n; i += NT) {
-          const T* li = g + i * ldg + kb;
-          T acc = v[i];
-          for (int k = 0; k < bs; ++k) acc = fma(-li[k], w[kb + k], acc);
-          v[i] = acc;
-        }
+        const T* gl = g + (kb + bs) * ldg + kb;
+        rowdot<1, false, 0, T>(n - kb - bs, bs,
+                  [&](int i, int k, T* acc) {
+                    acc[0] = fma(gl[i * ldg + k], w[kb + k], acc[0]);
+                  },
+                  [&](int i, T* acc) { v[kb + bs + i] -= acc[0]; });
         sync();
       }
     }
     for (int blk = nblk - 1; blk >= 0; --blk) {
       const int kb = blk * 32, bs = min(32, n - kb);
-      for (int r = tid; r < bs; r += NT) {
-        T acc = T(0);
-        for (int k = r; k < bs; ++k) acc = fma(g[(kb + k) * ldg + kb + r], w[kb + k], acc);
-        v[kb + r] = acc;
-      }
+      const T* gb = g + kb * ldg + kb;
+      rowdot<1, false, 0, T>(bs, bs,
+                [&](int r, int k, T* acc) {
+                  if (k >= r) acc[0] = fma(gb[k * ldg + r], w[kb + k], acc[0]);
+                },
+                [&](int r, T* acc) { v[kb + r] = acc[0]; });
       sync();
       if (kb > 0) {
-        for (int i = tid; i < kb; i += NT) {
-          T acc = w[i];
-          for (int k = 0; k < bs; ++k) acc = fma(-g[(kb + k) * ldg + i], v[kb + k], acc);
-          w[i] = acc;
-        }
+        const T* gc = g + kb * ldg;
+        rowdot<1, false, 0, T>(kb, bs,
+                  [&](int i, int k, T* acc) {
+                    acc[0] = fma(gc[k * ldg + i], v[kb + k], acc[0]);
+                  },
+                  [&](int i, T* acc) { w[i] -= acc[0]; });
         sync();
       }
     }
@@ -1008,8 +1105,14 @@ struct Ipm {
       sync();
       QTQP_TIC();
       kkt_residual(sol, krhs, res, mx[1], mx[2]);
+      // The reduction's barrier also orders every thread's res writes before
+      // the solve that reads them.
       reduce<0, 3>(dummy, mx);
-      sync();
+      if constexpr (NT <= 1024) {
+        if (NT / 32 == 1) sync();  // a one-warp reduction has no barrier
+      } else {
+        sync();
+      }
       QTQP_TOC(kPhResidual);
       out.rhs_norm = mx[0];
       out.final_res = mx[1];
@@ -1027,8 +1130,12 @@ struct Ipm {
       QTQP_TIC();
       double mx[2] = {0.0, 0.0};
       kkt_residual(sol, krhs, res, mx[0], mx[1]);
-      reduce<0, 2>(dummy, mx);
-      sync();
+      reduce<0, 2>(dummy, mx);  // its barrier orders the res writes (as above)
+      if constexpr (NT <= 1024) {
+        if (NT / 32 == 1) sync();
+      } else {
+        sync();
+      }
       QTQP_TOC(kPhResidual);
       rn = mx[0];
       out.nan = mx[1] > 0.0;
@@ -1494,10 +1601,15 @@ struct Ipm {
   // learned warm start of this instance (x and y in the original scaling,
   // active-row mask), or null for the plain method.
   // --------------------------------------------------------------------------
+  // start_*: a starting point in the original scaling (y, s positive on the
+  // inequality rows) that replaces the cold start (no reference counterpart:
+  // a re-solve started from an earlier solution), or null.
   __device__ void solve(qtqp_result* result, double* stats, double* x_out, double* y_out,
                         double* s_out, const double* warm_x = nullptr,
                         const double* warm_y = nullptr,
-                        const unsigned char* warm_act = nullptr) {
+                        const unsigned char* warm_act = nullptr,
+                        const double* start_x = nullptr, const double* start_y = nullptr,
+                        const double* start_s = nullptr) {
     const qtqp_options& op = *o;
     const uint64_t t_start = globaltimer_ns();
     double nb, nc;
@@ -1543,11 +1655,45 @@ struct Ipm {
     double* ct = vec(kCT);  // Mehrotra correction at [n, N)
     const double* q = vec(kQ);
     const double* de = vec(kDE);
+    // Starting point.  A learned warm start that was not accepted starts the
+    // method from its prediction when options.warm_shift > 0: x = x_hat,
+    // y = y_hat on the equality rows, y = max(y_hat, 0) + shift and
+    // s = max(b - A x_hat, 0) + shift on the inequality rows.  A given
+    // start_* point is taken as it is.  Both are equilibrated like the cold
+    // start (x/e, y/d, s*d).
+    const bool from_pred = warm_act != nullptr && op.warm_shift > 0.0;
+    const bool from_start = start_x != nullptr;
+    if (from_pred || from_start) {
+      const double sh = from_pred ? op.warm_shift : 0.0;
+      const double* px0 = from_start ? start_x : warm_x;
+      for (int k = tid; k < n; k += NT) xy[k] = px0[k] / de[k];
+      sync();
+      if (!from_start) {
+        a_times(xy, s);  // s[n + i] = (A_eq x)_i = d_i (A x_hat)_i
+        sync();
+      }
+      for (int k = own(n); k < N; k += NT) {
+        const int i = k - n;
+        const double yi = from_start ? start_y[i] : warm_y[i];
+        if (i < z) {
+          xy[k] = yi / de[k];
+          s[k] = 0.0;
+        } else if (from_start) {
+          xy[k] = yi / de[k];
+          s[k] = start_s[i] * de[k];
+        } else {
+          const double slack = fmax((q[k] - s[k]) / de[k], 0.0);  // b - A x_hat
+          xy[k] = (fmax(yi, 0.0) + sh) / de[k];
+          s[k] = (slack + sh) * de[k];
+        }
+      }
+    }
     // _init_variables (__init__.py:299-307): x = 0, y[z:] = s[z:] = 1, then
     // equilibrated (x/e, y/d, s*d); K^{-1} q starts at zero.
     for (int k = tid; k < N; k += NT) {
       kq[k] = 0.0;
-      if (k < n) {
+      if (from_pred || from_start) {
+      } else if (k < n) {
         xy[k] = 0.0 / de[k];
       } else if (k < n + z) {
         xy[k] = 0.0;

@@ -27,8 +27,9 @@ def test_device_ruiz_matches_reference(k):
   lib = _lib.load()
   g = golden_io.load("reference_units.npz")
   pre = f"ruiz{k}/"
-  a = golden_io.csc(g, pre + "a").toarray()
-  p = golden_io.csc(g, pre + "p").toarray()
+  # Row-major copies (a CSC matrix's toarray() is column-major).
+  a = np.ascontiguousarray(golden_io.csc(g, pre + "a").toarray())
+  p = np.ascontiguousarray(golden_io.csc(g, pre + "p").toarray())
   m, n = a.shape
   dev = dict(dtype=torch.float64, device="cuda")
   da, dp = torch.from_numpy(a).to(**dev), torch.from_numpy(p).to(**dev)

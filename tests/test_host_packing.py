@@ -2,7 +2,7 @@
 (CSR and CSC), P, b and c read back exactly from the int32/double pools at the
 offsets in its descriptor; problems built from the same A and P objects share
 one packed copy; the plan orders every instance once and sizes a workspace.
-Dense batch: A, P, b and c read back exactly from the row-major pools.
+Dense batch: A, P, b and c read back exactly from the column-major pools.
 """
 
 import numpy as np
@@ -71,24 +71,32 @@ def test_plan_orders_each_instance_once():
 
 
 def test_dense_pools_read_back_every_instance():
-  """The dense batch's pools (A m x n and P n x n row-major per instance; an
-  LP or an all-zero P packs no P) read back exactly at each descriptor's
-  offsets."""
+  """The dense batch's pools (A m x n and P n x n column-major per instance;
+  an LP or an all-zero P packs no P) read back exactly at each descriptor's
+  offsets, from DenseProblems and from QTQP objects alike; a QTQP whose CSC
+  matrices store every entry is packed from its value arrays in place."""
+  import qtqp_b200 as qb
   from qtqp_b200 import batch
-  probs = []
-  for i in range(5):
+  probs, qps = [], []
+  for i in range(6):
     a, b, c, z, p = problems.small_dense_instance(i)
+    if i == 4:  # a sparse A (not every entry stored) packs through a dense copy
+      a = sp.csc_matrix(np.where(np.abs(a.toarray()) > 0.5, a.toarray(), 0.0))
     probs.append(batch.DenseProblem(a.toarray(), b, c, z, p.toarray() if i != 2 else None))
-  hb = batch.HostBatch(probs, SolveOptions())
-  for i, pr in enumerate(probs):
-    d = hb.inst[i]
-    m, n = pr.a.shape
-    a0, p0 = int(d["a_off"]), int(d["p_off"])
-    np.testing.assert_array_equal(hb.a_pool[a0:a0 + m * n].reshape(m, n), pr.a)
-    assert int(d["has_p"]) == (pr.p is not None)
-    if pr.p is not None:
-      np.testing.assert_array_equal(hb.p_pool[p0:p0 + n * n].reshape(n, n), pr.p)
-    m0, n0 = int(d["m_off"]), int(d["n_off"])
-    np.testing.assert_array_equal(hb.b_pool[m0:m0 + m], pr.b)
-    np.testing.assert_array_equal(hb.c_pool[n0:n0 + n], pr.c)
-  assert hb.p_pool.size == sum(p.a.shape[1] ** 2 for p in probs if p.p is not None)
+    qps.append(qb.QTQP(a=a, b=b, c=c, z=z, p=p if i != 2 else None))
+  for src in (probs, qps):
+    hb = batch.HostBatch(src, SolveOptions())
+    for i, pr in enumerate(probs):
+      d = hb.inst[i]
+      m, n = pr.a.shape
+      a0, p0 = int(d["a_off"]), int(d["p_off"])
+      np.testing.assert_array_equal(hb.a_pool[a0:a0 + m * n].reshape(n, m).T, pr.a)
+      assert int(d["has_p"]) == (pr.p is not None)
+      if pr.p is not None:
+        np.testing.assert_array_equal(hb.p_pool[p0:p0 + n * n].reshape(n, n).T, pr.p)
+      m0, n0 = int(d["m_off"]), int(d["n_off"])
+      np.testing.assert_array_equal(hb.b_pool[m0:m0 + m], pr.b)
+      np.testing.assert_array_equal(hb.c_pool[n0:n0 + n], pr.c)
+    assert hb.p_pool.size == sum(p.a.shape[1] ** 2 for p in probs if p.p is not None)
+  assert all(getattr(q, "_dense_pack", None) is not None for i, q in enumerate(qps) if i != 4)
+  assert getattr(qps[4], "_dense_pack", None) is None
