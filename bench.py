@@ -57,7 +57,17 @@ def _args():
                   help="batch_small: 4096 uneven small dense QPs (default); dense_large: "
                        "one n=4096, m=8192 dense QP on the whole GPU; parametric: a T=50 "
                        "MPC family with the learned warm start")
-  ap.add_argument("--train", type=int, default=4096, help="parametric: training instances")
+  ap.add_argument("--train", type=int, default=16384,
+                  help="parametric: training instances (the family's stated split: 16384 "
+                       "train, 3616 held out)")
+  ap.add_argument("--warm-corrections", type=int, default=8,
+                  help="parametric: primal-dual corrections of the reduced KKT solve")
+  ap.add_argument("--warm-shift", type=float, default=0.1,
+                  help="parametric: a rejected prediction starts the IPM shifted by this "
+                       "(0: the cold start)")
+  ap.add_argument("--hinge", type=float, default=1.0,
+                  help="parametric: weight of the hinge term in the MLP training loss")
+  ap.add_argument("--epochs", type=int, default=60, help="parametric: training epochs")
   ap.add_argument("--mpc-horizon", type=int, default=500,
                   help="mpc: horizon T (n = 60 T); 500 is the workload, smaller horizons are "
                        "for profiling captures")
@@ -69,12 +79,22 @@ def _args():
                        "sizes are for profiling captures")
   ap.add_argument("--count", type=int, default=COUNT)
   ap.add_argument("--no-cpu-baseline", action="store_true")
+  ap.add_argument("--no-tune", action="store_true",
+                  help="batch_small: use the library's default launch shapes")
   return ap.parse_args()
 
 
-def _instances(rank: int, count: int):
-  from qtqp_b200 import problems
-  return [problems.small_dense_instance(rank * COUNT + i) for i in range(count)]
+def _instances(rank: int, count: int, world: int = 1):
+  """This rank's instances: all `count` at N = 1; at N > 1 its share of the
+  world x count instances, balanced by estimated work (weak scaling: about
+  `count` instances' work per GPU; only the rank's own instances are built)."""
+  from qtqp_b200 import distributed, problems
+  if world == 1:
+    return [problems.small_dense_instance(i) for i in range(count)]
+  total = world * count
+  costs = [distributed.instance_cost(*problems.small_dense_size(i)) for i in range(total)]
+  mine = distributed.shard_by_cost(costs, world)[rank]
+  return [problems.small_dense_instance(i) for i in mine]
 
 
 # ---------------------------------------------------------------------------
@@ -224,11 +244,21 @@ def run_ours(args) -> None:
   dev = torch.device("cuda", local)
   stream = torch.cuda.current_stream(dev)
 
-  insts = _instances(rank, args.count)
+  insts = _instances(rank, args.count, world)
   qps = [qb.QTQP(a=a, b=b, c=c, z=z, p=p) for a, b, c, z, p in insts]
 
+  # Launch shapes: the autotuner times each size class's candidate shapes on
+  # this GPU (outside the timed region) unless --no-tune.
+  from qtqp_b200 import autotune
+  tuning, t_tune = None, 0.0
+  if not args.no_tune:
+    t0 = time.perf_counter()
+    tuning = autotune.tune_dense_batch(qps, batch.SolveOptions(precision="fp64"), device=dev)
+    t_tune = time.perf_counter() - t0
+
   def prepare(precision):
-    hb = batch.HostBatch(qps, batch.SolveOptions(precision=precision), pinned=True)
+    hb = batch.HostBatch(qps, batch.SolveOptions(precision=precision), pinned=True,
+                         tuning=tuning)
     db = batch.DeviceBatch(hb, device=dev)
     db.upload(stream)
     torch.cuda.synchronize(dev)
@@ -264,6 +294,13 @@ def run_ours(args) -> None:
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
+  def sum_over_ranks(v):
+    if dist is None:
+      return v
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(round(t.item()))
+
   def solved_count(db):
     res, *_ = db.fetch()
     return int(np.sum(res["status"] == 0)), res
@@ -283,9 +320,12 @@ def run_ours(args) -> None:
 
   chosen = forms[args.precision]
   hb, db, res = chosen["hb"], chosen["db"], chosen["res"]
-  solved_total = chosen["solved"] * world
+  solved_total = sum_over_ranks(chosen["solved"])
   value = solved_total * args.steps / chosen["time"]
-  fp64_value = forms["fp64"]["solved"] * world * args.steps / forms["fp64"]["time"]
+  fp64_solved = sum_over_ranks(forms["fp64"]["solved"])
+  mixed_solved = sum_over_ranks(forms["mixed"]["solved"])
+  instances_total = sum_over_ranks(len(qps))
+  fp64_value = fp64_solved * args.steps / forms["fp64"]["time"]
   same_status = bool(np.array_equal(forms["fp64"]["res"]["status"], res["status"]))
 
   def ev_pair():
@@ -296,21 +336,21 @@ def run_ours(args) -> None:
   # unpacking), timed with CUDA events recorded before the call and after it
   # returns (the call synchronises).
   for _ in range(args.warmup):
-    qb.solve_batch(qps, precision=args.precision)
+    qb.solve_batch(qps, precision=args.precision, tuning=tuning)
   barrier()
   e_total, e2e_solved = 0.0, 0
   for _ in range(args.steps):
     flush.fill_(1)
     e0, e1 = ev_pair()
     e0.record(stream)
-    sols = qb.solve_batch(qps, precision=args.precision)
+    sols = qb.solve_batch(qps, precision=args.precision, tuning=tuning)
     e1.record(stream)
     e1.synchronize()
     e_total += e0.elapsed_time(e1) * 1e-3
     e2e_solved = sum(1 for x in sols if x.status == qb.SolutionStatus.SOLVED)
   barrier()
   e_total = max_over_ranks(e_total)
-  e2e_value = e2e_solved * world * args.steps / e_total
+  e2e_value = sum_over_ranks(e2e_solved) * args.steps / e_total
   h2d = hb.input_bytes
   d2h = db.output_bytes
 
@@ -375,15 +415,21 @@ def run_ours(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator of the workload's distribution)",
         "config": {"workload": WORKLOAD, "instances_per_gpu": args.count,
+                   "sharding": "one GPU" if world == 1 else
+                               "cost-balanced shares of world x 4096 (m n^2 + n^3/3)",
                    "precision": args.precision, "l2": "flushed between steps (256 MiB write);"
                    " inputs also exceed L2",
-                   "launch_groups": [list(g) for g in hb.groups]},
+                   "launch_groups": [list(g) for g in hb.groups],
+                   "autotuned": None if tuning is None else {
+                       "seconds": round(t_tune, 2),
+                       "table": [[e["n_lo"], e["n_hi"], e["block_threads"], e["lean"],
+                                  e["onchip"], e["default_ms"], e["ms"]] for e in tuning]}},
         "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
-        "mixed_value": forms["mixed"]["solved"] * world * args.steps / forms["mixed"]["time"],
+        "mixed_value": mixed_solved * args.steps / forms["mixed"]["time"],
         "mixed_statuses_identical_to_fp64": bool(np.array_equal(
             forms["fp64"]["res"]["status"], forms["mixed"]["res"]["status"])),
         "statuses_identical_to_fp64": same_status,
-        "solved_per_step": solved_total, "instances_per_step": args.count * world,
+        "solved_per_step": solved_total, "instances_per_step": instances_total,
         "mean_iterations": float(np.mean(iters)),
         "factorizations": {"fp32": int(res["fp32_factorizations"].sum()),
                            "fp64": int(res["fp64_factorizations"].sum())},
@@ -709,7 +755,7 @@ def run_parametric(args):
   local = int(os.environ.get("LOCAL_RANK", "0"))
   if rank != 0:
     return
-  test_count = args.count if args.count != COUNT else 512
+  test_count = args.count if args.count != COUNT else 3616
   from qtqp_b200 import problems
   fam = problems.parametric_mpc_family(count=args.train + test_count)
   thetas = fam[-1]
@@ -763,7 +809,8 @@ def run_parametric(args):
                                    [s_.s for s_ in sols])
   net = warmstart.WarmStartMLP(dim=thetas.shape[1], n=q0.n, m=q0.m, z=q0.z, seed=0, device=dev)
   t0 = time.perf_counter()
-  rep = net.train(thetas[keep], targets, epochs=30, batch=64, lr=2e-3)
+  rep = net.train(thetas[keep], targets, epochs=args.epochs, batch=64, lr=2e-3,
+                  hinge_weight=args.hinge, cosine=True)
   torch.cuda.synchronize(dev)
   t_train = time.perf_counter() - t0
   net.calibrate(thetas[keep], targets)
@@ -780,8 +827,9 @@ def run_parametric(args):
             for _ in range(args.steps))
     return t, db.fetch()[0]
   t_plain, r_plain = timed(batch.SolveOptions(precision="fp64"), lambda: None)
-  corr = 8  # the best measured budget of primal-dual corrections on this family
-  t_warm, r_warm = timed(batch.SolveOptions(precision=args.precision, warm_corrections=corr),
+  corr = args.warm_corrections
+  t_warm, r_warm = timed(batch.SolveOptions(precision=args.precision, warm_corrections=corr,
+                                            warm_shift=args.warm_shift),
                          lambda: net.predict_device(thetas[test]))
   solved_w = int(np.sum(r_warm["status"] == 0))
   solved_p = int(np.sum(r_plain["status"] == 0))
@@ -797,6 +845,8 @@ def run_parametric(args):
       "data": "synthetic (seeded generator of the family)",
       "config": {"workload": PARAM_WORKLOAD, "test_instances": test_count,
                  "train_instances": len(keep), "warm_corrections": corr,
+                 "warm_shift": args.warm_shift, "hinge_weight": args.hinge,
+                 "epochs": rep.epochs,
                  "chosen": f"{args.precision} + learned warm start; fp64_value: plain FP64"},
       "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
       "statuses_identical": bool(np.array_equal(r_plain["status"], r_warm["status"])),

@@ -112,7 +112,8 @@ typedef struct {
   int32_t block_threads; /* threads per block                             */
   int32_t smem_bytes;    /* dynamic shared memory per block               */
   int32_t slots;         /* banded batches: workspace slots (max blocks)   */
-  int32_t reserved;
+  int32_t lean;          /* dense batches: 1 = the register-capped kernel
+                            (more resident blocks), 0 = free registers     */
   uint64_t slot_off;     /* banded batches: byte offset of the first slot  */
   uint64_t slot_bytes;   /* banded batches: bytes per slot                 */
 } qtqp_launch_group;
@@ -153,6 +154,26 @@ int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
                           const qtqp_options* opt, int32_t* h_order,
                           int32_t block_threads, int32_t smem_bytes,
                           qtqp_batch_plan* plan);
+
+/* One entry of a launch-shape tuning table (no reference counterpart; the
+ * library's autotuner writes them, qtqp_b200/autotune.py): a launch group
+ * whose largest n lies in [n_lo, n_hi] runs with block_threads threads per
+ * block (32, 64, 128 or 256), the register-capped kernel when lean != 0, and
+ * A and P in shared memory when onchip != 0 and they fit (else only the Gram
+ * matrix and the vectors).  qtqp_dense_batch_plan_tuned plans like
+ * qtqp_dense_batch_plan and then applies the first matching entry to each
+ * group; groups no entry matches keep the default shape. */
+typedef struct {
+  int32_t n_lo, n_hi;
+  int32_t block_threads;
+  int32_t lean;
+  int32_t onchip;
+  int32_t reserved;
+} qtqp_batch_tuning;
+int qtqp_dense_batch_plan_tuned(qtqp_dense_instance* h_inst, int32_t count,
+                                const qtqp_options* opt, int32_t* h_order,
+                                const qtqp_batch_tuning* table, int32_t entries,
+                                qtqp_batch_plan* plan);
 
 /* Device-resident solve of the whole batch.
  * d_inst / d_order: the planned descriptors and order, copied to the device by
@@ -310,6 +331,16 @@ int qtqp_mlp_colsum(const float* d_d, int32_t rows, int32_t cols, float* d_db,
 /* dy = 2 (y - t) / count and *d_loss = sum (y - t)^2 (overwritten). */
 int qtqp_mlp_mse_grad(const float* d_y, const float* d_t, int64_t count,
                       float* d_dy, double* d_loss, void* stream);
+/* Hinge term on the sign of the inequality outputs, added to d_dy (after
+ * qtqp_mlp_mse_grad on the same buffers): columns [col0, cols) of the
+ * rows x cols output; d_zero[j - col0] is the column's decision point (the
+ * standardised value of y_i - s_i = 0); the target's side of it gives the
+ * sign s = +-1.  Adds weight * mean(relu(margin - s (y - zero))) to *d_loss
+ * and its gradient to d_dy. */
+int qtqp_mlp_hinge_grad(const float* d_y, const float* d_t, int32_t rows,
+                        int32_t cols, int32_t col0, const float* d_zero,
+                        float weight, float margin, float* d_dy, double* d_loss,
+                        void* stream);
 /* One Adam step (bias-corrected, step >= 1). */
 int qtqp_mlp_adam(float* d_p, const float* d_g, float* d_m, float* d_v,
                   int64_t count, float lr, float beta1, float beta2, float eps,
@@ -397,6 +428,24 @@ int qtqp_dense_equilibrate(int32_t n, int32_t m, const double* d_a,
                            const double* d_c, void* d_ws, double* d_d,
                            double* d_e, double* d_a_eq, double* d_p_eq,
                            void* stream);
+
+/* ---- self-test of the bounded device waits ------------------------------ *
+ * No reference counterpart.  Every spin-wait of the kernels gives up after a
+ * poll limit and reports an error instead of hanging (the grid barrier of the
+ * whole-GPU solves: QTQP_ERR_TIMEOUT from the solve; the tensor-core
+ * pipelines' mbarrier waits).  This makes one run out on purpose with a short
+ * limit (limit polls, at most 2^24) and writes the outcome to *d_status
+ * (QTQP_OK or QTQP_ERR_TIMEOUT):
+ *   mode 0: a cooperative grid of `blocks` blocks (2..64) where block
+ *           skip_block never reaches the barrier the others wait at
+ *           (skip_block = -1: every block arrives, a control run);
+ *           d_workspace: qtqp_wait_selftest_workspace_bytes() bytes;
+ *   mode 1: one block waits on an mbarrier that nothing arrives on.
+ * Nothing faults: the waits stop and the kernels return. */
+size_t qtqp_wait_selftest_workspace_bytes(void);
+int qtqp_wait_selftest(int32_t mode, int32_t blocks, int32_t skip_block,
+                       uint32_t limit, void* d_workspace, int32_t* d_status,
+                       void* stream);
 
 #ifdef __cplusplus
 }

@@ -200,13 +200,39 @@ class QTQP:
     return _batch.DenseProblem(a=self.a.toarray(), b=self.b, c=self.c, z=self.z, p=p)
 
   def band_problem(self):
-    """The presolved QP in the sparse form of the banded device solver."""
+    """The presolved QP in the sparse form of the banded device solver, its
+    variables in the band ordering (band_permutation) when there is one."""
     from . import band as _band  # pylint: disable=g-import-not-at-top
-    return _band.BandProblem(self.a, self.b, self.c, self.z, self.p if self.p.nnz else None)
+    perm = self.band_permutation()
+    if perm is None:
+      return _band.BandProblem(self.a, self.b, self.c, self.z, self.p if self.p.nnz else None)
+    a_p, p_p = self._permuted
+    return _band.BandProblem(a_p, self.b, self.c[perm], self.z, p_p)
+
+  def band_permutation(self):
+    """Ordering of the variables under which P + A^T D A is narrow-banded,
+    when the natural one is not: a reverse Cuthill-McKee ordering of the
+    Gram matrix's sparsity graph (a fill- and bandwidth-reducing ordering;
+    the banded device factorisation then works on the permuted QP, whose x
+    is permuted back).  None when the natural ordering is narrow or no
+    narrow ordering is found.  Computed once."""
+    if not hasattr(self, "_perm"):
+      self._perm, self._permuted = None, None
+      from . import band as _band  # pylint: disable=g-import-not-at-top
+      p = self.p if self.p.nnz else None
+      if self.n > 96 and 4 * (_band.gram_bandwidth(self.a, p) + 1) > self.n:
+        perm = _band.band_ordering(self.a, p)
+        if perm is not None:
+          a_p = sp.csc_matrix(self.a[:, perm])
+          p_p = sp.csc_matrix(p[perm][:, perm]) if p is not None else None
+          if 4 * (_band.gram_bandwidth(a_p, p_p) + 1) <= self.n:
+            self._perm, self._permuted = perm, (a_p, p_p)
+    return self._perm
 
   def storage_format(self, single: bool = False) -> str:
     """'band' when the Gram matrix P + A^T D A is narrow-banded (its
-    half-bandwidth at most n/4) and n > 96 -- 'band_grid' (the whole GPU,
+    half-bandwidth at most n/4, in the natural ordering or in the band
+    ordering of band_permutation) and n > 96 -- 'band_grid' (the whole GPU,
     partitioned band factorisation) instead for a QP solved on its own with
     n >= BAND_GRID_N; otherwise 'large' (the whole GPU on one dense QP) when
     n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on its own; else
@@ -214,7 +240,11 @@ class QTQP:
     if self.n <= 96:
       return "dense"
     from . import band as _band  # pylint: disable=g-import-not-at-top
-    bw = _band.gram_bandwidth(self.a, self.p if self.p.nnz else None)
+    p = self.p if self.p.nnz else None
+    bw = _band.gram_bandwidth(self.a, p)
+    if 4 * (bw + 1) > self.n and self.band_permutation() is not None:
+      a_p, p_p = self._permuted
+      bw = _band.gram_bandwidth(a_p, p_p)
     if 4 * (bw + 1) <= self.n:
       if single and self.n >= BAND_GRID_N and _band.grid_supported(bw, self.n):
         return "band_grid"
@@ -303,8 +333,27 @@ def _log_iteration(st: Dict[str, Any]) -> None:
         f" {infeas:>8.2e} | {st['mu']:>8.2e} | {solves:>8} | {st['time']:>8.2e} |")
 
 
+_TUNING = {}
+
+
+def _dense_tuning(tuning):
+  """The launch-shape table of the dense batch: 'auto' = the autotuner's
+  cached table for this GPU model (read once), None = the default plan, or
+  an explicit table."""
+  if tuning != "auto":
+    return tuning
+  if "auto" not in _TUNING:
+    from . import autotune  # pylint: disable=g-import-not-at-top
+    try:
+      _TUNING["auto"] = autotune.load()
+    except (OSError, ValueError):
+      _TUNING["auto"] = None
+  return _TUNING["auto"]
+
+
 def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: str = "auto",
-                warm_start=None, initial=None, initial_shift: float = 0.1, _opts=None,
+                warm_start=None, initial=None, initial_shift: float = 0.1, tuning="auto",
+                _opts=None,
                 _verbose: bool = False, _start: float | None = None,
                 **solve_kwargs) -> List[Solution]:
   """Solves independent QPs in one persistent GPU launch.
@@ -319,8 +368,10 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   when warm_shift > 0).  initial: one starting point per problem (a Solution,
   an (x, y, s) triple, or None for the cold start), e.g. the solutions of an
   earlier call on the same or nearby QPs; its inequality rows are moved
-  initial_shift inside the cone (dense storage only).  Returns one Solution
-  per problem, in order.
+  initial_shift inside the cone (dense storage only).  tuning: launch shapes
+  of the dense batch -- 'auto' (the autotuner's cached table for this GPU,
+  if any; see qtqp_b200.autotune), None (the library's default plan) or a
+  table.  Returns one Solution per problem, in order.
   """
   start = timeit.default_timer() if _start is None else _start
   if _opts is None:
@@ -379,7 +430,8 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     if not idx:
       continue
     if kind == "dense":
-      hb = _batch.HostBatch([problems[i] for i in idx], opts, pinned=True)
+      hb = _batch.HostBatch([problems[i] for i in idx], opts, pinned=True,
+                            tuning=_dense_tuning(tuning))
       db = _batch.DeviceBatch(hb, records=records)
     else:
       from . import band as _band  # pylint: disable=g-import-not-at-top
@@ -415,16 +467,32 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     iters = res["iterations"].tolist()
     for j, i in enumerate(idx):
       n0, m0, mj = n_off[j], m_off[j], ms[j]
-      out[i] = _make_solution(problems[i], xp[n0:n0 + ns[j]], yp[m0:m0 + mj],
+      x = xp[n0:n0 + ns[j]]
+      if kind == "band":
+        x = _unpermute(problems[i], x)
+      out[i] = _make_solution(problems[i], x, yp[m0:m0 + mj],
                               sp_[m0:m0 + mj], codes[j], iters[j],
                               None if st is None else st[j], opts, verbose, t_launch)
   for i, (r, x_pool, y_pool, s_pool, recs, d) in where.items():
     q = problems[i]
     n0, m0 = int(d["n_off"]), int(d["m_off"])
-    out[i] = _make_solution(q, x_pool[n0:n0 + q.n].copy(), y_pool[m0:m0 + q.m].copy(),
+    x = x_pool[n0:n0 + q.n].copy()
+    if kinds[i] == "band_grid":
+      x = _unpermute(q, x)
+    out[i] = _make_solution(q, x, y_pool[m0:m0 + q.m].copy(),
                             s_pool[m0:m0 + q.m].copy(), int(r["status"]),
                             int(r["iterations"]), recs, opts, verbose, t_launch)
   return out
+
+
+def _unpermute(q, x_band):
+  """x of q from the x of its band-ordered form (band_permutation)."""
+  perm = getattr(q, "_perm", None)
+  if perm is None:
+    return x_band
+  x = np.empty_like(x_band)
+  x[perm] = x_band
+  return x
 
 
 def _raise_device_error(code: int) -> None:

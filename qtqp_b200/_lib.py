@@ -35,6 +35,7 @@ EXPORTS = (
     "qtqp_device_sm_count",
     "qtqp_host_gather",
     "qtqp_dense_batch_plan",
+    "qtqp_dense_batch_plan_tuned",
     "qtqp_dense_batch_solve",
     "qtqp_dense_batch_solve_from",
     "qtqp_dense_batch_noalloc_max_workspace",
@@ -51,6 +52,7 @@ EXPORTS = (
     "qtqp_mlp_relu_grad",
     "qtqp_mlp_colsum",
     "qtqp_mlp_mse_grad",
+    "qtqp_mlp_hinge_grad",
     "qtqp_mlp_adam",
     "qtqp_mlp_decode",
     "qtqp_dense_large_workspace_bytes",
@@ -60,6 +62,8 @@ EXPORTS = (
     "qtqp_band_grid_default_parts",
     "qtqp_band_grid_workspace_bytes",
     "qtqp_band_grid_solve",
+    "qtqp_wait_selftest_workspace_bytes",
+    "qtqp_wait_selftest",
 )
 
 
@@ -124,8 +128,14 @@ MAX_GROUPS = 8
 class LaunchGroup(ctypes.Structure):
   _fields_ = [("begin", ctypes.c_int32), ("count", ctypes.c_int32),
               ("block_threads", ctypes.c_int32), ("smem_bytes", ctypes.c_int32),
-              ("slots", ctypes.c_int32), ("reserved", ctypes.c_int32),
+              ("slots", ctypes.c_int32), ("lean", ctypes.c_int32),
               ("slot_off", ctypes.c_uint64), ("slot_bytes", ctypes.c_uint64)]
+
+
+class BatchTuning(ctypes.Structure):
+  _fields_ = [("n_lo", ctypes.c_int32), ("n_hi", ctypes.c_int32),
+              ("block_threads", ctypes.c_int32), ("lean", ctypes.c_int32),
+              ("onchip", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class BatchPlan(ctypes.Structure):
@@ -171,6 +181,8 @@ def load() -> ctypes.CDLL:
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
     lib.qtqp_dense_batch_plan.argtypes = [vp, i32, ctypes.POINTER(Options), vp, i32, i32,
                                           ctypes.POINTER(BatchPlan)]
+    lib.qtqp_dense_batch_plan_tuned.argtypes = [vp, i32, ctypes.POINTER(Options), vp, vp, i32,
+                                                ctypes.POINTER(BatchPlan)]
     lib.qtqp_dense_batch_solve.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp, vp,
                                            vp, vp, vp, vp, vp, vp, sz,
                                            ctypes.POINTER(Options), vp]
@@ -193,6 +205,7 @@ def load() -> ctypes.CDLL:
     lib.qtqp_mlp_relu_grad.argtypes = [vp, vp, i64, vp]
     lib.qtqp_mlp_colsum.argtypes = [vp, i32, i32, vp, vp]
     lib.qtqp_mlp_mse_grad.argtypes = [vp, vp, i64, vp, vp, vp]
+    lib.qtqp_mlp_hinge_grad.argtypes = [vp, vp, i32, i32, i32, vp, f32, f32, vp, vp, vp]
     lib.qtqp_mlp_adam.argtypes = [vp, vp, vp, vp, i64, f32, f32, f32, f32, i32, vp]
     lib.qtqp_mlp_decode.argtypes = [vp, vp, vp, i32, i32, i32, i32, f64, vp, vp, vp, vp]
     lib.qtqp_dense_large_workspace_bytes.restype = sz
@@ -206,6 +219,9 @@ def load() -> ctypes.CDLL:
     lib.qtqp_band_grid_solve.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz,
                                          ctypes.POINTER(Options), vp]
     lib.qtqp_tc_split_tf32.argtypes = [vp, i64, vp, vp, vp]
+    lib.qtqp_wait_selftest_workspace_bytes.restype = sz
+    lib.qtqp_wait_selftest_workspace_bytes.argtypes = []
+    lib.qtqp_wait_selftest.argtypes = [i32, i32, i32, ctypes.c_uint32, vp, vp, vp]
     lib.qtqp_tc_gram_f32.argtypes = [i32, i32, vp, vp, i32, vp, i32, i32, vp, vp]
     lib.qtqp_kkt_dense_workspace_bytes.restype = sz
     lib.qtqp_kkt_dense_workspace_bytes.argtypes = [i32, i32]

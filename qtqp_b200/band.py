@@ -37,6 +37,28 @@ def gram_bandwidth(a: sp.spmatrix, p: sp.spmatrix | None) -> int:
   return bw
 
 
+def band_ordering(a: sp.spmatrix, p: sp.spmatrix | None):
+  """A reverse Cuthill-McKee ordering of the variables for the sparsity graph
+  of P + A^T A (variables adjacent when they share a row of A or an entry of
+  P), or None when A is dense or that graph holds more than a quarter of
+  the n x n entries (no narrow ordering to find)."""
+  from scipy.sparse import csgraph  # pylint: disable=g-import-not-at-top
+  m, n = a.shape
+  if a.nnz > 0.1 * float(m) * n:  # dense A: a dense Gram, no narrow ordering
+    return None
+  ab = sp.csr_matrix(a, dtype=np.float64, copy=True)
+  ab.data[:] = 1.0
+  g = (ab.T @ ab).tocsr()
+  if g.nnz > 0.25 * float(n) * n:
+    return None
+  if p is not None and p.nnz:
+    pb = sp.csr_matrix(p, dtype=np.float64, copy=True)
+    pb.data[:] = 1.0
+    g = (g + pb).tocsr()
+  g = g + sp.eye(n, format="csr")
+  return np.asarray(csgraph.reverse_cuthill_mckee(g, symmetric_mode=True), dtype=np.int64)
+
+
 class _Structure:
   """CSR / CSC / P arrays and bandwidth of one (A, P) pair."""
 

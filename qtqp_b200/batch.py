@@ -152,7 +152,7 @@ class HostBatch:
   """
 
   def __init__(self, problems: Sequence, opts: SolveOptions, block_threads: int = 0,
-               smem_bytes: int = 0, pinned: bool = False):
+               smem_bytes: int = 0, pinned: bool = False, tuning=None):
     lib = _lib.load()
     count = len(problems)
     self.count = count
@@ -192,21 +192,44 @@ class HostBatch:
                      out=self.b_pool[:self.m_total])
       np.concatenate([np.asarray(pr.c, dtype=np.float64) for pr in problems],
                      out=self.c_pool[:self.n_total])
-    order = np.zeros(max(count, 1), dtype=np.int32)
+    self.inst, self.opts = inst, opts
+    self.order = np.zeros(max(count, 1), dtype=np.int32)
+    self.replan(tuning, block_threads, smem_bytes)
+
+  def replan(self, tuning=None, block_threads: int = 0, smem_bytes: int = 0) -> None:
+    """(Re)plans the launch groups: the library's default shapes, a forced
+    shape (block_threads / smem_bytes), or a tuning table (a list of
+    {n_lo, n_hi, block_threads, lean, onchip} entries, see autotune.py)."""
+    lib = _lib.load()
     plan = _lib.BatchPlan()
-    copts = opts.to_c()
-    _lib.check(lib.qtqp_dense_batch_plan(inst.ctypes.data, count, ctypes.byref(copts),
-                                         order.ctypes.data, block_threads, smem_bytes,
-                                         ctypes.byref(plan)))
-    self.inst, self.order, self.plan = inst, order, plan
+    copts = self.opts.to_c()
+    if tuning:
+      table = (_lib.BatchTuning * len(tuning))(*[
+          _lib.BatchTuning(int(e["n_lo"]), int(e["n_hi"]), int(e["block_threads"]),
+                           int(e.get("lean", 0)), int(e.get("onchip", 0)), 0) for e in tuning])
+      _lib.check(lib.qtqp_dense_batch_plan_tuned(self.inst.ctypes.data, self.count,
+                                                 ctypes.byref(copts), self.order.ctypes.data,
+                                                 table, len(tuning), ctypes.byref(plan)))
+    else:
+      _lib.check(lib.qtqp_dense_batch_plan(self.inst.ctypes.data, self.count,
+                                           ctypes.byref(copts), self.order.ctypes.data,
+                                           block_threads, smem_bytes, ctypes.byref(plan)))
+    self.plan = plan
     self.workspace_bytes = int(plan.workspace_bytes)
-    self.opts = opts
+    self.tuning = tuning
 
   @property
   def groups(self):
     """(begin, count, block_threads, smem_bytes) of each launch group."""
     return [(g.begin, g.count, g.block_threads, g.smem_bytes)
             for g in self.plan.groups[:self.plan.num_groups]]
+
+  def group_n_range(self, g: int) -> tuple[int, int]:
+    """Smallest and largest n of launch group g."""
+    grp = self.plan.groups[g]
+    ids = self.order[grp.begin:grp.begin + grp.count]
+    ns = self.inst["n"][ids]
+    return int(ns.min()), int(ns.max())
 
   @property
   def input_bytes(self) -> int:
@@ -246,6 +269,30 @@ class DeviceBatch:
       self.h_pools = [torch.from_numpy(x).pin_memory() for x in
                       (hb.a_pool, hb.p_pool, hb.b_pool, hb.c_pool)]
     self._h_out = None
+
+  def refresh_plan(self) -> None:
+    """Re-uploads the descriptors and order and resizes the workspace after
+    the host batch was re-planned (HostBatch.replan)."""
+    torch = self.torch
+    hb = self.hb
+    self.inst = torch.from_numpy(hb.inst.view(np.uint8)).to(self.device)
+    self.order = torch.from_numpy(hb.order).to(self.device)
+    if self.workspace.numel() < hb.workspace_bytes:
+      self.workspace = torch.empty(hb.workspace_bytes, dtype=torch.uint8, device=self.device)
+
+  def launch_group(self, g: int, stream=None) -> None:
+    """Enqueues launch group g of the plan alone (for timing one group)."""
+    hb = self.hb
+    full = hb.plan
+    one = _lib.BatchPlan()
+    ctypes.memmove(ctypes.byref(one), ctypes.byref(full), ctypes.sizeof(one))
+    one.num_groups = 1
+    one.groups[0] = full.groups[g]
+    hb.plan = one
+    try:
+      self.launch(stream)
+    finally:
+      hb.plan = full
 
   def upload(self, stream=None) -> None:
     torch = self.torch

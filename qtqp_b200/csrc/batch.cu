@@ -10,12 +10,16 @@
 
 namespace qtqp {
 
-static int launch_nt(int nt, const BatchParams& p, int smem_total, cudaStream_t st) {
+static int launch_nt(int nt, int lean, const BatchParams& p, int smem_total, cudaStream_t st) {
   switch (nt) {
-    case 32: return launch_group_32(p, smem_total, st);
-    case 64: return launch_group_64(p, smem_total, st);
-    case 128: return launch_group_128(p, smem_total, st);
-    case 256: return launch_group_256(p, smem_total, st);
+    case 32: return lean ? launch_group_32_lean(p, smem_total, st)
+                         : launch_group_32(p, smem_total, st);
+    case 64: return lean ? launch_group_64_lean(p, smem_total, st)
+                         : launch_group_64(p, smem_total, st);
+    case 128: return lean ? launch_group_128_lean(p, smem_total, st)
+                          : launch_group_128(p, smem_total, st);
+    case 256: return lean ? launch_group_256_lean(p, smem_total, st)
+                          : launch_group_256(p, smem_total, st);
     default: return fail(QTQP_ERR_BAD_ARG, "block_threads must be 32, 64, 128 or 256");
   }
 }
@@ -65,10 +69,10 @@ static int fork_streams(ForkStreams** out, std::unique_lock<std::mutex>& lk) {
 
 using namespace qtqp;
 
-extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
-                                     const qtqp_options* opt, int32_t* h_order,
-                                     int32_t block_threads, int32_t smem_bytes,
-                                     qtqp_batch_plan* plan) {
+static int dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
+                            const qtqp_options* opt, int32_t* h_order, int32_t block_threads,
+                            int32_t smem_bytes, const qtqp_batch_tuning* table,
+                            int32_t entries, qtqp_batch_plan* plan) {
   if (h_inst == nullptr || h_order == nullptr || opt == nullptr || plan == nullptr ||
       count < 0)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_plan: null argument or negative count");
@@ -128,20 +132,42 @@ extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
   size_t off = kWsHeader;
   for (size_t g = 0; g < runs.size(); ++g) {
     const Run& r = runs[g];
-    int max_N = 0;
+    int max_N = 0, max_n = 0;
     size_t max_all = 0, max_gv = 0;
     for (int k = r.begin; k < r.begin + r.count; ++k) {
       const qtqp_dense_instance& d = h_inst[ord[k]];
       max_N = std::max(max_N, d.n + d.m);
+      max_n = std::max(max_n, d.n);
       const InstLayout L = plan_layout(d.n, d.m, 0);
       max_gv = std::max(max_gv, L.g_bytes + L.v_bytes);
       max_all = std::max(max_all, L.g_bytes + L.v_bytes + L.a_bytes + L.p_bytes);
     }
     int nt = threads_for(max_N);
     if (!block_threads && r.cls == 1 && max_N > 128) nt = 256;
+    // A tuning entry (first match on the group's largest n) replaces the
+    // default launch shape unless a shape is forced.
+    const qtqp_batch_tuning* tu = nullptr;
+    for (int e = 0; e < entries && !block_threads && !smem_bytes; ++e)
+      if (table[e].n_lo <= max_n && max_n <= table[e].n_hi) {
+        tu = &table[e];
+        break;
+      }
+    int lean = 0;
+    if (tu) {
+      nt = tu->block_threads;
+      lean = tu->lean != 0;
+    }
     const size_t red = red_bytes_rt(nt);
     size_t cap;
-    if (smem_bytes) {
+    if (tu) {
+      if (tu->onchip && max_all + red <= kSmemBlockMax) {
+        cap = max_all;
+      } else if (max_gv + red <= kSmemBlockMax) {
+        cap = max_gv;
+      } else {
+        cap = 0;
+      }
+    } else if (smem_bytes) {
       if (size_t(smem_bytes) < red || size_t(smem_bytes) > kSmemBlockMax)
         return fail(QTQP_ERR_BAD_ARG, "smem_bytes outside [reduction scratch, 227 KiB]");
       cap = size_t(smem_bytes) - red;
@@ -165,10 +191,33 @@ extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
       d.ws_off = int64_t(off);
       off += (L.global_bytes + 255) & ~size_t(255);
     }
-    plan->groups[g] = qtqp_launch_group{r.begin, r.count, nt, int32_t(cap + red)};
+    plan->groups[g] = qtqp_launch_group{r.begin, r.count, nt, int32_t(cap + red), 0, lean};
   }
   plan->workspace_bytes = off;
   return QTQP_OK;
+}
+
+extern "C" int qtqp_dense_batch_plan(qtqp_dense_instance* h_inst, int32_t count,
+                                     const qtqp_options* opt, int32_t* h_order,
+                                     int32_t block_threads, int32_t smem_bytes,
+                                     qtqp_batch_plan* plan) {
+  return dense_batch_plan(h_inst, count, opt, h_order, block_threads, smem_bytes, nullptr, 0,
+                          plan);
+}
+
+extern "C" int qtqp_dense_batch_plan_tuned(qtqp_dense_instance* h_inst, int32_t count,
+                                           const qtqp_options* opt, int32_t* h_order,
+                                           const qtqp_batch_tuning* table, int32_t entries,
+                                           qtqp_batch_plan* plan) {
+  if (entries < 0 || (entries > 0 && table == nullptr))
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_plan_tuned: bad tuning table");
+  for (int e = 0; e < entries; ++e) {
+    const int nt = table[e].block_threads;
+    if (nt != 32 && nt != 64 && nt != 128 && nt != 256)
+      return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_plan_tuned: entry " + std::to_string(e) +
+                                        ": block_threads must be 32, 64, 128 or 256");
+  }
+  return dense_batch_plan(h_inst, count, opt, h_order, 0, 0, table, entries, plan);
 }
 
 static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d_order,
@@ -238,7 +287,7 @@ static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d
       rc = cuda_check(cudaStreamWaitEvent(gs, fk->fork, 0), "cudaStreamWaitEvent");
       if (rc) return rc;
     }
-    rc = launch_nt(G.block_threads, p, G.smem_bytes, gs);
+    rc = launch_nt(G.block_threads, G.lean, p, G.smem_bytes, gs);
     if (rc) return rc;
     if (fk) {
       rc = cuda_check(cudaEventRecord(fk->join[g], gs), "cudaEventRecord");
@@ -411,7 +460,7 @@ extern "C" int qtqp_dense_batch_solve_noalloc(
     p.count = G.count;
     p.counter = static_cast<int*>(ws) + g;
     p.smem_cap = size_t(G.smem_bytes) - red;
-    rc = launch_nt(G.block_threads, p, G.smem_bytes, st);
+    rc = launch_nt(G.block_threads, G.lean, p, G.smem_bytes, st);
     if (rc) return rc;
   }
   return QTQP_OK;

@@ -49,15 +49,16 @@ inline size_t red_bytes_rt(int nt) {
   }
 }
 
-// Resident blocks per SM the compiler must allow for (it caps the registers
-// per thread at 64K / (NT * min blocks)); 1 leaves the register count free.
-#ifndef QTQP_BATCH_MIN_BLOCKS
-#define QTQP_BATCH_MIN_BLOCKS(NT) 1
-#endif
-
+// Each block size is compiled twice: MINB = 1 leaves the register count free
+// (fewest spills, fewest resident blocks), the lean variant asks the
+// compiler for kLeanBlocks<NT> resident blocks per SM (registers capped at
+// 64K / (NT * MINB), more warps in flight).  The launch group's `lean` field
+// picks one; the autotuner times both.
 template <int NT>
-__global__ void __launch_bounds__(NT, QTQP_BATCH_MIN_BLOCKS(NT))
-    dense_batch_kernel(const BatchParams p) {
+constexpr int kLeanBlocks = NT >= 256 ? 2 : (NT >= 128 ? 3 : (NT >= 64 ? 6 : 12));
+
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) dense_batch_kernel(const BatchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ qtqp_options sopt;
   __shared__ int next_idx;
@@ -99,9 +100,9 @@ __global__ void __launch_bounds__(NT, QTQP_BATCH_MIN_BLOCKS(NT))
 // Cost model used for ordering: Gram SYRK + Cholesky flops.
 inline double inst_cost(int n, int m) { return double(m) * n * n + double(n) * n * n / 3.0; }
 
-template <int NT>
+template <int NT, int MINB>
 inline int launch_group(const BatchParams& p, int smem_total, cudaStream_t stream) {
-  auto kern = dense_batch_kernel<NT>;
+  auto kern = dense_batch_kernel<NT, MINB>;
   int rc = cuda_check(
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_total),
       "cudaFuncSetAttribute");
@@ -119,9 +120,15 @@ inline int launch_group(const BatchParams& p, int smem_total, cudaStream_t strea
 }
 
 
+// One per translation unit (batch_nt*.cu), so that they compile in parallel;
+// lean != 0 selects the register-capped variant.
 int launch_group_32(const BatchParams& p, int smem_total, cudaStream_t stream);
 int launch_group_64(const BatchParams& p, int smem_total, cudaStream_t stream);
 int launch_group_128(const BatchParams& p, int smem_total, cudaStream_t stream);
 int launch_group_256(const BatchParams& p, int smem_total, cudaStream_t stream);
+int launch_group_32_lean(const BatchParams& p, int smem_total, cudaStream_t stream);
+int launch_group_64_lean(const BatchParams& p, int smem_total, cudaStream_t stream);
+int launch_group_128_lean(const BatchParams& p, int smem_total, cudaStream_t stream);
+int launch_group_256_lean(const BatchParams& p, int smem_total, cudaStream_t stream);
 
 }  // namespace qtqp

@@ -1,8 +1,8 @@
-// Instantiation of the batch kernel for 128-thread blocks.
+// Instantiation of the batch kernel for 128-thread blocks (free registers).
 #include "batch_kernel.cuh"
 
 namespace qtqp {
 int launch_group_128(const BatchParams& p, int smem_total, cudaStream_t stream) {
-  return launch_group<128>(p, smem_total, stream);
+  return launch_group<128, 1>(p, smem_total, stream);
 }
 }  // namespace qtqp

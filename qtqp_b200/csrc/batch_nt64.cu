@@ -1,8 +1,8 @@
-// Instantiation of the batch kernel for 64-thread blocks.
+// Instantiation of the batch kernel for 64-thread blocks (free registers).
 #include "batch_kernel.cuh"
 
 namespace qtqp {
 int launch_group_64(const BatchParams& p, int smem_total, cudaStream_t stream) {
-  return launch_group<64>(p, smem_total, stream);
+  return launch_group<64, 1>(p, smem_total, stream);
 }
 }  // namespace qtqp

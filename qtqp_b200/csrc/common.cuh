@@ -110,7 +110,7 @@ struct GridCtl {
   double part[2][kGridMaxBlocks][kRedMax];  // per-block partials (double-buffered)
 };
 
-__device__ __forceinline__ void grid_sync(GridCtl* g) {
+__device__ __forceinline__ void grid_sync(GridCtl* g, uint32_t limit = kGridWaitLimit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile GridCtl* vg = g;
@@ -125,7 +125,7 @@ __device__ __forceinline__ void grid_sync(GridCtl* g) {
       } else {
         uint32_t it = 0;
         while (vg->gen == gen && !vg->err) {
-          if (++it > kGridWaitLimit) {
+          if (++it > limit) {
             atomicExch(&g->err, 1);
             break;
           }

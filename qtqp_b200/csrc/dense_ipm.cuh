@@ -568,7 +568,21 @@ struct Ipm {
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-    if (mine) {
+    if constexpr (sizeof(T) == 8) {
+      // FP64 Gram on the FP64 tensor cores: each warp forms 8 x 8 lower
+      // blocks of A^T diag(1/Ry) A with mma.sync m8n8k4 (DMMA) over 4-row
+      // slices of A, writes them to g, and each thread then reads its tile.
+      gram_dmma(g);
+      if (mine) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int i = i0 + a, j = j0 + b;
+            if (i < n && j <= i) acc[a][b] = g[i * ldg + j];
+          }
+      }
+    } else if (mine) {
       for (int r = 0; r < m; ++r) {
         const double w = wsc[n + r];
         const double* row = A + r * lda;
@@ -611,16 +625,56 @@ struct Ipm {
     return info;
   }
 
+  // Lower 8 x 8 blocks of the FP64 Gram A^T diag(1/Ry) A into g (entries
+  // i >= j, i, j < n), one warp per block, on the FP64 tensor cores: for each
+  // 4-row slice of A, lane l holds a = A[r + l%4][I + l/4] / Ry and
+  // b = A[r + l%4][J + l/4] (dmma_8x8x4's fragment layout), rows past m and
+  // columns past n are zero.  Ends with a barrier.
+  __device__ __forceinline__ void gram_dmma(double* g) {
+    QTQP_LOCALS;
+    const double* wsc = vec(kPW);
+    const int lane = tid & 31, warp = tid >> 5;
+    const int lr = lane & 3, lc = lane >> 2;
+    const int n8 = (n + 7) >> 3;
+    const int nblk = n8 * (n8 + 1) / 2;
+    for (int t = warp; t < nblk; t += NT / 32) {
+      int bi8 = int((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+      while (bi8 * (bi8 + 1) / 2 > t) --bi8;
+      while ((bi8 + 1) * (bi8 + 2) / 2 <= t) ++bi8;
+      const int bj8 = t - bi8 * (bi8 + 1) / 2;
+      const int ci = bi8 * 8 + lc, cj = bj8 * 8 + lc;
+      const bool ci_ok = ci < n, cj_ok = cj < n;
+      double d[2] = {0.0, 0.0};
+      for (int r = 0; r < m; r += 4) {
+        const int rr = r + lr;
+        double a = 0.0, b = 0.0;
+        if (rr < m) {
+          const double* row = A + rr * lda;
+          const double w = wsc[n + rr];
+          if (ci_ok) a = row[ci] * w;
+          if (cj_ok) b = row[cj];
+        }
+        dmma_8x8x4(d, a, b);
+      }
+      const int i = bi8 * 8 + lc, j = bj8 * 8 + 2 * lr;
+      if (i < n) {
+        if (j <= i) g[i * ldg + j] = d[0];
+        if (j + 1 <= i) g[i * ldg + j + 1] = d[1];
+      }
+    }
+    sync();
+  }
+
   // Right-looking Cholesky of the register tiles of factorize_regs in 4-column
   // panels, one barrier per panel.  Panel k's off-diagonal tiles L_{i,k} =
   // G_{i,k} L_kk^{-T} are published in the double-buffered panel buffer PB;
   // every tile right of panel k is then updated by the rank-4 product
-  // L_{i,k} L_{j,k}^T.  The 4 x 4 diagonal factor L_kk is formed by every
-  // thread from the diagonal tile, which its owner publishes in g (its own,
-  // not yet written, region of the factor) one panel ahead, before its last
-  // update; each thread applies that update itself in the owner's order, so
-  // all copies agree to the bit, and a non-positive pivot stops every thread
-  // at the same column.  The diagonal of the result keeps 1 / l_jj, and every 32 x 32
+  // L_{i,k} L_{j,k}^T.  The 4 x 4 diagonal factor L_kk is formed by each
+  // thread of panel k from the diagonal tile, which its owner publishes in g
+  // (its own, not yet written, region of the factor) one panel ahead, before
+  // its last update; each of them applies that update itself in the owner's
+  // order, so all copies agree to the bit.  A non-positive pivot is recorded
+  // in shared memory and stops every thread after the panel's barrier.  The diagonal of the result keeps 1 / l_jj, and every 32 x 32
   // diagonal block of L is inverted in place afterwards (see chol_solve).
   // Returns 0 or the 1-based index of the first non-positive pivot.
   template <typename T>
@@ -641,13 +695,6 @@ struct Ipm {
     // live in pb[t & 1] at 17 elements per tile.
     T* const pb0 = reinterpret_cast<T*>(PB);
     const int pstride = 17 * nb;
-    auto get_rows = [&](int r0, int t, T (&l)[4][4]) {
-      const T* src = pb0 + (t & 1) * pstride + (r0 >> 2) * 17;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) l[a][c] = src[a * 4 + c];
-    };
     // The factor of diagonal tile t: D (as published, one update short when
     // t > 0) minus the rows of panel t-1, then the 4 x 4 Cholesky.  ld keeps
     // 1 / l on its diagonal.  Returns 0 or the failing 1-based column.
@@ -659,15 +706,18 @@ struct Ipm {
 #pragma unroll
         for (int b = 0; b < 4; ++b)
           d[a][b] = (b <= a && r0 + a < n) ? g[(r0 + a) * ldg + r0 + b] : T(0);
-      if (t > 0) {
-        T l[4][4];
-        get_rows(r0, t - 1, l);
+      if (t > 0) {  // the owner's last update, in the owner's order
+        const T* pr = pb0 + ((t - 1) & 1) * pstride + t * 17;
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int c = 0; c < 4; ++c) {
+          T l[4];
 #pragma unroll
-          for (int b = 0; b < 4; ++b)
+          for (int a = 0; a < 4; ++a) l[a] = pr[a * 4 + c];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) d[a][b] = fma(-l[a][c], l[b][c], d[a][b]);
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) d[a][b] = fma(-l[a], l[b], d[a][b]);
+        }
       }
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
@@ -713,33 +763,56 @@ struct Ipm {
 #pragma unroll
         for (int c = 0; c < 4; ++c) dst[a * 4 + c] = acc[a][c];
     };
+    // The panel owners factor the diagonal block (identically); one that
+    // meets a non-positive pivot records it in s_info, which every thread
+    // reads after the panel's barrier.
+    __shared__ int s_info;
+    if (tid == 0) s_info = 0;
     put_diag(0);
     put_diag(1);
     sync();
     int info = 0;
-    {
+    if (mine && bj == 0) {
       T ld[4][4];
-      info = diag_factor(0, ld);
-      if (info == 0 && mine && bj == 0) finish_panel(0, ld);
+      const int f = diag_factor(0, ld);
+      if (f != 0) {
+        s_info = f;
+      } else {
+        finish_panel(0, ld);
+      }
     }
     sync();
+    info = s_info;
     for (int kb = 0; info == 0 && kb + 1 < nb; ++kb) {
-      if (mine && bj > kb) {  // rank-4 update with panel kb
-        T li[4][4], lj[4][4];
-        get_rows(i0, kb, li);
-        get_rows(j0, kb, lj);
+      if (mine && bj > kb) {  // rank-4 update with panel kb, one column at a time
+        const T* pi = pb0 + (kb & 1) * pstride + bi * 17;
+        const T* pj = pb0 + (kb & 1) * pstride + bj * 17;
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int c = 0; c < 4; ++c) {
+          T li[4], lj[4];
 #pragma unroll
-          for (int b = 0; b < 4; ++b)
+          for (int a = 0; a < 4; ++a) {
+            li[a] = pi[a * 4 + c];
+            lj[a] = pj[a * 4 + c];
+          }
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b] = fma(-li[a][c], lj[b][c], acc[a][b]);
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(-li[a], lj[b], acc[a][b]);
+        }
       }
-      T ld[4][4];
-      info = diag_factor(kb + 1, ld);
-      if (info == 0 && mine && bj == kb + 1) finish_panel(kb + 1, ld);
+      if (mine && bj == kb + 1) {
+        T ld[4][4];
+        const int f = diag_factor(kb + 1, ld);
+        if (f != 0) {
+          s_info = f;
+        } else {
+          finish_panel(kb + 1, ld);
+        }
+      }
       if (kb + 2 < nb) put_diag(kb + 2);
       sync();
+      info = s_info;
     }
     if (info == 0 && mine) {
 #pragma unroll

@@ -1,6 +1,7 @@
 // Kernels of the warm-start MLP (no reference counterpart): a tiled FP32 GEMM
 // with fused bias and ReLU, the ReLU backward mask, column sums (bias
-// gradients), the MSE gradient with its loss, Adam, and the decoder that
+// gradients), the MSE gradient with its loss, the hinge term on the sign of
+// the inequality outputs, Adam, and the decoder that
 // turns network outputs into per-instance warm starts for the banded solver.
 #include <algorithm>
 #include <cmath>
@@ -134,6 +135,47 @@ __global__ void mse_grad_kernel(const float* __restrict__ y, const float* __rest
   }
 }
 
+// Hinge on the sign of the inequality outputs, added to dy after the MSE
+// gradient: for columns [col0, cols) of a rows x cols output, with the
+// column's decision point zero[j] (the standardised value of y_i - s_i = 0)
+// and the target's side sign = +1 (t > zero) or -1,
+//   loss += weight * mean relu(margin - sign (y - zero))  (as a sum, see below),
+//   dy   += -weight * sign * [margin - sign (y - zero) > 0] / (rows (cols - col0)).
+__global__ void hinge_grad_kernel(const float* __restrict__ y, const float* __restrict__ t,
+                                  int rows, int cols, int col0, const float* __restrict__ zero,
+                                  float weight, float margin, float* __restrict__ dy,
+                                  double* loss) {
+  __shared__ double part[32];
+  const int w = cols - col0;
+  const int64_t total = int64_t(rows) * w;
+  const float inv = 1.0f / float(total);
+  double acc = 0.0;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int r = int(e / w), j = col0 + int(e % w);
+    const size_t i = size_t(r) * cols + j;
+    const float z0 = zero[j - col0];
+    const float sg = t[i] > z0 ? 1.0f : -1.0f;
+    const float h = margin - sg * (y[i] - z0);
+    if (h > 0.0f) {
+      dy[i] -= weight * sg * inv;
+      acc += double(h);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    acc = lane < int(blockDim.x >> 5) ? part[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    // *loss holds a sum over all rows x cols outputs (the MSE kernel's sum of
+    // squares); scaled so that loss / (rows cols) = mse + weight mean(h).
+    if (lane == 0)
+      atomicAdd(loss, double(weight) * acc * (double(rows) * cols / double(total)));
+  }
+}
+
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g,
                             float* __restrict__ m, float* __restrict__ v, int64_t count, float lr,
                             float b1, float b2, float eps, float c1, float c2) {
@@ -249,4 +291,16 @@ extern "C" int qtqp_mlp_decode(const float* d_pred, const double* d_scale, const
   decode_kernel<<<grid_for(size_t(count) * (n + m)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       d_pred, d_scale, d_shift, n, m, z, count, threshold, d_x, d_y, d_active);
   return cuda_check(cudaGetLastError(), "decode_kernel launch");
+}
+
+extern "C" int qtqp_mlp_hinge_grad(const float* d_y, const float* d_t, int32_t rows,
+                                   int32_t cols, int32_t col0, const float* d_zero, float weight,
+                                   float margin, float* d_dy, double* d_loss, void* stream) {
+  if (rows < 1 || cols < 1 || col0 < 0 || col0 >= cols || d_y == nullptr || d_t == nullptr ||
+      d_zero == nullptr || d_dy == nullptr || d_loss == nullptr)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_mlp_hinge_grad: bad arguments");
+  hinge_grad_kernel<<<grid_for(size_t(rows) * (cols - col0)), 256, 0,
+                      static_cast<cudaStream_t>(stream)>>>(d_y, d_t, rows, cols, col0, d_zero,
+                                                            weight, margin, d_dy, d_loss);
+  return cuda_check(cudaGetLastError(), "hinge_grad_kernel launch");
 }

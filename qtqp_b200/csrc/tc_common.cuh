@@ -36,9 +36,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 }
 // Waits until the phase with the given parity has completed.  Returns false
 // when the wait gave up (the caller records the error and stops).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t limit = kWaitLimit) {
   const uint32_t addr = smem_u32(bar);
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

@@ -70,6 +70,13 @@ def small_dense_instance(i: int, base: int = 1001):
   return sp.csc_matrix(a_d), b, c, z, sp.csc_matrix(p_d)
 
 
+def small_dense_size(i: int, base: int = 1001) -> tuple[int, int]:
+  """(n, m) of small_dense_instance(i) without building it (the same first
+  draw of the same generator)."""
+  n = int(np.random.default_rng([base, i]).integers(8, 65))
+  return n, 2 * n
+
+
 def small_dense_batch(count: int = 4096):
   return [small_dense_instance(i) for i in range(count)]
 

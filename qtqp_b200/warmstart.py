@@ -13,8 +13,8 @@ method runs, so it is both the fallback and the arbiter.
 
 Training and inference run on the GPU through the library's hand-written
 kernels (qtqp_mlp_*: tiled FP32 GEMM with fused bias/ReLU, ReLU backward,
-column sums, MSE gradient, Adam, decoding); PyTorch only allocates device
-memory.
+column sums, MSE gradient, the hinge on the sign of the inequality outputs,
+Adam, decoding); PyTorch only allocates device memory.
 """
 
 from __future__ import annotations
@@ -94,9 +94,12 @@ class WarmStartMLP:
     self._gemm(h2, w3, y, bs, self.out, self.hidden, bias=b3)
     return h1, h2, y
 
-  def gradients(self, xb, tb, batch, dy=None, dh1=None, dh2=None, loss_buf=None):
-    """Forward + backward of the MSE on one minibatch; fills self.grads and
-    loss_buf (sum of squared errors).  Returns the network output."""
+  def gradients(self, xb, tb, batch, dy=None, dh1=None, dh2=None, loss_buf=None,
+                hinge_weight: float = 0.0, hinge_margin: float = 0.5, zero=None):
+    """Forward + backward of the MSE (plus, with hinge_weight > 0, the hinge
+    on the sign of each inequality output, zero: the decision points) on one
+    minibatch; fills self.grads and loss_buf (a sum over the outputs).
+    Returns the network output."""
     torch, lib, st = self.torch, self.lib, self._st()
     f32 = dict(dtype=torch.float32, device=self.device)
     dy = dy if dy is not None else torch.empty((batch, self.out), **f32)
@@ -107,6 +110,10 @@ class WarmStartMLP:
     h1, h2, y = self._forward(xb, batch)
     _lib.check(lib.qtqp_mlp_mse_grad(y.data_ptr(), tb.data_ptr(), y.numel(), dy.data_ptr(),
                                      loss_buf.data_ptr(), st))
+    if hinge_weight > 0.0 and self.m > self.z:
+      _lib.check(lib.qtqp_mlp_hinge_grad(y.data_ptr(), tb.data_ptr(), batch, self.out,
+                                         self.n + self.z, zero.data_ptr(), hinge_weight,
+                                         hinge_margin, dy.data_ptr(), loss_buf.data_ptr(), st))
     _, _, w2, _, w3, _ = self.params
     g1, gb1, g2, gb2, g3, gb3 = self.grads
     self._gemm(h2, dy, g3, self.hidden, self.out, batch, ta=1)        # dW3 = H2^T dY
@@ -127,10 +134,21 @@ class WarmStartMLP:
     self.shift = targets.mean(axis=0)
     self.scale = np.maximum(targets.std(axis=0), 1e-6)
 
+  def zero_points(self):
+    """Standardised value of y_i - s_i = 0 for each inequality output (the
+    decision point of its sign), FP32 on the device."""
+    c0 = self.n + self.z
+    z = (0.0 - self.shift[c0:]) / self.scale[c0:]
+    return self.torch.from_numpy(z.astype(np.float32)).to(self.device)
+
   def train(self, thetas: np.ndarray, targets: np.ndarray, epochs: int = 30, batch: int = 256,
-            lr: float = 1e-3, seed: int = 0) -> TrainReport:
-    """Adam on the MSE of the standardised targets; all math on the GPU.
-    The mean loss of each epoch is read back once per epoch."""
+            lr: float = 1e-3, seed: int = 0, hinge_weight: float = 0.0,
+            hinge_margin: float = 0.5, cosine: bool = False) -> TrainReport:
+    """Adam on the MSE of the standardised targets (plus, with hinge_weight
+    > 0, a hinge that pushes each inequality output to the target's side of
+    its decision point); all math on the GPU.  cosine: the learning rate
+    decays from lr to 0 over the run (cosine schedule).  The mean loss of
+    each epoch is read back once per epoch."""
     torch = self.torch
     if self.scale is None:
       self.fit_scaling(targets)
@@ -152,17 +170,21 @@ class WarmStartMLP:
     dh1 = torch.empty_like(dh2)
     losses = []
     lib, st = self.lib, self._st()
+    zero = self.zero_points() if hinge_weight > 0.0 else None
+    total_steps, done = epochs * nbatches, 0
     for _ in range(epochs):
       epoch_loss.zero_()
       for bidx in rng.permutation(nbatches):
         s0 = int(bidx) * batch
         self.gradients(x_all[s0:s0 + batch], t_all[s0:s0 + batch], batch, dy, dh1, dh2,
-                       loss_buf)
+                       loss_buf, hinge_weight, hinge_margin, zero)
         epoch_loss += loss_buf
         self.step += 1
+        rate = lr * 0.5 * (1.0 + np.cos(np.pi * done / total_steps)) if cosine else lr
+        done += 1
         for p, g, mm, vv in zip(self.params, self.grads, self.adam_m, self.adam_v):
           _lib.check(lib.qtqp_mlp_adam(p.data_ptr(), g.data_ptr(), mm.data_ptr(), vv.data_ptr(),
-                                       p.numel(), lr, 0.9, 0.999, 1e-8, self.step, st))
+                                       p.numel(), float(rate), 0.9, 0.999, 1e-8, self.step, st))
       losses.append(float(epoch_loss.item()) / (nbatches * batch * self.out))
     return TrainReport(epochs, losses[-1] if losses else float("nan"), losses)
 
@@ -184,18 +206,27 @@ class WarmStartMLP:
                                         wy.data_ptr(), act.data_ptr(), self._st()))
     return wx, wy, act
 
-  def calibrate(self, thetas: np.ndarray, targets: np.ndarray) -> float:
-    """Picks the threshold on the predicted y_i - s_i that minimises the mean
-    number of misclassified inequality rows on (thetas, targets); the truth
-    is the sign of the target.  Sets self.threshold and self.row_error_rate
-    (misclassified rows per inequality row at that threshold)."""
+  def calibrate(self, thetas: np.ndarray, targets: np.ndarray, tight_cost: float = 2.0) -> float:
+    """Picks the threshold on the predicted y_i - s_i that minimises the
+    weighted count of misclassified inequality rows on (thetas, targets): a
+    row wrongly held tight costs tight_cost, a row wrongly left free costs 1
+    (a tight row that should be free needs more corrections of the reduced
+    KKT solve to repair, so the threshold is biased up).  The truth is the
+    sign of the target.  Sets self.threshold and self.row_error_rate (the
+    plain fraction of misclassified rows at that threshold)."""
     n, z = self.n, self.z
     truth = targets[:, n + z:] > 0.0
     v = self.predict(thetas)[:, n + z:]
     spread = float(np.quantile(np.abs(v), 0.9)) if v.size else 1.0
     cands = np.concatenate([[0.0], spread * np.linspace(-0.5, 0.5, 41)])
-    errs = [np.mean((v > t) != truth) for t in cands]
-    best = int(np.argmin(errs))
+    costs, errs = [], []
+    for t in cands:
+      pred = v > t
+      false_tight = np.mean(pred & ~truth)
+      false_free = np.mean(~pred & truth)
+      costs.append(tight_cost * false_tight + false_free)
+      errs.append(false_tight + false_free)
+    best = int(np.argmin(costs))
     self.threshold = float(cands[best])
     self.row_error_rate = float(errs[best])
     return self.threshold

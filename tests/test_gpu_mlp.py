@@ -60,6 +60,34 @@ def test_gradients_and_adam_match_oracle():
   np.testing.assert_allclose(p0.cpu().numpy(), want_p, rtol=1e-5, atol=1e-7)
 
 
+def test_hinge_gradients_match_oracle():
+  """MSE + hinge on the sign of the inequality outputs: the device loss and
+  gradients against the FP64 oracle (tests/mlp_oracle.py hinge_gradients)."""
+  import torch
+  n, m, z, dim, weight, margin = 4, 6, 2, 5, 0.7, 0.5
+  net = warmstart.WarmStartMLP(dim=dim, n=n, m=m, z=z, hidden=16, seed=4)
+  rng = np.random.default_rng(3)
+  raw = rng.normal(size=(40, n + m))
+  net.fit_scaling(raw)
+  x = rng.normal(size=(9, dim)).astype(np.float32)
+  t = ((raw[:9] - net.shift) / net.scale).astype(np.float32)
+  zero = net.zero_points()
+  xb, tb = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+  loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+  net.gradients(xb, tb, 9, loss_buf=loss, hinge_weight=weight, hinge_margin=margin, zero=zero)
+  params = [p.astype(np.float64) for p in net.params_host()]
+  cols = np.arange(n + z, n + m)
+  z64 = zero.cpu().numpy().astype(np.float64)
+  sign = np.where(t[:, cols] > z64, 1.0, -1.0)
+  want = mlp_oracle.hinge_gradients(params, x.astype(np.float64), t.astype(np.float64), cols,
+                                    z64, sign, weight, margin)
+  for g, w in zip(net.grads, want):
+    np.testing.assert_allclose(g.cpu().numpy(), w, rtol=1e-3, atol=1e-5)
+  want_loss = mlp_oracle.hinge_loss(params, x.astype(np.float64), t.astype(np.float64), cols,
+                                    z64, sign, weight, margin)
+  np.testing.assert_allclose(loss.item() / t.size, want_loss, rtol=1e-4)
+
+
 def test_decode_matches_oracle():
   net = warmstart.WarmStartMLP(dim=3, n=4, m=6, z=2, hidden=8, seed=5)
   rng = np.random.default_rng(2)

@@ -259,3 +259,54 @@ def test_solve_batch_checks_arguments_before_device_work():
   wrong = types.SimpleNamespace(n=band_q.n + 1, m=band_q.m)
   with pytest.raises(ValueError, match="model's"):
     qb.solve_batch([band_q], storage="band", warm_start=(wrong, np.zeros((1, 32))))
+
+
+def test_device_errors_map_to_the_reference_exceptions():
+  """The error codes of a device solve become the exceptions the reference
+  raises (LinAlgError for a failed Cholesky, ValueError for NaNs) and a
+  RuntimeError for a grid barrier that gave up."""
+  from qtqp_b200 import _lib
+  with pytest.raises(np.linalg.LinAlgError):
+    qb._raise_device_error(_lib.QTQP_ERR_NOT_SPD)
+  with pytest.raises(ValueError, match="NaNs"):
+    qb._raise_device_error(_lib.QTQP_ERR_NAN)
+  with pytest.raises(RuntimeError, match="timed out"):
+    qb._raise_device_error(_lib.QTQP_ERR_TIMEOUT)
+
+
+def _shuffled_mpc(horizon, seed=0):
+  a, b, c, z, p = problems.mpc_feasible(horizon)
+  perm = np.random.default_rng(seed).permutation(a.shape[1])
+  return sp.csc_matrix(a[:, perm]), b, c[perm], z, sp.csc_matrix(p[perm][:, perm])
+
+
+def test_band_ordering_of_a_shuffled_banded_qp():
+  """A stage-ordered QP with its variables shuffled is not banded as given;
+  the reverse Cuthill-McKee ordering of its Gram graph makes it narrow again,
+  so it takes the banded path in that ordering, and x maps back."""
+  from qtqp_b200 import band
+  a, b, c, z, p = _shuffled_mpc(10)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert 4 * (band.gram_bandwidth(a, p) + 1) > q.n
+  assert q.storage_format() == "band"
+  perm = q.band_permutation()
+  assert sorted(perm.tolist()) == list(range(q.n))
+  bp = q.band_problem()
+  assert 4 * (bp.bw + 1) <= q.n
+  np.testing.assert_array_equal(bp.a.toarray(), a.toarray()[:, perm])
+  np.testing.assert_array_equal(bp.c, c[perm])
+  x = np.arange(q.n, dtype=float)
+  np.testing.assert_array_equal(qb._unpermute(q, x[perm]), x)
+  # the oracle on the band-ordered QP, mapped back, is the QP's own solution
+  r_band = orc.solve(bp.a, bp.b, bp.c, bp.z, bp.p, backend="superlu")
+  r_orig = orc.solve(a, b, c, z, p, backend="superlu")
+  assert r_band.status == r_orig.status == "solved"
+  np.testing.assert_allclose(qb._unpermute(q, r_band.x), r_orig.x, atol=1e-8)
+
+
+def test_dense_and_naturally_banded_qps_keep_their_paths():
+  a, b, c, z, p = problems.sparse_qp_n200()
+  assert qb.QTQP(a=a, b=b, c=c, z=z, p=p).storage_format() == "dense"
+  a, b, c, z, p = problems.mpc_feasible(10)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert q.storage_format() == "band" and q.band_permutation() is None
