@@ -341,6 +341,20 @@ int qtqp_mlp_hinge_grad(const float* d_y, const float* d_t, int32_t rows,
                         int32_t cols, int32_t col0, const float* d_zero,
                         float weight, float margin, float* d_dy, double* d_loss,
                         void* stream);
+/* Forward-pass GEMM of the MLP on the tensor cores (tcgen05, BF16 inputs,
+ * FP32 accumulation): C = A B^T (+ bias per column) (ReLU if relu != 0), A
+ * M x K and B N x K BF16 row-major (K a multiple of 8, 16-byte aligned), C
+ * M x N FP32 (leading dimension ldc) and, when d_c16 is not NULL, its BF16
+ * copy (leading dimension ldc16) for the next layer.  *d_err (device int32)
+ * is set to 1 if a bounded pipeline wait gave up (the tile is not written). */
+int qtqp_mlp_gemm_bf16(int32_t M, int32_t N, int32_t K, const void* d_a,
+                       const void* d_bt, float* d_c, int32_t ldc,
+                       const float* d_bias, int32_t relu, void* d_c16,
+                       int32_t ldc16, int32_t* d_err, void* stream);
+/* FP32 rows x cols row-major -> BF16 (round to nearest even), transposed
+ * (cols x rows) when transpose != 0. */
+int qtqp_mlp_to_bf16(const float* d_src, int32_t rows, int32_t cols,
+                     int32_t transpose, void* d_dst, void* stream);
 /* One Adam step (bias-corrected, step >= 1). */
 int qtqp_mlp_adam(float* d_p, const float* d_g, float* d_m, float* d_v,
                   int64_t count, float lr, float beta1, float beta2, float eps,

@@ -53,6 +53,8 @@ EXPORTS = (
     "qtqp_mlp_colsum",
     "qtqp_mlp_mse_grad",
     "qtqp_mlp_hinge_grad",
+    "qtqp_mlp_gemm_bf16",
+    "qtqp_mlp_to_bf16",
     "qtqp_mlp_adam",
     "qtqp_mlp_decode",
     "qtqp_dense_large_workspace_bytes",
@@ -206,6 +208,8 @@ def load() -> ctypes.CDLL:
     lib.qtqp_mlp_colsum.argtypes = [vp, i32, i32, vp, vp]
     lib.qtqp_mlp_mse_grad.argtypes = [vp, vp, i64, vp, vp, vp]
     lib.qtqp_mlp_hinge_grad.argtypes = [vp, vp, i32, i32, i32, vp, f32, f32, vp, vp, vp]
+    lib.qtqp_mlp_gemm_bf16.argtypes = [i32, i32, i32, vp, vp, vp, i32, vp, i32, vp, i32, vp, vp]
+    lib.qtqp_mlp_to_bf16.argtypes = [vp, i32, i32, i32, vp, vp]
     lib.qtqp_mlp_adam.argtypes = [vp, vp, vp, vp, i64, f32, f32, f32, f32, i32, vp]
     lib.qtqp_mlp_decode.argtypes = [vp, vp, vp, i32, i32, i32, i32, f64, vp, vp, vp, vp]
     lib.qtqp_dense_large_workspace_bytes.restype = sz

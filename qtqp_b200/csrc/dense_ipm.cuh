@@ -49,10 +49,13 @@ enum VecId : int {
 __host__ __device__ inline int odd_ld(int n) { return (n & 1) ? n : n + 1; }
 __host__ __device__ inline size_t round16(size_t b) { return (b + 15) & ~size_t(15); }
 
-// Panel buffer of the tile Cholesky (tile_cholesky): two panels of (n+3)/4
-// tiles of 4 x 4, each tile padded to 17 elements so that lanes reading
-// different tiles hit different banks.
-__host__ __device__ inline size_t panel_buf_elems(int n) { return size_t(34) * ((n + 3) >> 2); }
+// Panel buffer (PB): the tile Cholesky's two panels of (n+3)/4 tiles of
+// 4 x 4, each tile padded to 17 elements so that lanes reading different
+// tiles hit different banks; outside the factorisation, the staged column
+// sums of fused_products (up to 8 warps x n) and a vector of n.
+__host__ __device__ inline size_t panel_buf_elems(int n) {
+  return size_t(34) * ((n + 3) >> 2) + size_t(2) * n;
+}
 
 struct InstLayout {
   int lda, ldp, ldg, np;  // leading dims (doubles) and padded vector length
@@ -1085,6 +1088,80 @@ struct Ipm {
     QTQP_TOC(kPhSolve);
   }
 
+  // One pass over A (and P) for the products a dense block needs together,
+  // for n <= 64: the column sums c_k = sum_{i<m} A_ik wy_i + sum_{i<n} P_ik
+  // wp_i (k < n; the P part only when has_p and wp is given), staged per warp
+  // in the panel buffer PB
+  // (PB[w * n + k]; the caller sums the warps' rows after a barrier), and
+  // the row products (A vx)_i, passed to row_epi(i, value) by one lane each.
+  // Each warp takes 16 rows of A at a time, lane l columns l and l + 32; the
+  // 16 row sums are reduced across the warp in 16 shuffles (each step sends
+  // half of the values to the partner lane and keeps the other half).
+  static constexpr bool kFused = FMT == kFmtDense && NT <= 1024;
+  __device__ __forceinline__ bool fused_ok() const { return kFused && n <= 64; }
+  template <typename RowEpi>
+  __device__ void fused_products(const double* vx, const double* wy, const double* wp,
+                                 RowEpi row_epi) const {
+    QTQP_LOCALS;
+    constexpr int NW = NT / 32;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int c0 = lane, c1 = lane + 32;
+    const bool ok0 = c0 < n, ok1 = c1 < n;
+    const double x0 = ok0 ? vx[c0] : 0.0, x1 = ok1 ? vx[c1] : 0.0;
+    double cs0 = 0.0, cs1 = 0.0;
+    const int rsel = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 +
+                     ((lane >> 1) & 1);  // the row of the 16 this lane ends with
+    for (int base = warp * 16; base < m; base += NW * 16) {
+      double t[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int i = base + r;
+        double a0 = 0.0, a1 = 0.0, w = 0.0;
+        if (i < m) {
+          const double* row = A + i * lda;
+          a0 = ok0 ? row[c0] : 0.0;
+          a1 = ok1 ? row[c1] : 0.0;
+          w = wy[i];
+        }
+        cs0 = fma(a0, w, cs0);
+        cs1 = fma(a1, w, cs1);
+        t[r] = fma(a0, x0, a1 * x1);
+      }
+#pragma unroll
+      for (int half = 8, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+        const bool hi = (lane & bit) != 0;
+#pragma unroll
+        for (int j = 0; j < half; ++j) {
+          const double send = hi ? t[j] : t[j + half];
+          const double keep = hi ? t[j + half] : t[j];
+          t[j] = keep + __shfl_xor_sync(0xffffffffu, send, bit);
+        }
+      }
+      t[0] += __shfl_xor_sync(0xffffffffu, t[0], 1);
+      const int i = base + rsel;
+      if ((lane & 1) == 0 && i < m) row_epi(i, t[0]);
+    }
+    if (has_p && wp != nullptr) {
+      for (int i = warp; i < n; i += NW) {
+        const double* row = P + i * ldp;
+        const double w = wp[i];
+        if (ok0) cs0 = fma(row[c0], w, cs0);
+        if (ok1) cs1 = fma(row[c1], w, cs1);
+      }
+    }
+    double* stage = PB + warp * n;
+    if (ok0) stage[c0] = cs0;
+    if (ok1) stage[c1] = cs1;
+  }
+  // Column sum k of fused_products (after a barrier).
+  __device__ __forceinline__ double fused_colsum(int k) const {
+    constexpr int NW = NT / 32;
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) t += PB[w * n + k];
+    return t;
+  }
+
   // res = krhs - K_reg v + corr o v (direct.py:256, 266 with the matvec of
   // solvers_dense.py:118-128).  Reads all of v; returns this thread's partial
   // max |res| and NaN flag of v (combined by the caller's reduction).
@@ -1095,6 +1172,27 @@ struct Ipm {
       return;
     }
     QTQP_LOCALS;
+    if (fused_ok()) {
+      const double* reg = vec(kREG);
+      const double* corr = vec(kCORR);
+      fused_products(v, v + n, v, [&](int i, double ax) {
+        const int kk = n + i;
+        const double kv = ax - (-reg[kk]) * v[kk];
+        const double rk = krhs[kk] - kv + corr[kk] * v[kk];
+        res[kk] = rk;
+        mres = nanmax(mres, fabs(rk));
+        vnan = fmax(vnan, (v[kk] != v[kk]) ? 1.0 : 0.0);
+      });
+      sync();
+      for (int k = tid; k < n; k += NT) {
+        const double kv = fused_colsum(k) + reg[k] * v[k];
+        const double rk = krhs[k] - kv + corr[k] * v[k];
+        res[k] = rk;
+        mres = nanmax(mres, fabs(rk));
+        vnan = fmax(vnan, (v[k] != v[k]) ? 1.0 : 0.0);
+      }
+      return;
+    }
     const double* reg = vec(kREG);
     const double* corr = vec(kCORR);
     const double* Ap = A;
@@ -1416,6 +1514,18 @@ struct Ipm {
     if constexpr (FMT == kFmtBand) {
       for (int k = tid; k < n; k += NT) epi_x(k, band_at_col(xy, k), band_poff_row(xy, k));
       for (int k = tid; k < m; k += NT) epi_y(k, band_a_row(xy, k));
+    } else if (fused_ok()) {
+      // A^T y and A x in one pass over A; P x as row dots.  P x goes to the
+      // panel buffer behind the warps' staged column sums.
+      double* pxs = PB + (NT / 32) * n;
+      if (hp) {
+        rowdot<1>(n, n,
+                  [&](int k, int i, double* acc) { acc[0] = fma(Pp[i * lp + k], xy[i], acc[0]); },
+                  [&](int k, double* acc) { pxs[k] = acc[0]; });
+      }
+      fused_products(xy, xy + nn, nullptr, [&](int i, double ax) { epi_y(i, ax); });
+      sync();
+      for (int k = tid; k < n; k += NT) epi_x(k, fused_colsum(k), hp ? pxs[k] : 0.0);
     } else {
       rowdot<2>(n, m + plen,
                 [&](int k, int i, double* acc) {

@@ -179,6 +179,26 @@ int make_map_f32(CUtensorMap* map, const float* ptr, int rows, int cols, int ld)
   return QTQP_OK;
 }
 
+// Row-major BF16 rows x cols (leading dimension cols) as 128 x 64 boxes
+// (128 bytes per row) with the 128-byte swizzle; columns past `cols` and rows
+// past `rows` load as zeros.
+int make_map_bf16(CUtensorMap* map, const void* ptr, int rows, int cols) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return fail(QTQP_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  const cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(cols) * 2};
+  const cuuint32_t box[2] = {64, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return fail(QTQP_ERR_CUDA, "cuTensorMapEncodeTiled (bf16) failed (code " + std::to_string(r) +
+                                   ")");
+  return QTQP_OK;
+}
+
 int launch_gram_tf32(int n, int k, const float* hi, const float* lo, int ld, float* c, int ldc,
                      int split, int* d_err, cudaStream_t st) {
   CUtensorMap mh, ml;

@@ -14,7 +14,10 @@ method runs, so it is both the fallback and the arbiter.
 Training and inference run on the GPU through the library's hand-written
 kernels (qtqp_mlp_*: tiled FP32 GEMM with fused bias/ReLU, ReLU backward,
 column sums, MSE gradient, the hinge on the sign of the inequality outputs,
-Adam, decoding); PyTorch only allocates device memory.
+Adam, decoding); PyTorch only allocates device memory.  Inference
+(predict_device) runs the three layers on the tensor cores in BF16 with FP32
+accumulation (qtqp_mlp_gemm_bf16: tcgen05, TMA-fed, fused bias / ReLU and the
+next layer's BF16 input); training keeps FP32 weights and gradients.
 """
 
 from __future__ import annotations
@@ -67,6 +70,8 @@ class WarmStartMLP:
     self.adam_m = [torch.zeros(s, dtype=torch.float32, device=dev) for s in shapes]
     self.adam_v = [torch.zeros(s, dtype=torch.float32, device=dev) for s in shapes]
     self.step = 0
+    self.bf16 = True   # inference on the tensor cores in BF16
+    self._wt16 = None  # BF16 W^T copies of the weights (refresh_bf16)
     self.scale = self.shift = None  # standardisation of the targets (FP64)
     self.threshold = 0.0
     self.row_error_rate = None
@@ -93,6 +98,55 @@ class WarmStartMLP:
     self._gemm(h1, w2, h2, bs, self.hidden, self.hidden, bias=b2, relu=1)
     self._gemm(h2, w3, y, bs, self.out, self.hidden, bias=b3)
     return h1, h2, y
+
+  def refresh_bf16(self) -> None:
+    """BF16 copies of the weights, transposed (out x in: the K-major B
+    operand of the tensor-core GEMM), taken from the FP32 weights."""
+    torch = self.torch
+    w1, _, w2, _, w3, _ = self.params
+    self._wt16 = []
+    for w in (w1, w2, w3):
+      k, n = w.shape
+      wt = torch.empty((n, k), dtype=torch.bfloat16, device=self.device)
+      _lib.check(self.lib.qtqp_mlp_to_bf16(w.data_ptr(), k, n, 1, wt.data_ptr(), self._st()))
+      self._wt16.append(wt)
+
+  def _gemm_bf16(self, a16, wt16, bias, relu, out_bf16: bool):
+    """A (rows x K, BF16) times W (W^T given, N x K) + bias (ReLU) on the
+    tensor cores: FP32 output and, when out_bf16, its BF16 copy."""
+    torch = self.torch
+    rows, k = a16.shape
+    n = wt16.shape[0]
+    c = torch.empty((rows, n), dtype=torch.float32, device=self.device)
+    c16 = torch.empty((rows, n), dtype=torch.bfloat16, device=self.device) if out_bf16 else None
+    err = torch.zeros(1, dtype=torch.int32, device=self.device)
+    _lib.check(self.lib.qtqp_mlp_gemm_bf16(rows, n, k, a16.data_ptr(), wt16.data_ptr(),
+                                           c.data_ptr(), n, bias.data_ptr(), int(relu),
+                                           None if c16 is None else c16.data_ptr(), n,
+                                           err.data_ptr(), self._st()))
+    return c, c16, err
+
+  def _forward_bf16(self, x, bs):
+    """The forward pass on the tensor cores (BF16 in, FP32 accumulate);
+    returns the FP32 output."""
+    torch = self.torch
+    if self._wt16 is None:
+      self.refresh_bf16()
+    _, b1, _, b2, _, b3 = self.params
+    k_in = ((self.dim + 7) // 8) * 8  # K of the first layer padded to 8 (16 bytes)
+    x16 = torch.zeros((bs, k_in), dtype=torch.bfloat16, device=self.device)
+    x16[:, :self.dim] = x.to(torch.bfloat16)
+    w1t = self._wt16[0]
+    if k_in != self.dim:
+      w1p = torch.zeros((w1t.shape[0], k_in), dtype=torch.bfloat16, device=self.device)
+      w1p[:, :self.dim] = w1t
+      w1t = w1p
+    _, h1, e1 = self._gemm_bf16(x16, w1t, b1, True, True)
+    _, h2, e2 = self._gemm_bf16(h1, self._wt16[1], b2, True, True)
+    y, _, e3 = self._gemm_bf16(h2, self._wt16[2], b3, False, False)
+    if int((e1 + e2 + e3).item()) != 0:
+      raise RuntimeError("qtqp_mlp_gemm_bf16: a tensor-core pipeline wait timed out")
+    return y
 
   def gradients(self, xb, tb, batch, dy=None, dh1=None, dh2=None, loss_buf=None,
                 hinge_weight: float = 0.0, hinge_margin: float = 0.5, zero=None):
@@ -186,6 +240,7 @@ class WarmStartMLP:
           _lib.check(lib.qtqp_mlp_adam(p.data_ptr(), g.data_ptr(), mm.data_ptr(), vv.data_ptr(),
                                        p.numel(), float(rate), 0.9, 0.999, 1e-8, self.step, st))
       losses.append(float(epoch_loss.item()) / (nbatches * batch * self.out))
+    self._wt16 = None  # the BF16 copies follow the new weights
     return TrainReport(epochs, losses[-1] if losses else float("nan"), losses)
 
   def predict_device(self, thetas: np.ndarray, threshold: float | None = None):
@@ -194,7 +249,7 @@ class WarmStartMLP:
     torch = self.torch
     count = thetas.shape[0]
     x = torch.from_numpy(np.ascontiguousarray(thetas, np.float32)).to(self.device)
-    _, _, pred = self._forward(x, count)
+    pred = self._forward_bf16(x, count) if self.bf16 else self._forward(x, count)[2]
     scale = torch.from_numpy(self.scale).to(self.device)
     shift = torch.from_numpy(self.shift).to(self.device)
     wx = torch.empty(count * self.n, dtype=torch.float64, device=self.device)
@@ -236,7 +291,8 @@ class WarmStartMLP:
     (count x (n + m))."""
     torch = self.torch
     x = torch.from_numpy(np.ascontiguousarray(thetas, np.float32)).to(self.device)
-    _, _, pred = self._forward(x, thetas.shape[0])
+    count = thetas.shape[0]
+    pred = self._forward_bf16(x, count) if self.bf16 else self._forward(x, count)[2]
     return pred.cpu().numpy().astype(np.float64) * self.scale + self.shift
 
   def params_host(self):
@@ -257,4 +313,5 @@ class WarmStartMLP:
       p.copy_(net.torch.from_numpy(d[f"arr_{i}"]))
     net.scale, net.shift = d["scale"], d["shift"]
     net.threshold = float(d["threshold"])
+    net._wt16 = None
     return net

@@ -88,6 +88,43 @@ def test_hinge_gradients_match_oracle():
   np.testing.assert_allclose(loss.item() / t.size, want_loss, rtol=1e-4)
 
 
+@pytest.mark.parametrize("m,n,k", [(300, 256, 32), (64, 11000, 256), (129, 130, 40)])
+def test_bf16_tensor_core_gemm(m, n, k):
+  """qtqp_mlp_gemm_bf16 (tcgen05, BF16 inputs, FP32 accumulation) against an
+  FP64 product of the same BF16-rounded operands, with bias, ReLU and the
+  BF16 copy of the output."""
+  import torch
+  lib = _lib.load()
+  rng = np.random.default_rng(m + n + k)
+  a = torch.from_numpy(rng.normal(size=(m, k)).astype(np.float32)).cuda().to(torch.bfloat16)
+  bt = torch.from_numpy(rng.normal(size=(n, k)).astype(np.float32)).cuda().to(torch.bfloat16)
+  bias = torch.from_numpy(rng.normal(size=n).astype(np.float32)).cuda()
+  c = torch.empty((m, n), dtype=torch.float32, device="cuda")
+  c16 = torch.empty((m, n), dtype=torch.bfloat16, device="cuda")
+  err = torch.zeros(1, dtype=torch.int32, device="cuda")
+  _lib.check(lib.qtqp_mlp_gemm_bf16(m, n, k, a.data_ptr(), bt.data_ptr(), c.data_ptr(), n,
+                                    bias.data_ptr(), 1, c16.data_ptr(), n, err.data_ptr(), 0))
+  torch.cuda.synchronize()
+  assert int(err.item()) == 0
+  a64 = a.float().cpu().numpy().astype(np.float64)
+  b64 = bt.float().cpu().numpy().astype(np.float64)
+  want = np.maximum(a64 @ b64.T + bias.cpu().numpy(), 0.0)
+  scale = np.sqrt(k)  # size of a K-term sum of unit products
+  np.testing.assert_allclose(c.cpu().numpy(), want, rtol=0, atol=1e-4 * scale + 1e-4)
+  np.testing.assert_allclose(c16.float().cpu().numpy(), want, rtol=1e-2, atol=1e-2)
+
+
+def test_bf16_forward_matches_fp32_forward():
+  """The MLP's inference on the tensor cores (BF16) against its FP32 forward
+  pass: the same outputs up to BF16 input rounding."""
+  import torch
+  net = warmstart.WarmStartMLP(dim=32, n=40, m=60, z=10, hidden=256, seed=2)
+  x = torch.from_numpy(np.random.default_rng(5).normal(size=(300, 32)).astype(np.float32)).cuda()
+  y32 = net._forward(x, 300)[2].cpu().numpy()
+  y16 = net._forward_bf16(x, 300).cpu().numpy()
+  assert np.max(np.abs(y16 - y32)) <= 3e-2 * max(1.0, np.max(np.abs(y32)))
+
+
 def test_decode_matches_oracle():
   net = warmstart.WarmStartMLP(dim=3, n=4, m=6, z=2, hidden=8, seed=5)
   rng = np.random.default_rng(2)
