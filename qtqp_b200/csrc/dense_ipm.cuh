@@ -635,7 +635,7 @@ struct Ipm {
   // columns past n are zero.  Ends with a barrier.
   __device__ __forceinline__ void gram_dmma(double* g) {
     QTQP_LOCALS;
-    const double* wsc = vec(kPW);
+    const double* iry = vec(kPI) + n;  // 1 / Ry
     const int lane = tid & 31, warp = tid >> 5;
     const int lr = lane & 3, lc = lane >> 2;
     const int n8 = (n + 7) >> 3;
@@ -653,8 +653,7 @@ struct Ipm {
         double a = 0.0, b = 0.0;
         if (rr < m) {
           const double* row = A + rr * lda;
-          const double w = wsc[n + rr];
-          if (ci_ok) a = row[ci] * w;
+          if (ci_ok) a = row[ci] * iry[rr];
           if (cj_ok) b = row[cj];
         }
         dmma_8x8x4(d, a, b);
