@@ -133,7 +133,7 @@ int qtqp_device_sm_count(void);
 
 /* Host-only helper (no device work, no CUDA call): copies `count` host
  * blocks, h_src[i] (an address) of h_bytes[i] bytes, to h_dst + h_dst_off[i],
- * on `threads` host threads (0: up to 8).  Packs the batch pools below from
+ * on `threads` host threads (0: up to 16).  Packs the batch pools below from
  * the thousands of per-QP arrays a batch arrives as (the reference packs
  * nothing: its solver handles one QP at a time, src/qtqp/__init__.py:183-246). */
 int qtqp_host_gather(int32_t count, const uint64_t* h_src, const int64_t* h_bytes,

@@ -54,8 +54,15 @@ inline size_t red_bytes_rt(int nt) {
 // compiler for kLeanBlocks<NT> resident blocks per SM (registers capped at
 // 64K / (NT * MINB), more warps in flight).  The launch group's `lean` field
 // picks one; the autotuner times both.
+#ifdef QTQP_PHASE_TIMERS
+// Profiling builds use relocatable device code, where a phase function is
+// compiled once for every kernel that calls it: no register-capped variant.
+template <int NT>
+constexpr int kLeanBlocks = 1;
+#else
 template <int NT>
 constexpr int kLeanBlocks = NT >= 256 ? 2 : (NT >= 128 ? 3 : (NT >= 64 ? 6 : 12));
+#endif
 
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) dense_batch_kernel(const BatchParams p) {

@@ -536,20 +536,25 @@ struct Ipm {
       return large_factorize<T>(*this);
     } else {
       const int nb = (n + 3) >> 2;
-      if (nb * (nb + 1) / 2 <= NT) return factorize_regs<T>();
+      if (nb * (nb + 1) / 2 <= 2 * NT) return factorize_regs<T>();
       return factorize_mem<T>();
     }
   }
 
-  // One thread per 4x4 tile of the lower triangle of G: the tile is formed
-  // in registers by the Gram product, and the Cholesky runs on the registers.
-  // Column k (as left by step k-1) is broadcast through a double-buffered
-  // vector in memory together with its pivot d, 1/d and sqrt(d); each step is
-  // one barrier and 16 independent FMAs per thread:
-  //   g_ij -= g_ik g_jk / d   (j > k),   l_ik = g_ik / sqrt(d),  l_kk = sqrt(d).
-  // The finished L is written to G for the solves.
+  // Register-tiled factorisation: each thread owns TPT (1 or 2) 4x4 tiles of
+  // the lower triangle of G (tile t = tid + q NT, q < TPT); the Gram product
+  // fills them (the FP64 one on the FP64 tensor cores through g, see
+  // gram_dmma; the FP32 one on the registers), then tile_cholesky factors
+  // them in place.  The finished L is written to G for the solves.
   template <typename T>
   __device__ int factorize_regs() {
+    const int nb = (n + 3) >> 2;
+    if (nb * (nb + 1) / 2 <= NT) return factorize_tiles<T, 1>();
+    return factorize_tiles<T, 2>();
+  }
+
+  template <typename T, int TPT>
+  __device__ int factorize_tiles() {
     QTQP_LOCALS;
     QTQP_TIC();
     T* g = reinterpret_cast<T*>(G);
@@ -557,73 +562,95 @@ struct Ipm {
     const double* wsc = vec(kPW);
     const int nb = (n + 3) >> 2;
     const int tiles = nb * (nb + 1) / 2;
-    const bool mine = tid < tiles;
-    int bi = 0, bj = 0;
-    if (mine) {
-      bi = int((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
-      while (bi * (bi + 1) / 2 > tid) --bi;
-      while ((bi + 1) * (bi + 2) / 2 <= tid) ++bi;
-      bj = tid - bi * (bi + 1) / 2;
+    bool mine[TPT];
+    int bi[TPT], bj[TPT];
+    T acc[TPT][4][4];
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) {
+      const int t = tid + q * NT;
+      mine[q] = t < tiles;
+      bi[q] = bj[q] = 0;
+      if (mine[q]) {
+        int b = int((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+        while (b * (b + 1) / 2 > t) --b;
+        while ((b + 1) * (b + 2) / 2 <= t) ++b;
+        bi[q] = b;
+        bj[q] = t - b * (b + 1) / 2;
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[q][a][b] = T(0);
     }
-    const int i0 = bi * 4, j0 = bj * 4;
-    T acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
     if constexpr (sizeof(T) == 8) {
       // FP64 Gram on the FP64 tensor cores: each warp forms 8 x 8 lower
       // blocks of A^T diag(1/Ry) A with mma.sync m8n8k4 (DMMA) over 4-row
-      // slices of A, writes them to g, and each thread then reads its tile.
+      // slices of A, writes them to g, and each thread then reads its tiles.
       gram_dmma(g);
-      if (mine) {
+#pragma unroll
+      for (int q = 0; q < TPT; ++q) {
+        if (!mine[q]) continue;
+        const int i0 = bi[q] * 4, j0 = bj[q] * 4;
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
             const int i = i0 + a, j = j0 + b;
-            if (i < n && j <= i) acc[a][b] = g[i * ldg + j];
+            if (i < n && j <= i) acc[q][a][b] = g[i * ldg + j];
           }
       }
-    } else if (mine) {
-      for (int r = 0; r < m; ++r) {
-        const double w = wsc[n + r];
-        const double* row = A + r * lda;
-        T ai[4], aj[4];
+    } else {
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          ai[a] = (i0 + a < n) ? T(row[i0 + a] * w) : T(0);
-          aj[a] = (j0 + a < n) ? T(row[j0 + a] * w) : T(0);
+      for (int q = 0; q < TPT; ++q) {
+        if (!mine[q]) continue;
+        const int i0 = bi[q] * 4, j0 = bj[q] * 4;
+        for (int r = 0; r < m; ++r) {
+          const double w = wsc[n + r];
+          const double* row = A + r * lda;
+          T ai[4], aj[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            ai[a] = (i0 + a < n) ? T(row[i0 + a] * w) : T(0);
+            aj[a] = (j0 + a < n) ? T(row[j0 + a] * w) : T(0);
+          }
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[q][a][b] = fma(ai[a], aj[b], acc[q][a][b]);
         }
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = fma(ai[a], aj[b], acc[a][b]);
       }
     }
     double dmax[1] = {0.0};
     double dummy[1] = {0.0};
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int q = 0; q < TPT; ++q) {
+      if (!mine[q]) continue;
+      const int i0 = bi[q] * 4, j0 = bj[q] * 4;
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int i = i0 + a, j = j0 + b;
-        if (mine && i < n && j <= i) {
-          double base = P[i * ldp + j];
-          if (i == j) base += reg[i];
-          acc[a][b] = T(base) + acc[a][b];
-          if (i == j) dmax[0] = nanmax(dmax[0], double(acc[a][b]));
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int i = i0 + a, j = j0 + b;
+          if (i < n && j <= i) {
+            double base = P[i * ldp + j];
+            if (i == j) base += reg[i];
+            acc[q][a][b] = T(base) + acc[q][a][b];
+            if (i == j) dmax[0] = nanmax(dmax[0], double(acc[q][a][b]));
+          }
         }
       }
     }
     reduce<0, 1>(dummy, dmax);
     const double jit = (sizeof(T) == 8 ? 1e-14 : 2.384185791015625e-07) * dmax[0];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-      if (mine && bi == bj && i0 + a < n) acc[a][a] = T(double(acc[a][a]) + jit);
+    for (int q = 0; q < TPT; ++q)
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (mine[q] && bi[q] == bj[q] && bi[q] * 4 + a < n)
+          acc[q][a][a] = T(double(acc[q][a][a]) + jit);
     QTQP_TOC(kPhGram);
     QTQP_RETIC();
-    const int info = tile_cholesky<T>(acc, mine, bi, bj, g);
+    const int info = tile_cholesky<T, TPT>(acc, mine, bi, bj, g);
     QTQP_TOC(kPhChol);
     return info;
   }
@@ -667,36 +694,42 @@ struct Ipm {
     sync();
   }
 
-  // Right-looking Cholesky of the register tiles of factorize_regs in 4-column
-  // panels, one barrier per panel.  Panel k's off-diagonal tiles L_{i,k} =
-  // G_{i,k} L_kk^{-T} are published in the double-buffered panel buffer PB;
-  // every tile right of panel k is then updated by the rank-4 product
-  // L_{i,k} L_{j,k}^T.  The 4 x 4 diagonal factor L_kk is formed by each
-  // thread of panel k from the diagonal tile, which its owner publishes in g
-  // (its own, not yet written, region of the factor) one panel ahead, before
-  // its last update; each of them applies that update itself in the owner's
-  // order, so all copies agree to the bit.  A non-positive pivot is recorded
-  // in shared memory and stops every thread after the panel's barrier.  The diagonal of the result keeps 1 / l_jj, and every 32 x 32
-  // diagonal block of L is inverted in place afterwards (see chol_solve).
-  // Returns 0 or the 1-based index of the first non-positive pivot.
-  template <typename T>
-  __device__ int tile_cholesky(T (&acc)[4][4], bool mine, int bi, int bj, T* g) {
+  // Right-looking Cholesky of the register tiles of factorize_tiles in
+  // 4-column panels, one barrier per panel.  Panel k's off-diagonal tiles
+  // L_{i,k} = G_{i,k} L_kk^{-T} are published in the double-buffered panel
+  // buffer PB; every tile right of panel k is then updated by the rank-4
+  // product L_{i,k} L_{j,k}^T.  The 4 x 4 diagonal factor L_kk is formed by
+  // each thread that owns a tile of panel k from the diagonal tile, which its
+  // owner publishes in g (its own, not yet written, region of the factor) one
+  // panel ahead, before its last update; each of them applies that update
+  // itself in the owner's order, so all copies agree to the bit.  A
+  // non-positive pivot is recorded in shared memory and stops every thread
+  // after the panel's barrier.  The diagonal of the result keeps 1 / l_jj,
+  // and every 32 x 32 diagonal block of L is inverted in place afterwards
+  // (see chol_solve).  Returns 0 or the 1-based index of the first
+  // non-positive pivot.
+  template <typename T, int TPT>
+  __device__ int tile_cholesky(T (&acc)[TPT][4][4], const bool (&mine)[TPT],
+                               const int (&bi)[TPT], const int (&bj)[TPT], T* g) {
     QTQP_LOCALS;
     const int nb = (n + 3) >> 2;
-    const int i0 = bi * 4, j0 = bj * 4;
-    // Lower entries of a diagonal tile into g (its own region).
-    auto put_diag = [&](int t) {
-      if (!mine || bi != t || bj != t) return;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (b <= a && i0 + a < n) g[(i0 + a) * ldg + j0 + b] = acc[a][b];
-    };
     // Panel t's tiles (L values; exactly zero in rows and columns beyond n)
     // live in pb[t & 1] at 17 elements per tile.
     T* const pb0 = reinterpret_cast<T*>(PB);
     const int pstride = 17 * nb;
+    // Lower entries of a diagonal tile into g (its own region).
+    auto put_diag = [&](int t) {
+#pragma unroll
+      for (int q = 0; q < TPT; ++q) {
+        if (!mine[q] || bi[q] != t || bj[q] != t) continue;
+        const int i0 = bi[q] * 4, j0 = bj[q] * 4;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b)
+            if (b <= a && i0 + a < n) g[(i0 + a) * ldg + j0 + b] = acc[q][a][b];
+      }
+    };
     // The factor of diagonal tile t: D (as published, one update short when
     // t > 0) minus the rows of panel t-1, then the 4 x 4 Cholesky.  ld keeps
     // 1 / l on its diagonal.  Returns 0 or the failing 1-based column.
@@ -739,56 +772,64 @@ struct Ipm {
       }
       return 0;
     };
-    // This thread's tile of panel t (already updated by panels < t) becomes
-    // L_{i,t} = tile L_tt^{-T}; the diagonal tile becomes L_tt itself.
-    auto finish_panel = [&](int t, const T (&ld)[4][4]) {
-      if (bi == t) {
+    // Tile q of panel t (already updated by panels < t) becomes
+    // L_{i,t} = tile L_tt^{-T}, published in the panel buffer; the diagonal
+    // tile becomes L_tt itself.
+    auto finish_panel = [&](int q, int t, const T (&ld)[4][4]) {
+      if (bi[q] == t) {
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int c = 0; c < 4; ++c) acc[a][c] = ld[a][c];
+          for (int c = 0; c < 4; ++c) acc[q][a][c] = ld[a][c];
         return;
       }
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          T x = acc[a][c];
+          T x = acc[q][a][c];
 #pragma unroll
-          for (int q = 0; q < c; ++q) x = fma(-acc[a][q], ld[c][q], x);
-          acc[a][c] = x * ld[c][c];  // ld[c][c] = 1 / l_cc (0 beyond n)
+          for (int e = 0; e < c; ++e) x = fma(-acc[q][a][e], ld[c][e], x);
+          acc[q][a][c] = x * ld[c][c];  // ld[c][c] = 1 / l_cc (0 beyond n)
         }
       }
-      T* dst = pb0 + (t & 1) * pstride + bi * 17;
+      T* dst = pb0 + (t & 1) * pstride + bi[q] * 17;
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) dst[a * 4 + c] = acc[a][c];
+        for (int c = 0; c < 4; ++c) dst[a * 4 + c] = acc[q][a][c];
     };
-    // The panel owners factor the diagonal block (identically); one that
-    // meets a non-positive pivot records it in s_info, which every thread
-    // reads after the panel's barrier.
+    // Panel t for the tiles of this thread that belong to it.
+    auto do_panel = [&](int t, int* s_info) {
+      bool need = false;
+#pragma unroll
+      for (int q = 0; q < TPT; ++q) need = need || (mine[q] && bj[q] == t);
+      if (!need) return;
+      T ld[4][4];
+      const int f = diag_factor(t, ld);
+      if (f != 0) {
+        *s_info = f;
+        return;
+      }
+#pragma unroll
+      for (int q = 0; q < TPT; ++q)
+        if (mine[q] && bj[q] == t) finish_panel(q, t, ld);
+    };
     __shared__ int s_info;
     if (tid == 0) s_info = 0;
     put_diag(0);
     put_diag(1);
     sync();
-    int info = 0;
-    if (mine && bj == 0) {
-      T ld[4][4];
-      const int f = diag_factor(0, ld);
-      if (f != 0) {
-        s_info = f;
-      } else {
-        finish_panel(0, ld);
-      }
-    }
+    do_panel(0, &s_info);
     sync();
-    info = s_info;
+    int info = s_info;
     for (int kb = 0; info == 0 && kb + 1 < nb; ++kb) {
-      if (mine && bj > kb) {  // rank-4 update with panel kb, one column at a time
-        const T* pi = pb0 + (kb & 1) * pstride + bi * 17;
-        const T* pj = pb0 + (kb & 1) * pstride + bj * 17;
+#pragma unroll
+      for (int q = 0; q < TPT; ++q) {
+        if (!mine[q] || bj[q] <= kb) continue;
+        // rank-4 update with panel kb, one column at a time
+        const T* pi = pb0 + (kb & 1) * pstride + bi[q] * 17;
+        const T* pj = pb0 + (kb & 1) * pstride + bj[q] * 17;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           T li[4], lj[4];
@@ -800,30 +841,27 @@ struct Ipm {
 #pragma unroll
           for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = fma(-li[a], lj[b], acc[a][b]);
+            for (int b = 0; b < 4; ++b) acc[q][a][b] = fma(-li[a], lj[b], acc[q][a][b]);
         }
       }
-      if (mine && bj == kb + 1) {
-        T ld[4][4];
-        const int f = diag_factor(kb + 1, ld);
-        if (f != 0) {
-          s_info = f;
-        } else {
-          finish_panel(kb + 1, ld);
-        }
-      }
+      do_panel(kb + 1, &s_info);
       if (kb + 2 < nb) put_diag(kb + 2);
       sync();
       info = s_info;
     }
-    if (info == 0 && mine) {
+    if (info == 0) {
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int q = 0; q < TPT; ++q) {
+        if (!mine[q]) continue;
+        const int i0 = bi[q] * 4, j0 = bj[q] * 4;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int i = i0 + a, j = j0 + b;
-          if (i < n && j <= i) g[i * ldg + j] = acc[a][b];
-        }
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int i = i0 + a, j = j0 + b;
+            if (i < n && j <= i) g[i * ldg + j] = acc[q][a][b];
+          }
+      }
     }
     sync();
     if (info == 0) invert_diag_blocks<T>(g);

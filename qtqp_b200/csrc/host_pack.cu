@@ -31,7 +31,8 @@ extern "C" int qtqp_host_gather(int32_t count, const uint64_t* h_src, const int6
         std::memcpy(dst + h_dst_off[i], reinterpret_cast<const void*>(h_src[i]),
                     size_t(h_bytes[i]));
   };
-  int nt = threads > 0 ? threads : int(std::min(8u, std::max(1u, std::thread::hardware_concurrency())));
+  int nt = threads > 0 ? threads
+                       : int(std::min(16u, std::max(1u, std::thread::hardware_concurrency())));
   if (total < (int64_t(1) << 20)) nt = 1;  // small pools: threads cost more than they save
   nt = std::min<int>(nt, count);
   if (nt <= 1) {

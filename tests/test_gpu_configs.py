@@ -9,8 +9,9 @@ SCIPY_DENSE for the large dense QP and SCIPY for the parametric family):
 * 32 held-out instances (16384..16415) of the T=50 parametric MPC family
   (n=3000, m=8000): the reference's statuses and objectives through the plain
   batched path and through the learned warm start (a network trained on the
-  plain method's solutions of instances 0..1023), whose statuses must also
-  equal the plain path's.
+  plain method's solutions of instances 0..1023; rejected predictions start
+  the plain method cold, or from the prediction with warm_shift), whose
+  statuses must also equal the plain path's.
 """
 
 import numpy as np
@@ -83,11 +84,12 @@ def test_parametric_t50_plain_and_warm_started_match_reference():
   net = warmstart.WarmStartMLP(dim=thetas.shape[1], n=q0.n, m=q0.m, z=q0.z, seed=0)
   net.train(thetas[keep], targets, epochs=30, batch=64, lr=2e-3)
   net.calibrate(thetas[keep], targets)
-  warm = qb.solve_batch(test_qps, warm_start=(net, thetas[idx]),
-                        warm_corrections=WARM_CORRECTIONS)
-  for q, s, sp_, st, fo in zip(test_qps, warm, plain, ref_status, ref_obj):
-    assert s.status == sp_.status
-    assert s.status.value == st
-    kkt_checks.assert_status_certificate(s, q.a, q.b, q.c, q.p, q.z)
-    if st == "solved":
-      assert abs(_objective(q, s.x) - fo) <= OBJ_TOL * max(1.0, abs(fo))
+  for shift in (0.0, 0.1):  # 0.1: a rejected prediction starts the IPM at the prediction
+    warm = qb.solve_batch(test_qps, warm_start=(net, thetas[idx]),
+                          warm_corrections=WARM_CORRECTIONS, warm_shift=shift)
+    for q, s, sp_, st, fo in zip(test_qps, warm, plain, ref_status, ref_obj):
+      assert s.status == sp_.status
+      assert s.status.value == st
+      kkt_checks.assert_status_certificate(s, q.a, q.b, q.c, q.p, q.z)
+      if st == "solved":
+        assert abs(_objective(q, s.x) - fo) <= OBJ_TOL * max(1.0, abs(fo))

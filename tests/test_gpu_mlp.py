@@ -127,6 +127,7 @@ def test_bf16_forward_matches_fp32_forward():
 
 def test_decode_matches_oracle():
   net = warmstart.WarmStartMLP(dim=3, n=4, m=6, z=2, hidden=8, seed=5)
+  net.bf16 = False  # decode is checked exactly against the FP32 forward pass
   rng = np.random.default_rng(2)
   thetas = rng.normal(size=(5, 3))
   targets = rng.normal(size=(5, 10))

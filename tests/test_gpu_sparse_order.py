@@ -39,7 +39,7 @@ def _check(q, sol):
 
 
 def test_reordered_batch_matches_oracle():
-  qps = [_shuffled_mpc(8, s) for s in range(4)]
+  qps = [_shuffled_mpc(12, s) for s in range(4)]  # n = 720: the reordered band fits n / 4
   assert all(q.storage_format() == "band" and q.band_permutation() is not None for q in qps)
   sols = qb.solve_batch(qps, collect_stats=True)
   for q, s in zip(qps, sols):
