@@ -192,6 +192,23 @@ int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst,
                            size_t workspace_bytes, const qtqp_options* opt,
                            void* stream);
 
+/* Launch group `group` of the plan alone, on `stream` (the same arguments as
+ * qtqp_dense_batch_solve; only that group's work counter is reset).  A caller
+ * that packs and copies the batch group by group launches each group as soon
+ * as its data is on the device, on a stream of its own, while it packs the
+ * next one; the groups' instances do not overlap, so the launches may run
+ * concurrently. */
+int qtqp_dense_batch_solve_group(const qtqp_dense_instance* d_inst,
+                                 const int32_t* d_order,
+                                 const qtqp_batch_plan* plan, int32_t group,
+                                 const double* d_a_pool, const double* d_p_pool,
+                                 const double* d_b_pool, const double* d_c_pool,
+                                 double* d_x_pool, double* d_y_pool,
+                                 double* d_s_pool, qtqp_result* d_results,
+                                 qtqp_iter_stats* d_stats, void* d_workspace,
+                                 size_t workspace_bytes, const qtqp_options* opt,
+                                 void* stream);
+
 /* qtqp_dense_batch_solve started from given points instead of the cold
  * start of _init_variables (src/qtqp/__init__.py:299-307; the reference has
  * no warm start -- its re-solve, tests/test_qtqp.py:1578-1598, starts cold

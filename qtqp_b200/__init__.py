@@ -430,15 +430,21 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     if not idx:
       continue
     if kind == "dense":
+      # Packed group by group while earlier groups already solve (below),
+      # unless starting points are given.
       hb = _batch.HostBatch([problems[i] for i in idx], opts, pinned=True,
-                            tuning=_dense_tuning(tuning))
+                            tuning=_dense_tuning(tuning), defer=initial is None)
       db = _batch.DeviceBatch(hb, records=records)
     else:
       from . import band as _band  # pylint: disable=g-import-not-at-top
       hb = _band.HostBandBatch([problems[i].band_problem() for i in idx], opts)
       db = _band.DeviceBandBatch(hb, records=records)
-    db.upload()
     t_launch = timeit.default_timer() - start
+    if kind == "dense" and initial is None:
+      db.solve_pipelined()
+      per[kind] = (idx, *db.fetch(), hb.inst)
+      continue
+    db.upload()
     if warm_start is not None:
       model, thetas = warm_start
       db.launch(warm=model.predict_device(np.asarray(thetas)))

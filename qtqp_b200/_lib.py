@@ -38,6 +38,7 @@ EXPORTS = (
     "qtqp_dense_batch_plan_tuned",
     "qtqp_dense_batch_solve",
     "qtqp_dense_batch_solve_from",
+    "qtqp_dense_batch_solve_group",
     "qtqp_dense_batch_noalloc_max_workspace",
     "qtqp_dense_batch_solve_noalloc",
     "qtqp_band_batch_plan",
@@ -191,6 +192,9 @@ def load() -> ctypes.CDLL:
     lib.qtqp_dense_batch_solve_from.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp, vp,
                                                 vp, vp, vp, vp, vp, vp, vp, sz,
                                                 ctypes.POINTER(Options), vp, vp, vp, vp]
+    lib.qtqp_dense_batch_solve_group.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), i32, vp, vp,
+                                                 vp, vp, vp, vp, vp, vp, vp, vp, sz,
+                                                 ctypes.POINTER(Options), vp]
     lib.qtqp_dense_batch_noalloc_max_workspace.restype = sz
     lib.qtqp_dense_batch_noalloc_max_workspace.argtypes = []
     lib.qtqp_dense_batch_solve_noalloc.argtypes = [vp, vp, ctypes.POINTER(BatchPlan), vp, vp,

@@ -152,8 +152,7 @@ class HostBatch:
   """
 
   def __init__(self, problems: Sequence, opts: SolveOptions, block_threads: int = 0,
-               smem_bytes: int = 0, pinned: bool = False, tuning=None):
-    lib = _lib.load()
+               smem_bytes: int = 0, pinned: bool = False, tuning=None, defer: bool = False):
     count = len(problems)
     self.count = count
     packs = [_pack_of(pr) for pr in problems]
@@ -164,12 +163,21 @@ class HostBatch:
     inst["n"], inst["m"] = ns, ms
     inst["z"] = np.fromiter((pk.z for pk in packs), np.int64, count)
     inst["has_p"] = has_p
-    a_sz, p_sz = ms * ns, np.where(has_p, ns * ns, 0)
-    inst["a_off"] = np.cumsum(a_sz) - a_sz
-    inst["p_off"] = np.cumsum(p_sz) - p_sz
     inst["n_off"] = np.cumsum(ns) - ns
     inst["m_off"] = np.cumsum(ms) - ms
     inst["st_off"] = np.arange(count, dtype=np.int64) * opts.max_iter
+    self.inst, self.opts = inst, opts
+    self.order = np.zeros(max(count, 1), dtype=np.int32)
+    self.replan(tuning, block_threads, smem_bytes)
+    # A and P are laid out in processing order, so that each launch group's
+    # data is one contiguous range of the pools (packed and copied per group
+    # by DeviceBatch.solve_pipelined).
+    pos = self.order[:count]
+    a_sz, p_sz = ms * ns, np.where(has_p, ns * ns, 0)
+    a_ord, p_ord = a_sz[pos], p_sz[pos]
+    inst["a_off"][pos] = np.cumsum(a_ord) - a_ord
+    inst["p_off"][pos] = np.cumsum(p_ord) - p_ord
+    self._a_sz, self._p_sz, self._packs = a_sz, p_sz, packs
     a_total, p_total = int(a_sz.sum()), int(p_sz.sum())
     self.n_total, self.m_total = int(ns.sum()), int(ms.sum())
     self.pinned = pinned
@@ -183,18 +191,39 @@ class HostBatch:
       self.a_pool, self.p_pool, self.b_pool, self.c_pool = (np.empty(k) for k in sizes)
     if p_total == 0:
       self.p_pool[:] = 0.0
-    _gather(lib, self.a_pool, [pk.a_ptr for pk in packs], 8 * a_sz, 8 * inst["a_off"])
-    sel = np.nonzero(has_p)[0]
-    _gather(lib, self.p_pool, [packs[i].p_ptr for i in sel], 8 * p_sz[sel],
-            8 * inst["p_off"][sel])
     if count:
       np.concatenate([np.asarray(pr.b, dtype=np.float64) for pr in problems],
                      out=self.b_pool[:self.m_total])
       np.concatenate([np.asarray(pr.c, dtype=np.float64) for pr in problems],
                      out=self.c_pool[:self.n_total])
-    self.inst, self.opts = inst, opts
-    self.order = np.zeros(max(count, 1), dtype=np.int32)
-    self.replan(tuning, block_threads, smem_bytes)
+    self.gathered = False
+    if not defer:
+      self.gather_all()
+
+  def gather_group(self, g: int):
+    """Packs the A and P values of launch group g into the pools; returns
+    their element ranges ((a_lo, a_hi), (p_lo, p_hi))."""
+    lib = _lib.load()
+    grp = self.plan.groups[g]
+    ids = self.order[grp.begin:grp.begin + grp.count]
+    inst, packs = self.inst, self._packs
+    a_sz, p_sz = self._a_sz[ids], self._p_sz[ids]
+    a_off, p_off = inst["a_off"][ids], inst["p_off"][ids]
+    _gather(lib, self.a_pool, [packs[i].a_ptr for i in ids], 8 * a_sz, 8 * a_off)
+    sel = np.nonzero(p_sz)[0]
+    _gather(lib, self.p_pool, [packs[ids[k]].p_ptr for k in sel], 8 * p_sz[sel],
+            8 * p_off[sel])
+    if not len(ids):
+      return (0, 0), (0, 0)
+    a_rng = (int(a_off[0]), int(a_off[-1] + a_sz[-1]))
+    p_rng = (int(p_off[0]), int(p_off[-1] + p_sz[-1]))
+    return a_rng, p_rng
+
+  def gather_all(self) -> None:
+    """Packs every group's A and P values."""
+    for g in range(self.plan.num_groups):
+      self.gather_group(g)
+    self.gathered = True
 
   def replan(self, tuning=None, block_threads: int = 0, smem_bytes: int = 0) -> None:
     """(Re)plans the launch groups: the library's default shapes, a forced
@@ -270,6 +299,47 @@ class DeviceBatch:
                       (hb.a_pool, hb.p_pool, hb.b_pool, hb.c_pool)]
     self._h_out = None
 
+  def solve_pipelined(self, stream=None) -> None:
+    """Packs, copies and launches the batch group by group: each launch group
+    is packed on the host (the largest instances first), copied to the
+    device and launched on a stream of its own, while the host packs the next
+    group; the outputs are complete on `stream` when the call returns (no
+    synchronisation).  The host batch must have been built with defer=True."""
+    torch = self.torch
+    lib = _lib.load()
+    hb = self.hb
+    st = stream or torch.cuda.current_stream(self.device)
+    with torch.cuda.stream(st):
+      for dst, src in ((self.b, self.h_pools[2]), (self.c, self.h_pools[3])):
+        dst.copy_(src, non_blocking=True)
+    ready = torch.cuda.Event()
+    ready.record(st)
+    streams = _side_streams(torch, self.device, hb.plan.num_groups)
+    args_tail = (self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(),
+                 self.results.data_ptr(),
+                 self.stats.data_ptr() if self.stats is not None else None,
+                 self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts))
+    done = []
+    for g in range(hb.plan.num_groups):
+      (a_lo, a_hi), (p_lo, p_hi) = hb.gather_group(g)
+      sg = streams[g]
+      sg.wait_event(ready)
+      with torch.cuda.stream(sg):
+        if a_hi > a_lo:
+          self.a[a_lo:a_hi].copy_(self.h_pools[0][a_lo:a_hi], non_blocking=True)
+        if p_hi > p_lo:
+          self.p[p_lo:p_hi].copy_(self.h_pools[1][p_lo:p_hi], non_blocking=True)
+      _lib.check(lib.qtqp_dense_batch_solve_group(
+          self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan), g,
+          self.a.data_ptr(), self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),
+          *args_tail, _lib.stream_handle(sg)))
+      ev = torch.cuda.Event()
+      ev.record(sg)
+      done.append(ev)
+    hb.gathered = True
+    for ev in done:
+      st.wait_event(ev)
+
   def refresh_plan(self) -> None:
     """Re-uploads the descriptors and order and resizes the workspace after
     the host batch was re-planned (HostBatch.replan)."""
@@ -296,6 +366,8 @@ class DeviceBatch:
 
   def upload(self, stream=None) -> None:
     torch = self.torch
+    if not self.hb.gathered:
+      self.hb.gather_all()
     with torch.cuda.stream(stream or torch.cuda.current_stream(self.device)):
       for dst, src in zip((self.a, self.p, self.b, self.c), self.h_pools):
         dst.copy_(src, non_blocking=True)
@@ -404,3 +476,15 @@ def start_points(hb: HostBatch, problems: Sequence, points: Sequence, shift: flo
     y0[m0 + z:m0 + m] = np.maximum(y[z:], 0.0) + shift
     s0[m0 + z:m0 + m] = np.maximum(sl[z:], 0.0) + shift
   return x0, y0, s0
+
+
+_SIDE_STREAMS: dict = {}
+
+
+def _side_streams(torch, device, count: int):
+  """`count` reusable side streams of `device` (created once per device)."""
+  key = str(device)
+  have = _SIDE_STREAMS.setdefault(key, [])
+  while len(have) < count:
+    have.append(torch.cuda.Stream(device=device))
+  return have[:count]

@@ -227,7 +227,7 @@ static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d
                              double* d_s_pool, qtqp_result* d_results, qtqp_iter_stats* d_stats,
                              void* d_workspace, size_t workspace_bytes, const qtqp_options* opt,
                              const double* d_x0_pool, const double* d_y0_pool,
-                             const double* d_s0_pool, void* stream) {
+                             const double* d_s0_pool, void* stream, int only = -1) {
   if (plan == nullptr || opt == nullptr)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve: null plan/options");
   if (plan->num_groups == 0) return QTQP_OK;
@@ -242,8 +242,15 @@ static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d
   if (opt->max_iter < 1 || opt->max_iterative_refinement_steps < 1 ||
       !(opt->step_size_scale > 0.0 && opt->step_size_scale < 1.0))
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve: invalid options");
+  if (only >= plan->num_groups)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_group: group index out of range");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int rc = cuda_check(cudaMemsetAsync(d_workspace, 0, kWsHeader, st), "cudaMemsetAsync");
+  // The work counters must start at zero: every group's, or the one group's
+  // (the others may belong to launches still running on other streams).
+  int rc = only < 0 ? cuda_check(cudaMemsetAsync(d_workspace, 0, kWsHeader, st), "cudaMemsetAsync")
+                    : cuda_check(cudaMemsetAsync(static_cast<int*>(d_workspace) + only, 0,
+                                                 sizeof(int), st),
+                                 "cudaMemsetAsync");
   if (rc) return rc;
   BatchParams base;
   base.inst = d_inst;
@@ -264,7 +271,7 @@ static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d
   const int ng = plan->num_groups;
   ForkStreams* fk = nullptr;
   std::unique_lock<std::mutex> fork_lock;  // held until every join is enqueued
-  if (ng > 1) {
+  if (ng > 1 && only < 0) {
     rc = fork_streams(&fk, fork_lock);
     if (rc) return rc;
     rc = cuda_check(cudaEventRecord(fk->fork, st), "cudaEventRecord");
@@ -272,7 +279,7 @@ static int dense_batch_solve(const qtqp_dense_instance* d_inst, const int32_t* d
   }
   for (int g = 0; g < ng; ++g) {
     const qtqp_launch_group& G = plan->groups[g];
-    if (G.count <= 0) continue;
+    if (G.count <= 0 || (only >= 0 && g != only)) continue;
     const size_t red = red_bytes_rt(G.block_threads);
     if (size_t(G.smem_bytes) < red)
       return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve: group smem below scratch");
@@ -310,6 +317,19 @@ extern "C" int qtqp_dense_batch_solve(const qtqp_dense_instance* d_inst, const i
   return dense_batch_solve(d_inst, d_order, plan, d_a_pool, d_p_pool, d_b_pool, d_c_pool,
                            d_x_pool, d_y_pool, d_s_pool, d_results, d_stats, d_workspace,
                            workspace_bytes, opt, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" int qtqp_dense_batch_solve_group(
+    const qtqp_dense_instance* d_inst, const int32_t* d_order, const qtqp_batch_plan* plan,
+    int32_t group, const double* d_a_pool, const double* d_p_pool, const double* d_b_pool,
+    const double* d_c_pool, double* d_x_pool, double* d_y_pool, double* d_s_pool,
+    qtqp_result* d_results, qtqp_iter_stats* d_stats, void* d_workspace,
+    size_t workspace_bytes, const qtqp_options* opt, void* stream) {
+  if (group < 0)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_batch_solve_group: negative group index");
+  return dense_batch_solve(d_inst, d_order, plan, d_a_pool, d_p_pool, d_b_pool, d_c_pool,
+                           d_x_pool, d_y_pool, d_s_pool, d_results, d_stats, d_workspace,
+                           workspace_bytes, opt, nullptr, nullptr, nullptr, stream, group);
 }
 
 extern "C" int qtqp_dense_batch_solve_from(
