@@ -404,6 +404,8 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
                        f"{len(problems)} problems")
   _lib.require_device()
   records = bool(verbose or opts.collect_stats)
+  if problems and initial is None and not records and all(k == "dense" for k in kinds):
+    return _solve_dense_streamed(problems, opts, _dense_tuning(tuning))
   per = {}  # kind -> (indices, results, x, y, s, stats, inst)
   where = {}
   t_launch = 0.0
@@ -499,6 +501,35 @@ def _unpermute(q, x_band):
   x = np.empty_like(x_band)
   x[perm] = x_band
   return x
+
+
+def _solve_dense_streamed(problems, opts, tuning) -> List[Solution]:
+  """All-dense batch without records: packed, copied and launched group by
+  group (DeviceBatch.solve_pipelined), and each group's Solutions built as
+  soon as its launch finishes, while the others still run."""
+  hb = _batch.HostBatch(problems, opts, pinned=True, tuning=tuning, defer=True)
+  db = _batch.DeviceBatch(hb, records=False)
+  db.solve_pipelined()
+  out: List[Solution | None] = [None] * len(problems)
+  errs = []
+  n_off, m_off = hb.inst["n_off"], hb.inst["m_off"]
+  for g, res, n0, x, m0, y, s in db.fetch_groups():
+    grp = hb.plan.groups[g]
+    ids = hb.order[grp.begin:grp.begin + grp.count].tolist()
+    codes = res["status"][ids].tolist()
+    bad = res["error"][ids]
+    if bad.any():
+      errs += [(ids[k], int(bad[k])) for k in np.nonzero(bad)[0]]
+    iters = res["iterations"][ids].tolist()
+    for j, i in enumerate(ids):
+      q = problems[i]
+      a = int(n_off[i]) - n0
+      b = int(m_off[i]) - m0
+      out[i] = _make_solution(q, x[a:a + q.n], y[b:b + q.m], s[b:b + q.m], codes[j], iters[j],
+                              None, opts, False, 0.0)
+  if errs:
+    _raise_device_error(min(errs)[1])
+  return out
 
 
 def _raise_device_error(code: int) -> None:

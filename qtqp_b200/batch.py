@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import time
 from typing import Sequence
 
 import numpy as np
@@ -163,20 +164,18 @@ class HostBatch:
     inst["n"], inst["m"] = ns, ms
     inst["z"] = np.fromiter((pk.z for pk in packs), np.int64, count)
     inst["has_p"] = has_p
-    inst["n_off"] = np.cumsum(ns) - ns
-    inst["m_off"] = np.cumsum(ms) - ms
     inst["st_off"] = np.arange(count, dtype=np.int64) * opts.max_iter
     self.inst, self.opts = inst, opts
     self.order = np.zeros(max(count, 1), dtype=np.int32)
     self.replan(tuning, block_threads, smem_bytes)
-    # A and P are laid out in processing order, so that each launch group's
-    # data is one contiguous range of the pools (packed and copied per group
-    # by DeviceBatch.solve_pipelined).
+    # Every pool is laid out in processing order, so that each launch group's
+    # inputs and outputs are contiguous ranges (packed, copied and read back
+    # per group by DeviceBatch.solve_pipelined / fetch_groups).
     pos = self.order[:count]
     a_sz, p_sz = ms * ns, np.where(has_p, ns * ns, 0)
-    a_ord, p_ord = a_sz[pos], p_sz[pos]
-    inst["a_off"][pos] = np.cumsum(a_ord) - a_ord
-    inst["p_off"][pos] = np.cumsum(p_ord) - p_ord
+    for key, sz in (("a_off", a_sz), ("p_off", p_sz), ("n_off", ns), ("m_off", ms)):
+      srt = sz[pos]
+      inst[key][pos] = np.cumsum(srt) - srt
     self._a_sz, self._p_sz, self._packs = a_sz, p_sz, packs
     a_total, p_total = int(a_sz.sum()), int(p_sz.sum())
     self.n_total, self.m_total = int(ns.sum()), int(ms.sum())
@@ -192,9 +191,9 @@ class HostBatch:
     if p_total == 0:
       self.p_pool[:] = 0.0
     if count:
-      np.concatenate([np.asarray(pr.b, dtype=np.float64) for pr in problems],
+      np.concatenate([np.asarray(problems[i].b, dtype=np.float64) for i in pos],
                      out=self.b_pool[:self.m_total])
-      np.concatenate([np.asarray(pr.c, dtype=np.float64) for pr in problems],
+      np.concatenate([np.asarray(problems[i].c, dtype=np.float64) for i in pos],
                      out=self.c_pool[:self.n_total])
     self.gathered = False
     if not defer:
@@ -320,6 +319,7 @@ class DeviceBatch:
                  self.stats.data_ptr() if self.stats is not None else None,
                  self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts))
     done = []
+    self._group_done = done
     for g in range(hb.plan.num_groups):
       (a_lo, a_hi), (p_lo, p_hi) = hb.gather_group(g)
       sg = streams[g]
@@ -339,6 +339,41 @@ class DeviceBatch:
     hb.gathered = True
     for ev in done:
       st.wait_event(ev)
+
+  def fetch_groups(self):
+    """After solve_pipelined: yields (g, results, x, y, s) for each launch
+    group as soon as its launch has finished (polling, the other groups may
+    still run): the full results array (only group g's entries are final)
+    and group g's contiguous output ranges, as numpy arrays owned by the
+    caller."""
+    torch = self.torch
+    hb = self.hb
+    copy_stream = _side_streams(torch, self.device, QTQP_COPY_STREAM + 1)[QTQP_COPY_STREAM]
+    pending = list(range(hb.plan.num_groups))
+    while pending:
+      ready = [g for g in pending if self._group_done[g].query()]
+      if not ready:
+        time.sleep(2e-5)
+        continue
+      for g in ready:
+        pending.remove(g)
+        grp = hb.plan.groups[g]
+        ids = hb.order[grp.begin:grp.begin + grp.count]
+        if not len(ids):
+          continue
+        n0 = int(hb.inst["n_off"][ids[0]])
+        n1 = int(hb.inst["n_off"][ids[-1]] + hb.inst["n"][ids[-1]])
+        m0 = int(hb.inst["m_off"][ids[0]])
+        m1 = int(hb.inst["m_off"][ids[-1]] + hb.inst["m"][ids[-1]])
+        copy_stream.wait_event(self._group_done[g])
+        with torch.cuda.stream(copy_stream):
+          res = self.results.to("cpu", non_blocking=True)
+          x = self.x[n0:n1].to("cpu", non_blocking=True)
+          y = self.y[m0:m1].to("cpu", non_blocking=True)
+          sl = self.s[m0:m1].to("cpu", non_blocking=True)
+        copy_stream.synchronize()
+        yield (g, res.numpy().view(_lib.RESULT_DTYPE)[:hb.count], n0, x.numpy(), m0,
+               y.numpy(), sl.numpy())
 
   def refresh_plan(self) -> None:
     """Re-uploads the descriptors and order and resizes the workspace after
@@ -479,6 +514,7 @@ def start_points(hb: HostBatch, problems: Sequence, points: Sequence, shift: flo
 
 
 _SIDE_STREAMS: dict = {}
+QTQP_COPY_STREAM = 8  # the side stream after the 8 launch groups' ones: read-backs
 
 
 def _side_streams(torch, device, count: int):
