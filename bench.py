@@ -38,10 +38,10 @@ CPU_SAMPLE = 1024          # instances in the CPU-baseline sample
 REF_SAMPLE = 1024          # instances per step of the reference arm
 HBM_FALLBACK_GBS = 6650.0  # only if MEASURED_PEAKS.json is absent
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), nominal; for context only
-# DRAM bytes (read + write) of one batch solve of this workload (all its group
-# launches), per precision form, from one ncu capture of
+# DRAM bytes (read + write) of one batch solve of this workload (all 8 group
+# launches, the autotuned FP64 plan), from one ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum; None where no capture exists.
-NCU_TRAFFIC_BYTES = {"fp64": None, "mixed": 171.6e6}
+NCU_TRAFFIC_BYTES = {"fp64": 414.5e6, "mixed": None}
 
 
 def _args():
@@ -399,7 +399,8 @@ def run_ours(args) -> None:
       "frac": achieved / peak, "peak_source": peak_kind,
       "traffic": NCU_TRAFFIC_BYTES.get(args.precision),
       "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum over one batch "
-                         f"solve, {args.precision} form") if NCU_TRAFFIC_BYTES.get(
+                         f"solve (8 launches), {args.precision} form, autotuned plan"
+                         ) if NCU_TRAFFIC_BYTES.get(
                              args.precision) else "no capture of this form",
       "kernel": "dense_batch_kernel",
       "algorithmic_bytes_per_launch": alg_bytes,

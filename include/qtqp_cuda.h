@@ -393,14 +393,17 @@ int qtqp_mlp_decode(const float* d_pred, const double* d_scale,
  * (grid barriers and reductions), with a blocked Gram + Cholesky factor
  * (Gram on tcgen05 tensor cores, TF32 hi + lo split, when opt->precision is
  * QTQP_PREC_MIXED; FP64 otherwise) and blocked triangular solves.
- * A: m x n row-major FP64, P: n x n row-major FP64 (null if has_p == 0);
- * b, c inputs; x, y, s, *d_result outputs (as the batch); d_stats:
+ * flags: QTQP_LARGE_HAS_P (P is given) | QTQP_LARGE_COLMAJOR (A and P are
+ * column-major -- the value order of a dense CSC matrix -- else row-major).
+ * A: m x n FP64, P: n x n FP64 (null without QTQP_LARGE_HAS_P); b, c inputs; x, y, s, *d_result outputs (as the batch); d_stats:
  * qtqp_iter_stats[max_iter] or NULL.  The workspace (>=
  * qtqp_dense_large_workspace_bytes(n, m), 1024-byte aligned) is private.
  * m * n < 2^31.  A grid barrier that waits too long ends the solve with
  * status FAILED and error QTQP_ERR_TIMEOUT. */
 size_t qtqp_dense_large_workspace_bytes(int32_t n, int32_t m);
-int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t has_p,
+#define QTQP_LARGE_HAS_P 1
+#define QTQP_LARGE_COLMAJOR 2
+int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t flags,
                            const double* d_a, const double* d_p,
                            const double* d_b, const double* d_c, double* d_x,
                            double* d_y, double* d_s, qtqp_result* d_result,

@@ -120,6 +120,24 @@ class _PresolveState:
   b_dropped: np.ndarray
 
 
+def _max_asymmetry(p: sp.csc_matrix) -> float:
+  """max |P - P^T| (__init__.py:240-245 computes it as a sparse difference).
+  A CSC matrix that stores all n x n entries in canonical order holds P^T
+  row-major in its data array, compared with its transpose in row blocks;
+  anything else takes the sparse difference."""
+  n = p.shape[0]
+  if p.nnz == n * n and p.has_canonical_format:
+    d = p.data.reshape(n, n)  # d[j, i] = P[i, j]
+    worst, bs = 0.0, 256  # square blocks: both sides stay in cache
+    for r0 in range(0, n, bs):
+      for c0 in range(r0, n, bs):
+        blk = d[r0:r0 + bs, c0:c0 + bs] - d[c0:c0 + bs, r0:r0 + bs].T
+        worst = max(worst, float(np.max(np.abs(blk), initial=0.0)))
+    return worst
+  asym = p - p.T
+  return float(np.max(np.abs(asym.data), initial=0.0)) if asym.nnz else 0.0
+
+
 class QTQP:
   """Primal-dual interior point method for QPs (src/qtqp/__init__.py:168-307).
 
@@ -154,8 +172,7 @@ class QTQP:
         raise ValueError(f"p must have shape ({self.n}, {self.n}), got {p.shape}")
       if not np.all(np.isfinite(p.data)):
         raise ValueError("QP matrix 'p' must contain only finite values.")
-      asym = p - p.T
-      if asym.nnz and np.max(np.abs(asym.data), initial=0.0) > 1e-12:
+      if _max_asymmetry(p) > 1e-12:
         raise ValueError("QP matrix 'p' must be symmetric.")
       self.p = p
 
@@ -241,6 +258,8 @@ class QTQP:
       return "dense"
     from . import band as _band  # pylint: disable=g-import-not-at-top
     p = self.p if self.p.nnz else None
+    if _band.wide_by_counts(self.a, p, self.n):  # no ordering makes it narrow
+      return "large" if self.n >= (LARGE_N_SINGLE if single else LARGE_N) else "dense"
     bw = _band.gram_bandwidth(self.a, p)
     if 4 * (bw + 1) > self.n and self.band_permutation() is not None:
       a_p, p_p = self._permuted
@@ -411,7 +430,7 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   t_launch = 0.0
   for i in [i for i, k in enumerate(kinds) if k == "large"]:
     from . import large as _large  # pylint: disable=g-import-not-at-top
-    dl = _large.DeviceLarge(problems[i].dense_problem(), opts, records=records)
+    dl = _large.DeviceLarge(problems[i], opts, records=records)
     dl.upload()
     t_launch = timeit.default_timer() - start
     dl.launch()

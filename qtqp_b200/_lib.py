@@ -25,6 +25,9 @@ QTQP_ERR_NAN = -5
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+# qtqp_dense_large_solve flags.
+LARGE_HAS_P = 1
+LARGE_COLMAJOR = 2
 
 STATS_DOUBLES = 64
 

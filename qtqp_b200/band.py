@@ -19,22 +19,39 @@ from .batch import SolveOptions
 
 
 def gram_bandwidth(a: sp.spmatrix, p: sp.spmatrix | None) -> int:
-  """Half-bandwidth of P + A^T D A for any positive diagonal D."""
+  """Half-bandwidth of P + A^T D A for any positive diagonal D: the widest
+  column span of a row of A, or of P's entries from the diagonal."""
   a = sp.csr_matrix(a)
   bw = 0
   if a.nnz:
-    rows = np.repeat(np.arange(a.shape[0]), np.diff(a.indptr))
-    lo = np.full(a.shape[0], np.iinfo(np.int64).max)
-    hi = np.full(a.shape[0], -1)
-    np.minimum.at(lo, rows, a.indices)
-    np.maximum.at(hi, rows, a.indices)
-    ok = hi >= 0
-    if np.any(ok):
-      bw = int(np.max(hi[ok] - lo[ok]))
+    if not a.has_sorted_indices:
+      a = a.sorted_indices()
+    cnt = np.diff(a.indptr)
+    rows = np.flatnonzero(cnt)
+    lo = a.indices[a.indptr[rows]]
+    hi = a.indices[a.indptr[rows + 1] - 1]
+    bw = int(np.max(hi - lo))
   if p is not None and p.nnz:
     pc = sp.coo_matrix(p)
     bw = max(bw, int(np.max(np.abs(pc.row - pc.col))))
   return bw
+
+
+def wide_by_counts(a: sp.spmatrix, p: sp.spmatrix | None, n: int) -> bool:
+  """True when the Gram matrix has half-bandwidth above n/4 - 1 in every
+  ordering of the variables, read from entry counts alone: a row of A with k
+  entries spans at least k columns, and a column of P with k entries reaches
+  at least (k - 1) / 2 from the diagonal."""
+  if a.nnz:
+    rows = np.bincount(a.indices, minlength=a.shape[0]) if a.format == "csc" else \
+        np.diff(sp.csr_matrix(a).indptr)
+    if 4 * int(rows.max()) > n:
+      return True
+  if p is not None and p.nnz:
+    cols = np.diff(sp.csc_matrix(p).indptr)
+    if 2 * (int(cols.max()) + 1) > n:
+      return True
+  return False
 
 
 def band_ordering(a: sp.spmatrix, p: sp.spmatrix | None):

@@ -11,7 +11,7 @@ namespace qtqp {
 int make_map_f32(CUtensorMap* map, const float* ptr, int rows, int cols, int ld);  // tc_gram.cu
 
 struct LargeParams {
-  int n, m, z, has_p;
+  int n, m, z, flags;
   const double* a;  // m x n row-major
   const double* p;  // n x n row-major (or null)
   const double* b;
@@ -56,7 +56,8 @@ __global__ void __launch_bounds__(kGridBT, 1)
   s.m = p.m;
   s.N = p.n + p.m;
   s.z = p.z;
-  s.has_p = p.has_p != 0;
+  s.has_p = (p.flags & QTQP_LARGE_HAS_P) != 0;
+  s.colmajor = (p.flags & QTQP_LARGE_COLMAJOR) != 0;
   s.A0 = p.a;
   s.P0 = p.p;
   s.b0 = p.b;
@@ -111,7 +112,7 @@ extern "C" size_t qtqp_dense_large_workspace_bytes(int32_t n, int32_t m) {
   return plan_large_layout(n, m).total;
 }
 
-extern "C" int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t has_p,
+extern "C" int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t flags,
                                       const double* d_a, const double* d_p, const double* d_b,
                                       const double* d_c, double* d_x, double* d_y, double* d_s,
                                       qtqp_result* d_result, qtqp_iter_stats* d_stats,
@@ -119,6 +120,9 @@ extern "C" int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t h
                                       const qtqp_options* opt, void* stream) {
   if (n < 1 || m < 1 || z < 0 || z >= m)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_large_solve: needs n, m >= 1 and 0 <= z < m");
+  if (flags & ~(QTQP_LARGE_HAS_P | QTQP_LARGE_COLMAJOR))
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_large_solve: unknown flags");
+  const bool has_p = (flags & QTQP_LARGE_HAS_P) != 0;
   if (n > kLB * kLargeBlocks)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_dense_large_solve: n must be at most " +
                                       std::to_string(kLB * kLargeBlocks));
@@ -169,7 +173,7 @@ extern "C" int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t h
   p.n = n;
   p.m = m;
   p.z = z;
-  p.has_p = has_p;
+  p.flags = flags;
   p.a = d_a;
   p.p = has_p ? d_p : nullptr;
   p.b = d_b;

@@ -15,29 +15,35 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .batch import DenseProblem, SolveOptions
+from . import batch as _batch
+from .batch import SolveOptions
 
 
 class DeviceLarge:
-  """Device buffers of one large dense QP and its workspace (torch tensors)."""
+  """Device buffers of one large dense QP and its workspace (torch tensors).
 
-  def __init__(self, prob: DenseProblem, opts: SolveOptions, device=None,
-               records: bool | None = None):
+  prob is a QTQP (its CSC matrices are read column by column: a CSC matrix
+  holding every entry is used in place, anything else is expanded column-major
+  once) or a DenseProblem.  A and P travel to the device column-major and the
+  solve reads them so; no host transpose."""
+
+  def __init__(self, prob, opts: SolveOptions, device=None, records: bool | None = None):
     torch = _lib.require_device()
     self.torch, self.prob, self.opts = torch, prob, opts
     dev = torch.device(device or "cuda")
     self.device = dev
-    m, n = prob.a.shape
-    self.n, self.m, self.z = n, m, int(prob.z)
-    self.has_p = prob.p is not None and bool(np.any(prob.p))
+    pk = _batch._pack_of(prob)  # pylint: disable=protected-access
+    n, m = pk.n, pk.m
+    self.n, self.m, self.z = n, m, int(pk.z)
+    self.has_p = pk.p_vals is not None
+    self.flags = _lib.LARGE_COLMAJOR | (_lib.LARGE_HAS_P if self.has_p else 0)
     f64 = dict(dtype=torch.float64, device=dev)
-    self.h_a = torch.from_numpy(np.ascontiguousarray(prob.a, dtype=np.float64)).pin_memory()
-    self.h_p = (torch.from_numpy(np.ascontiguousarray(prob.p, dtype=np.float64)).pin_memory()
-                if self.has_p else None)
+    self.h_a = torch.from_numpy(pk.a_vals).pin_memory()
+    self.h_p = torch.from_numpy(pk.p_vals).pin_memory() if self.has_p else None
     self.h_b = torch.from_numpy(np.ascontiguousarray(prob.b, dtype=np.float64)).pin_memory()
     self.h_c = torch.from_numpy(np.ascontiguousarray(prob.c, dtype=np.float64)).pin_memory()
-    self.a = torch.empty((m, n), **f64)
-    self.p = torch.empty((n, n), **f64) if self.has_p else None
+    self.a = torch.empty(m * n, **f64)
+    self.p = torch.empty(n * n, **f64) if self.has_p else None
     self.b = torch.empty(m, **f64)
     self.c = torch.empty(n, **f64)
     self.x = torch.empty(n, **f64)
@@ -72,7 +78,7 @@ class DeviceLarge:
     st = stream or torch.cuda.current_stream(self.device)
     lib = _lib.load()
     _lib.check(lib.qtqp_dense_large_solve(
-        self.n, self.m, self.z, int(self.has_p), self.a.data_ptr(),
+        self.n, self.m, self.z, self.flags, self.a.data_ptr(),
         self.p.data_ptr() if self.p is not None else None, self.b.data_ptr(),
         self.c.data_ptr(), self.x.data_ptr(), self.y.data_ptr(), self.s.data_ptr(),
         self.result.data_ptr(), self.stats.data_ptr() if self.stats is not None else None,

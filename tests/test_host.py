@@ -310,3 +310,52 @@ def test_dense_and_naturally_banded_qps_keep_their_paths():
   a, b, c, z, p = problems.mpc_feasible(10)
   q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
   assert q.storage_format() == "band" and q.band_permutation() is None
+
+
+def test_symmetry_check_of_full_csc_matches_the_sparse_difference():
+  """The blocked check of a CSC matrix storing all n x n entries gives the
+  reference's max |P - P^T| (__init__.py:240-245), including the rejection."""
+  from qtqp_b200 import _max_asymmetry
+  rng = np.random.default_rng(4)
+  for n in (1, 2, 3, 7, 255, 256, 257, 600):
+    m = rng.normal(size=(n, n))
+    s = m + m.T
+    bad = s.copy()
+    bad[rng.integers(n), rng.integers(n)] += 1e-6
+    for x in (s, bad):
+      xc = sp.csc_matrix(x)
+      assert xc.nnz == n * n
+      d = xc - xc.T
+      ref = float(np.max(np.abs(d.data), initial=0.0)) if d.nnz else 0.0
+      assert _max_asymmetry(xc) == pytest.approx(ref, abs=1e-15)
+  a = sp.csc_matrix(rng.normal(size=(6, 4)))
+  p = np.eye(4)
+  p[0, 3] = 1e-9
+  with pytest.raises(ValueError, match="symmetric"):
+    qb.QTQP(a=a, b=np.ones(6), c=np.zeros(4), z=1, p=sp.csc_matrix(p))
+
+
+def test_storage_of_dense_qps_is_decided_from_entry_counts():
+  """A row of A with more than n/4 entries (or a column of P with more than
+  n/2 - 1) rules out every banded ordering; the routing then skips the
+  bandwidth and ordering passes."""
+  from qtqp_b200 import band
+  a, b, c, z, p = problems.large_dense(n=256, m=512, z=64, rank=8)
+  assert band.wide_by_counts(sp.csc_matrix(a), sp.csc_matrix(p), 256)
+  q = qb.QTQP(a=sp.csc_matrix(a), b=b, c=c, z=z, p=sp.csc_matrix(p))
+  assert q.storage_format(single=True) == ("large" if 256 >= qb.LARGE_N_SINGLE else "dense")
+  a, b, c, z, p = problems.mpc_feasible(10)
+  assert not band.wide_by_counts(a, p, a.shape[1])
+  wide_p = sp.csc_matrix(np.ones((8, 8)))
+  assert band.wide_by_counts(sp.csc_matrix((3, 8)), wide_p, 8)
+  # Counts never exceed what the bandwidth itself implies.
+  rng = np.random.default_rng(2)
+  for _ in range(20):
+    n = int(rng.integers(4, 40))
+    a = sp.random(int(rng.integers(1, 60)), n, density=float(rng.uniform(0.02, 0.5)),
+                  format="csc", random_state=rng)
+    dense = a.toarray() != 0
+    spans = [np.flatnonzero(r).max() - np.flatnonzero(r).min() for r in dense if r.any()]
+    assert band.gram_bandwidth(a, None) == (max(spans) if spans else 0)
+    if band.wide_by_counts(a, None, n):
+      assert 4 * (band.gram_bandwidth(a, None) + 1) > n
