@@ -329,6 +329,66 @@ int qtqp_band_grid_solve(const qtqp_band_instance* h_inst, int32_t parts,
                          void* d_workspace, size_t workspace_bytes,
                          const qtqp_options* opt, void* stream);
 
+/* ---- one sparse QP on the whole GPU: supernodal Cholesky ----------------- *
+ * For QPs whose Gram matrix P + A^T D A is neither small and dense nor
+ * narrow-banded: the role of the sparse direct backends behind the plugin
+ * interface (src/qtqp/solvers_sparse.py:96-121 SuperLU,
+ * src/qtqp/solvers_gpu.py:27-116 cuDSS), on the dense backend's Gram
+ * reduction (src/qtqp/solvers_dense.py:99-116).
+ *
+ * Host symbolic stage: qtqp_sparse_analyze orders G's pattern (the union of
+ * P's pattern and one clique per row of A; ordering 1 = minimum degree on the
+ * quotient graph with approximate degrees, 0 = the given order), composes the
+ * ordering with a postorder of the elimination tree, finds supernodes (at
+ * most 64 columns wide), their row structures and left-looking update lists,
+ * maps whole subtrees to the `blocks` blocks of the grid solve
+ * (qtqp_sparse_grid_blocks()) and the supernodes above them to levels, and
+ * maps G's lower entries to positions in the factor.  A and P are CSC
+ * (int32 column pointers and row indices; P may be NULL).  The plan stays on
+ * the host until qtqp_sparse_free; qtqp_sparse_export writes the column order
+ * (perm[new] = old, n entries) and the plan's two pools (desc.n32 int32 and
+ * desc.n64 int64 elements; the offsets in desc), which the caller copies to
+ * the device unchanged. */
+typedef struct qtqp_sparse_desc {
+  int32_t n, nsuper, blocks, top_levels;
+  int32_t max_rows, max_width, tree_levels, reserved;
+  int64_t nvals;    /* factor values (column-major blocks of the supernodes) */
+  int64_t ngram;    /* lower entries of G, diagonal included */
+  int64_t nrows, nupd, nranges, ntop;
+  int64_t nnz_l;    /* stored lower entries of L */
+  double flops;     /* multiply-adds x 2 of one numeric factorisation */
+  int64_t o_first, o_colsn, o_rows, o_upd_ptr, o_upd_src, o_upd_off, o_upd_cnt,
+      o_cta_ptr, o_cta_range, o_top_ptr, o_top_list, o_gcol, o_grow; /* int32 pool */
+  int64_t o_rowptr, o_valptr, o_gpos;                             /* int64 pool */
+  int64_t n32, n64;
+} qtqp_sparse_desc;
+int qtqp_sparse_analyze(int32_t n, int32_t m, const int32_t* h_a_colptr,
+                        const int32_t* h_a_rowind, const int32_t* h_p_colptr,
+                        const int32_t* h_p_rowind, int32_t ordering, int32_t blocks,
+                        void** h_plan, qtqp_sparse_desc* h_desc);
+int qtqp_sparse_export(const void* h_plan, const qtqp_sparse_desc* h_desc,
+                       int32_t* h_perm, int32_t* h_pool32, int64_t* h_pool64);
+void qtqp_sparse_free(void* h_plan);
+/* Grid solve: the banded backend's device IPM (same algorithm, options and
+ * outputs as qtqp_band_grid_solve) with the supernodal factor.  h_inst
+ * describes the QP in the pools exactly as for the banded backend, with its
+ * columns in the plan's order (bw is ignored); d_sn32 / d_sn64 are the
+ * exported pools on the device (16-byte aligned).  FP64 and mixed precision;
+ * no learned warm start.  Every wait is bounded (status FAILED, error
+ * QTQP_ERR_TIMEOUT). */
+int32_t qtqp_sparse_grid_blocks(void);
+size_t qtqp_sparse_grid_workspace_bytes(const qtqp_band_instance* h_inst,
+                                        const qtqp_sparse_desc* h_desc);
+int qtqp_sparse_grid_solve(const qtqp_band_instance* h_inst,
+                           const qtqp_sparse_desc* h_desc, const int32_t* d_sn32,
+                           const int64_t* d_sn64, const int32_t* d_ipool,
+                           const double* d_vpool, const double* d_b_pool,
+                           const double* d_c_pool, double* d_x_pool, double* d_y_pool,
+                           double* d_s_pool, qtqp_result* d_result,
+                           qtqp_iter_stats* d_stats, void* d_workspace,
+                           size_t workspace_bytes, const qtqp_options* opt,
+                           void* stream);
+
 /* ---- learned warm start: MLP kernels (no reference counterpart) --------- *
  * theta -> 256 -> 256 -> (n + m) MLP, FP32, all matrices row-major.  Used to
  * train the network on plain-method solutions of a parametric family and to

@@ -34,6 +34,11 @@ __version__ = "0.0.5+b200"
 # own switches earlier.
 LARGE_N = 1024
 LARGE_N_SINGLE = 256
+# A QP with n >= SPARSE_N whose Gram matrix is not narrow-banded, whose A has
+# at most 10 % nonzeros and whose supernodal factor holds at most SPARSE_FILL
+# of a dense factor's entries gets the supernodal factorisation.
+SPARSE_N = 256
+SPARSE_FILL = 0.25
 BAND_GRID_N = 1024  # a banded QP solved on its own from this size: the whole GPU
 
 _HEADER = ("| iter |      pcost |      dcost |     pres |     dres |      gap |"
@@ -246,28 +251,43 @@ class QTQP:
             self._perm, self._permuted = perm, (a_p, p_p)
     return self._perm
 
+  def sparse_plan(self):
+    """The symbolic plan of the supernodal factorisation of this QP's Gram
+    matrix (qtqp_b200.sparse.SparsePlan: minimum-degree ordering,
+    supernodes, schedule).  Computed once."""
+    plan = getattr(self, "_sparse", None)
+    if plan is None or plan[0] is not self.a or plan[1] is not self.p:
+      from . import sparse as _sparse  # pylint: disable=g-import-not-at-top
+      plan = (self.a, self.p, _sparse.SparsePlan(self.a, self.p if self.p.nnz else None))
+      self._sparse = plan
+    return plan[2]
+
   def storage_format(self, single: bool = False) -> str:
     """'band' when the Gram matrix P + A^T D A is narrow-banded (its
     half-bandwidth at most n/4, in the natural ordering or in the band
     ordering of band_permutation) and n > 96 -- 'band_grid' (the whole GPU,
     partitioned band factorisation) instead for a QP solved on its own with
-    n >= BAND_GRID_N; otherwise 'large' (the whole GPU on one dense QP) when
-    n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on its own; else
-    'dense' (one thread block per QP)."""
+    n >= BAND_GRID_N; otherwise 'sparse' (the whole GPU, supernodal
+    factorisation) for a sparse QP with n >= SPARSE_N whose factor stays
+    sparse (sparse_plan); otherwise 'large' (the whole GPU on one dense QP)
+    when n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on its own;
+    else 'dense' (one thread block per QP)."""
     if self.n <= 96:
       return "dense"
     from . import band as _band  # pylint: disable=g-import-not-at-top
     p = self.p if self.p.nnz else None
-    if _band.wide_by_counts(self.a, p, self.n):  # no ordering makes it narrow
-      return "large" if self.n >= (LARGE_N_SINGLE if single else LARGE_N) else "dense"
-    bw = _band.gram_bandwidth(self.a, p)
-    if 4 * (bw + 1) > self.n and self.band_permutation() is not None:
-      a_p, p_p = self._permuted
-      bw = _band.gram_bandwidth(a_p, p_p)
-    if 4 * (bw + 1) <= self.n:
-      if single and self.n >= BAND_GRID_N and _band.grid_supported(bw, self.n):
-        return "band_grid"
-      return "band"
+    if not _band.wide_by_counts(self.a, p, self.n):  # else no ordering makes it narrow
+      bw = _band.gram_bandwidth(self.a, p)
+      if 4 * (bw + 1) > self.n and self.band_permutation() is not None:
+        a_p, p_p = self._permuted
+        bw = _band.gram_bandwidth(a_p, p_p)
+      if 4 * (bw + 1) <= self.n:
+        if single and self.n >= BAND_GRID_N and _band.grid_supported(bw, self.n):
+          return "band_grid"
+        return "band"
+    if (self.n >= SPARSE_N and self.a.nnz <= 0.1 * float(self.m) * self.n and
+        self.sparse_plan().fill_fraction() <= SPARSE_FILL):
+      return "sparse"
     return "large" if self.n >= (LARGE_N_SINGLE if single else LARGE_N) else "dense"
 
   def solve(self, *, atol: float = 1e-7, rtol: float = 1e-8, atol_infeas: float = 1e-8,
@@ -378,9 +398,9 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   """Solves independent QPs in one persistent GPU launch.
 
   Accepts the keyword arguments of QTQP.solve (verbose defaults to False)
-  plus warm_corrections and warm_shift.  storage: 'auto' (per problem:
-  banded when the Gram matrix is narrow-banded, else dense), 'dense' or
-  'band'.  warm_start: (WarmStartMLP, thetas) for instances of a parametric
+  plus warm_corrections and warm_shift.  storage: 'auto' (per problem,
+  QTQP.storage_format), 'dense', 'band', 'large', 'band_grid' or 'sparse'
+  (the last three solve one problem at a time on the whole GPU).  warm_start: (WarmStartMLP, thetas) for instances of a parametric
   family, all on the banded path -- each instance first solves the KKT system
   on the predicted active set and keeps that point only if the plain
   termination test passes, else the plain method runs (from the prediction
@@ -404,9 +424,9 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
   # go to their own device batches; each large problem gets the whole GPU in
   # turn.
   kinds = [q.storage_format() if storage == "auto" else storage for q in problems]
-  if any(k not in ("dense", "band", "large", "band_grid") for k in kinds):
-    raise ValueError("storage must be 'auto', 'dense', 'band', 'large' or 'band_grid', "
-                     f"got {storage!r}")
+  if any(k not in ("dense", "band", "large", "band_grid", "sparse") for k in kinds):
+    raise ValueError("storage must be 'auto', 'dense', 'band', 'large', 'band_grid' or "
+                     f"'sparse', got {storage!r}")
   if initial is not None:
     if len(initial) != len(problems):
       raise ValueError(f"initial: {len(initial)} points for {len(problems)} problems")
@@ -446,6 +466,19 @@ def solve_batch(problems: Sequence[QTQP], *, precision: str = "fp64", storage: s
     dg.launch()
     res, xp, yp, sp_, st = dg.fetch()
     where[i] = (res[0], xp, yp, sp_, None if st is None else st[0], hb.inst[0])
+  for i in [i for i, k in enumerate(kinds) if k == "sparse"]:
+    from . import sparse as _sparse  # pylint: disable=g-import-not-at-top
+    q = problems[i]
+    plan = q.sparse_plan()
+    dsg = _sparse.DeviceSparseGrid(
+        plan.permuted(q.a, q.b, q.c, q.z, q.p if q.p.nnz else None), plan, opts,
+        records=records)
+    dsg.upload()
+    t_launch = timeit.default_timer() - start
+    dsg.launch()
+    res, xp, yp, sp_, st = dsg.fetch()
+    where[i] = (res[0], plan.unpermute(xp[:q.n]), yp, sp_, None if st is None else st[0],
+                dsg.pools.inst[0])
   for kind in ("dense", "band"):
     idx = [i for i, k in enumerate(kinds) if k == kind]
     if not idx:

@@ -70,6 +70,12 @@ EXPORTS = (
     "qtqp_band_grid_solve",
     "qtqp_wait_selftest_workspace_bytes",
     "qtqp_wait_selftest",
+    "qtqp_sparse_analyze",
+    "qtqp_sparse_export",
+    "qtqp_sparse_free",
+    "qtqp_sparse_grid_blocks",
+    "qtqp_sparse_grid_workspace_bytes",
+    "qtqp_sparse_grid_solve",
 )
 
 
@@ -241,6 +247,18 @@ def load() -> ctypes.CDLL:
     lib.qtqp_kkt_dense_solve.argtypes = [i32, i32, vp, vp, vp, vp]
     lib.qtqp_kkt_dense_matvec.argtypes = [i32, i32, vp, vp, vp, vp]
     lib.qtqp_dense_equilibrate.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.qtqp_sparse_analyze.argtypes = [i32, i32, vp, vp, vp, vp, i32, i32,
+                                        ctypes.POINTER(vp), ctypes.POINTER(SparseDesc)]
+    lib.qtqp_sparse_export.argtypes = [vp, ctypes.POINTER(SparseDesc), vp, vp, vp]
+    lib.qtqp_sparse_free.restype = None
+    lib.qtqp_sparse_free.argtypes = [vp]
+    lib.qtqp_sparse_grid_blocks.restype = i32
+    lib.qtqp_sparse_grid_blocks.argtypes = []
+    lib.qtqp_sparse_grid_workspace_bytes.restype = sz
+    lib.qtqp_sparse_grid_workspace_bytes.argtypes = [vp, ctypes.POINTER(SparseDesc)]
+    lib.qtqp_sparse_grid_solve.argtypes = [vp, ctypes.POINTER(SparseDesc), vp, vp, vp, vp, vp,
+                                           vp, vp, vp, vp, vp, vp, vp, sz,
+                                           ctypes.POINTER(Options), vp]
     for name in EXPORTS:  # every declared entry point must resolve
       getattr(lib, name)
     _lib = lib
@@ -281,3 +299,17 @@ class BandInstance(ctypes.Structure):
 BAND_DTYPE = np.dtype([(name, np.int32 if ct is ctypes.c_int32 else np.int64)
                        for name, ct in BandInstance._fields_])
 assert BAND_DTYPE.itemsize == ctypes.sizeof(BandInstance)
+
+
+class SparseDesc(ctypes.Structure):
+  """qtqp_sparse_desc: sizes and pool offsets of a supernodal symbolic plan."""
+  _fields_ = ([(f, ctypes.c_int32) for f in ("n", "nsuper", "blocks", "top_levels", "max_rows",
+                                              "max_width", "tree_levels", "reserved")] +
+              [(f, ctypes.c_int64) for f in ("nvals", "ngram", "nrows", "nupd", "nranges",
+                                              "ntop", "nnz_l")] +
+              [("flops", ctypes.c_double)] +
+              [(f, ctypes.c_int64) for f in ("o_first", "o_colsn", "o_rows", "o_upd_ptr",
+                                              "o_upd_src", "o_upd_off", "o_upd_cnt",
+                                              "o_cta_ptr", "o_cta_range", "o_top_ptr",
+                                              "o_top_list", "o_gcol", "o_grow", "o_rowptr",
+                                              "o_valptr", "o_gpos", "n32", "n64")])

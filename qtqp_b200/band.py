@@ -122,11 +122,11 @@ class BandProblem:
     self.bw = self.structure.bw
 
 
-class HostBandBatch:
-  """Packed int32/double pools, descriptors and plan of a banded batch."""
+class BandPools:
+  """Descriptors and packed int32 / double pools of sparse QPs (A as CSR and
+  CSC, P as CSR), the input layout of the banded and supernodal solves."""
 
-  def __init__(self, problems: Sequence[BandProblem], opts: SolveOptions, num_sms: int = 0):
-    lib = _lib.load()
+  def __init__(self, problems: Sequence[BandProblem], opts: SolveOptions):
     count = len(problems)
     self.count = count
     inst = np.zeros(count, dtype=_lib.BAND_DTYPE)
@@ -178,12 +178,22 @@ class HostBandBatch:
     self.b_pool = np.concatenate([pr.b for pr in problems]) if count else np.zeros(1)
     self.c_pool = np.concatenate([pr.c for pr in problems]) if count else np.zeros(1)
     self.n_total, self.m_total = n_off, m_off
+    self.inst, self.opts = inst, opts
+
+
+class HostBandBatch(BandPools):
+  """Packed int32/double pools, descriptors and plan of a banded batch."""
+
+  def __init__(self, problems: Sequence[BandProblem], opts: SolveOptions, num_sms: int = 0):
+    super().__init__(problems, opts)
+    lib = _lib.load()
+    count = self.count
     order = np.zeros(max(count, 1), dtype=np.int32)
     plan = _lib.BatchPlan()
     copts = opts.to_c()
-    _lib.check(lib.qtqp_band_batch_plan(inst.ctypes.data, count, ctypes.byref(copts), num_sms,
-                                        order.ctypes.data, ctypes.byref(plan)))
-    self.inst, self.order, self.plan, self.opts = inst, order, plan, opts
+    _lib.check(lib.qtqp_band_batch_plan(self.inst.ctypes.data, count, ctypes.byref(copts),
+                                        num_sms, order.ctypes.data, ctypes.byref(plan)))
+    self.order, self.plan = order, plan
     self.workspace_bytes = int(plan.workspace_bytes)
 
   @property

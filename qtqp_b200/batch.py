@@ -88,15 +88,18 @@ class _Pack:
   """Column-major FP64 values of one QP's A and P (P: None when it is zero)
   and their host addresses, ready for the gather into the batch pools."""
 
-  __slots__ = ("src_a", "src_p", "n", "m", "z", "a_vals", "p_vals", "a_ptr", "p_ptr")
+  __slots__ = ("src_a", "src_p", "n", "m", "z", "a_vals", "p_vals", "a_ptr", "p_ptr", "b", "c",
+               "b_ptr", "c_ptr")
 
-  def __init__(self, src_a, src_p, n, m, z, a_vals, p_vals):
+  def __init__(self, src_a, src_p, n, m, z, a_vals, p_vals, b, c):
     self.src_a, self.src_p = src_a, src_p
     self.n, self.m, self.z = n, m, z
     self.a_vals = a_vals
     self.p_vals = p_vals
     self.a_ptr = a_vals.ctypes.data
     self.p_ptr = 0 if p_vals is None else p_vals.ctypes.data
+    self.b, self.c = b, c  # FP64, contiguous: gathered like A and P
+    self.b_ptr, self.c_ptr = b.ctypes.data, c.ctypes.data
 
 
 def _colmajor_values(mat, rows: int, cols: int) -> tuple[np.ndarray, bool]:
@@ -119,19 +122,29 @@ def _pack_of(pr) -> _Pack:
     a_vals, _ = _colmajor_values(pr.a, m, n)
     has_p = pr.p is not None and bool(np.any(pr.p != 0))
     p_vals = _colmajor_values(pr.p, n, n)[0] if has_p else None
-    return _Pack(None, None, n, m, pr.z, a_vals, p_vals)
+    return _Pack(None, None, n, m, pr.z, a_vals, p_vals, _f64(pr.b), _f64(pr.c))
   pk = getattr(pr, "_dense_pack", None)
-  if pk is not None and pk.src_a is pr.a and pk.src_p is pr.p:
+  if (pk is not None and pk.src_a is pr.a and pk.src_p is pr.p and pk.b is pr.b and
+      pk.c is pr.c):
     return pk
   n, m = pr.n, pr.m
   a_vals, a_view = _colmajor_values(pr.a, m, n)
   p_vals, p_view = None, True
   if pr.p.nnz and np.any(pr.p.data != 0):  # the device needs P when it is non-zero
     p_vals, p_view = _colmajor_values(pr.p, n, n)
-  pk = _Pack(pr.a, pr.p, n, m, pr.z, a_vals, p_vals)
-  if a_view and p_view:  # values read in place: valid while the matrices are
+  b, c = _f64(pr.b), _f64(pr.c)
+  pk = _Pack(pr.a, pr.p, n, m, pr.z, a_vals, p_vals, b, c)
+  if a_view and p_view and b is pr.b and c is pr.c:  # read in place: valid while they are
     pr._dense_pack = pk  # pylint: disable=protected-access
   return pk
+
+
+def _f64(v) -> np.ndarray:
+  """v itself when it is a contiguous FP64 vector, else such a copy."""
+  if (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.ndim == 1 and
+      v.flags.c_contiguous):
+    return v
+  return np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
 
 
 def _gather(lib, pool: np.ndarray, ptrs, nbytes, offs) -> None:
@@ -190,33 +203,36 @@ class HostBatch:
       self.a_pool, self.p_pool, self.b_pool, self.c_pool = (np.empty(k) for k in sizes)
     if p_total == 0:
       self.p_pool[:] = 0.0
-    if count:
-      np.concatenate([np.asarray(problems[i].b, dtype=np.float64) for i in pos],
-                     out=self.b_pool[:self.m_total])
-      np.concatenate([np.asarray(problems[i].c, dtype=np.float64) for i in pos],
-                     out=self.c_pool[:self.n_total])
     self.gathered = False
     if not defer:
       self.gather_all()
 
   def gather_group(self, g: int):
-    """Packs the A and P values of launch group g into the pools; returns
-    their element ranges ((a_lo, a_hi), (p_lo, p_hi))."""
+    """Packs the A, P, b and c values of launch group g into the pools;
+    returns the element ranges ((a_lo, a_hi), (p_lo, p_hi), (m_lo, m_hi),
+    (n_lo, n_hi)) of its A, P, b and c."""
     lib = _lib.load()
     grp = self.plan.groups[g]
     ids = self.order[grp.begin:grp.begin + grp.count]
+    if not len(ids):
+      return (0, 0), (0, 0), (0, 0), (0, 0)
     inst, packs = self.inst, self._packs
+    sel = [packs[i] for i in ids.tolist()]
     a_sz, p_sz = self._a_sz[ids], self._p_sz[ids]
     a_off, p_off = inst["a_off"][ids], inst["p_off"][ids]
-    _gather(lib, self.a_pool, [packs[i].a_ptr for i in ids], 8 * a_sz, 8 * a_off)
-    sel = np.nonzero(p_sz)[0]
-    _gather(lib, self.p_pool, [packs[ids[k]].p_ptr for k in sel], 8 * p_sz[sel],
-            8 * p_off[sel])
-    if not len(ids):
-      return (0, 0), (0, 0)
+    n_sz, m_sz = inst["n"][ids], inst["m"][ids]
+    n_off, m_off = inst["n_off"][ids], inst["m_off"][ids]
+    _gather(lib, self.a_pool, [pk.a_ptr for pk in sel], 8 * a_sz, 8 * a_off)
+    has = np.nonzero(p_sz)[0]
+    _gather(lib, self.p_pool, [sel[k].p_ptr for k in has.tolist()], 8 * p_sz[has],
+            8 * p_off[has])
+    _gather(lib, self.b_pool, [pk.b_ptr for pk in sel], 8 * m_sz, 8 * m_off)
+    _gather(lib, self.c_pool, [pk.c_ptr for pk in sel], 8 * n_sz, 8 * n_off)
     a_rng = (int(a_off[0]), int(a_off[-1] + a_sz[-1]))
     p_rng = (int(p_off[0]), int(p_off[-1] + p_sz[-1]))
-    return a_rng, p_rng
+    m_rng = (int(m_off[0]), int(m_off[-1] + m_sz[-1]))
+    n_rng = (int(n_off[0]), int(n_off[-1] + n_sz[-1]))
+    return a_rng, p_rng, m_rng, n_rng
 
   def gather_all(self) -> None:
     """Packs every group's A and P values."""
@@ -308,9 +324,6 @@ class DeviceBatch:
     lib = _lib.load()
     hb = self.hb
     st = stream or torch.cuda.current_stream(self.device)
-    with torch.cuda.stream(st):
-      for dst, src in ((self.b, self.h_pools[2]), (self.c, self.h_pools[3])):
-        dst.copy_(src, non_blocking=True)
     ready = torch.cuda.Event()
     ready.record(st)
     streams = _side_streams(torch, self.device, hb.plan.num_groups)
@@ -321,14 +334,13 @@ class DeviceBatch:
     done = []
     self._group_done = done
     for g in range(hb.plan.num_groups):
-      (a_lo, a_hi), (p_lo, p_hi) = hb.gather_group(g)
+      rngs = hb.gather_group(g)
       sg = streams[g]
       sg.wait_event(ready)
       with torch.cuda.stream(sg):
-        if a_hi > a_lo:
-          self.a[a_lo:a_hi].copy_(self.h_pools[0][a_lo:a_hi], non_blocking=True)
-        if p_hi > p_lo:
-          self.p[p_lo:p_hi].copy_(self.h_pools[1][p_lo:p_hi], non_blocking=True)
+        for dst, src, (lo, hi) in zip((self.a, self.p, self.b, self.c), self.h_pools, rngs):
+          if hi > lo:
+            dst[lo:hi].copy_(src[lo:hi], non_blocking=True)
       _lib.check(lib.qtqp_dense_batch_solve_group(
           self.inst.data_ptr(), self.order.data_ptr(), ctypes.byref(hb.plan), g,
           self.a.data_ptr(), self.p.data_ptr(), self.b.data_ptr(), self.c.data_ptr(),

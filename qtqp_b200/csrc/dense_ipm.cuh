@@ -178,6 +178,8 @@ enum MatFormat : int {
   kFmtBand = 1,   // sparse A (CSR + CSC), sparse P (CSR), banded Gram / factor
   kFmtLarge = 2,  // one large dense QP on the whole GPU (grid mode, NT > 1024):
                   // dense A / P in global memory, blocked Gram + Cholesky
+  kFmtSparse = 3, // one sparse QP on the whole GPU (grid mode): A and P as in
+                  // kFmtBand, a supernodal Cholesky of the Gram matrix
 };
 
 // ----------------------------------------------------------------------------
@@ -194,9 +196,17 @@ template <typename T, class S>
 __device__ int bandp_factorize(S& s);
 template <typename T, class S>
 __device__ void bandp_solve(S& s, T* v, T* w);
+// Supernodal factorisation / solve of grid mode (sparse_grid.cuh).
+struct SnFactor;
+template <typename T, class S>
+__device__ int sparse_factorize(S& s);
+template <typename T, class S>
+__device__ void sparse_solve(S& s, T* v, T* w);
 
 template <int NT, int FMT = kFmtDense>
 struct Ipm {
+  // Sparse A and P (CSR / CSC) with a banded or supernodal Gram factor.
+  static constexpr bool kSparseA = FMT == kFmtBand || FMT == kFmtSparse;
   int tid;
   int n, m, z, N;
   bool has_p;
@@ -246,6 +256,8 @@ struct Ipm {
   double* bp_wl;
   double* bp_sep;
   double* bp_vec;
+  // Supernodal factor of grid mode (FMT == kFmtSparse).
+  const SnFactor* sn;
 
   // Grid mode (NT > 1024, FMT == kFmtLarge): the group is a cooperative grid
   // of NT / kGridBT blocks; barriers and reductions go through gctl.
@@ -387,7 +399,7 @@ struct Ipm {
   // multiplied by (d_i * e_j), the clip bounds are [1e-3, 1e3].
   // --------------------------------------------------------------------------
   QTQP_PHASE void load_and_equilibrate(bool equilibrate, double& nb, double& nc) {
-    if constexpr (FMT == kFmtBand) {
+    if constexpr (kSparseA) {
       band_load_and_equilibrate(equilibrate, nb, nc);
       return;
     }
@@ -530,7 +542,7 @@ struct Ipm {
   // --------------------------------------------------------------------------
   template <typename T>
   QTQP_PHASE int factorize() {
-    if constexpr (FMT == kFmtBand) {
+    if constexpr (kSparseA) {
       return band_factorize<T>();
     } else if constexpr (FMT == kFmtLarge) {
       return large_factorize<T>(*this);
@@ -1078,7 +1090,7 @@ struct Ipm {
   // before other threads read it).
   // --------------------------------------------------------------------------
   QTQP_PHASE void kkt_solve(const double* r, double* out, bool accumulate, bool fp64) {
-    if constexpr (FMT == kFmtBand) {
+    if constexpr (kSparseA) {
       band_kkt_solve(r, out, accumulate, fp64);
       return;
     }
@@ -1204,7 +1216,7 @@ struct Ipm {
   // max |res| and NaN flag of v (combined by the caller's reduction).
   QTQP_PHASE void kkt_residual(const double* v, const double* krhs, double* res, double& mres,
                                double& vnan) const {
-    if constexpr (FMT == kFmtBand) {
+    if constexpr (kSparseA) {
       band_kkt_residual(v, krhs, res, mres, vnan);
       return;
     }
@@ -1421,7 +1433,7 @@ struct Ipm {
         sm[3] = fma(kr[k], t, sm[3]);
         sm[4] = fma(px[k], kr[k], sm[4]);
       };
-      if constexpr (FMT == kFmtBand) {
+      if constexpr (kSparseA) {
         for (int k = tid; k < n; k += NT) epi(k, band_poff_row(kr, k));
       } else {
         const double* Pp = P;
@@ -1548,7 +1560,7 @@ struct Ipm {
       mx[6] = nanmax(mx[6], fabs(so));
       mx[8] = nanmax(mx[8], fabs(yo));
     };
-    if constexpr (FMT == kFmtBand) {
+    if constexpr (kSparseA) {
       for (int k = tid; k < n; k += NT) epi_x(k, band_at_col(xy, k), band_poff_row(xy, k));
       for (int k = tid; k < m; k += NT) epi_y(k, band_a_row(xy, k));
     } else if (fused_ok()) {
@@ -1689,7 +1701,7 @@ struct Ipm {
   // out[n + i] = (A v)_i (equilibrated A).  Exit: needs a barrier before
   // other threads read out.
   __device__ void a_times(const double* v, double* out) const {
-    if constexpr (FMT == kFmtBand) {
+    if constexpr (kSparseA) {
       for (int k = own(n); k < N; k += NT) out[k] = band_a_row(v, k - n);
     } else {
       const double* Ap = A;
@@ -2007,7 +2019,7 @@ struct Ipm {
             sm[3] = fma(xy[k], b, sm[3]);
             sm[4] = fma(b, kq[k], sm[4]);
           };
-          if constexpr (FMT == kFmtBand) {
+          if constexpr (kSparseA) {
             for (int k = tid; k < n; k += NT) epi(k, band_poff_row(kq, k), band_poff_row(xy, k));
           } else {
             const double* Pp = P;
@@ -2480,7 +2492,9 @@ struct Ipm {
   // factor keeps 1 / l_kk.
   template <typename T>
   __device__ int band_factorize() {
-    if constexpr (NT > 1024) {
+    if constexpr (FMT == kFmtSparse) {
+      return sparse_factorize<T>(*this);
+    } else if constexpr (NT > 1024) {
       return bandp_factorize<T>(*this);
     } else {
       if (bwin == nullptr) return band_factorize_global<T>();
@@ -2797,7 +2811,9 @@ struct Ipm {
   // (band_grid.cuh).
   template <typename T>
   __device__ void band_chol_solve(T* v, T* w) {
-    if constexpr (NT > 1024) {
+    if constexpr (FMT == kFmtSparse) {
+      sparse_solve<T>(*this, v, w);
+    } else if constexpr (NT > 1024) {
       bandp_solve<T>(*this, v, w);
     } else {
       if (bwin == nullptr) {

@@ -245,3 +245,87 @@ def unbounded(m: int, n: int, z: int, seed):
   c = -c / (c @ x)
   b = rng.normal(size=m)
   return sp.csc_matrix(a), b, c, z, sp.csc_matrix(p)
+
+
+# ---------------------------------------------------------------------------
+# Sparse QPs whose Gram matrix is neither dense nor banded (the supernodal
+# path): random sparse rows, and min-cost flows on a grid network.
+# ---------------------------------------------------------------------------
+def sparse_rows(m: int, n: int, per_row: int, rng) -> sp.csc_matrix:
+  """m x n, each row with `per_row` N(0,1) entries in random columns (every
+  column hit at least once)."""
+  cols = np.concatenate([rng.permutation(n), rng.integers(0, n, size=m * per_row - n)])
+  cols = cols[:m * per_row] if m * per_row >= n else cols
+  rows = np.repeat(np.arange(m), per_row)[:cols.size]
+  a = sp.csc_matrix((rng.normal(size=cols.size), (rows, cols)), shape=(m, n))
+  a.sum_duplicates()
+  return a
+
+
+def sparse_feasible(n: int, m: int, z: int, seed, per_row: int = 3, lp: bool = False):
+  """Sparse feasible QP: A with `per_row` entries per row, P = 0.1 G^T G + 1e-2 I
+  with G two entries per row (P = 0 if lp), b and c from a known optimal pair."""
+  rng = np.random.default_rng(seed)
+  a = sparse_rows(m, n, per_row, rng)
+  if lp:
+    p = sp.csc_matrix((n, n))
+  else:
+    g = sparse_rows(n, n, 2, rng)
+    p = sp.csc_matrix(0.1 * (g.T @ g) + 1e-2 * sp.eye(n))
+  b, c = _feasible_pair(rng, a, p, z)
+  return a, b, c, z, p
+
+
+def sparse_infeasible(n: int, m: int, z: int, seed, per_row: int = 3):
+  """Sparse primal-infeasible QP: two inequality rows a x <= b1, -a x <= b2
+  with b1 + b2 = -1 (the Farkas ray y = e_i + e_j)."""
+  a, b, c, z, p = sparse_feasible(n, m, z, seed, per_row)
+  a = sp.lil_matrix(a)
+  i, j = m - 2, m - 1
+  a[j, :] = -a[i, :]
+  b = b.copy()
+  b[j] = -1.0 - b[i]
+  return sp.csc_matrix(a), b, c, z, p
+
+
+def sparse_unbounded(n: int, m: int, z: int, seed, per_row: int = 3):
+  """Sparse dual-infeasible QP: variable k has no entry in P or in the
+  equality rows, entries <= 0 in the inequality rows, and c_k = -1, so
+  x = t e_k stays feasible with the objective going to -inf."""
+  rng = np.random.default_rng(seed)
+  a, b, c, z, p = sparse_feasible(n, m, z, seed, per_row)
+  k = n - 1
+  a = sp.lil_matrix(a)
+  col = a[:, k].toarray().ravel()
+  col[:z] = 0.0
+  col[z:] = -np.abs(col[z:])
+  a[:, k] = col.reshape(-1, 1)
+  p = sp.lil_matrix(p)
+  p[k, :] = 0.0
+  p[:, k] = 0.0
+  c = c.copy()
+  c[k] = -1.0
+  b = b + rng.random(m)  # keeps the QP feasible (x0 with slack)
+  return sp.csc_matrix(a), b, c, z, sp.csc_matrix(p)
+
+
+def grid_flow(k: int, seed: int = 1005):
+  """Min-cost flow with quadratic edge costs on a k x k grid network (both
+  directions of every grid edge): node conservation E x = d (equalities) and
+  0 <= x <= u (inequalities), from a known optimal pair.  n = 4 k (k - 1)."""
+  rng = np.random.default_rng(seed)
+  idx = np.arange(k * k).reshape(k, k)
+  e = ([(idx[i, j], idx[i, j + 1]) for i in range(k) for j in range(k - 1)] +
+       [(idx[i, j], idx[i + 1, j]) for i in range(k - 1) for j in range(k)])
+  e = e + [(v, u) for u, v in e]
+  n, nodes = len(e), k * k
+  tail = np.array([u for u, _ in e])
+  head = np.array([v for _, v in e])
+  inc = sp.csc_matrix((np.concatenate([-np.ones(n), np.ones(n)]),
+                       (np.concatenate([tail, head]), np.tile(np.arange(n), 2))),
+                      shape=(nodes, n))
+  eye = sp.eye(n, format="csc")
+  a = sp.csc_matrix(sp.vstack([inc, -eye, eye]))
+  p = sp.csc_matrix(sp.diags(rng.uniform(0.1, 1.0, size=n)))
+  b, c = _feasible_pair(rng, a, p, nodes)
+  return a, b, c, nodes, p

@@ -141,3 +141,40 @@ def test_band_grid_solve_rejects_bad_arguments(lib):
   bad.max_iter = 0
   assert call(o=ctypes.byref(bad)) == _lib.QTQP_ERR_BAD_ARG
   assert b"invalid options" in lib.qtqp_last_error()
+
+
+def test_sparse_grid_solve_rejects_bad_arguments(lib):
+  """The supernodal whole-GPU entry point checks its plan against the
+  instance and its pointers, sizes and options before any device work."""
+  from qtqp_b200 import band, sparse
+  a, b, c, z, p = problems.sparse_feasible(300, 320, 30, 4, per_row=2)
+  plan = sparse.SparsePlan(a, p)
+  prob = plan.permuted(a, b, c, z, p)
+  pools = band.BandPools([prob], batch.SolveOptions())
+  inst = np.ascontiguousarray(pools.inst[:1])
+  desc = plan.desc
+  ws_bytes = lib.qtqp_sparse_grid_workspace_bytes(inst.ctypes.data, ctypes.byref(desc))
+  assert ws_bytes > 8 * desc.nvals
+  assert lib.qtqp_sparse_grid_blocks() == desc.blocks
+  opts = batch.SolveOptions().to_c()
+  fake = 1 << 20  # a non-null device-looking address, never dereferenced
+  def call(d=desc, pools_=fake, ws=fake, nbytes=ws_bytes, o=ctypes.byref(opts)):
+    return lib.qtqp_sparse_grid_solve(inst.ctypes.data, ctypes.byref(d), pools_, pools_,
+                                      pools_, pools_, pools_, pools_, pools_, pools_, pools_,
+                                      pools_, None, ws, nbytes, o, None)
+  assert call(pools_=None) == _lib.QTQP_ERR_BAD_ARG
+  assert b"null argument" in lib.qtqp_last_error()
+  assert call(nbytes=ws_bytes - 1) == _lib.QTQP_ERR_BAD_ARG
+  assert b"workspace smaller" in lib.qtqp_last_error()
+  assert call(ws=fake + 8) == _lib.QTQP_ERR_BAD_ARG
+  assert b"16-byte aligned" in lib.qtqp_last_error()
+  other = sparse.SparsePlan(*problems.sparse_feasible(301, 320, 30, 4, per_row=2)[::4]).desc
+  assert call(d=other) == _lib.QTQP_ERR_BAD_ARG
+  assert b"does not match" in lib.qtqp_last_error()
+  warm = batch.SolveOptions(warm_corrections=2).to_c()
+  assert call(o=ctypes.byref(warm)) == _lib.QTQP_ERR_BAD_ARG
+  assert b"warm starts" in lib.qtqp_last_error()
+  bad = batch.SolveOptions().to_c()
+  bad.max_iter = 0
+  assert call(o=ctypes.byref(bad)) == _lib.QTQP_ERR_BAD_ARG
+  assert b"invalid options" in lib.qtqp_last_error()

@@ -250,7 +250,7 @@ def test_solve_batch_checks_arguments_before_device_work():
   a, b, c, z, p = problems.feasible(12, 8, 2, 3)
   dense_q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
   with pytest.raises(ValueError, match="storage must be"):
-    qb.solve_batch([dense_q], storage="sparse")
+    qb.solve_batch([dense_q], storage="supernodal")
   model = types.SimpleNamespace(n=dense_q.n, m=dense_q.m)
   with pytest.raises(ValueError, match="banded path"):
     qb.solve_batch([dense_q], storage="dense", warm_start=(model, np.zeros((1, 32))))
