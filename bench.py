@@ -53,10 +53,13 @@ def _args():
   ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
                   help="form whose throughput is the headline value (both are measured)")
   ap.add_argument("--workload", default="batch_small",
-                  choices=["batch_small", "dense_large", "mpc", "parametric"],
+                  choices=["batch_small", "dense_large", "mpc", "parametric", "sparse"],
                   help="batch_small: 4096 uneven small dense QPs (default); dense_large: "
                        "one n=4096, m=8192 dense QP on the whole GPU; parametric: a T=50 "
-                       "MPC family with the learned warm start")
+                       "MPC family with the learned warm start; sparse: one min-cost flow "
+                       "QP on a grid network (supernodal factorisation)")
+  ap.add_argument("--grid", type=int, default=60,
+                  help="sparse: side of the grid network (n = 4 k (k - 1) edges)")
   ap.add_argument("--train", type=int, default=16384,
                   help="parametric: training instances (the family's stated split: 16384 "
                        "train, 3616 held out)")
@@ -749,6 +752,133 @@ def run_mpc(args):
           flush=True)
 
 
+SPARSE_WORKLOAD = ("one min-cost flow QP on a k x k grid network (both directions of every "
+                   "edge, quadratic costs): n = 4 k (k - 1), node conservation equalities, "
+                   "0 <= x <= u")
+
+
+def run_sparse(args):
+  """One sparse QP per step on the supernodal whole-GPU path (replicas only
+  for N > 1)."""
+  rank = int(os.environ.get("RANK", "0"))
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  from qtqp_b200 import problems
+  k = args.grid
+  a, b, c, z, p = problems.grid_flow(k)
+  workload = SPARSE_WORKLOAD.replace("k x k", f"{k} x {k}")
+  if args.impl == "reference":
+    if rank != 0:
+      return
+    from oracle import qtqp_oracle as orc
+    times = []
+    for step in range(args.warmup + args.steps):
+      t0 = time.perf_counter()
+      r = orc.solve(a, b, c, z, p, backend="superlu")
+      if step >= args.warmup:
+        times.append(time.perf_counter() - t0)
+    t_cpu = sum(times) / len(times)
+    cpu = {"value": 1.0 / t_cpu, "unit": "QPs/s", "cores": 1, "kind": "port",
+           "sample": f"one whole solve per step, {args.steps} steps, oracle restatement "
+                     "(SuperLU KKT)"}
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": 1.0 / t_cpu, "unit": "QPs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_cpu, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload, "status": r.status}, "cpu_baseline": cpu,
+        "e2e": {"value": 1.0 / t_cpu, "unit": "QPs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}), flush=True)
+    return
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    from oracle import qtqp_oracle as orc
+    t0 = time.perf_counter()
+    orc.solve(a, b, c, z, p, backend="superlu")
+    t_cpu = time.perf_counter() - t0
+    cpu = {"value": 1.0 / t_cpu, "unit": "QPs/s", "cores": 1, "kind": "port",
+           "sample": "one whole solve, oracle restatement (SuperLU KKT)"}
+  else:
+    cpu = None
+  import torch
+  import qtqp_b200 as qb
+  from qtqp_b200 import batch, sparse
+  torch.cuda.set_device(local)
+  dev = torch.device("cuda", local)
+  stream = torch.cuda.current_stream(dev)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  t0 = time.perf_counter()
+  plan = q.sparse_plan()
+  t_plan = time.perf_counter() - t0
+  prob = plan.permuted(q.a, q.b, q.c, q.z, q.p if q.p.nnz else None)
+  forms = {}
+  for precision in ("fp64", "mixed"):
+    dg = sparse.DeviceSparseGrid(prob, plan, batch.SolveOptions(precision=precision), device=dev)
+    dg.upload(stream)
+    for _ in range(args.warmup):
+      dg.launch(stream)
+    torch.cuda.synchronize(dev)
+    clocks = _Clocks(local) if precision == args.precision else None
+    t = sum(_ev_time(stream, lambda: dg.launch(stream)) for _ in range(args.steps))
+    ck = clocks.stop() if clocks else None
+    forms[precision] = dict(dg=dg, time=t, res=dg.fetch()[0][0], clocks=ck)
+  chosen = forms[args.precision]
+  dg, res = chosen["dg"], chosen["res"]
+  value = int(res["status"] == 0) * args.steps / chosen["time"]
+  fp64, mixed = forms["fp64"], forms["mixed"]
+  # End to end through the public API: solve_batch on the QTQP (its symbolic
+  # plan is cached on it after the first call), host packing, copies, solve,
+  # read-back and the Solution, timed with CUDA events.
+  qb.solve_batch([q], storage="sparse", precision=args.precision)
+  e_total = sum(_ev_time(stream, lambda: qb.solve_batch([q], storage="sparse",
+                                                        precision=args.precision))
+                for _ in range(args.steps))
+  t_launch = chosen["time"] / args.steps
+  d = plan.desc
+  iters = int(res["iterations"])
+  nnz = int(dg.pools.inst["nnz_a"][0])
+  n_, m_ = int(dg.pools.inst["n"][0]), int(dg.pools.inst["m"][0])
+  # Algorithmic bytes per IPM iteration: the SpMV bytes of A x in CSR (12 nnz
+  # + 4 (rows + 1) + 8 (cols + rows)), twice (A x and A^T y), plus the
+  # supernodal factor written and read (8 bytes per stored value each).
+  per_iter = 2 * (12 * nnz + 4 * (m_ + 1) + 8 * (n_ + m_)) + 2 * 8 * int(d.nvals)
+  achieved = per_iter * iters / t_launch / 1e9
+  peak, peak_kind = _peaks()
+  nfact = int(res["fp32_factorizations"] + res["fp64_factorizations"])
+  if rank == 0:
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_launch, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator of the workload's distribution)",
+        "config": {"workload": workload, "n": n_, "m": m_, "precision": args.precision,
+                   "supernodes": int(d.nsuper), "top_levels": int(d.top_levels),
+                   "nnz_l": int(d.nnz_l), "fill_of_dense": plan.fill_fraction(),
+                   "symbolic_seconds": t_plan,
+                   "parallelism": "replicas" if world > 1 else "one QP per GPU"},
+        "fp64_value": int(fp64["res"]["status"] == 0) * args.steps / fp64["time"],
+        "mixed_value": int(mixed["res"]["status"] == 0) * args.steps / mixed["time"],
+        "statuses_identical": bool(fp64["res"]["status"] == mixed["res"]["status"]),
+        "iterations": iters,
+        "factorizations": {"fp32": int(res["fp32_factorizations"]),
+                           "fp64": int(res["fp64_factorizations"])},
+        "kkt_tflops": d.flops * nfact / t_launch / 1e12,
+        "e2e": {"value": int(res["status"] == 0) * args.steps / e_total, "unit": "QPs/s",
+                "h2d_bytes_per_step": dg.input_bytes,
+                "d2h_bytes_per_step": 8 * (n_ + 2 * m_) + _lib_result_bytes(),
+                "path": "qtqp.solve_batch([QTQP], storage='sparse') -> [Solution]"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "kernel": "sparse_grid_kernel",
+                     "algorithmic_bytes_per_launch": per_iter * iters},
+        "cpu_baseline": cpu, "clocks": chosen["clocks"], "gpu_launches": args.steps}),
+          flush=True)
+
+
+def _lib_result_bytes() -> int:
+  from qtqp_b200 import _lib
+  return int(_lib.RESULT_DTYPE.itemsize)
+
+
 def run_parametric(args):
   """Plain FP64 batch vs mixed precision + learned warm start on held-out
   instances of the parametric family (training is outside the timed region)."""
@@ -866,6 +996,8 @@ def main():
     run_dense_large(args)
   elif args.workload == "parametric":
     run_parametric(args)
+  elif args.workload == "sparse":
+    run_sparse(args)
   elif args.workload == "mpc":
     run_mpc(args)
   elif args.impl == "reference":

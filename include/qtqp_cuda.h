@@ -356,9 +356,11 @@ typedef struct qtqp_sparse_desc {
   int64_t ngram;    /* lower entries of G, diagonal included */
   int64_t nrows, nupd, nranges, ntop;
   int64_t nnz_l;    /* stored lower entries of L */
+  int64_t top_row_slabs; /* 64-row work items of the supernodes above the subtrees */
   double flops;     /* multiply-adds x 2 of one numeric factorisation */
   int64_t o_first, o_colsn, o_rows, o_upd_ptr, o_upd_src, o_upd_off, o_upd_cnt,
-      o_cta_ptr, o_cta_range, o_top_ptr, o_top_list, o_gcol, o_grow; /* int32 pool */
+      o_cta_ptr, o_cta_range, o_top_ptr, o_top_list, o_top_slab, o_gcol,
+      o_grow;                                                     /* int32 pool */
   int64_t o_rowptr, o_valptr, o_gpos;                             /* int64 pool */
   int64_t n32, n64;
 } qtqp_sparse_desc;

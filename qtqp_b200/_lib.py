@@ -306,10 +306,11 @@ class SparseDesc(ctypes.Structure):
   _fields_ = ([(f, ctypes.c_int32) for f in ("n", "nsuper", "blocks", "top_levels", "max_rows",
                                               "max_width", "tree_levels", "reserved")] +
               [(f, ctypes.c_int64) for f in ("nvals", "ngram", "nrows", "nupd", "nranges",
-                                              "ntop", "nnz_l")] +
+                                              "ntop", "nnz_l", "top_row_slabs")] +
               [("flops", ctypes.c_double)] +
               [(f, ctypes.c_int64) for f in ("o_first", "o_colsn", "o_rows", "o_upd_ptr",
                                               "o_upd_src", "o_upd_off", "o_upd_cnt",
                                               "o_cta_ptr", "o_cta_range", "o_top_ptr",
-                                              "o_top_list", "o_gcol", "o_grow", "o_rowptr",
+                                              "o_top_list", "o_top_slab", "o_gcol", "o_grow",
+                                              "o_rowptr",
                                               "o_valptr", "o_gpos", "n32", "n64")])

@@ -234,6 +234,15 @@ class HostBatch:
     n_rng = (int(n_off[0]), int(n_off[-1] + n_sz[-1]))
     return a_rng, p_rng, m_rng, n_rng
 
+  def launch_order(self) -> list[int]:
+    """Launch groups in increasing order of their packed A and P bytes."""
+    sizes = []
+    for g in range(self.plan.num_groups):
+      grp = self.plan.groups[g]
+      ids = self.order[grp.begin:grp.begin + grp.count]
+      sizes.append((int(self._a_sz[ids].sum() + self._p_sz[ids].sum()), g))
+    return [g for _, g in sorted(sizes)]
+
   def gather_all(self) -> None:
     """Packs every group's A and P values."""
     for g in range(self.plan.num_groups):
@@ -316,10 +325,16 @@ class DeviceBatch:
 
   def solve_pipelined(self, stream=None) -> None:
     """Packs, copies and launches the batch group by group: each launch group
-    is packed on the host (the largest instances first), copied to the
-    device and launched on a stream of its own, while the host packs the next
-    group; the outputs are complete on `stream` when the call returns (no
-    synchronisation).  The host batch must have been built with defer=True."""
+    is packed on the host, copied to the device and launched on a stream of
+    its own, while the host packs the next group; the outputs are complete on
+    `stream` when the call returns (no synchronisation).  The host batch must
+    have been built with defer=True.
+
+    Groups go in increasing order of their packed bytes (Johnson's rule for a
+    two-stage flow shop whose stages are host packing and device solving:
+    packing takes less time than solving for every group here, so the
+    cheapest packing goes first and the device starts at once, while the
+    host packs the big groups behind the running ones)."""
     torch = self.torch
     lib = _lib.load()
     hb = self.hb
@@ -331,9 +346,9 @@ class DeviceBatch:
                  self.results.data_ptr(),
                  self.stats.data_ptr() if self.stats is not None else None,
                  self.workspace.data_ptr(), hb.workspace_bytes, ctypes.byref(self._copts))
-    done = []
+    done = [None] * hb.plan.num_groups
     self._group_done = done
-    for g in range(hb.plan.num_groups):
+    for g in hb.launch_order():
       rngs = hb.gather_group(g)
       sg = streams[g]
       sg.wait_event(ready)
@@ -347,7 +362,7 @@ class DeviceBatch:
           *args_tail, _lib.stream_handle(sg)))
       ev = torch.cuda.Event()
       ev.record(sg)
-      done.append(ev)
+      done[g] = ev
     hb.gathered = True
     for ev in done:
       st.wait_event(ev)

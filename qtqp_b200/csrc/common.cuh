@@ -100,6 +100,11 @@ __device__ __forceinline__ void group_sync() {
 // ----------------------------------------------------------------------------
 constexpr int kGridMaxBlocks = 256;
 constexpr int kGridBT = 256;  // threads per block of a grid-mode solve
+// Supernodal factorisation: the widest supernode (its diagonal block stays in
+// shared memory) and the rows of a top-level supernode per work item.  Both
+// the host symbolic stage and the device phases use them.
+constexpr int kSnMaxWidth = 64;
+constexpr int kSnSlabRows = 64;
 constexpr uint32_t kGridWaitLimit = 1u << 25;
 
 struct GridCtl {
@@ -271,7 +276,10 @@ enum Phase : int {
   // Sub-phases of the partitioned banded factorisation and solves.
   kPhBpInterior, kPhBpChain, kPhBpFwd, kPhBpChains, kPhBpBwd,
   // Steps of one reduction level (per participating block).
-  kPhBpCrStage, kPhBpCrSweep, kPhBpCrGemm, kPhBpCrGather, kNumPhases
+  kPhBpCrStage, kPhBpCrSweep, kPhBpCrGemm, kPhBpCrGather,
+  // Sub-phases of the supernodal factorisation and solves (subtrees / top levels).
+  kPhSnSub, kPhSnTop, kPhSnFwdSub, kPhSnFwdTop, kPhSnBwdTop, kPhSnBwdSub,
+  kPhSnTopUpd, kPhSnTopDiag, kPhSnTopPanel, kNumPhases
 };
 #ifdef QTQP_PHASE_TIMERS
 extern __device__ unsigned long long g_phase_cycles[kNumPhases];

@@ -28,15 +28,22 @@ struct SparseGridParams {
 __host__ __device__ inline size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct SparseLayout {
-  size_t band_off, vals_off, ctl_off, info_off, total;
+  size_t band_off, vals_off, z_off, parts_off, ctl_off, info_off, total;
 };
+// Workspace: the banded backend's vectors and working values, the factor
+// (nvals), the forward products (one per stored row), the backward partial
+// sums (kSnMaxW per top-level row slab), the grid's barrier state and the
+// factorisation status.
 __host__ __device__ inline SparseLayout plan_sparse_layout(int n, int m, int nnz_a, int nnz_p,
-                                                           int64_t nvals) {
+                                                           int64_t nvals, int64_t nrows,
+                                                           int64_t nslabs) {
   SparseLayout L;
   const BandLayout B = plan_band_layout(n, m, 0, nnz_a, nnz_p);
   L.band_off = 0;
   L.vals_off = round256(B.total);
-  L.ctl_off = round256(L.vals_off + size_t(nvals) * 8);
+  L.z_off = round256(L.vals_off + size_t(nvals) * 8);
+  L.parts_off = round256(L.z_off + size_t(nrows) * 8);
+  L.ctl_off = round256(L.parts_off + size_t(nslabs) * kSnMaxW * 8);
   L.info_off = round256(L.ctl_off + sizeof(GridCtl));
   L.total = L.info_off + 256;
   return L;
@@ -48,11 +55,14 @@ __global__ void __launch_bounds__(kGridBT, 1) sparse_grid_kernel(const SparseGri
   __shared__ SnFactor sf;
   extern __shared__ double snmem[];
   const qtqp_band_instance& d = p.d;
-  const SparseLayout L = plan_sparse_layout(d.n, d.m, d.nnz_a, d.nnz_p, p.f.nvals);
+  const SparseLayout L =
+      plan_sparse_layout(d.n, d.m, d.nnz_a, d.nnz_p, p.f.nvals, p.f.nrows, p.f.nslabs);
   if (threadIdx.x == 0) {
     sopt = p.opt;
     sf = p.f;
     sf.vals = reinterpret_cast<double*>(p.ws + L.vals_off);
+    sf.zbuf = reinterpret_cast<double*>(p.ws + L.z_off);
+    sf.pbuf = reinterpret_cast<double*>(p.ws + L.parts_off);
   }
   __syncthreads();
   Ipm<kSparseGridNT, kFmtSparse> s;
@@ -89,6 +99,10 @@ __global__ void __launch_bounds__(kGridBT, 1) sparse_grid_kernel(const SparseGri
   }
 }
 
+// Row slabs of the top-level supernodes: the plan's top_slab[ntop] (also in
+// the descriptor, so that the host needs no pool to size the workspace).
+static int64_t top_slabs(const qtqp_sparse_desc& sd) { return sd.top_row_slabs; }
+
 static int check_sparse(const qtqp_band_instance* h, const qtqp_sparse_desc* sd, const char* who) {
   if (h == nullptr || sd == nullptr)
     return fail(QTQP_ERR_BAD_ARG, std::string(who) + ": null instance or plan");
@@ -114,7 +128,9 @@ extern "C" size_t qtqp_sparse_grid_workspace_bytes(const qtqp_band_instance* h_i
                                                    const qtqp_sparse_desc* h_desc) {
   if (check_sparse(h_inst, h_desc, "qtqp_sparse_grid_workspace_bytes") != QTQP_OK) return 0;
   const qtqp_band_instance& d = *h_inst;
-  return plan_sparse_layout(d.n, d.m, d.nnz_a, d.nnz_p, h_desc->nvals).total;
+  return plan_sparse_layout(d.n, d.m, d.nnz_a, d.nnz_p, h_desc->nvals, h_desc->nrows,
+                            top_slabs(*h_desc))
+      .total;
 }
 
 extern "C" int qtqp_sparse_grid_solve(const qtqp_band_instance* h_inst,
@@ -139,7 +155,8 @@ extern "C" int qtqp_sparse_grid_solve(const qtqp_band_instance* h_inst,
     return fail(QTQP_ERR_BAD_ARG, "qtqp_sparse_grid_solve: warm starts are not supported");
   const qtqp_band_instance& d = *h_inst;
   const qtqp_sparse_desc& sd = *h_desc;
-  const SparseLayout L = plan_sparse_layout(d.n, d.m, d.nnz_a, d.nnz_p, sd.nvals);
+  const SparseLayout L = plan_sparse_layout(d.n, d.m, d.nnz_a, d.nnz_p, sd.nvals, sd.nrows,
+                                            top_slabs(sd));
   if (workspace_bytes < L.total)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_sparse_grid_solve: workspace smaller than "
                                   "qtqp_sparse_grid_workspace_bytes(inst, plan)");
@@ -176,6 +193,8 @@ extern "C" int qtqp_sparse_grid_solve(const qtqp_band_instance* h_inst,
   f.top_levels = sd.top_levels;
   f.nvals = sd.nvals;
   f.ngram = sd.ngram;
+  f.nrows = sd.nrows;
+  f.nslabs = top_slabs(sd);
   f.first = d_sn32 + sd.o_first;
   f.colsn = d_sn32 + sd.o_colsn;
   f.rows = d_sn32 + sd.o_rows;
@@ -187,6 +206,7 @@ extern "C" int qtqp_sparse_grid_solve(const qtqp_band_instance* h_inst,
   f.cta_range = d_sn32 + sd.o_cta_range;
   f.top_ptr = d_sn32 + sd.o_top_ptr;
   f.top_list = d_sn32 + sd.o_top_list;
+  f.top_slab = d_sn32 + sd.o_top_slab;
   f.gcol = d_sn32 + sd.o_gcol;
   f.grow = d_sn32 + sd.o_grow;
   f.rowptr = d_sn64 + sd.o_rowptr;

@@ -13,22 +13,26 @@
 //    G is computed (a merge of columns i and j of A, plus P and the diagonal)
 //    and written to its position; the dense backend's relative jitter
 //    (1e-14 max diag) is added to the diagonal;
-//  * factorisation, left-looking per supernode s (one block): for every
-//    descendant d with rows in s's column range (the update list: d, the
-//    first such row `off` of R_d and their number `cnt`), L_s[rows, cols] -=
-//    L_d[off:, :] L_d[off:off+cnt, :]^T, scattered by the position of each
-//    row of R_d in R_s; then the Cholesky of the diagonal block in shared
-//    memory and the triangular solve of the rows below it.  The diagonal
-//    keeps 1 / l_jj;
-//  * solves: forward, per supernode, gathers the rows of L in its columns
-//    from its update list, then solves with its diagonal block; backward
-//    gathers x over R_s below the block, then solves with the transposed
-//    block.  No atomics: every result has a single writer, so the results
-//    are reproducible run to run.
+//  * factorisation, left-looking per supernode s: for every descendant d
+//    with rows in s's column range (the update list: d, the first such row
+//    `off` of R_d and their number `cnt`), L_s[rows, cols] -= L_d[off:, :]
+//    L_d[off:off+cnt, :]^T, scattered by the position of each row of R_d in
+//    R_s; then the Cholesky of the diagonal block in shared memory and the
+//    triangular solve of the rows below it.  The diagonal keeps 1 / l_jj;
+//  * forward solve: each supernode subtracts the stored products z_d =
+//    L_d[r, :] y_d of its descendants' rows in its columns, solves with its
+//    diagonal block, and stores its own products z_s for the rows below;
+//  * backward solve: partial sums L_s[slab, :]^T x[rows] per row slab, then
+//    per supernode their sum in slab order and the transposed block solve.
+// No atomics: every result has a single writer and sums run in a fixed
+// order, so the results are reproducible run to run.
 // Order: each block first runs the subtrees the symbolic stage gave it (their
-// supernodes in postorder, no grid barrier), then the supernodes above the
-// subtrees run level by level with one grid barrier per level; the backward
-// solve runs the same schedule in reverse.
+// supernodes in postorder, no grid barrier; a supernode is one block's work).
+// Above the subtrees, each level is spread over the whole grid in 64-row
+// slabs: the factorisation in three steps (updates of every slab, diagonal
+// blocks, rows below), each solve direction in two (diagonal solves and the
+// slabs' products / partial sums), with a grid barrier after each step.  The
+// backward solve runs the schedule in reverse.
 #pragma once
 
 #include "dense_ipm.cuh"
@@ -37,10 +41,11 @@ namespace qtqp {
 
 constexpr int kSparseGridBlocks = 128;
 constexpr int kSparseGridNT = kSparseGridBlocks * kGridBT;
-constexpr int kSnMaxW = 64;             // widest supernode (the symbolic stage's cap)
+constexpr int kSnMaxW = kSnMaxWidth;    // widest supernode (the symbolic stage's cap)
 constexpr int kSnLd = kSnMaxW + 1;      // leading dimension of the diagonal block in smem
 constexpr int kSnStageK = 32;           // descendant columns staged per pass
 constexpr int kSnCg = 8;                // target columns per thread in an update pass
+constexpr int kSnSlab = kSnSlabRows;    // rows of a top-level supernode per work item
 // Dynamic shared memory of a block: the diagonal block, its reciprocal
 // diagonal, the staged descendant rows, and the partial sums of the solves.
 constexpr size_t kSparseSmemElems =
@@ -51,7 +56,7 @@ constexpr size_t kSparseSmem = kSparseSmemElems * sizeof(double);
 // and the factor's value storage.
 struct SnFactor {
   int n, nsuper, top_levels;
-  int64_t nvals, ngram;
+  int64_t nvals, ngram, nrows, nslabs;
   const int32_t* first;
   const int32_t* colsn;
   const int32_t* rows;
@@ -63,12 +68,15 @@ struct SnFactor {
   const int32_t* cta_range;
   const int32_t* top_ptr;
   const int32_t* top_list;
+  const int32_t* top_slab;  // prefix counts of row slabs over top_list (ntop + 1)
   const int32_t* gcol;
   const int32_t* grow;
   const int64_t* rowptr;
   const int64_t* valptr;
   const int64_t* gpos;
   double* vals;
+  double* zbuf;  // forward products per stored row (nrows)
+  double* pbuf;  // backward partial sums per top-level row slab (kSnMaxW each)
 };
 
 // Position of `key` in the sorted rows[0 .. len) (present by construction).
@@ -127,89 +135,132 @@ __device__ double sn_gram_entry(const S& s, int i, int j) {
   return acc;
 }
 
-// Left-looking factorisation of supernode `sn` by the calling block.
+// Updates of rows [r0, r1) of supernode sn's block from all its descendants
+// (the calling block): L_s[r, j] -= sum over the descendants d holding both
+// row R_s[r] and column f + j of L_d[row, :] . L_d[col, :].  Each thread owns
+// one target row and kSnCg target columns and walks the update list in order
+// (binary searches in the sorted structures find the row and the columns in
+// R_d), so no two threads write the same entry, the sum runs in a fixed
+// order, and no barrier separates the descendants.
 template <typename T>
-__device__ void sn_factor_one(const SnFactor& F, T* L, double* smem, int* info, int sn) {
+__device__ void sn_update_rows(const SnFactor& F, T* L, double* smem, int sn, int r0, int r1) {
+  (void)smem;
   const int t = threadIdx.x;
   const int f = F.first[sn], w = F.first[sn + 1] - f;
   const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
   const int32_t* R = F.rows + F.rowptr[sn];
   T* Ls = L + F.valptr[sn];
-  double* D = smem;                       // w x w (ld kSnLd)
-  double* rdiag = D + kSnMaxW * kSnLd;    // 1 / l_jj
-  double* C = rdiag + kSnMaxW;            // staged descendant rows (ld kSnStageK + 1)
-  constexpr int ldc = kSnStageK + 1;
-  // Updates from the descendants.
-  for (int u = F.upd_ptr[sn]; u < F.upd_ptr[sn + 1]; ++u) {
-    const int d = F.upd_src[u], off = F.upd_off[u], cnt = F.upd_cnt[u];
-    const int wd = F.first[d + 1] - F.first[d];
-    const int nrd = int(F.rowptr[d + 1] - F.rowptr[d]);
-    const int32_t* Rd = F.rows + F.rowptr[d];
-    const T* Ld = L + F.valptr[d];
-    const int rem = nrd - off;
-    const int ngrp = (cnt + kSnCg - 1) / kSnCg;
-    for (int k0 = 0; k0 < wd; k0 += kSnStageK) {
-      const int kc = min(kSnStageK, wd - k0);
-      for (int idx = t; idx < cnt * kc; idx += blockDim.x) {
-        const int c = idx % cnt, k = idx / cnt;
-        C[c * ldc + k] = double(Ld[size_t(off + c) + size_t(k0 + k) * nrd]);
-      }
-      __syncthreads();
-      for (int item = t; item < rem * ngrp; item += blockDim.x) {
-        const int r = item % rem, cg = item / rem;
-        const int row = off + r;
-        double acc[kSnCg];
+  const int u0 = F.upd_ptr[sn], u1 = F.upd_ptr[sn + 1];
+  const int ngrp = (w + kSnCg - 1) / kSnCg;
+  const int rows = r1 - r0;
+  for (int item = t; item < rows * ngrp; item += blockDim.x) {
+    const int r = r0 + item % rows, cg = item / rows;
+    const int key = R[r];
+    const int ck0 = f + cg * kSnCg, ck1 = min(ck0 + kSnCg, f + w);
+    if (key < ck0) continue;  // the block's upper triangle
+    double acc[kSnCg];
 #pragma unroll
-        for (int q = 0; q < kSnCg; ++q) acc[q] = 0.0;
-        const int c0 = cg * kSnCg;
-        for (int k = 0; k < kc; ++k) {
-          const double a = double(Ld[size_t(row) + size_t(k0 + k) * nrd]);
+    for (int q = 0; q < kSnCg; ++q) acc[q] = 0.0;
+    for (int u = u0; u < u1; ++u) {
+      const int off = F.upd_off[u], cnt = F.upd_cnt[u];
+      const int d = F.upd_src[u];
+      const int nrd = int(F.rowptr[d + 1] - F.rowptr[d]);
+      const int32_t* Rd = F.rows + F.rowptr[d] + off;
+      const int i = sn_find(Rd, nrd - off, key);
+      if (i >= nrd - off || Rd[i] != key) continue;
+      int c = sn_find(Rd, cnt, ck0);
+      const int c1 = sn_find(Rd, cnt, ck1);
+      if (c >= c1) continue;
+      const int wd = F.first[d + 1] - F.first[d];
+      const T* Ld = L + F.valptr[d] + off;
+      const T* Li = Ld + i;
 #pragma unroll
-          for (int q = 0; q < kSnCg; ++q)
-            if (c0 + q < cnt) acc[q] = fma(a, C[(c0 + q) * ldc + k], acc[q]);
-        }
-        const int pos = sn_find(R, nr, Rd[row]);
-#pragma unroll
-        for (int q = 0; q < kSnCg; ++q) {
-          const int c = c0 + q;
-          if (c < cnt) {
-            T* dst = Ls + size_t(pos) + size_t(Rd[off + c] - f) * nr;
-            *dst = T(double(*dst) - acc[q]);
-          }
+      for (int q = 0; q < kSnCg; ++q) {
+        if (c < c1 && Rd[c] == ck0 + q) {
+          const T* Lc = Ld + c;
+          double sum = 0.0;
+          for (int k = 0; k < wd; ++k)
+            sum = fma(double(Li[size_t(k) * nrd]), double(Lc[size_t(k) * nrd]), sum);
+          acc[q] += sum;
+          ++c;
         }
       }
-      __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < kSnCg; ++q) {
+      if (ck0 + q < ck1 && ck0 + q <= key) {
+        T* dst = Ls + size_t(r) + size_t(cg * kSnCg + q) * nr;
+        *dst = T(double(*dst) - acc[q]);
+      }
     }
   }
-  // Cholesky of the diagonal block (left-looking by columns).
+  __syncthreads();
+}
+
+// Cholesky of supernode sn's diagonal block (the calling block): the factor
+// goes back to L with 1 / l_jj on the diagonal, and stays in shared memory
+// (D, rdiag) for sn_panel_rows.
+template <typename T>
+__device__ void sn_diag(const SnFactor& F, T* L, double* smem, int* info, int sn) {
+  const int t = threadIdx.x;
+  const int f = F.first[sn], w = F.first[sn + 1] - f;
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  T* Ls = L + F.valptr[sn];
+  double* D = smem;                     // w x w (ld kSnLd)
+  double* rdiag = D + kSnMaxW * kSnLd;  // 1 / l_jj
   for (int idx = t; idx < w * w; idx += blockDim.x) {
     const int c = idx / w, r = idx % w;
     if (r >= c) D[r * kSnLd + c] = double(Ls[size_t(r) + size_t(c) * nr]);
   }
   __syncthreads();
-  for (int k = 0; k < w; ++k) {
-    for (int i = k + t; i < w; i += blockDim.x) {
-      double acc = D[i * kSnLd + k];
-      for (int p = 0; p < k; ++p) acc = fma(-D[i * kSnLd + p], D[k * kSnLd + p], acc);
-      D[i * kSnLd + k] = acc;
+  if (t < 32) {  // one warp, right-looking by columns (warp-synchronous)
+    for (int k = 0; k < w; ++k) {
+      const double dk = D[k * kSnLd + k];
+      const double rk = dk > 0.0 ? 1.0 / sqrt(dk) : __longlong_as_double(0x7ff8000000000000ll);
+      for (int i = k + 1 + t; i < w; i += 32) D[i * kSnLd + k] *= rk;
+      if (t == 0) {
+        rdiag[k] = rk;
+        if (!(dk > 0.0)) atomicCAS(info, 0, f + k + 1);
+      }
+      __syncwarp();
+      for (int i = k + 1 + t; i < w; i += 32) {
+        const double lik = D[i * kSnLd + k];
+        for (int j = k + 1; j <= i; ++j) D[i * kSnLd + j] = fma(-lik, D[j * kSnLd + k], D[i * kSnLd + j]);
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    const double dk = D[k * kSnLd + k];
-    const double rk = dk > 0.0 ? 1.0 / sqrt(dk) : __longlong_as_double(0x7ff8000000000000ll);
-    for (int i = k + 1 + t; i < w; i += blockDim.x) D[i * kSnLd + k] *= rk;
-    if (t == 0) {
-      rdiag[k] = rk;
-      if (!(dk > 0.0)) atomicCAS(info, 0, f + k + 1);
-    }
-    __syncthreads();
   }
+  __syncthreads();
   for (int idx = t; idx < w * w; idx += blockDim.x) {
     const int c = idx / w, r = idx % w;
     if (r > c) Ls[size_t(r) + size_t(c) * nr] = T(D[r * kSnLd + c]);
     if (r == c) Ls[size_t(r) + size_t(c) * nr] = T(rdiag[c]);
   }
-  // Rows below the block: x L_bb^T = a, forward substitution per row.
-  for (int r = w + t; r < nr; r += blockDim.x) {
+  __syncthreads();
+}
+
+// Rows [r0, r1) (all at or below the diagonal block) of supernode sn: the
+// triangular solve x L_bb^T = a, forward substitution per row.  load: read
+// the factored diagonal block back from L into shared memory first (another
+// block factored it).
+template <typename T>
+__device__ void sn_panel_rows(const SnFactor& F, T* L, double* smem, int sn, int r0, int r1,
+                              bool load) {
+  const int t = threadIdx.x;
+  const int w = F.first[sn + 1] - F.first[sn];
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  T* Ls = L + F.valptr[sn];
+  double* D = smem;
+  double* rdiag = D + kSnMaxW * kSnLd;
+  if (load) {
+    for (int idx = t; idx < w * w; idx += blockDim.x) {
+      const int c = idx / w, r = idx % w;
+      if (r > c) D[r * kSnLd + c] = double(Ls[size_t(r) + size_t(c) * nr]);
+      if (r == c) rdiag[c] = double(Ls[size_t(r) + size_t(c) * nr]);
+    }
+    __syncthreads();
+  }
+  for (int r = max(r0, w) + t; r < r1; r += blockDim.x) {
     for (int k = 0; k < w; ++k) {
       double acc = double(Ls[size_t(r) + size_t(k) * nr]);
       for (int p = 0; p < k; ++p)
@@ -220,16 +271,55 @@ __device__ void sn_factor_one(const SnFactor& F, T* L, double* smem, int* info, 
   __syncthreads();
 }
 
-// Forward solve of supernode `sn`: v[cols] -= L[cols, cols of descendants]
-// y, then y_cols = L_bb^{-1} v[cols].
+// Left-looking factorisation of supernode `sn` by the calling block alone.
 template <typename T>
-__device__ void sn_fwd_one(const SnFactor& F, const T* L, double* smem, T* v, int sn) {
+__device__ void sn_factor_one(const SnFactor& F, T* L, double* smem, int* info, int sn) {
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  sn_update_rows<T>(F, L, smem, sn, 0, nr);
+  sn_diag<T>(F, L, smem, info, sn);
+  sn_panel_rows<T>(F, L, smem, sn, 0, nr, false);
+}
+
+// The supernode and row range [r0, r1) of work item `item` of a top level
+// whose supernodes are top_list[q0 .. q1) and whose row slabs (kSnSlab rows
+// each) are numbered top_slab[q0] .. top_slab[q1] - 1.
+__device__ __forceinline__ void sn_slab_item(const SnFactor& F, int q0, int q1, int item,
+                                             int& sn, int& r0, int& r1) {
+  int lo = q0, hi = q1 - 1;  // the last q with top_slab[q] <= item
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (F.top_slab[mid] <= item) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  sn = F.top_list[lo];
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  r0 = (item - F.top_slab[lo]) * kSnSlab;
+  r1 = min(nr, r0 + kSnSlab);
+}
+
+// Forward solve, step 1 for supernode `sn` (the calling block): v[cols] -=
+// the products z of its descendants with the rows in its columns (z_d[r] =
+// L_d[r, :] y_d, stored per row of R_d by step 2), then y_cols = L_bb^{-1}
+// v[cols] on one warp with the diagonal block in shared memory.  The
+// contributions are summed in a fixed order (thread groups over the update
+// list, then the groups in turn), so the result does not depend on timing.
+template <typename T>
+__device__ void sn_fwd_diag(const SnFactor& F, const T* L, double* smem, const double* z, T* v,
+                            int sn) {
   const int t = threadIdx.x;
   const int f = F.first[sn], w = F.first[sn + 1] - f;
   const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
   const T* Ls = L + F.valptr[sn];
+  double* D = smem;  // the diagonal block (factor, 1 / l_jj on the diagonal)
   double* part = smem + kSnMaxW * kSnLd + kSnMaxW + kSnMaxW * (kSnStageK + 1);
   double* yb = part + kGridBT;
+  for (int idx = t; idx < w * w; idx += blockDim.x) {
+    const int c = idx / w, r = idx % w;
+    if (r >= c) D[r * kSnLd + c] = double(Ls[size_t(r) + size_t(c) * nr]);
+  }
   const int W32 = w <= 32 ? 32 : 64;
   const int G = blockDim.x / W32;
   const int j = t % W32, g = t / W32;
@@ -237,23 +327,17 @@ __device__ void sn_fwd_one(const SnFactor& F, const T* L, double* smem, T* v, in
   if (j < w) {
     for (int u = F.upd_ptr[sn] + g; u < F.upd_ptr[sn + 1]; u += G) {
       const int d = F.upd_src[u], off = F.upd_off[u], cnt = F.upd_cnt[u];
-      const int fd = F.first[d], wd = F.first[d + 1] - fd;
-      const int nrd = int(F.rowptr[d + 1] - F.rowptr[d]);
       const int32_t* Rd = F.rows + F.rowptr[d] + off;
       const int c = sn_find(Rd, cnt, f + j);
-      if (c < cnt && Rd[c] == f + j) {
-        const T* Ld = L + F.valptr[d] + off + c;
-        for (int k = 0; k < wd; ++k)
-          acc = fma(double(Ld[size_t(k) * nrd]), double(v[fd + k]), acc);
-      }
+      if (c < cnt && Rd[c] == f + j) acc += z[F.rowptr[d] + off + c];
     }
   }
   part[t] = acc;
   __syncthreads();
   if (t < w) {
-    double b = double(v[f + t]);
-    for (int q = 0; q < G; ++q) b -= part[q * W32 + t];
-    yb[t] = b;
+    double bv = double(v[f + t]);
+    for (int q = 0; q < G; ++q) bv -= part[q * W32 + t];
+    yb[t] = bv;
   }
   __syncthreads();
   if (t < 32) {  // one warp: lane l holds rows l and l + 32
@@ -261,7 +345,7 @@ __device__ void sn_fwd_one(const SnFactor& F, const T* L, double* smem, T* v, in
     double r1 = t + 32 < w ? yb[t + 32] : 0.0;
     for (int k = 0; k < w; ++k) {
       const double mine = k < 32 ? r0 : r1;
-      const double yk = __shfl_sync(0xffffffffu, mine, k & 31) * double(Ls[size_t(k) * nr + k]);
+      const double yk = __shfl_sync(0xffffffffu, mine, k & 31) * D[k * kSnLd + k];
       if (t == (k & 31)) {
         if (k < 32) {
           r0 = yk;
@@ -269,32 +353,86 @@ __device__ void sn_fwd_one(const SnFactor& F, const T* L, double* smem, T* v, in
           r1 = yk;
         }
       }
-      if (t > k && t < w) r0 = fma(-double(Ls[size_t(t) + size_t(k) * nr]), yk, r0);
-      if (t + 32 > k && t + 32 < w) r1 = fma(-double(Ls[size_t(t + 32) + size_t(k) * nr]), yk, r1);
+      if (t > k && t < w) r0 = fma(-D[t * kSnLd + k], yk, r0);
+      if (t + 32 > k && t + 32 < w) r1 = fma(-D[(t + 32) * kSnLd + k], yk, r1);
     }
-    if (t < w) v[f + t] = T(r0);
-    if (t + 32 < w) v[f + t + 32] = T(r1);
+    if (t < w) {
+      v[f + t] = T(r0);
+      yb[t] = r0;
+    }
+    if (t + 32 < w) {
+      v[f + t + 32] = T(r1);
+      yb[t + 32] = r1;
+    }
   }
   __syncthreads();
 }
 
-// Backward solve of supernode `sn`: v[cols] -= L[below, cols]^T x[R below],
-// then x_cols = L_bb^{-T} v[cols].
+// Forward solve, step 2: z[r] = L_s[r, :] y_s for the rows [r0, r1) of
+// supernode sn below its diagonal block.  y_s is read from v (from_smem:
+// from the yb slots that sn_fwd_diag of this block left in shared memory).
 template <typename T>
-__device__ void sn_bwd_one(const SnFactor& F, const T* L, double* smem, T* v, int sn) {
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarp = blockDim.x >> 5;
+__device__ void sn_fwd_rows(const SnFactor& F, const T* L, double* smem, double* z, const T* v,
+                            int sn, int r0, int r1, bool from_smem) {
+  const int t = threadIdx.x;
   const int f = F.first[sn], w = F.first[sn + 1] - f;
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  const T* Ls = L + F.valptr[sn];
+  double* yb = smem + kSnMaxW * kSnLd + kSnMaxW + kSnMaxW * (kSnStageK + 1) + kGridBT;
+  if (!from_smem) {
+    for (int k = t; k < w; k += blockDim.x) yb[k] = double(v[f + k]);
+    __syncthreads();
+  }
+  double* zs = z + F.rowptr[sn];
+  for (int r = max(r0, w) + t; r < r1; r += blockDim.x) {
+    double acc = 0.0;
+    for (int k = 0; k < w; ++k) acc = fma(double(Ls[size_t(r) + size_t(k) * nr]), yb[k], acc);
+    zs[r] = acc;
+  }
+  __syncthreads();
+}
+
+// Backward solve, step 1: partial sums p[j] = sum_{r in [r0, r1), r >= w}
+// L_s[r, j] x[R_s[r]] of supernode sn (the calling block), to `out` (w
+// values).
+template <typename T>
+__device__ void sn_bwd_rows(const SnFactor& F, const T* L, const T* v, int sn, int r0, int r1,
+                            double* out) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarp = blockDim.x >> 5;
+  const int w = F.first[sn + 1] - F.first[sn];
   const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
   const int32_t* R = F.rows + F.rowptr[sn];
   const T* Ls = L + F.valptr[sn];
-  double* yb = smem + kSnMaxW * kSnLd + kSnMaxW + kSnMaxW * (kSnStageK + 1) + kGridBT;
   for (int j = warp; j < w; j += nwarp) {
     double acc = 0.0;
-    for (int r = w + lane; r < nr; r += 32)
+    for (int r = max(r0, w) + lane; r < r1; r += 32)
       acc = fma(double(Ls[size_t(r) + size_t(j) * nr]), double(v[R[r]]), acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) yb[j] = double(v[f + j]) - acc;
+    if (lane == 0) out[j] = acc;
+  }
+  __syncthreads();
+}
+
+// Backward solve, step 2: y_cols = v[cols] - (the partial sums of parts
+// slabs, in order), then x_cols = L_bb^{-T} y_cols on one warp.
+template <typename T>
+__device__ void sn_bwd_diag(const SnFactor& F, const T* L, double* smem, const double* parts,
+                            int nparts, T* v, int sn) {
+  const int t = threadIdx.x;
+  const int f = F.first[sn], w = F.first[sn + 1] - f;
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  const T* Ls = L + F.valptr[sn];
+  double* D = smem;
+  double* yb = smem + kSnMaxW * kSnLd + kSnMaxW + kSnMaxW * (kSnStageK + 1) + kGridBT;
+  for (int idx = t; idx < w * w; idx += blockDim.x) {
+    const int c = idx / w, r = idx % w;
+    if (r >= c) D[r * kSnLd + c] = double(Ls[size_t(r) + size_t(c) * nr]);
+  }
+  if (t < w) {
+    double bv = double(v[f + t]);
+    for (int q = 0; q < nparts; ++q) bv -= parts[q * kSnMaxW + t];
+    yb[t] = bv;
   }
   __syncthreads();
   if (t < 32) {
@@ -302,7 +440,7 @@ __device__ void sn_bwd_one(const SnFactor& F, const T* L, double* smem, T* v, in
     double r1 = t + 32 < w ? yb[t + 32] : 0.0;
     for (int k = w - 1; k >= 0; --k) {
       const double mine = k < 32 ? r0 : r1;
-      const double xk = __shfl_sync(0xffffffffu, mine, k & 31) * double(Ls[size_t(k) * nr + k]);
+      const double xk = __shfl_sync(0xffffffffu, mine, k & 31) * D[k * kSnLd + k];
       if (t == (k & 31)) {
         if (k < 32) {
           r0 = xk;
@@ -311,8 +449,8 @@ __device__ void sn_bwd_one(const SnFactor& F, const T* L, double* smem, T* v, in
         }
       }
       // rows j < k: v_j -= L[k][j] x_k
-      if (t < k) r0 = fma(-double(Ls[size_t(k) + size_t(t) * nr]), xk, r0);
-      if (t + 32 < k) r1 = fma(-double(Ls[size_t(k) + size_t(t + 32) * nr]), xk, r1);
+      if (t < k) r0 = fma(-D[k * kSnLd + t], xk, r0);
+      if (t + 32 < k) r1 = fma(-D[k * kSnLd + t + 32], xk, r1);
     }
     if (t < w) v[f + t] = T(r0);
     if (t + 32 < w) v[f + t + 32] = T(r1);
@@ -356,12 +494,36 @@ __device__ int sparse_factorize(S& s) {
     for (int sn = F.cta_range[2 * q]; sn <= F.cta_range[2 * q + 1]; ++sn)
       sn_factor_one<T>(F, L, smem, s.linfo, sn);
   s.sync();
+  QTQP_TOC(kPhSnSub);
+  QTQP_RETIC();
+  // Above the subtrees, each level in three steps over the whole grid: the
+  // updates of every row slab, the diagonal blocks, the rows below them.
   for (int l = 0; l < F.top_levels; ++l) {
-    for (int q = F.top_ptr[l] + b; q < F.top_ptr[l + 1]; q += gridDim.x)
-      sn_factor_one<T>(F, L, smem, s.linfo, F.top_list[q]);
+    const int q0 = F.top_ptr[l], q1 = F.top_ptr[l + 1];
+    const int items = F.top_slab[q1] - F.top_slab[q0];
+    QTQP_TIC();
+    for (int it = b; it < items; it += gridDim.x) {
+      int sn, r0, r1;
+      sn_slab_item(F, q0, q1, F.top_slab[q0] + it, sn, r0, r1);
+      sn_update_rows<T>(F, L, smem, sn, r0, r1);
+    }
     s.sync();
+    QTQP_TOC(kPhSnTopUpd);
+    QTQP_RETIC();
+    for (int q = q0 + b; q < q1; q += gridDim.x) sn_diag<T>(F, L, smem, s.linfo, F.top_list[q]);
+    s.sync();
+    QTQP_TOC(kPhSnTopDiag);
+    QTQP_RETIC();
+    for (int it = b; it < items; it += gridDim.x) {
+      int sn, r0, r1;
+      sn_slab_item(F, q0, q1, F.top_slab[q0] + it, sn, r0, r1);
+      const int w = F.first[sn + 1] - F.first[sn];
+      if (r1 > w) sn_panel_rows<T>(F, L, smem, sn, r0, r1, true);
+    }
+    s.sync();
+    QTQP_TOC(kPhSnTopPanel);
   }
-  QTQP_TOC(kPhChol);
+  QTQP_TOC(kPhSnTop);
   return *reinterpret_cast<volatile int*>(s.linfo);
 }
 
@@ -371,27 +533,63 @@ __device__ void sparse_solve(S& s, T* v, T* w) {
   const SnFactor& F = *s.sn;
   const T* L = reinterpret_cast<const T*>(F.vals);
   double* smem = s.bwin;
+  double* z = F.zbuf;
+  double* parts = F.pbuf;
   const int b = blockIdx.x;
   QTQP_TIC();
+  // Forward: the blocks' subtrees, then the top levels (the diagonal solves,
+  // then every row slab's products).
   for (int q = F.cta_ptr[b]; q < F.cta_ptr[b + 1]; ++q)
-    for (int sn = F.cta_range[2 * q]; sn <= F.cta_range[2 * q + 1]; ++sn)
-      sn_fwd_one<T>(F, L, smem, v, sn);
+    for (int sn = F.cta_range[2 * q]; sn <= F.cta_range[2 * q + 1]; ++sn) {
+      sn_fwd_diag<T>(F, L, smem, z, v, sn);
+      sn_fwd_rows<T>(F, L, smem, z, v, sn, 0, int(F.rowptr[sn + 1] - F.rowptr[sn]), true);
+    }
   s.sync();
+  QTQP_TOC(kPhSnFwdSub);
+  QTQP_RETIC();
   for (int l = 0; l < F.top_levels; ++l) {
-    for (int q = F.top_ptr[l] + b; q < F.top_ptr[l + 1]; q += gridDim.x)
-      sn_fwd_one<T>(F, L, smem, v, F.top_list[q]);
+    const int q0 = F.top_ptr[l], q1 = F.top_ptr[l + 1];
+    for (int q = q0 + b; q < q1; q += gridDim.x) sn_fwd_diag<T>(F, L, smem, z, v, F.top_list[q]);
     s.sync();
+    if (l + 1 < F.top_levels) {  // the last level's products have no reader
+      const int items = F.top_slab[q1] - F.top_slab[q0];
+      for (int it = b; it < items; it += gridDim.x) {
+        int sn, r0, r1;
+        sn_slab_item(F, q0, q1, F.top_slab[q0] + it, sn, r0, r1);
+        const int w = F.first[sn + 1] - F.first[sn];
+        if (r1 > w) sn_fwd_rows<T>(F, L, smem, z, v, sn, r0, r1, false);
+      }
+      s.sync();
+    }
   }
+  QTQP_TOC(kPhSnFwdTop);
+  QTQP_RETIC();
+  // Backward: the top levels in reverse (every row slab's partial sums, then
+  // the diagonal solves), then the subtrees in reverse.
   for (int l = F.top_levels - 1; l >= 0; --l) {
-    for (int q = F.top_ptr[l] + b; q < F.top_ptr[l + 1]; q += gridDim.x)
-      sn_bwd_one<T>(F, L, smem, v, F.top_list[q]);
+    const int q0 = F.top_ptr[l], q1 = F.top_ptr[l + 1];
+    const int items = F.top_slab[q1] - F.top_slab[q0];
+    for (int it = b; it < items; it += gridDim.x) {
+      int sn, r0, r1;
+      sn_slab_item(F, q0, q1, F.top_slab[q0] + it, sn, r0, r1);
+      sn_bwd_rows<T>(F, L, v, sn, r0, r1, parts + size_t(F.top_slab[q0] + it) * kSnMaxW);
+    }
+    s.sync();
+    for (int q = q0 + b; q < q1; q += gridDim.x)
+      sn_bwd_diag<T>(F, L, smem, parts + size_t(F.top_slab[q]) * kSnMaxW,
+                     F.top_slab[q + 1] - F.top_slab[q], v, F.top_list[q]);
     s.sync();
   }
+  QTQP_TOC(kPhSnBwdTop);
+  QTQP_RETIC();
+  double* own = smem + kSnMaxW * kSnLd + kSnMaxW;  // one partial row (the staging area)
   for (int q = F.cta_ptr[b + 1] - 1; q >= F.cta_ptr[b]; --q)
-    for (int sn = F.cta_range[2 * q + 1]; sn >= F.cta_range[2 * q]; --sn)
-      sn_bwd_one<T>(F, L, smem, v, sn);
+    for (int sn = F.cta_range[2 * q + 1]; sn >= F.cta_range[2 * q]; --sn) {
+      sn_bwd_rows<T>(F, L, v, sn, 0, int(F.rowptr[sn + 1] - F.rowptr[sn]), own);
+      sn_bwd_diag<T>(F, L, smem, own, 1, v, sn);
+    }
   s.sync();
-  QTQP_TOC(kPhSolve);
+  QTQP_TOC(kPhSnBwdSub);
 }
 
 }  // namespace qtqp

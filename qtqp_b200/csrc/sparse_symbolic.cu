@@ -44,8 +44,6 @@ namespace qtqp {
 
 namespace {
 
-constexpr int kSnMaxWidth = 64;  // widest supernode (the diagonal block stays in shared memory)
-
 using Adj = std::vector<std::vector<int>>;
 
 // ----------------------------------------------------------------------------
@@ -252,7 +250,7 @@ struct Plan {
   std::vector<int32_t> first, rows, colsn;
   std::vector<int64_t> rowptr, valptr;
   std::vector<int32_t> upd_ptr, upd_src, upd_off, upd_cnt;
-  std::vector<int32_t> cta_ptr, cta_range, top_ptr, top_list;
+  std::vector<int32_t> cta_ptr, cta_range, top_ptr, top_list, top_slab;
   std::vector<int32_t> gcol, grow;
   std::vector<int64_t> gpos;
   int max_rows = 0, max_width = 0, tree_levels = 0;
@@ -650,6 +648,13 @@ static int build_plan(int n, int m, const int32_t* ap, const int32_t* ai, const 
     for (int s = 0; s < S; ++s)
       if (top[s]) P.top_list[fl[tlev[s]]++] = s;
   }
+  // Row slabs of the top supernodes (work items of the grid), prefix counts.
+  P.top_slab.assign(P.top_list.size() + 1, 0);
+  for (size_t q = 0; q < P.top_list.size(); ++q) {
+    const int s = P.top_list[q];
+    const int nr = int(P.rowptr[s + 1] - P.rowptr[s]);
+    P.top_slab[q + 1] = P.top_slab[q] + (nr + kSnSlabRows - 1) / kSnSlabRows;
+  }
   // G's lower entries (diagonal first in each column) and their positions.
   for (int j = 0; j < n; ++j) {
     const int s = P.colsn[j];
@@ -720,6 +725,7 @@ extern "C" int qtqp_sparse_analyze(int32_t n, int32_t m, const int32_t* h_a_colp
   d.nranges = int64_t(P->cta_range.size() / 2);
   d.ntop = int64_t(P->top_list.size());
   d.nnz_l = P->nnz_l;
+  d.top_row_slabs = P->top_slab.back();
   d.flops = P->flops;
   int64_t o = 0;
   auto put = [&](int64_t& off, size_t count) {
@@ -737,6 +743,7 @@ extern "C" int qtqp_sparse_analyze(int32_t n, int32_t m, const int32_t* h_a_colp
   put(d.o_cta_range, P->cta_range.size());
   put(d.o_top_ptr, P->top_ptr.size());
   put(d.o_top_list, P->top_list.size());
+  put(d.o_top_slab, P->top_slab.size());
   put(d.o_gcol, P->gcol.size());
   put(d.o_grow, P->grow.size());
   d.n32 = o;
@@ -782,6 +789,7 @@ extern "C" int qtqp_sparse_export(const void* h_plan, const qtqp_sparse_desc* h_
   cp(d.o_cta_range, P.cta_range);
   cp(d.o_top_ptr, P.top_ptr);
   cp(d.o_top_list, P.top_list);
+  cp(d.o_top_slab, P.top_slab);
   cp(d.o_gcol, P.gcol);
   cp(d.o_grow, P.grow);
   cp64(d.o_rowptr, P.rowptr);

@@ -81,7 +81,8 @@ class SparsePlan:
     sizes = {"first": d.nsuper + 1, "colsn": d.n, "rows": d.nrows, "upd_ptr": d.nsuper + 1,
              "upd_src": d.nupd, "upd_off": d.nupd, "upd_cnt": d.nupd,
              "cta_ptr": d.blocks + 1, "cta_range": 2 * d.nranges,
-             "top_ptr": d.top_levels + 1, "top_list": d.ntop, "gcol": d.ngram,
+             "top_ptr": d.top_levels + 1, "top_list": d.ntop, "top_slab": d.ntop + 1,
+             "gcol": d.ngram,
              "grow": d.ngram, "rowptr": d.nsuper + 1, "valptr": d.nsuper + 1,
              "gpos": d.ngram}
     off = int(getattr(d, "o_" + name))

@@ -29,6 +29,7 @@ WORKLOADS = {
     "dense_large": ["--workload", "dense_large", "--large-n", "64"],
     "mpc": ["--workload", "mpc", "--mpc-horizon", "20"],
     "parametric": ["--workload", "parametric", "--train", "64", "--count", "16"],
+    "sparse": ["--workload", "sparse", "--grid", "8"],
 }
 
 

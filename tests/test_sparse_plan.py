@@ -106,6 +106,10 @@ def test_update_lists_and_schedule(case):
       seen[s] += 1
       when[s] = lvl
   assert np.all(seen == 1)
+  slab = plan.section("top_slab")  # row slabs (64 rows) of the top supernodes, prefix counts
+  assert slab[0] == 0 and slab.size == top_list.size + 1
+  for q, s in enumerate(top_list):
+    assert slab[q + 1] - slab[q] == -(-(rowptr[s + 1] - rowptr[s]) // 64)
   for s in range(ns):
     if parent[s] >= 0 and when[parent[s]] >= 0 and when[s] >= 0:
       assert when[s] < when[parent[s]]
