@@ -24,6 +24,10 @@ from . import batch as _batch
 
 CANDIDATES = [(nt, lean, onchip) for nt in (64, 128, 256) for lean in (0, 1)
               for onchip in (0, 1)]
+# Single-warp blocks (barriers become warp syncs) are tried for the classes of
+# small QPs only, where one warp has enough work.
+SMALL_N = 32
+SMALL_CANDIDATES = [(32, lean, onchip) for lean in (0, 1) for onchip in (0, 1)]
 
 
 def cache_path() -> str:
@@ -73,7 +77,8 @@ def tune_dense_batch(problems, opts: _batch.SolveOptions | None = None, candidat
     ids = hb.order[grp.begin:grp.begin + grp.count]
     status_ref = db.fetch()[0]["status"][ids].copy()
     best = (t_default, None)
-    for nt, lean, onchip in (candidates or CANDIDATES):
+    cands = candidates or (CANDIDATES + (SMALL_CANDIDATES if n_hi <= SMALL_N else []))
+    for nt, lean, onchip in cands:
       entry = {"n_lo": n_lo, "n_hi": n_hi, "block_threads": nt, "lean": lean,
                "onchip": onchip}
       hb.replan([entry])

@@ -470,76 +470,82 @@ __device__ int large_cholesky(S& s, T* g) {
   if (s.tid == 0) *info = 0;
   s.sync();
   QTQP_TIC();
+  // (a) Factor the diagonal block starting at column k0 (the calling CTA):
+  // in shared memory, 32 columns at a time, then back to g with the four
+  // 32 x 32 sub-block inverses (also to global memory, for the panel step).
+  auto factor_diag = [&](int k0) {
+    QTQP_TIC();
+    stage_block(sm, g, npad, k0, k0, true);
+    __syncthreads();
+    QTQP_TOC(kPhNormalize);
+    int bad = 0;
+    for (int q = 0; q < 4 && !bad; ++q) {
+      const int o = 32 * q;
+      QTQP_RETIC();
+      if (warp == 0) {
+        const int b = warp_chol32(sm, o, sinv + q * 32 * kSubPitch, lane);
+        if (lane == 0) *sflag = b ? o + b : 0;
+      }
+      __syncthreads();
+      QTQP_TOC(kPhStep);
+      QTQP_RETIC();
+      bad = *sflag;
+      if (bad) break;
+      // Rows below the sub-block: x = row inv(L_qq)^T (thread per row).
+      const T* iq = sinv + q * 32 * kSubPitch;
+      const int rows = kLB - o - 32;
+      if (int(threadIdx.x) < rows) {
+        T* row = sm + (o + 32 + threadIdx.x) * kPitch + o;
+        T v[32];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) v[l] = row[l];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          T acc = T(0);
+#pragma unroll
+          for (int l = 0; l <= j; ++l) acc = fma(v[l], iq[j * kSubPitch + l], acc);
+          row[j] = acc;
+        }
+      }
+      __syncthreads();
+      // Trailing lower part of the block: a_ij -= sum_l a_il a_jl.
+      const int t0 = o + 32, tn = kLB - t0, cnt = tn * (tn + 1) / 2;
+      for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        int i = int((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+        while (i * (i + 1) / 2 > e) --i;
+        while ((i + 1) * (i + 2) / 2 <= e) ++i;
+        const int j = e - i * (i + 1) / 2;
+        const T* ri = sm + (t0 + i) * kPitch + o;
+        const T* rj = sm + (t0 + j) * kPitch + o;
+        T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+        for (int l = 0; l < 32; l += 2) {
+          acc0 = fma(ri[l], rj[l], acc0);
+          acc1 = fma(ri[l + 1], rj[l + 1], acc1);
+        }
+        sm[(t0 + i) * kPitch + t0 + j] -= acc0 + acc1;
+      }
+      __syncthreads();
+      QTQP_TOC(kPhOther);
+    }
+    if (bad) {
+      if (threadIdx.x == 0) atomicCAS(info, 0, k0 + bad);
+    } else {
+      for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
+        const int r = e >> 7, c = e & 127;
+        if (c <= r) g[size_t(k0 + r) * npad + k0 + c] = sm[r * kPitch + c];
+      }
+      for (int e = threadIdx.x; e < 4 * 32 * kSubPitch; e += blockDim.x) ginv[e] = sinv[e];
+    }
+    __syncthreads();
+  };
   for (int k = 0; k < nblk; ++k) {
     const int k0 = k * kLB;
     QTQP_RETIC();
-    // (a) diagonal block.
-    if (int(blockIdx.x) == k % int(gridDim.x)) {
-      QTQP_TIC();
-      stage_block(sm, g, npad, k0, k0, true);
-      __syncthreads();
-      QTQP_TOC(kPhNormalize);
-      int bad = 0;
-      for (int q = 0; q < 4 && !bad; ++q) {
-        const int o = 32 * q;
-        QTQP_RETIC();
-        if (warp == 0) {
-          const int b = warp_chol32(sm, o, sinv + q * 32 * kSubPitch, lane);
-          if (lane == 0) *sflag = b ? o + b : 0;
-        }
-        __syncthreads();
-        QTQP_TOC(kPhStep);
-        QTQP_RETIC();
-        bad = *sflag;
-        if (bad) break;
-        // Rows below the sub-block: x = row inv(L_qq)^T (thread per row).
-        const T* iq = sinv + q * 32 * kSubPitch;
-        const int rows = kLB - o - 32;
-        if (int(threadIdx.x) < rows) {
-          T* row = sm + (o + 32 + threadIdx.x) * kPitch + o;
-          T v[32];
-#pragma unroll
-          for (int l = 0; l < 32; ++l) v[l] = row[l];
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            T acc = T(0);
-#pragma unroll
-            for (int l = 0; l <= j; ++l) acc = fma(v[l], iq[j * kSubPitch + l], acc);
-            row[j] = acc;
-          }
-        }
-        __syncthreads();
-        // Trailing lower part of the block: a_ij -= sum_l a_il a_jl.
-        const int t0 = o + 32, tn = kLB - t0, cnt = tn * (tn + 1) / 2;
-        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-          int i = int((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
-          while (i * (i + 1) / 2 > e) --i;
-          while ((i + 1) * (i + 2) / 2 <= e) ++i;
-          const int j = e - i * (i + 1) / 2;
-          const T* ri = sm + (t0 + i) * kPitch + o;
-          const T* rj = sm + (t0 + j) * kPitch + o;
-          T acc0 = T(0), acc1 = T(0);
-#pragma unroll
-          for (int l = 0; l < 32; l += 2) {
-            acc0 = fma(ri[l], rj[l], acc0);
-            acc1 = fma(ri[l + 1], rj[l + 1], acc1);
-          }
-          sm[(t0 + i) * kPitch + t0 + j] -= acc0 + acc1;
-        }
-        __syncthreads();
-        QTQP_TOC(kPhOther);
-      }
-      if (bad) {
-        if (threadIdx.x == 0) atomicCAS(info, 0, k0 + bad);
-      } else {
-        for (int e = threadIdx.x; e < kLB * kLB; e += blockDim.x) {
-          const int r = e >> 7, c = e & 127;
-          if (c <= r) g[size_t(k0 + r) * npad + k0 + c] = sm[r * kPitch + c];
-        }
-        for (int e = threadIdx.x; e < 4 * 32 * kSubPitch; e += blockDim.x) ginv[e] = sinv[e];
-      }
-    }
-    s.sync();
+    // (a) diagonal block: only for the first one; every later one is
+    // factored during the previous step's trailing update (lookahead).
+    if (k == 0 && blockIdx.x == 0) factor_diag(k0);
+    if (k == 0) s.sync();
     QTQP_TOC(kPhLgDiag);
     QTQP_RETIC();
     if (*reinterpret_cast<volatile int*>(info) != 0) break;
@@ -602,7 +608,13 @@ __device__ int large_cholesky(S& s, T* g) {
         }
         cp_async_commit();
       };
-      for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+      // Lookahead: the CTA that owns the next diagonal block updates tile 0
+      // (that block) first and factors it at once; the other tiles go round
+      // robin over the other CTAs.
+      const int G = int(gridDim.x), owner = (k + 1) % G, me = int(blockIdx.x);
+      const int first_t = me == owner ? 0 : 1 + (me - owner - 1 + G) % G;
+      const int step_t = me == owner ? tiles : G - 1;
+      for (int t = first_t; t < tiles; t += (t == 0 ? tiles : step_t)) {
         int ti = 0;
         while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
         const int tj = t - ti * (ti + 1) / 2;
@@ -685,6 +697,10 @@ __device__ int large_cholesky(S& s, T* g) {
               if (j <= i) g[size_t(i) * npad + j] -= acc[a][b];
             }
           }
+        }
+        if (t == 0) {  // the next diagonal block is final: factor it now
+          __syncthreads();
+          factor_diag(base);
         }
       }
     }

@@ -135,16 +135,17 @@ __device__ double sn_gram_entry(const S& s, int i, int j) {
   return acc;
 }
 
-// Updates of rows [r0, r1) of supernode sn's block from all its descendants
-// (the calling block): L_s[r, j] -= sum over the descendants d holding both
-// row R_s[r] and column f + j of L_d[row, :] . L_d[col, :].  Each thread owns
-// one target row and kSnCg target columns and walks the update list in order
-// (binary searches in the sorted structures find the row and the columns in
-// R_d), so no two threads write the same entry, the sum runs in a fixed
-// order, and no barrier separates the descendants.
+// Updates of rows [r0, r1) (at most kSnSlab of them) of supernode sn's block
+// from all its descendants (the calling block): L_s[r, j] -= the sum, over
+// the descendants d holding both row R_s[r] and column f + j, of
+// L_d[row, :] . L_d[col, :].  Each thread owns up to two (target row, kSnCg
+// target columns) items and keeps their sums in registers while the block
+// walks the update list in order: per descendant, the rows of R_d inside the
+// slab (a range found by two binary searches, the same in every thread), then
+// each item's row and columns in it.  No two threads write the same entry,
+// every sum runs in a fixed order, and no barrier separates the descendants.
 template <typename T>
-__device__ void sn_update_rows(const SnFactor& F, T* L, double* smem, int sn, int r0, int r1) {
-  (void)smem;
+__device__ void sn_update_slab(const SnFactor& F, T* L, int sn, int r0, int r1) {
   const int t = threadIdx.x;
   const int f = F.first[sn], w = F.first[sn + 1] - f;
   const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
@@ -153,48 +154,76 @@ __device__ void sn_update_rows(const SnFactor& F, T* L, double* smem, int sn, in
   const int u0 = F.upd_ptr[sn], u1 = F.upd_ptr[sn + 1];
   const int ngrp = (w + kSnCg - 1) / kSnCg;
   const int rows = r1 - r0;
-  for (int item = t; item < rows * ngrp; item += blockDim.x) {
-    const int r = r0 + item % rows, cg = item / rows;
-    const int key = R[r];
-    const int ck0 = f + cg * kSnCg, ck1 = min(ck0 + kSnCg, f + w);
-    if (key < ck0) continue;  // the block's upper triangle
-    double acc[kSnCg];
+  const int lo_key = R[r0], hi_key = R[r1 - 1];
+  constexpr int kItems = kSnSlab * ((kSnMaxW + kSnCg - 1) / kSnCg) / kGridBT;
+  static_assert(kItems * kGridBT >= kSnSlab * ((kSnMaxW + kSnCg - 1) / kSnCg), "items");
+  int key[kItems], ck0[kItems], ck1[kItems];
+  double acc[kItems][kSnCg];
 #pragma unroll
-    for (int q = 0; q < kSnCg; ++q) acc[q] = 0.0;
-    for (int u = u0; u < u1; ++u) {
-      const int off = F.upd_off[u], cnt = F.upd_cnt[u];
-      const int d = F.upd_src[u];
-      const int nrd = int(F.rowptr[d + 1] - F.rowptr[d]);
-      const int32_t* Rd = F.rows + F.rowptr[d] + off;
-      const int i = sn_find(Rd, nrd - off, key);
-      if (i >= nrd - off || Rd[i] != key) continue;
-      int c = sn_find(Rd, cnt, ck0);
-      const int c1 = sn_find(Rd, cnt, ck1);
-      if (c >= c1) continue;
-      const int wd = F.first[d + 1] - F.first[d];
-      const T* Ld = L + F.valptr[d] + off;
+  for (int it = 0; it < kItems; ++it) {
+    const int item = t + it * kGridBT;
+    key[it] = -1;
+    if (item < rows * ngrp) {
+      const int r = r0 + item % rows, cg = item / rows;
+      ck0[it] = f + cg * kSnCg;
+      ck1[it] = min(ck0[it] + kSnCg, f + w);
+      if (R[r] >= ck0[it]) key[it] = R[r];  // else entirely in the upper triangle
+    }
+#pragma unroll
+    for (int q = 0; q < kSnCg; ++q) acc[it][q] = 0.0;
+  }
+  for (int u = u0; u < u1; ++u) {
+    const int off = F.upd_off[u], cnt = F.upd_cnt[u];
+    const int d = F.upd_src[u];
+    const int nrd = int(F.rowptr[d + 1] - F.rowptr[d]);
+    const int32_t* Rd = F.rows + F.rowptr[d] + off;
+    const int a = sn_find(Rd, nrd - off, lo_key);
+    const int b = sn_find(Rd, nrd - off, hi_key + 1);
+    if (a >= b) continue;  // none of d's rows in this slab
+    const int wd = F.first[d + 1] - F.first[d];
+    const T* Ld = L + F.valptr[d] + off;
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      if (key[it] < 0) continue;
+      const int i = a + sn_find(Rd + a, b - a, key[it]);
+      if (i >= b || Rd[i] != key[it]) continue;
+      int c = sn_find(Rd, cnt, ck0[it]);
+      const int c1 = sn_find(Rd, cnt, ck1[it]);
       const T* Li = Ld + i;
 #pragma unroll
       for (int q = 0; q < kSnCg; ++q) {
-        if (c < c1 && Rd[c] == ck0 + q) {
+        if (c < c1 && Rd[c] == ck0[it] + q) {
           const T* Lc = Ld + c;
           double sum = 0.0;
           for (int k = 0; k < wd; ++k)
             sum = fma(double(Li[size_t(k) * nrd]), double(Lc[size_t(k) * nrd]), sum);
-          acc[q] += sum;
+          acc[it][q] += sum;
           ++c;
         }
       }
     }
+  }
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    if (key[it] < 0) continue;
+    const int item = t + it * kGridBT;
+    const int r = r0 + item % rows, cg = item / rows;
 #pragma unroll
     for (int q = 0; q < kSnCg; ++q) {
-      if (ck0 + q < ck1 && ck0 + q <= key) {
+      if (ck0[it] + q < ck1[it] && ck0[it] + q <= key[it]) {
         T* dst = Ls + size_t(r) + size_t(cg * kSnCg + q) * nr;
-        *dst = T(double(*dst) - acc[q]);
+        *dst = T(double(*dst) - acc[it][q]);
       }
     }
   }
   __syncthreads();
+}
+
+// All rows [r0, r1) of supernode sn, slab by slab.
+template <typename T>
+__device__ void sn_update_rows(const SnFactor& F, T* L, double* smem, int sn, int r0, int r1) {
+  (void)smem;
+  for (int lo = r0; lo < r1; lo += kSnSlab) sn_update_slab<T>(F, L, sn, lo, min(r1, lo + kSnSlab));
 }
 
 // Cholesky of supernode sn's diagonal block (the calling block): the factor
@@ -213,24 +242,63 @@ __device__ void sn_diag(const SnFactor& F, T* L, double* smem, int* info, int sn
     if (r >= c) D[r * kSnLd + c] = double(Ls[size_t(r) + size_t(c) * nr]);
   }
   __syncthreads();
-  if (t < 32) {  // one warp, right-looking by columns (warp-synchronous)
-    for (int k = 0; k < w; ++k) {
-      const double dk = D[k * kSnLd + k];
-      const double rk = dk > 0.0 ? 1.0 / sqrt(dk) : __longlong_as_double(0x7ff8000000000000ll);
-      for (int i = k + 1 + t; i < w; i += 32) D[i * kSnLd + k] *= rk;
-      if (t == 0) {
-        rdiag[k] = rk;
-        if (!(dk > 0.0)) atomicCAS(info, 0, f + k + 1);
+  // Right-looking in panels of 8 columns: warp 0 factors a panel in
+  // registers (lane l holds rows p0 + l and p0 + l + 32 of the panel's
+  // columns; pivots and multipliers by shuffles), then the whole block
+  // applies its rank-8 update to the rest.  Two barriers per panel.
+  const int lane = t & 31;
+  for (int p0 = 0; p0 < w; p0 += 8) {
+    const int pw = min(8, w - p0);
+    if (t < 32) {
+      const int ra = p0 + lane, rb = p0 + lane + 32;
+      double va[8], vb[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        va[c] = (c < pw && ra < w) ? D[ra * kSnLd + p0 + c] : 0.0;
+        vb[c] = (c < pw && rb < w) ? D[rb * kSnLd + p0 + c] : 0.0;
       }
-      __syncwarp();
-      for (int i = k + 1 + t; i < w; i += 32) {
-        const double lik = D[i * kSnLd + k];
-        for (int j = k + 1; j <= i; ++j) D[i * kSnLd + j] = fma(-lik, D[j * kSnLd + k], D[i * kSnLd + j]);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < pw) {
+          const double dk = __shfl_sync(0xffffffffu, va[c], c);  // pivot row p0 + c = lane c
+          const double rk = dk > 0.0 ? 1.0 / sqrt(dk) : __longlong_as_double(0x7ff8000000000000ll);
+          if (lane > c) va[c] *= rk;
+          vb[c] *= rk;
+          if (lane == c) va[c] = dk > 0.0 ? dk * rk : va[c];  // l_kk (kept in D, 1 / l_kk in rdiag)
+          if (lane == 0) {
+            rdiag[p0 + c] = rk;
+            if (!(dk > 0.0)) atomicCAS(info, 0, f + p0 + c + 1);
+          }
+#pragma unroll
+          for (int c2 = c + 1; c2 < 8; ++c2) {
+            if (c2 < pw) {
+              const double l2 = __shfl_sync(0xffffffffu, va[c], c2);  // L[p0 + c2][p0 + c]
+              if (lane >= c2) va[c2] = fma(-va[c], l2, va[c2]);
+              vb[c2] = fma(-vb[c], l2, vb[c2]);
+            }
+          }
+        }
       }
-      __syncwarp();
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < pw && ra < w && lane >= c) D[ra * kSnLd + p0 + c] = va[c];
+        if (c < pw && rb < w) D[rb * kSnLd + p0 + c] = vb[c];
+      }
     }
+    __syncthreads();
+    // Trailing update of rows and columns >= p0 + pw.
+    const int t0 = p0 + pw, tn = w - t0;
+    for (int idx = t; idx < tn * tn; idx += blockDim.x) {
+      const int i = t0 + idx / tn, j = t0 + idx % tn;
+      if (j > i) continue;
+      double sum = 0.0;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < pw) sum = fma(D[i * kSnLd + p0 + c], D[j * kSnLd + p0 + c], sum);
+      D[i * kSnLd + j] -= sum;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   for (int idx = t; idx < w * w; idx += blockDim.x) {
     const int c = idx / w, r = idx % w;
     if (r > c) Ls[size_t(r) + size_t(c) * nr] = T(D[r * kSnLd + c]);

@@ -51,7 +51,7 @@ def test_every_candidate_shape_solves_the_same():
   db.launch()
   ref = db.fetch()[0]["status"].copy()
   n_hi = int(hb.inst["n"].max())
-  for nt, lean, onchip in autotune.CANDIDATES:
+  for nt, lean, onchip in autotune.CANDIDATES + autotune.SMALL_CANDIDATES:
     hb.replan([{"n_lo": 0, "n_hi": n_hi, "block_threads": nt, "lean": lean,
                 "onchip": onchip}])
     db.refresh_plan()
