@@ -34,11 +34,15 @@ __version__ = "0.0.5+b200"
 # own switches earlier.
 LARGE_N = 1024
 LARGE_N_SINGLE = 256
-# A QP with n >= SPARSE_N whose Gram matrix is not narrow-banded, whose A has
-# at most 10 % nonzeros and whose supernodal factor holds at most SPARSE_FILL
-# of a dense factor's entries gets the supernodal factorisation.
+# A QP with n >= SPARSE_N whose A has at most 10 % nonzeros and whose
+# supernodal factor holds at most SPARSE_FILL of a dense factor's entries gets
+# the supernodal factorisation when it is not narrow-banded, or when it is
+# solved on its own and its band is too wide for the partitioned band path.
+# (Measured on a B200: at 7 % fill the supernodal and the whole-GPU dense
+# paths take about the same time; at 1.2 % the supernodal path is 8x faster
+# than the dense one and 37x faster than the one-block banded one.)
 SPARSE_N = 256
-SPARSE_FILL = 0.25
+SPARSE_FILL = 0.05
 BAND_GRID_N = 1024  # a banded QP solved on its own from this size: the whole GPU
 
 _HEADER = ("| iter |      pcost |      dcost |     pres |     dres |      gap |"
@@ -267,15 +271,18 @@ class QTQP:
     half-bandwidth at most n/4, in the natural ordering or in the band
     ordering of band_permutation) and n > 96 -- 'band_grid' (the whole GPU,
     partitioned band factorisation) instead for a QP solved on its own with
-    n >= BAND_GRID_N; otherwise 'sparse' (the whole GPU, supernodal
-    factorisation) for a sparse QP with n >= SPARSE_N whose factor stays
-    sparse (sparse_plan); otherwise 'large' (the whole GPU on one dense QP)
-    when n >= LARGE_N, or n >= LARGE_N_SINGLE for a QP solved on its own;
-    else 'dense' (one thread block per QP)."""
+    n >= BAND_GRID_N and a band narrow enough for it; 'sparse' (the whole GPU,
+    supernodal factorisation) for a sparse QP with n >= SPARSE_N whose factor
+    stays sparse (sparse_plan) and that is either not banded or banded but
+    solved on its own without the partitioned band path; otherwise 'large'
+    (the whole GPU on one dense QP) when n >= LARGE_N, or n >= LARGE_N_SINGLE
+    for a QP solved on its own; else 'dense' (one thread block per QP)."""
     if self.n <= 96:
       return "dense"
     from . import band as _band  # pylint: disable=g-import-not-at-top
     p = self.p if self.p.nnz else None
+    sparse_ok = lambda: (self.n >= SPARSE_N and self.a.nnz <= 0.1 * float(self.m) * self.n and
+                         self.sparse_plan().fill_fraction() <= SPARSE_FILL)
     if not _band.wide_by_counts(self.a, p, self.n):  # else no ordering makes it narrow
       bw = _band.gram_bandwidth(self.a, p)
       if 4 * (bw + 1) > self.n and self.band_permutation() is not None:
@@ -284,11 +291,13 @@ class QTQP:
       if 4 * (bw + 1) <= self.n:
         if single and self.n >= BAND_GRID_N and _band.grid_supported(bw, self.n):
           return "band_grid"
+        if single and sparse_ok():
+          return "sparse"
         return "band"
-    if (self.n >= SPARSE_N and self.a.nnz <= 0.1 * float(self.m) * self.n and
-        self.sparse_plan().fill_fraction() <= SPARSE_FILL):
+    large = self.n >= (LARGE_N_SINGLE if single else LARGE_N)
+    if (single or large) and sparse_ok():
       return "sparse"
-    return "large" if self.n >= (LARGE_N_SINGLE if single else LARGE_N) else "dense"
+    return "large" if large else "dense"
 
   def solve(self, *, atol: float = 1e-7, rtol: float = 1e-8, atol_infeas: float = 1e-8,
             rtol_infeas: float = 1e-9, max_iter: int = 100, step_size_scale: float = 0.99,
@@ -555,30 +564,34 @@ def _unpermute(q, x_band):
   return x
 
 
+_ARENA = _batch.PinnedArena()
+
+
 def _solve_dense_streamed(problems, opts, tuning) -> List[Solution]:
   """All-dense batch without records: packed, copied and launched group by
   group (DeviceBatch.solve_pipelined), and each group's Solutions built as
   soon as its launch finishes, while the others still run."""
-  hb = _batch.HostBatch(problems, opts, pinned=True, tuning=tuning, defer=True)
-  db = _batch.DeviceBatch(hb, records=False)
-  db.solve_pipelined()
   out: List[Solution | None] = [None] * len(problems)
   errs = []
-  n_off, m_off = hb.inst["n_off"], hb.inst["m_off"]
-  for g, res, n0, x, m0, y, s in db.fetch_groups():
-    grp = hb.plan.groups[g]
-    ids = hb.order[grp.begin:grp.begin + grp.count].tolist()
-    codes = res["status"][ids].tolist()
-    bad = res["error"][ids]
-    if bad.any():
-      errs += [(ids[k], int(bad[k])) for k in np.nonzero(bad)[0]]
-    iters = res["iterations"][ids].tolist()
-    for j, i in enumerate(ids):
-      q = problems[i]
-      a = int(n_off[i]) - n0
-      b = int(m_off[i]) - m0
-      out[i] = _make_solution(q, x[a:a + q.n], y[b:b + q.m], s[b:b + q.m], codes[j], iters[j],
-                              None, opts, False, 0.0)
+  with _ARENA.lock:  # the pinned pools are reused from call to call
+    hb = _batch.HostBatch(problems, opts, pinned=_ARENA, tuning=tuning, defer=True)
+    db = _batch.DeviceBatch(hb, records=False)
+    db.solve_pipelined()
+    n_off, m_off = hb.inst["n_off"], hb.inst["m_off"]
+    for g, res, n0, x, m0, y, s in db.fetch_groups():
+      grp = hb.plan.groups[g]
+      ids = hb.order[grp.begin:grp.begin + grp.count].tolist()
+      codes = res["status"][ids].tolist()
+      bad = res["error"][ids]
+      if bad.any():
+        errs += [(ids[k], int(bad[k])) for k in np.nonzero(bad)[0]]
+      iters = res["iterations"][ids].tolist()
+      for j, i in enumerate(ids):
+        q = problems[i]
+        a = int(n_off[i]) - n0
+        b = int(m_off[i]) - m0
+        out[i] = _make_solution(q, x[a:a + q.n], y[b:b + q.m], s[b:b + q.m], codes[j],
+                                iters[j], None, opts, False, 0.0)
   if errs:
     _raise_device_error(min(errs)[1])
   return out

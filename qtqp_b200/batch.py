@@ -156,13 +156,34 @@ def _gather(lib, pool: np.ndarray, ptrs, nbytes, offs) -> None:
                                     offs.ctypes.data, pool.ctypes.data, 0))
 
 
+class PinnedArena:
+  """Pinned host buffers kept across calls (grown, never shrunk), for a caller
+  that builds one batch at a time: allocating and page-locking 150 MB of
+  pools on every call costs more than the packing itself.  Whoever holds
+  `lock` owns the buffers until it releases it."""
+
+  def __init__(self):
+    import threading  # pylint: disable=g-import-not-at-top
+    self.lock = threading.Lock()
+    self._bufs = {}
+
+  def get(self, slot: str, count: int):
+    import torch  # pylint: disable=g-import-not-at-top
+    t = self._bufs.get(slot)
+    if t is None or t.numel() < count:
+      t = torch.empty(max(count, 1), dtype=torch.float64, pin_memory=True)
+      self._bufs[slot] = t
+    return t[:count]
+
+
 class HostBatch:
   """Packed host pools of a batch: A and P column-major per instance, b, c.
 
   problems: QTQP objects (their CSC values are gathered in place when every
   entry is stored) or DenseProblems.  pinned=True allocates the pools in
   pinned host memory (torch), so that they are copied to the device
-  asynchronously without a staging copy.
+  asynchronously without a staging copy; pinned=<PinnedArena> takes them
+  from the arena (the caller holds its lock while the batch lives).
   """
 
   def __init__(self, problems: Sequence, opts: SolveOptions, block_threads: int = 0,
@@ -195,7 +216,11 @@ class HostBatch:
     self.pinned = pinned
     self.h_pools = None
     sizes = (max(a_total, 1), max(p_total, 1), max(self.m_total, 1), max(self.n_total, 1))
-    if pinned:
+    self.arena = pinned if isinstance(pinned, PinnedArena) else None
+    if isinstance(pinned, PinnedArena):
+      self.h_pools = [pinned.get(slot, k) for slot, k in zip("apbc", sizes)]
+      self.a_pool, self.p_pool, self.b_pool, self.c_pool = (t.numpy() for t in self.h_pools)
+    elif pinned:
       import torch  # pylint: disable=g-import-not-at-top
       self.h_pools = [torch.empty(k, dtype=torch.float64, pin_memory=True) for k in sizes]
       self.a_pool, self.p_pool, self.b_pool, self.c_pool = (t.numpy() for t in self.h_pools)
@@ -393,6 +418,20 @@ class DeviceBatch:
         m0 = int(hb.inst["m_off"][ids[0]])
         m1 = int(hb.inst["m_off"][ids[-1]] + hb.inst["m"][ids[-1]])
         copy_stream.wait_event(self._group_done[g])
+        if hb.arena is not None:  # through the arena's pinned buffers into numpy arrays
+          nres = (self.results.numel() + 7) // 8
+          rb = hb.arena.get("out_res", nres).view(torch.uint8)[:self.results.numel()]
+          xb, yb = hb.arena.get("out_x", n1 - n0), hb.arena.get("out_y", m1 - m0)
+          sb = hb.arena.get("out_s", m1 - m0)
+          with torch.cuda.stream(copy_stream):
+            rb.copy_(self.results, non_blocking=True)
+            xb.copy_(self.x[n0:n1], non_blocking=True)
+            yb.copy_(self.y[m0:m1], non_blocking=True)
+            sb.copy_(self.s[m0:m1], non_blocking=True)
+          copy_stream.synchronize()
+          yield (g, rb.numpy().view(_lib.RESULT_DTYPE)[:hb.count].copy(), n0,
+                 xb.numpy().copy(), m0, yb.numpy().copy(), sb.numpy().copy())
+          continue
         with torch.cuda.stream(copy_stream):
           res = self.results.to("cpu", non_blocking=True)
           x = self.x[n0:n1].to("cpu", non_blocking=True)

@@ -81,9 +81,10 @@ def test_sparse_certificates(precision):
 
 
 def test_auto_routing_and_reproducibility():
-  """A sparse QP that no band ordering narrows goes to the supernodal path
-  on its own; two solves give identical bits (no atomics in the factor)."""
-  a, b, c, z, p = problems.sparse_feasible(1200, 1300, 100, 9, per_row=2)
+  """A grid-network QP whose band is too wide for the partitioned band path
+  goes to the supernodal path when solved on its own; two solves give
+  identical bits (no atomics in the factor)."""
+  a, b, c, z, p = problems.grid_flow(32)
   q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
   assert q.storage_format(single=True) == "sparse"
   s1 = q.solve(verbose=False)

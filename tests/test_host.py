@@ -359,3 +359,20 @@ def test_storage_of_dense_qps_is_decided_from_entry_counts():
     assert band.gram_bandwidth(a, None) == (max(spans) if spans else 0)
     if band.wide_by_counts(a, None, n):
       assert 4 * (band.gram_bandwidth(a, None) + 1) > n
+
+
+def test_storage_routing_of_sparse_problems():
+  """A grid network's QP solved on its own goes to the supernodal path when
+  its band is too wide for the partitioned band path (in a batch it stays
+  banded); a random sparse QP whose factor fills 25 % of a dense one stays
+  dense; a long MPC horizon keeps the partitioned band path."""
+  a, b, c, z, p = problems.grid_flow(32)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert q.sparse_plan().fill_fraction() < qb.SPARSE_FILL
+  assert q.storage_format(single=True) == "sparse"
+  assert q.storage_format() == "band"
+  a, b, c, z, p = problems.sparse_feasible(1200, 1300, 100, 9)
+  q = qb.QTQP(a=a, b=b, c=c, z=z, p=p)
+  assert q.storage_format(single=True) == "large"
+  a, b, c, z, p = problems.mpc_feasible(30)
+  assert qb.QTQP(a=a, b=b, c=c, z=z, p=p).storage_format(single=True) == "band_grid"
