@@ -18,6 +18,9 @@ _ROOT = os.path.dirname(_HERE)
 _CSRC = os.path.join(_HERE, "csrc")
 _INC = os.path.join(_ROOT, "include")
 LIB_PATH = os.path.join(_HERE, "libqtqp_cuda.so")
+# The profiling build: per-phase SM-cycle counters (-DQTQP_PHASE_TIMERS, read
+# with qtqp_phase_cycles; qtqp_b200.phases reports them).
+PHASE_LIB_PATH = os.path.join(_HERE, "libqtqp_cuda_phase.so")
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -40,22 +43,29 @@ def _deps() -> list[str]:
   return files
 
 
-def up_to_date() -> bool:
-  if not os.path.exists(LIB_PATH):
+def up_to_date(path: str = LIB_PATH) -> bool:
+  if not os.path.exists(path):
     return False
-  t = os.path.getmtime(LIB_PATH)
+  t = os.path.getmtime(path)
   return all(os.path.getmtime(f) <= t for f in _deps())
 
 
-def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
-  """Compiles every .cu under csrc/ (in parallel) into libqtqp_cuda.so."""
-  if not force and not debug and up_to_date():
-    return LIB_PATH
+def build(force: bool = False, debug: bool = False, verbose: bool = False,
+          phase_timers: bool = False) -> str:
+  """Compiles every .cu under csrc/ (in parallel) into libqtqp_cuda.so, or,
+  with phase_timers, into the profiling build libqtqp_cuda_phase.so (per-phase
+  cycle counters; relocatable device code, since the counters are one device
+  array shared by every kernel)."""
+  out = PHASE_LIB_PATH if phase_timers else LIB_PATH
+  if not force and not debug and up_to_date(out):
+    return out
   import concurrent.futures
   import tempfile
   common = [_nvcc(), *ARCH_FLAGS, "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
             "-I", _INC, "-I", _CSRC, "--expt-relaxed-constexpr"]
   common += ["-O0", "-G"] if debug else ["-O3"]
+  if phase_timers:
+    common += ["-DQTQP_PHASE_TIMERS", "-rdc=true"]
   if verbose:
     common += ["-Xptxas", "-v"]
   with tempfile.TemporaryDirectory(prefix="qtqp_build_") as tmp:
@@ -71,14 +81,15 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
         if verbose:
           sys.stderr.write(proc.stderr)
         objs.append(obj)
-    link = [_nvcc(), *ARCH_FLAGS, "-shared", "-o", LIB_PATH + ".tmp", *objs]
+    link = [_nvcc(), *ARCH_FLAGS, *(["-rdc=true"] if phase_timers else []), "-shared", "-o",
+            out + ".tmp", *objs]
     proc = subprocess.run(link, capture_output=True, text=True)
     if proc.returncode != 0:
       raise RuntimeError(f"nvcc link failed:\n{proc.stderr}\n{proc.stdout}")
-  os.replace(LIB_PATH + ".tmp", LIB_PATH)
-  return LIB_PATH
+  os.replace(out + ".tmp", out)
+  return out
 
 
 if __name__ == "__main__":
-  build(force=True, debug="--debug" in sys.argv, verbose="-v" in sys.argv)
-  print(LIB_PATH)
+  print(build(force=True, debug="--debug" in sys.argv, verbose="-v" in sys.argv,
+              phase_timers="--phase-timers" in sys.argv))
