@@ -28,12 +28,12 @@ struct SparseGridParams {
 __host__ __device__ inline size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct SparseLayout {
-  size_t band_off, vals_off, z_off, parts_off, ctl_off, info_off, total;
+  size_t band_off, vals_off, z_off, parts_off, upd_off, ctl_off, info_off, total;
 };
 // Workspace: the banded backend's vectors and working values, the factor
 // (nvals), the forward products (one per stored row), the backward partial
-// sums (kSnMaxW per top-level row slab), the grid's barrier state and the
-// factorisation status.
+// sums (kSnMaxW per top-level row slab), the partial updates of split row
+// slabs, the grid's barrier state and the factorisation status.
 __host__ __device__ inline SparseLayout plan_sparse_layout(int n, int m, int nnz_a, int nnz_p,
                                                            int64_t nvals, int64_t nrows,
                                                            int64_t nslabs) {
@@ -43,7 +43,8 @@ __host__ __device__ inline SparseLayout plan_sparse_layout(int n, int m, int nnz
   L.vals_off = round256(B.total);
   L.z_off = round256(L.vals_off + size_t(nvals) * 8);
   L.parts_off = round256(L.z_off + size_t(nrows) * 8);
-  L.ctl_off = round256(L.parts_off + size_t(nslabs) * kSnMaxW * 8);
+  L.upd_off = round256(L.parts_off + size_t(nslabs) * kSnMaxW * 8);
+  L.ctl_off = round256(L.upd_off + size_t(kSparseGridBlocks) * kSnSlab * kSnMaxW * 8);
   L.info_off = round256(L.ctl_off + sizeof(GridCtl));
   L.total = L.info_off + 256;
   return L;
@@ -63,6 +64,7 @@ __global__ void __launch_bounds__(kGridBT, 1) sparse_grid_kernel(const SparseGri
     sf.vals = reinterpret_cast<double*>(p.ws + L.vals_off);
     sf.zbuf = reinterpret_cast<double*>(p.ws + L.z_off);
     sf.pbuf = reinterpret_cast<double*>(p.ws + L.parts_off);
+    sf.ubuf = reinterpret_cast<double*>(p.ws + L.upd_off);
   }
   __syncthreads();
   Ipm<kSparseGridNT, kFmtSparse> s;

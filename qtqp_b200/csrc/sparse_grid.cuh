@@ -46,6 +46,7 @@ constexpr int kSnLd = kSnMaxW + 1;      // leading dimension of the diagonal blo
 constexpr int kSnStageK = 32;           // descendant columns staged per pass
 constexpr int kSnCg = 8;                // target columns per thread in an update pass
 constexpr int kSnSlab = kSnSlabRows;    // rows of a top-level supernode per work item
+constexpr int kSnMaxSplit = 8;          // blocks sharing one slab's update list, at most
 // Dynamic shared memory of a block: the diagonal block, its reciprocal
 // diagonal, the staged descendant rows, and the partial sums of the solves.
 constexpr size_t kSparseSmemElems =
@@ -77,6 +78,7 @@ struct SnFactor {
   double* vals;
   double* zbuf;  // forward products per stored row (nrows)
   double* pbuf;  // backward partial sums per top-level row slab (kSnMaxW each)
+  double* ubuf;  // partial updates of split row slabs (kSparseGridBlocks x kSnSlab x kSnMaxW)
 };
 
 // Position of `key` in the sorted rows[0 .. len) (present by construction).
@@ -144,14 +146,18 @@ __device__ double sn_gram_entry(const S& s, int i, int j) {
 // slab (a range found by two binary searches, the same in every thread), then
 // each item's row and columns in it.  No two threads write the same entry,
 // every sum runs in a fixed order, and no barrier separates the descendants.
+//
+// [u0, u1) is the part of the update list to apply; out == nullptr subtracts
+// the sums from the block, else they go to out (kSnSlab x kSnMaxW, row r - r0
+// at out[(r - r0) * kSnMaxW + col]) for sn_add_partials.
 template <typename T>
-__device__ void sn_update_slab(const SnFactor& F, T* L, int sn, int r0, int r1) {
+__device__ void sn_update_slab(const SnFactor& F, T* L, int sn, int r0, int r1, int u0, int u1,
+                               double* out) {
   const int t = threadIdx.x;
   const int f = F.first[sn], w = F.first[sn + 1] - f;
   const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
   const int32_t* R = F.rows + F.rowptr[sn];
   T* Ls = L + F.valptr[sn];
-  const int u0 = F.upd_ptr[sn], u1 = F.upd_ptr[sn + 1];
   const int ngrp = (w + kSnCg - 1) / kSnCg;
   const int rows = r1 - r0;
   const int lo_key = R[r0], hi_key = R[r1 - 1];
@@ -211,19 +217,47 @@ __device__ void sn_update_slab(const SnFactor& F, T* L, int sn, int r0, int r1) 
 #pragma unroll
     for (int q = 0; q < kSnCg; ++q) {
       if (ck0[it] + q < ck1[it] && ck0[it] + q <= key[it]) {
-        T* dst = Ls + size_t(r) + size_t(cg * kSnCg + q) * nr;
-        *dst = T(double(*dst) - acc[it][q]);
+        const int col = cg * kSnCg + q;
+        if (out != nullptr) {
+          out[(r - r0) * kSnMaxW + col] = acc[it][q];
+        } else {
+          T* dst = Ls + size_t(r) + size_t(col) * nr;
+          *dst = T(double(*dst) - acc[it][q]);
+        }
       }
     }
   }
   __syncthreads();
 }
 
-// All rows [r0, r1) of supernode sn, slab by slab.
+// All rows [r0, r1) of supernode sn, slab by slab, from its whole update list.
 template <typename T>
 __device__ void sn_update_rows(const SnFactor& F, T* L, double* smem, int sn, int r0, int r1) {
   (void)smem;
-  for (int lo = r0; lo < r1; lo += kSnSlab) sn_update_slab<T>(F, L, sn, lo, min(r1, lo + kSnSlab));
+  for (int lo = r0; lo < r1; lo += kSnSlab)
+    sn_update_slab<T>(F, L, sn, lo, min(r1, lo + kSnSlab), F.upd_ptr[sn], F.upd_ptr[sn + 1],
+                      nullptr);
+}
+
+// Subtracts from rows [r0, r1) of supernode sn the partial sums that `parts`
+// blocks left in part[0 .. parts) (sn_update_slab with out), in that order.
+template <typename T>
+__device__ void sn_add_partials(const SnFactor& F, T* L, int sn, int r0, int r1,
+                                const double* part, int parts) {
+  const int f = F.first[sn], w = F.first[sn + 1] - f;
+  const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+  const int32_t* R = F.rows + F.rowptr[sn];
+  T* Ls = L + F.valptr[sn];
+  const int rows = r1 - r0;
+  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
+    const int rl = e % rows, col = e / rows;
+    if (f + col > R[r0 + rl]) continue;  // the block's upper triangle
+    double sum = 0.0;
+    for (int c = 0; c < parts; ++c) sum += part[size_t(c) * kSnSlab * kSnMaxW + rl * kSnMaxW + col];
+    T* dst = Ls + size_t(r0 + rl) + size_t(col) * nr;
+    *dst = T(double(*dst) - sum);
+  }
+  __syncthreads();
 }
 
 // Cholesky of supernode sn's diagonal block (the calling block): the factor
@@ -368,15 +402,60 @@ __device__ __forceinline__ void sn_slab_item(const SnFactor& F, int q0, int q1, 
   r1 = min(nr, r0 + kSnSlab);
 }
 
+// The forward contributions of the update list's entries [ua, ub) to the
+// columns of supernode sn, per thread group (thread t: column t % W32, group
+// t / W32 over every G-th entry; W32 = 32 or 64 by the width), into
+// part[t]; ends with a barrier.
+__device__ __forceinline__ void sn_fwd_gather_block(const SnFactor& F, const double* z, int sn,
+                                                    int ua, int ub, double* part) {
+  const int t = threadIdx.x;
+  const int f = F.first[sn], w = F.first[sn + 1] - f;
+  const int W32 = w <= 32 ? 32 : 64;
+  const int G = blockDim.x / W32;
+  const int j = t % W32, g = t / W32;
+  double acc = 0.0;
+  if (j < w) {
+    for (int u = ua + g; u < ub; u += G) {
+      const int d = F.upd_src[u], off = F.upd_off[u], cnt = F.upd_cnt[u];
+      const int32_t* Rd = F.rows + F.rowptr[d] + off;
+      const int c = sn_find(Rd, cnt, f + j);
+      if (c < cnt && Rd[c] == f + j) acc += z[F.rowptr[d] + off + c];
+    }
+  }
+  part[t] = acc;
+  __syncthreads();
+}
+
+// sn_fwd_gather_block over [ua, ub), its groups summed in order into out[j]
+// (j < the supernode's width), for sn_fwd_diag's `parts`.
+__device__ __forceinline__ void sn_fwd_gather(const SnFactor& F, const double* z, double* smem,
+                                              int sn, int ua, int ub, double* out) {
+  const int t = threadIdx.x;
+  const int w = F.first[sn + 1] - F.first[sn];
+  const int W32 = w <= 32 ? 32 : 64;
+  const int G = blockDim.x / W32;
+  double* part = smem + kSnMaxW * kSnLd + kSnMaxW + kSnMaxW * (kSnStageK + 1);
+  sn_fwd_gather_block(F, z, sn, ua, ub, part);
+  if (t < w) {
+    double sum = 0.0;
+    for (int q = 0; q < G; ++q) sum += part[q * W32 + t];
+    out[t] = sum;
+  }
+  __syncthreads();
+}
+
 // Forward solve, step 1 for supernode `sn` (the calling block): v[cols] -=
 // the products z of its descendants with the rows in its columns (z_d[r] =
 // L_d[r, :] y_d, stored per row of R_d by step 2), then y_cols = L_bb^{-1}
 // v[cols] on one warp with the diagonal block in shared memory.  The
 // contributions are summed in a fixed order (thread groups over the update
 // list, then the groups in turn), so the result does not depend on timing.
+//
+// parts != nullptr: the contributions were gathered by sn_fwd_gather into
+// parts[0 .. nparts) (kSnMaxW values each) and are subtracted in that order.
 template <typename T>
 __device__ void sn_fwd_diag(const SnFactor& F, const T* L, double* smem, const double* z, T* v,
-                            int sn) {
+                            int sn, const double* parts = nullptr, int nparts = 0) {
   const int t = threadIdx.x;
   const int f = F.first[sn], w = F.first[sn + 1] - f;
   const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
@@ -390,21 +469,16 @@ __device__ void sn_fwd_diag(const SnFactor& F, const T* L, double* smem, const d
   }
   const int W32 = w <= 32 ? 32 : 64;
   const int G = blockDim.x / W32;
-  const int j = t % W32, g = t / W32;
-  double acc = 0.0;
-  if (j < w) {
-    for (int u = F.upd_ptr[sn] + g; u < F.upd_ptr[sn + 1]; u += G) {
-      const int d = F.upd_src[u], off = F.upd_off[u], cnt = F.upd_cnt[u];
-      const int32_t* Rd = F.rows + F.rowptr[d] + off;
-      const int c = sn_find(Rd, cnt, f + j);
-      if (c < cnt && Rd[c] == f + j) acc += z[F.rowptr[d] + off + c];
+  if (parts == nullptr) {
+    sn_fwd_gather_block(F, z, sn, F.upd_ptr[sn], F.upd_ptr[sn + 1], part);
+    if (t < w) {
+      double bv = double(v[f + t]);
+      for (int q = 0; q < G; ++q) bv -= part[q * W32 + t];
+      yb[t] = bv;
     }
-  }
-  part[t] = acc;
-  __syncthreads();
-  if (t < w) {
+  } else if (t < w) {
     double bv = double(v[f + t]);
-    for (int q = 0; q < G; ++q) bv -= part[q * W32 + t];
+    for (int q = 0; q < nparts; ++q) bv -= parts[q * kSnMaxW + t];
     yb[t] = bv;
   }
   __syncthreads();
@@ -566,26 +640,47 @@ __device__ int sparse_factorize(S& s) {
   QTQP_RETIC();
   // Above the subtrees, each level in three steps over the whole grid: the
   // updates of every row slab, the diagonal blocks, the rows below them.
+  // A level with fewer row slabs than half the grid splits each slab's
+  // update list over `split` blocks; their partial sums are added (in order)
+  // by the diagonal step (slab 0 of each supernode) and the row step (the
+  // other slabs), so the split costs no extra barrier.
+  const int G = int(gridDim.x);
   for (int l = 0; l < F.top_levels; ++l) {
     const int q0 = F.top_ptr[l], q1 = F.top_ptr[l + 1];
     const int items = F.top_slab[q1] - F.top_slab[q0];
+    const int split = 2 * items > G ? 1 : min(kSnMaxSplit, G / items);
     QTQP_TIC();
-    for (int it = b; it < items; it += gridDim.x) {
+    for (int it = b; it < items * split; it += G) {
+      const int slab = it / split, part = it % split;
       int sn, r0, r1;
-      sn_slab_item(F, q0, q1, F.top_slab[q0] + it, sn, r0, r1);
-      sn_update_rows<T>(F, L, smem, sn, r0, r1);
+      sn_slab_item(F, q0, q1, F.top_slab[q0] + slab, sn, r0, r1);
+      const int ua = F.upd_ptr[sn], len = F.upd_ptr[sn + 1] - ua;
+      sn_update_slab<T>(F, L, sn, r0, r1, ua + len * part / split, ua + len * (part + 1) / split,
+                        split > 1 ? F.ubuf + size_t(it) * kSnSlab * kSnMaxW : nullptr);
     }
     s.sync();
     QTQP_TOC(kPhSnTopUpd);
     QTQP_RETIC();
-    for (int q = q0 + b; q < q1; q += gridDim.x) sn_diag<T>(F, L, smem, s.linfo, F.top_list[q]);
+    for (int q = q0 + b; q < q1; q += G) {
+      const int sn = F.top_list[q];
+      if (split > 1) {
+        const int slab = F.top_slab[q] - F.top_slab[q0];
+        const int nr = int(F.rowptr[sn + 1] - F.rowptr[sn]);
+        sn_add_partials<T>(F, L, sn, 0, min(nr, kSnSlab),
+                           F.ubuf + size_t(slab) * split * kSnSlab * kSnMaxW, split);
+      }
+      sn_diag<T>(F, L, smem, s.linfo, sn);
+    }
     s.sync();
     QTQP_TOC(kPhSnTopDiag);
     QTQP_RETIC();
-    for (int it = b; it < items; it += gridDim.x) {
+    for (int it = b; it < items; it += G) {
       int sn, r0, r1;
       sn_slab_item(F, q0, q1, F.top_slab[q0] + it, sn, r0, r1);
       const int w = F.first[sn + 1] - F.first[sn];
+      if (split > 1 && r0 > 0)
+        sn_add_partials<T>(F, L, sn, r0, r1, F.ubuf + size_t(it) * split * kSnSlab * kSnMaxW,
+                           split);
       if (r1 > w) sn_panel_rows<T>(F, L, smem, sn, r0, r1, true);
     }
     s.sync();
@@ -615,9 +710,28 @@ __device__ void sparse_solve(S& s, T* v, T* w) {
   s.sync();
   QTQP_TOC(kPhSnFwdSub);
   QTQP_RETIC();
+  const int G = int(gridDim.x);
   for (int l = 0; l < F.top_levels; ++l) {
     const int q0 = F.top_ptr[l], q1 = F.top_ptr[l + 1];
-    for (int q = q0 + b; q < q1; q += gridDim.x) sn_fwd_diag<T>(F, L, smem, z, v, F.top_list[q]);
+    // Long update lists are gathered by several blocks first (one more
+    // barrier), each on a contiguous part, then summed in order.
+    int ulen = 0;
+    for (int q = q0; q < q1; ++q) ulen += F.upd_ptr[F.top_list[q] + 1] - F.upd_ptr[F.top_list[q]];
+    const int nq = q1 - q0;
+    const int split = ulen < 8 * kGridBT / 32 * nq || 2 * nq > G ? 1 : min(kSnMaxSplit, G / nq);
+    if (split > 1) {
+      for (int it = b; it < nq * split; it += G) {
+        const int q = q0 + it / split, part = it % split;
+        const int sn = F.top_list[q];
+        const int ua = F.upd_ptr[sn], len = F.upd_ptr[sn + 1] - ua;
+        sn_fwd_gather(F, z, smem, sn, ua + len * part / split, ua + len * (part + 1) / split,
+                      F.ubuf + size_t(it) * kSnMaxW);
+      }
+      s.sync();
+    }
+    for (int q = q0 + b; q < q1; q += G)
+      sn_fwd_diag<T>(F, L, smem, z, v, F.top_list[q],
+                     split > 1 ? F.ubuf + size_t(q - q0) * split * kSnMaxW : nullptr, split);
     s.sync();
     if (l + 1 < F.top_levels) {  // the last level's products have no reader
       const int items = F.top_slab[q1] - F.top_slab[q0];

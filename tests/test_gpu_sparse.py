@@ -93,3 +93,19 @@ def test_auto_routing_and_reproducibility():
   assert np.array_equal(s1.x, s2.x) and np.array_equal(s1.y, s2.y)
   ref = orc.solve(a, b, c, z, p, backend="superlu")
   assert kkt_checks.objective_rel_err(s1.x, ref.x, c, p) <= OBJ_TOL
+
+
+@pytest.mark.parametrize("case", ["grid_flow_40", "random_3000"])
+def test_larger_sparse_qps_match_oracle(case):
+  """Sizes whose top levels split their row slabs' update lists and their
+  forward gathers over several blocks (long update lists, few slabs)."""
+  if case == "grid_flow_40":
+    a, b, c, z, p = problems.grid_flow(40)
+  else:
+    a, b, c, z, p = problems.sparse_feasible(3000, 3000, 300, 77, per_row=2)
+  q, sol = _solve(a, b, c, z, p)
+  ref = orc.solve(a, b, c, z, p, backend="superlu")
+  assert sol.status.value == ref.status
+  kkt_checks.assert_status_certificate(sol, a, b, c, p, z)
+  assert kkt_checks.objective_rel_err(sol.x, ref.x, c, p) <= OBJ_TOL
+  assert abs(len(sol.stats) - len(ref.stats)) <= 1
