@@ -38,11 +38,11 @@ LARGE_N_SINGLE = 256
 # supernodal factor holds at most SPARSE_FILL of a dense factor's entries gets
 # the supernodal factorisation when it is not narrow-banded, or when it is
 # solved on its own and its band is too wide for the partitioned band path.
-# (Measured on a B200: at 7 % fill the supernodal and the whole-GPU dense
-# paths take about the same time; at 1.2 % the supernodal path is 8x faster
-# than the dense one and 37x faster than the one-block banded one.)
+# (Measured on a B200: at 7 % fill the supernodal path takes 0.76-0.82 of the
+# whole-GPU dense path's time; at 1.2 % it is 45x faster than the one-block
+# banded path.)
 SPARSE_N = 256
-SPARSE_FILL = 0.05
+SPARSE_FILL = 0.10
 BAND_GRID_N = 1024  # a banded QP solved on its own from this size: the whole GPU
 
 _HEADER = ("| iter |      pcost |      dcost |     pres |     dres |      gap |"

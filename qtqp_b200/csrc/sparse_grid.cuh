@@ -648,7 +648,11 @@ __device__ int sparse_factorize(S& s) {
   for (int l = 0; l < F.top_levels; ++l) {
     const int q0 = F.top_ptr[l], q1 = F.top_ptr[l + 1];
     const int items = F.top_slab[q1] - F.top_slab[q0];
-    const int split = 2 * items > G ? 1 : min(kSnMaxSplit, G / items);
+    int ulen = 0;  // update list entries of the level (the same in every block)
+    for (int q = q0; q < q1; ++q) ulen += F.upd_ptr[F.top_list[q] + 1] - F.upd_ptr[F.top_list[q]];
+    // At least 8 list entries per part on average: short lists stay whole.
+    const int split = 2 * items > G ? 1
+                                    : max(1, min(min(kSnMaxSplit, G / items), ulen / (8 * (q1 - q0))));
     QTQP_TIC();
     for (int it = b; it < items * split; it += G) {
       const int slab = it / split, part = it % split;
