@@ -580,7 +580,11 @@ static int build_plan(int n, int m, const int32_t* ap, const int32_t* ai, const 
       const double rem = double(P.rowptr[d + 1] - P.rowptr[d]) - P.upd_off[u];
       wk += rem * P.upd_cnt[u] * wd;
     }
-    work[s] = wk + 64.0;  // a fixed cost per supernode (barriers, bookkeeping)
+    // A supernode also costs a fixed latency (its barriers and dependent loads,
+    // tens of microseconds on one block), worth about 2e5 multiply-adds of
+    // a block's throughput; without it, blocks given many small supernodes
+    // finish their subtrees last.
+    work[s] = wk + 2e5;
     P.flops += 2.0 * wk;
     P.nnz_l += int64_t(nr * w - w * (w - 1) / 2);
   }
