@@ -38,8 +38,8 @@ LARGE_N_SINGLE = 256
 # supernodal factor holds at most SPARSE_FILL of a dense factor's entries gets
 # the supernodal factorisation when it is not narrow-banded, or when it is
 # solved on its own and its band is too wide for the partitioned band path.
-# (Measured on a B200: at 7 % fill the supernodal path takes 0.76-0.82 of the
-# whole-GPU dense path's time; at 1.2 % it is 45x faster than the one-block
+# (Measured on a B200: at 7 % fill the supernodal path takes 0.45-0.72 of the
+# whole-GPU dense path's time; at 1.2 % it is 40x faster than the one-block
 # banded path.)
 SPARSE_N = 256
 SPARSE_FILL = 0.10

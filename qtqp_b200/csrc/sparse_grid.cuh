@@ -46,7 +46,7 @@ constexpr int kSnLd = kSnMaxW + 1;      // leading dimension of the diagonal blo
 constexpr int kSnStageK = 32;           // descendant columns staged per pass
 constexpr int kSnCg = 8;                // target columns per thread in an update pass
 constexpr int kSnSlab = kSnSlabRows;    // rows of a top-level supernode per work item
-constexpr int kSnMaxSplit = 8;          // blocks sharing one slab's update list, at most
+constexpr int kSnMaxSplit = 32;         // blocks sharing one slab's update list, at most
 // Dynamic shared memory of a block: the diagonal block, its reciprocal
 // diagonal, the staged descendant rows, and the partial sums of the solves.
 constexpr size_t kSparseSmemElems =
