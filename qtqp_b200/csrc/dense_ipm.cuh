@@ -191,6 +191,9 @@ template <typename T, class S>
 __device__ int large_factorize(S& s);
 template <typename T, class S>
 __device__ void large_chol_solve(S& s, T* v, T* w);
+template <class S, class RowEpi, class ColEpi>
+__device__ void large_products(S& s, const double* vx, const double* vy, const double* vs,
+                               const double* vp, RowEpi row_epi, ColEpi col_epi);
 // Partitioned banded factorisation / solve of grid mode (band_grid.cuh).
 template <typename T, class S>
 __device__ int bandp_factorize(S& s);
@@ -275,6 +278,7 @@ struct Ipm {
   float* g32l;
   double* linv;
   double* sinv;  // sub-block inverses of the current panel step
+  double* colpart;  // per-block column sums of large_products (gridDim x npad)
   float* xhi;
   float* xlo;
   const void* map_hi;
@@ -335,7 +339,7 @@ struct Ipm {
         // U independent partial sums per lane keep U loads (and U FMA
         // chains) in flight: grid mode streams A and P from HBM; a block's
         // loads come from shared memory or L2.
-        constexpr int U = NT > 1024 ? 8 : QTQP_ROWDOT_UNROLL;
+        constexpr int U = NT > 1024 ? 16 : QTQP_ROWDOT_UNROLL;
         AccT part[U][NACC];
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -1102,18 +1106,21 @@ struct Ipm {
     const double* Ap = A;
     const int ld = lda, nn = n;
     // g = r_x + A^T (r_y / Ry)
+    auto put_g = [&](int k, double g) {
+      if (fp64) {
+        tmp[k] = g;
+      } else {
+        t32[k] = float(g);
+      }
+    };
+    // (In grid mode a lane group per column streams A with many loads in
+    // flight; a row pass with per-block column sums measured slower here,
+    // where no row dot rides along.)
     rowdot<1>(n, m,
               [&](int k, int i, double* acc) {
                 acc[0] = fma(Ap[i * ld + k], iry[nn + i] * r[nn + i], acc[0]);
               },
-              [&](int k, double* acc) {
-                const double g = r[k] + acc[0];
-                if (fp64) {
-                  tmp[k] = g;
-                } else {
-                  t32[k] = float(g);
-                }
-              });
+              [&](int k, double* acc) { put_g(k, r[k] + acc[0]); });
     sync();
     if (fp64) {
       chol_solve<double>(G, tmp, vec(kW));
@@ -1244,6 +1251,29 @@ struct Ipm {
     }
     const double* reg = vec(kREG);
     const double* corr = vec(kCORR);
+    if constexpr (FMT == kFmtLarge) {
+      // One pass over A (and P): row dots A v_x and column sums
+      // A^T v_y + P v_x (large_ipm.cuh); the column epilogue runs after a
+      // grid barrier, in the thread that owns column k.
+      const int nn = n;
+      large_products(*this, v, v + n, nullptr, has_p ? v : nullptr,
+                     [&](int i, double ax) {
+                       const int kk = nn + i;
+                       const double kv = ax - (-reg[kk]) * v[kk];
+                       const double rk = krhs[kk] - kv + corr[kk] * v[kk];
+                       res[kk] = rk;
+                       mres = nanmax(mres, fabs(rk));
+                       vnan = fmax(vnan, (v[kk] != v[kk]) ? 1.0 : 0.0);
+                     },
+                     [&](int k, double cs) {
+                       const double kv = cs + reg[k] * v[k];
+                       const double rk = krhs[k] - kv + corr[k] * v[k];
+                       res[k] = rk;
+                       mres = nanmax(mres, fabs(rk));
+                       vnan = fmax(vnan, (v[k] != v[k]) ? 1.0 : 0.0);
+                     });
+      return;
+    }
     const double* Ap = A;
     const double* Pp = P;
     const int la = lda, lp = ldp, nn = n, mm = m;

@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(kGridBT, 1)
   s.sinv = reinterpret_cast<double*>(p.ws + L.sinv_off);
   s.xhi = reinterpret_cast<float*>(p.ws + L.xhi_off);
   s.xlo = reinterpret_cast<float*>(p.ws + L.xlo_off);
+  s.colpart = reinterpret_cast<double*>(p.ws + L.cp_off);
   s.map_hi = &map_hi;
   s.map_lo = &map_lo;
   s.arena = arena;

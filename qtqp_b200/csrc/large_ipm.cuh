@@ -40,7 +40,7 @@ __host__ __device__ inline int round_up(int v, int q) { return (v + q - 1) / q *
 struct LargeLayout {
   int n, m, npad, mpad, nblk, np;
   size_t ctl_off, info_off, v_off, a_off, p_off, g64_off, g32_off, linv_off, sinv_off, xhi_off,
-      xlo_off, total;
+      xlo_off, cp_off, total;
 };
 __host__ __device__ inline LargeLayout plan_large_layout(int n, int m) {
   LargeLayout L;
@@ -74,8 +74,105 @@ __host__ __device__ inline LargeLayout plan_large_layout(int n, int m) {
   off += al(size_t(L.npad) * L.mpad * 4);
   L.xlo_off = off;
   off += al(size_t(L.npad) * L.mpad * 4);
+  L.cp_off = off;  // per-block column sums of large_products
+  off += al(size_t(kLargeBlocks) * L.npad * 8);
   L.total = off;
   return L;
+}
+
+// ---------------------------------------------------------------------------
+// One pass over the rows of A (and P) for the products a KKT residual needs
+// together: the row dots (A vx)_i, passed to row_epi(i, value) by one thread
+// each (none when vx is null), and the column sums c_k = sum_i A_ik vy_i
+// vs_i (vs null: 1) + sum_i P_ik vp_i (when vp is given; P is symmetric, so
+// that is (P vp)_k), passed to col_epi(k, c_k) by the thread k % NT after a
+// grid barrier.  The rows of the stacked matrix
+// [A; P] are cut into one contiguous band per block, and each band into
+// chunks of kPrRows rows; within a tile of kPrTile columns each warp takes
+// kPrCpl x 32 consecutive columns (lane l: columns l + 32 t), so every row is
+// read once, coalesced, with kPrCpl loads in flight per lane, and each lane
+// keeps its columns' sums in registers over the chunk.  The row dots of a
+// chunk are combined over warps and tiles in shared memory; the blocks'
+// column sums go to global memory and are added in block order.  Every sum
+// runs in a fixed order, so the results are the same on every run.
+// ---------------------------------------------------------------------------
+constexpr int kPrCpl = 16;                         // columns per lane in a tile
+constexpr int kPrTile = (kGridBT / 32) * 32 * kPrCpl;  // 4096 columns
+constexpr int kPrRows = 256;                       // rows per chunk (rowpart in smem)
+// The products' shared memory starts behind the diagonal-block inverse (128
+// x 129 doubles) and the partial sums (128) that large_chol_solve keeps
+// resident in the arena from the factorisation on.
+constexpr size_t kPrSmemOff = (size_t(kLB) * (kLB + 1) + kLB) * sizeof(double);
+static_assert(kPrSmemOff + (size_t(kPrRows) * (kGridBT / 32) + kPrTile) * sizeof(double) <=
+                  kArenaBytes, "the products' shared memory exceeds the arena");
+
+template <class S, class RowEpi, class ColEpi>
+__device__ void large_products(S& s, const double* vx, const double* vy, const double* vs,
+                               const double* vp, RowEpi row_epi, ColEpi col_epi) {
+  constexpr int NW = kGridBT / 32;
+  const int n = s.n, m = s.m, lda = s.lda, ldp = s.ldp;
+  const double* A = s.A;
+  const double* P = s.P;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rows = m + (vp != nullptr ? n : 0);
+  const int band = (rows + G - 1) / G;
+  const int r0 = min(rows, b * band), r1 = min(rows, r0 + band);
+  double* rowpart = reinterpret_cast<double*>(s.arena + kPrSmemOff);  // kPrRows x NW
+  double* xs = rowpart + kPrRows * NW;                    // vx of one tile
+  double* part = s.colpart + size_t(b) * s.npad;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) part[k] = 0.0;
+  __syncthreads();
+  for (int c0 = r0; c0 < r1; c0 += kPrRows) {
+    const int c1 = min(r1, c0 + kPrRows);
+    for (int e = threadIdx.x; e < (c1 - c0) * NW; e += blockDim.x) rowpart[e] = 0.0;
+    for (int t0 = 0; t0 < n; t0 += kPrTile) {
+      if (vx != nullptr)
+        for (int k = threadIdx.x; k < kPrTile; k += blockDim.x)
+          xs[k] = t0 + k < n ? vx[t0 + k] : 0.0;
+      __syncthreads();
+      const int cb = t0 + warp * 32 * kPrCpl + lane;  // this lane's first column
+      double acc[kPrCpl];
+#pragma unroll
+      for (int t = 0; t < kPrCpl; ++t) acc[t] = 0.0;
+      for (int i = c0; i < c1; ++i) {
+        const bool arow = i < m;
+        const double* Mi = arow ? A + size_t(i) * lda : P + size_t(i - m) * ldp;
+        const double wi = arow ? (vs != nullptr ? vy[i] * vs[i] : vy[i]) : vp[i - m];
+        double a[kPrCpl];
+#pragma unroll
+        for (int t = 0; t < kPrCpl; ++t) a[t] = cb + 32 * t < n ? Mi[cb + 32 * t] : 0.0;
+        double d = 0.0;
+#pragma unroll
+        for (int t = 0; t < kPrCpl; ++t) acc[t] = fma(a[t], wi, acc[t]);
+        if (arow && vx != nullptr) {  // the row dot (the same branch for the whole warp)
+#pragma unroll
+          for (int t = 0; t < kPrCpl; ++t) d = fma(a[t], xs[cb - t0 + 32 * t], d);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+          if (lane == 0) rowpart[(i - c0) * NW + warp] += d;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < kPrCpl; ++t)
+        if (cb + 32 * t < n) part[cb + 32 * t] += acc[t];
+      __syncthreads();
+    }
+    for (int i = c0 + threadIdx.x; i < c1 && vx != nullptr; i += blockDim.x) {
+      if (i >= m) continue;
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) v += rowpart[(i - c0) * NW + w];
+      row_epi(i, v);
+    }
+    __syncthreads();
+  }
+  s.sync();
+  for (int k = s.tid; k < n; k += kLargeNT) {
+    double v = 0.0;
+    for (int bb = 0; bb < G; ++bb) v += s.colpart[size_t(bb) * s.npad + k];
+    col_epi(k, v);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -801,6 +898,8 @@ __device__ void large_chol_solve(S& s, T* v, T* w) {
   // memory (pitch kPitch) since the factorisation.
   const T* rinv = reinterpret_cast<const T*>(s.arena);
   T* red = reinterpret_cast<T*>(s.arena) + kLB * kPitch;  // [kLB] partials of the owner
+  static_assert((size_t(kLB) * kPitch + kLB) * sizeof(double) <= kPrSmemOff,
+                "large_products would overwrite the resident inverse");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int WPB = kGridBT / 32;
   const int G = gridDim.x;
