@@ -527,16 +527,20 @@ int qtqp_dense_equilibrate(int32_t n, int32_t m, const double* d_a,
 
 /* ---- self-test of the bounded device waits ------------------------------ *
  * No reference counterpart.  Every spin-wait of the kernels gives up after a
- * poll limit and reports an error instead of hanging (the grid barrier of the
- * whole-GPU solves: QTQP_ERR_TIMEOUT from the solve; the tensor-core
- * pipelines' mbarrier waits).  This makes one run out on purpose with a short
+ * poll limit and reports an error instead of hanging (the grid barrier and
+ * the per-block flags of the whole-GPU solves: QTQP_ERR_TIMEOUT from the
+ * solve; the tensor-core pipelines' mbarrier waits).  This makes one run out on purpose with a short
  * limit (limit polls, at most 2^24) and writes the outcome to *d_status
  * (QTQP_OK or QTQP_ERR_TIMEOUT):
  *   mode 0: a cooperative grid of `blocks` blocks (2..64) where block
  *           skip_block never reaches the barrier the others wait at
  *           (skip_block = -1: every block arrives, a control run);
  *           d_workspace: qtqp_wait_selftest_workspace_bytes() bytes;
- *   mode 1: one block waits on an mbarrier that nothing arrives on.
+ *   mode 1: one block waits on an mbarrier that nothing arrives on;
+ *   mode 2: a cooperative grid of `blocks` blocks (2..64) where block b
+ *           waits for block b - 1's flag, then sets its own, and block
+ *           skip_block never sets its flag (-1: a control run); the same
+ *           workspace as mode 0.
  * Nothing faults: the waits stop and the kernels return. */
 size_t qtqp_wait_selftest_workspace_bytes(void);
 int qtqp_wait_selftest(int32_t mode, int32_t blocks, int32_t skip_block,

@@ -110,8 +110,9 @@ constexpr uint32_t kGridWaitLimit = 1u << 25;
 struct GridCtl {
   unsigned int count;  // arrivals in the current generation
   unsigned int gen;    // completed barriers
-  int err;             // 1: a barrier wait gave up
+  int err;             // 1: a barrier or flag wait gave up
   int pad;
+  unsigned int flag[kGridMaxBlocks];        // per-block publication flags (flags_ready)
   double part[2][kGridMaxBlocks][kRedMax];  // per-block partials (double-buffered)
 };
 
@@ -141,6 +142,53 @@ __device__ __forceinline__ void grid_sync(GridCtl* g, uint32_t limit = kGridWait
     }
   }
   __syncthreads();
+}
+
+// Point-to-point hand-off between the blocks of a cooperative grid.  Block c
+// publishes a result by writing it, fencing, and storing a generation number
+// to flag[c] with release semantics (flag_publish); a consumer's warp polls
+// the flags with acquire loads (flags_ready).  Generations only grow within a
+// launch and the flags start at zero with the rest of GridCtl, so a flag is
+// never reset.  A wait that exceeds `limit` polls sets the sticky err flag;
+// every later wait then returns at once, as grid_sync does.
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Called by one whole warp.  Looks at flag[c], flag[c + dir], ... (up to 32
+// of them, stopping before index `end`, dir = +1 or -1) and returns how many
+// consecutive ones, starting at c, have reached `gen`; waits (bounded) until
+// that is at least one.  Returns 0 only when the wait gave up or an earlier
+// wait had (err set).  Every lane returns the same value.
+__device__ __forceinline__ int flags_ready(GridCtl* g, int c, int dir, int end, unsigned int gen,
+                                           uint32_t limit = kGridWaitLimit) {
+  const int lane = threadIdx.x & 31;
+  const int i = c + dir * lane;
+  const bool in = dir > 0 ? i < end : i > end;
+  for (uint32_t it = 0;; ++it) {
+    const bool ok = in && ld_acquire_gpu(&g->flag[i]) >= gen;
+    const unsigned int mask = __ballot_sync(0xffffffffu, ok);
+    if (mask & 1u) return mask == 0xffffffffu ? 32 : __ffs(~mask) - 1;
+    int err = lane == 0 ? *reinterpret_cast<volatile int*>(&g->err) : 0;
+    err = __shfl_sync(0xffffffffu, err, 0);
+    if (err) return 0;
+    if (it >= limit) {
+      if (lane == 0) atomicExch(&g->err, 1);
+      return 0;
+    }
+    if (it >= 256) __nanosleep(64);  // each poll is an L2 round trip; back off later
+  }
+}
+
+// Called by thread 0 after a __syncthreads that follows the block's writes
+// (each writing thread fenced its own stores with __threadfence()).
+__device__ __forceinline__ void flag_publish(GridCtl* g, int c, unsigned int gen) {
+  st_release_gpu(&g->flag[c], gen);
 }
 
 // NS sums and NM maxima over every thread of the grid; all threads receive

@@ -286,6 +286,7 @@ struct Ipm {
   unsigned char* arena;
   uint32_t tmem;
   uint32_t tc_load, tc_mma, tc_tiles;
+  uint32_t tri_gen;  // flag generations used by the whole-GPU triangular solves
 
   __device__ __forceinline__ void sync() const {
     if constexpr (NT > 1024) {

@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(kGridBT, 1)
   s.arena = arena;
   s.tmem = tmem_slot;
   s.tc_load = s.tc_mma = s.tc_tiles = 0;
+  s.tri_gen = 0;
   s.red = red;
   s.phase = 0;
   s.o = &sopt;

@@ -14,7 +14,8 @@
 //             FP64, 8 x 8 register tiles in FP32); then the inverse of every
 //             diagonal block.
 //   Solves    block forward / backward substitution with the inverted
-//             diagonal blocks, one grid barrier per 128-block step.
+//             diagonal blocks; CTA j owns block row j and waits on per-block
+//             flags for the blocks it needs, one grid barrier per solve.
 //
 // Padding: the factor is npad x npad (npad = n rounded up to 128) with an
 // identity on the padded diagonal; X is npad x mpad with zero padding.
@@ -880,13 +881,19 @@ __device__ int large_factorize(S& s) {
 }
 
 // ---------------------------------------------------------------------------
-// L L^T v = v in place (v, w: n entries of T; w is scratch).  Forward:
-// z_b = inv(L_bb) (v_b - sum_{c<b} L_bc z_c) into w; backward:
-// x_b = inv(L_bb)^T (z_b - sum_{c>b} L_cb^T x_c) into v.  Step b: the CTA that
-// owns block b+1 (b-1 backward) applies z_b to that block and immediately
-// forms its next z, while the other CTAs apply z_b to the remaining rows;
-// one grid barrier per step.  Every inner loop keeps several independent
-// loads in flight (the factor streams from HBM / L2).
+// L L^T v = v in place (v, w: n entries of T; w is scratch), block by block
+// with flags instead of grid barriers.  CTA j (j < nb) owns block row j and
+// keeps inv(L_jj) resident in shared memory since the factorisation.
+//   Forward:  z_j = inv(L_jj) (v_j - sum_{c<j} L_jc z_c) into w.  CTA j adds
+//             L_jc z_c as soon as flag c shows z_c published, in the order
+//             c = 0, 1, ..., so only the last product L_{j,j-1} z_{j-1} and
+//             the diagonal step lie on the chain from one block to the next.
+//   Backward: x_j = inv(L_jj)^T (z_j - sum_{c>j} L_cj^T x_c) into v, the
+//             same way from c = nb-1 down.
+// Every sum runs in a fixed order (c ascending or descending, then the
+// lanes' and warps' partials in a fixed tree), so results do not depend on
+// timing.  Flag generations: 2t - 1 (forward) and 2t (backward) for the t-th
+// solve of the launch.  One grid barrier at the end.
 // ---------------------------------------------------------------------------
 template <typename T, class S>
 __device__ void large_chol_solve(S& s, T* v, T* w) {
@@ -894,164 +901,184 @@ __device__ void large_chol_solve(S& s, T* v, T* w) {
   const int nb = (n + kLB - 1) / kLB;
   const T* g = sizeof(T) == 4 ? reinterpret_cast<const T*>(s.g32l)
                               : reinterpret_cast<const T*>(s.g64);
-  // CTA b owns block b (nb <= gridDim.x); inv(L_bb) is resident in its shared
-  // memory (pitch kPitch) since the factorisation.
+  constexpr int WPB = kGridBT / 32;
+  static_assert(WPB * 16 == kLB, "one warp per 16 rows of a block");
+  // Shared memory: inv(L_bb) (pitch kPitch), then the block's right-hand side
+  // (kLB), the warps' column partials of the backward step (WPB x kLB), and
+  // the hand-off of the polling warp's result.
   const T* rinv = reinterpret_cast<const T*>(s.arena);
-  T* red = reinterpret_cast<T*>(s.arena) + kLB * kPitch;  // [kLB] partials of the owner
+  T* red = reinterpret_cast<T*>(s.arena) + kLB * kPitch;
+  T* cpart = red + kLB;
+  volatile int* sready = reinterpret_cast<volatile int*>(cpart + WPB * kLB);
   static_assert((size_t(kLB) * kPitch + kLB) * sizeof(double) <= kPrSmemOff,
                 "large_products would overwrite the resident inverse");
+  static_assert((size_t(kLB) * kPitch + kLB + WPB * kLB) * sizeof(double) + sizeof(int) <=
+                    kArenaBytes, "the solve's shared memory exceeds the arena");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int WPB = kGridBT / 32;
-  const int G = gridDim.x;
+  const int j = blockIdx.x;
   auto bsz = [&](int b) { return min(kLB, n - b * kLB); };
-  // z_b = inv(L_bb) v_b by CTA b (thread r < bs; v_b staged in red).
-  auto diag_fwd = [&](int b) {
-    const int b0 = b * kLB, bs = bsz(b);
-    if (int(threadIdx.x) < bs) red[threadIdx.x] = v[b0 + threadIdx.x];
-    __syncthreads();
-    if (int(threadIdx.x) < bs) {
-      const int r = threadIdx.x;
-      const T* ir = rinv + r * kPitch;
-      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-      int c = 0;
-      for (; c + 3 <= r; c += 4) {
-        a0 = fma(ir[c + 0], red[c + 0], a0);
-        a1 = fma(ir[c + 1], red[c + 1], a1);
-        a2 = fma(ir[c + 2], red[c + 2], a2);
-        a3 = fma(ir[c + 3], red[c + 3], a3);
-      }
-      for (; c <= r; ++c) a0 = fma(ir[c], red[c], a0);
-      w[b0 + r] = (a0 + a1) + (a2 + a3);
+  s.tri_gen += 1;
+  const unsigned int gen_fwd = 2 * s.tri_gen - 1, gen_bwd = 2 * s.tri_gen;
+  GridCtl* gc = s.gctl;
+  // The polling warp's count of consecutive published blocks from c (dir +1
+  // or -1, stopping before `end`), passed to the whole CTA; `none` when the
+  // wait gave up (the solve then runs to its end on whatever is there, and the
+  // sticky error reports it).
+  auto ready_until = [&](int c, int dir, int end) {
+    if (warp == 0) {
+      const int k = flags_ready(gc, c, dir, end, dir > 0 ? gen_fwd : gen_bwd);
+      if (lane == 0) *sready = k > 0 ? c + dir * k : end;
     }
     __syncthreads();
+    const int r = *sready;
+    __syncthreads();
+    return r;
   };
-  // x_b = inv(L_bb)^T w_b by CTA b (thread r < bs; w_b staged in red).
-  auto diag_bwd = [&](int b) {
-    const int b0 = b * kLB, bs = bsz(b);
-    if (int(threadIdx.x) < bs) red[threadIdx.x] = w[b0 + threadIdx.x];
-    __syncthreads();
-    if (int(threadIdx.x) < bs) {
-      const int r = threadIdx.x;
-      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-      int c = r;
-      for (; c + 3 < bs; c += 4) {
-        a0 = fma(rinv[(c + 0) * kPitch + r], red[c + 0], a0);
-        a1 = fma(rinv[(c + 1) * kPitch + r], red[c + 1], a1);
-        a2 = fma(rinv[(c + 2) * kPitch + r], red[c + 2], a2);
-        a3 = fma(rinv[(c + 3) * kPitch + r], red[c + 3], a3);
-      }
-      for (; c < bs; ++c) a0 = fma(rinv[c * kPitch + r], red[c], a0);
-      v[b0 + r] = (a0 + a1) + (a2 + a3);
+  // Brings the 128 x 128 block of g at (row block rb, column block cb) into
+  // L2 ahead of the step that has it on the chain between blocks (L_{j,j-1}
+  // forward, L_{j+1,j} backward), one 128-byte line per request.
+  auto prefetch_block = [&](int rb, int cb) {
+    constexpr int kLines = kLB * int(sizeof(T)) / 128;  // lines per block row
+    const int rows = bsz(rb);
+    for (int e = threadIdx.x; e < rows * kLines; e += blockDim.x) {
+      const T* p = g + size_t(rb * kLB + e / kLines) * npad + cb * kLB +
+                   (e % kLines) * (128 / int(sizeof(T)));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }
-    __syncthreads();
   };
-  // v_i -= L_ib z_b for rows [lo, hi): each warp takes 4 rows at a time,
-  // lanes split the 128 columns (4 each), then 4 shuffle reductions.
-  auto fwd_rows = [&](int b, int lo, int hi, int wfirst, int wcount) {
-    const int b0 = b * kLB, bs = bsz(b);
-    T z[4];
+  QTQP_TIC();
+  if (j < nb) {
+    const int b0 = j * kLB, bs = bsz(j);
+    const int r0 = 16 * warp;  // this warp's 16 rows of the block
+    if (j > 1) prefetch_block(j, j - 1);
+    // Forward: lane partials of rows r0 + r over columns lane + 32 q.
+    T acc[16];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int c = lane + 32 * q;
-      z[q] = c < bs ? w[b0 + c] : T(0);
-    }
-    for (int i = lo + 4 * wfirst; i < hi; i += 4 * wcount) {
-      T acc[4];
+    for (int r = 0; r < 16; ++r) acc[r] = T(0);
+    for (int c = 0; c < j;) {
+      const int hi = ready_until(c, 1, j);
+      for (; c < hi; ++c) {
+        T z[4];
 #pragma unroll
-      for (int rr = 0; rr < 4; ++rr) {
-        acc[rr] = T(0);
-        if (i + rr < hi) {
-          const T* li = g + size_t(i + rr) * npad + b0;
+        for (int q = 0; q < 4; ++q) z[q] = __ldcg(w + c * kLB + lane + 32 * q);
+        const T* lr = g + size_t(b0 + r0) * npad + c * kLB + lane;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int c = lane + 32 * q;
-            if (c < bs) acc[rr] = fma(li[c], z[q], acc[rr]);
+        for (int r = 0; r < 16; ++r) {
+          if (r0 + r < bs) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[r] = fma(lr[size_t(r) * npad + 32 * q], z[q], acc[r]);
           }
         }
       }
+    }
+    // Sum the 16 rows over the warp: each exchange step sends half of the
+    // values to the partner lane and keeps the other half, so lane l ends with
+    // row rsel(l) (lanes l and l ^ 1 hold the same row).
 #pragma unroll
-      for (int rr = 0; rr < 4; ++rr)
-        for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
-      if (lane < 4 && i + lane < hi) {
-        T a = acc[0];
-        if (lane == 1) a = acc[1];
-        if (lane == 2) a = acc[2];
-        if (lane == 3) a = acc[3];
-        v[i + lane] -= a;
+    for (int half = 8, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+      const bool up = (lane & bit) != 0;
+#pragma unroll
+      for (int q = 0; q < half; ++q) {
+        const T send = up ? acc[q] : acc[q + half];
+        const T keep = up ? acc[q + half] : acc[q];
+        acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, bit);
       }
     }
-  };
-  // w_i -= sum_{l in [l0, l1)} L_li x_l for column i (one thread per column,
-  // coalesced over i), returned as the partial sum.
-  auto bwd_col = [&](int b, int i, int l0, int l1) {
-    const int b0 = b * kLB;
-    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-    int l = l0;
-    for (; l + 3 < l1; l += 4) {
-      a0 = fma(g[size_t(b0 + l + 0) * npad + i], v[b0 + l + 0], a0);
-      a1 = fma(g[size_t(b0 + l + 1) * npad + i], v[b0 + l + 1], a1);
-      a2 = fma(g[size_t(b0 + l + 2) * npad + i], v[b0 + l + 2], a2);
-      a3 = fma(g[size_t(b0 + l + 3) * npad + i], v[b0 + l + 3], a3);
+    acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
+    const int rsel = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 +
+                     ((lane >> 1) & 1);
+    if ((lane & 1) == 0 && r0 + rsel < bs) red[r0 + rsel] = v[b0 + r0 + rsel] - acc[0];
+    __syncthreads();
+    {
+      // z_r = sum_{c <= r} inv(L_jj)_rc u_c by two threads per row: the
+      // half-warp h of warp w takes rows 16 w .. 16 w + 15 and the columns
+      // c = h (mod 2) (distinct banks across the half-warp, u_c broadcast).
+      const int r = r0 + (lane & 15), h = lane >> 4;
+      const T* ir = rinv + r * kPitch;
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+      if (r < bs) {
+        int c = h;
+        for (; c + 6 <= r; c += 8) {
+          a0 = fma(ir[c + 0], red[c + 0], a0);
+          a1 = fma(ir[c + 2], red[c + 2], a1);
+          a2 = fma(ir[c + 4], red[c + 4], a2);
+          a3 = fma(ir[c + 6], red[c + 6], a3);
+        }
+        for (; c <= r; c += 2) a0 = fma(ir[c], red[c], a0);
+      }
+      T zr = (a0 + a1) + (a2 + a3);
+      zr += __shfl_xor_sync(0xffffffffu, zr, 16);
+      if (h == 0 && r < bs) {
+        w[b0 + r] = zr;
+        __threadfence();
+      }
     }
-    for (; l < l1; ++l) a0 = fma(g[size_t(b0 + l) * npad + i], v[b0 + l], a0);
-    return (a0 + a1) + (a2 + a3);
-  };
-  // Forward.
-  QTQP_TIC();
-  if (blockIdx.x == 0) diag_fwd(0);
-  s.sync();
-  for (int b = 0; b + 1 < nb; ++b) {
-    const int own = (b + 1) % G;
-    const int nxt0 = (b + 1) * kLB, nxt1 = min(n, nxt0 + kLB);
-    if (int(blockIdx.x) == own) {
-      fwd_rows(b, nxt0, nxt1, warp, WPB);
-      __syncthreads();
-      diag_fwd(b + 1);
-    } else {
-      const int cta = (int(blockIdx.x) - own - 1 + G) % G;  // 0 .. G-2
-      fwd_rows(b, nxt1, n, cta * WPB + warp, (G - 1) * WPB);
-    }
-    s.sync();
+    __syncthreads();
+    if (threadIdx.x == 0) flag_publish(gc, j, gen_fwd);
   }
   QTQP_TOC(kPhLgFwd);
   QTQP_RETIC();
-  // Backward.
-  if (int(blockIdx.x) == (nb - 1) % G) diag_bwd(nb - 1);
-  s.sync();
-  for (int b = nb - 1; b > 0; --b) {
-    const int own = (b - 1) % G;
-    const int prv0 = (b - 1) * kLB, bs = bsz(b);
-    if (int(blockIdx.x) == own) {
-      // 128 columns x 2 halves of the block's rows, combined in shared memory.
-      const int col = threadIdx.x & (kLB - 1), half = threadIdx.x >> 7;
-      const int mid = bs / 2;
-      const T part = bwd_col(b, prv0 + col, half ? mid : 0, half ? bs : mid);
-      if (half) red[kLB + col] = part;
-      __syncthreads();
-      if (!half) w[prv0 + col] -= part + red[kLB + col];
-      __syncthreads();
-      diag_bwd(b - 1);
-    } else {
-      // 32 columns per CTA, the block's rows split over the 8 warps (16 each),
-      // partial sums combined in a fixed order.
-      const int cta = (int(blockIdx.x) - own - 1 + G) % G;
-      const int col = threadIdx.x & 31, part = threadIdx.x >> 5;
-      const int l0 = min(bs, 16 * part), l1 = min(bs, 16 * part + 16);
-      for (int c0 = 32 * cta; c0 < prv0; c0 += 32 * (G - 1)) {
-        const int i = c0 + col;
-        red[part * 32 + col] = i < prv0 ? bwd_col(b, i, l0, l1) : T(0);
-        __syncthreads();
-        if (part == 0 && i < prv0) {
-          T t = red[col];
+  if (j < nb) {
+    const int b0 = j * kLB, bs = bsz(j);
+    const int r0 = 16 * warp;
+    if (j + 1 < nb) prefetch_block(j + 1, j);
+    // Backward: lane partials of columns lane + 32 q of block j over this
+    // warp's 16 rows of every later block.
+    T acc[4];
 #pragma unroll
-          for (int q = 1; q < kGridBT / 32; ++q) t += red[q * 32 + col];
-          w[i] -= t;
+    for (int q = 0; q < 4; ++q) acc[q] = T(0);
+    for (int c = nb - 1; c > j;) {
+      const int lo = ready_until(c, -1, j);
+      for (; c > lo; --c) {
+        const int cb0 = c * kLB, cbs = bsz(c);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          if (r0 + r < cbs) {
+            const T xi = __ldcg(v + cb0 + r0 + r);
+            const T* lr = g + size_t(cb0 + r0 + r) * npad + b0 + lane;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = fma(lr[32 * q], xi, acc[q]);
+          }
         }
-        __syncthreads();
       }
     }
-    s.sync();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cpart[warp * kLB + lane + 32 * q] = acc[q];
+    __syncthreads();
+    if (int(threadIdx.x) < bs) {
+      const int k = threadIdx.x;
+      T t = T(0);
+#pragma unroll
+      for (int q = 0; q < WPB; ++q) t += cpart[q * kLB + k];
+      red[k] = w[b0 + k] - t;  // w_j: this CTA's forward result
+    }
+    __syncthreads();
+    {
+      // x_r = sum_{c >= r} inv(L_jj)_cr u_c, two threads per row as forward
+      // (half-warp h: the columns c >= r with c = r + h (mod 2)).
+      const int r = r0 + (lane & 15), h = lane >> 4;
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+      if (r < bs) {
+        int c = r + h;
+        for (; c + 6 < bs; c += 8) {
+          a0 = fma(rinv[(c + 0) * kPitch + r], red[c + 0], a0);
+          a1 = fma(rinv[(c + 2) * kPitch + r], red[c + 2], a1);
+          a2 = fma(rinv[(c + 4) * kPitch + r], red[c + 4], a2);
+          a3 = fma(rinv[(c + 6) * kPitch + r], red[c + 6], a3);
+        }
+        for (; c < bs; c += 2) a0 = fma(rinv[c * kPitch + r], red[c], a0);
+      }
+      T xr = (a0 + a1) + (a2 + a3);
+      xr += __shfl_xor_sync(0xffffffffu, xr, 16);
+      if (h == 0 && r < bs) {
+        v[b0 + r] = xr;
+        __threadfence();
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) flag_publish(gc, j, gen_bwd);
   }
+  s.sync();
   QTQP_TOC(kPhLgBwd);
 }
 

@@ -8,7 +8,11 @@
 // can check that the error comes back and that the GPU stays usable:
 //   mode 0: a cooperative grid where one host-chosen block never reaches the
 //           barrier the others wait at;
-//   mode 1: a wait on an mbarrier that nothing arrives on.
+//   mode 1: a wait on an mbarrier that nothing arrives on;
+//   mode 2: the per-block flags of the whole-GPU triangular solves
+//           (flags_ready / flag_publish): a cooperative grid where block b
+//           waits for block b - 1's flag and then publishes its own, and a
+//           host-chosen block never publishes.
 // Nothing faults: the waits simply stop and the kernels return.
 #include "common.cuh"
 #include "tc_common.cuh"
@@ -34,6 +38,15 @@ __global__ void __launch_bounds__(kSelftestThreads)
   if (threadIdx.x == 0 && !tc::mbar_wait(&bar, 0, limit)) *status = QTQP_ERR_TIMEOUT;
 }
 
+__global__ void __launch_bounds__(kSelftestThreads)
+    flag_wait_selftest_kernel(GridCtl* g, int skip_block, uint32_t limit) {
+  const int b = blockIdx.x;
+  if (b == skip_block) return;  // never publishes
+  if (b > 0 && threadIdx.x < 32) flags_ready(g, b - 1, 1, b, 1u, limit);
+  __syncthreads();
+  if (threadIdx.x == 0) flag_publish(g, b, 1u);
+}
+
 __global__ void grid_status_kernel(const GridCtl* g, int* status) {
   *status = g->err ? QTQP_ERR_TIMEOUT : QTQP_OK;
 }
@@ -57,7 +70,8 @@ extern "C" int qtqp_wait_selftest(int32_t mode, int32_t blocks, int32_t skip_blo
     mbar_wait_selftest_kernel<<<1, kSelftestThreads, 0, st>>>(limit, d_status);
     return cuda_check(cudaGetLastError(), "mbar_wait_selftest_kernel launch");
   }
-  if (mode != 0) return fail(QTQP_ERR_BAD_ARG, "qtqp_wait_selftest: mode must be 0 or 1");
+  if (mode != 0 && mode != 2)
+    return fail(QTQP_ERR_BAD_ARG, "qtqp_wait_selftest: mode must be 0, 1 or 2");
   if (d_workspace == nullptr || blocks < 2 || blocks > 64 || skip_block < -1 ||
       skip_block >= blocks)
     return fail(QTQP_ERR_BAD_ARG, "qtqp_wait_selftest: need a workspace, 2..64 blocks and "
@@ -77,10 +91,19 @@ extern "C" int qtqp_wait_selftest(int32_t mode, int32_t blocks, int32_t skip_blo
   rc = cuda_check(cudaMemsetAsync(g, 0, sizeof(GridCtl), st), "cudaMemsetAsync");
   if (rc) return rc;
   int skip = skip_block, rounds = 4;
-  void* args[] = {&g, &skip, &rounds, &limit};
-  rc = cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(grid_wait_selftest_kernel),
-                                              dim3(blocks), dim3(kSelftestThreads), args, 0, st),
-                  "grid_wait_selftest_kernel launch");
+  if (mode == 0) {
+    void* args[] = {&g, &skip, &rounds, &limit};
+    rc = cuda_check(
+        cudaLaunchCooperativeKernel(reinterpret_cast<void*>(grid_wait_selftest_kernel),
+                                    dim3(blocks), dim3(kSelftestThreads), args, 0, st),
+        "grid_wait_selftest_kernel launch");
+  } else {
+    void* args[] = {&g, &skip, &limit};
+    rc = cuda_check(
+        cudaLaunchCooperativeKernel(reinterpret_cast<void*>(flag_wait_selftest_kernel),
+                                    dim3(blocks), dim3(kSelftestThreads), args, 0, st),
+        "flag_wait_selftest_kernel launch");
+  }
   if (rc) return rc;
   grid_status_kernel<<<1, 1, 0, st>>>(g, d_status);
   return cuda_check(cudaGetLastError(), "grid_status_kernel launch");
