@@ -451,8 +451,10 @@ int qtqp_mlp_decode(const float* d_pred, const double* d_scale,
 /* ---- one large dense QP on the whole GPU ---------------------------------- *
  * Replaces QTQP._solve_impl (src/qtqp/__init__.py:351-614) with the dense
  * KKT backend (src/qtqp/solvers_dense.py:25-145) for a single large QP: the
- * same device IPM as the batch, run by one cooperative launch of 128 blocks
- * (grid barriers and reductions), with a blocked Gram + Cholesky factor
+ * same device IPM as the batch, run by one cooperative launch of
+ * qtqp_dense_large_blocks() blocks, one per SM of a B200 (grid barriers and
+ * reductions; the triangular solves hand blocks over through per-block
+ * flags), with a blocked Gram + Cholesky factor
  * (Gram on tcgen05 tensor cores, TF32 hi + lo split, when opt->precision is
  * QTQP_PREC_MIXED; FP64 otherwise) and blocked triangular solves.
  * flags: QTQP_LARGE_HAS_P (P is given) | QTQP_LARGE_COLMAJOR (A and P are
@@ -460,9 +462,11 @@ int qtqp_mlp_decode(const float* d_pred, const double* d_scale,
  * A: m x n FP64, P: n x n FP64 (null without QTQP_LARGE_HAS_P); b, c inputs; x, y, s, *d_result outputs (as the batch); d_stats:
  * qtqp_iter_stats[max_iter] or NULL.  The workspace (>=
  * qtqp_dense_large_workspace_bytes(n, m), 1024-byte aligned) is private.
- * m * n < 2^31.  A grid barrier that waits too long ends the solve with
- * status FAILED and error QTQP_ERR_TIMEOUT. */
+ * n <= 128 * qtqp_dense_large_blocks(), m * n < 2^31.  A grid barrier or
+ * flag wait that waits too long ends the solve with status FAILED and error
+ * QTQP_ERR_TIMEOUT. */
 size_t qtqp_dense_large_workspace_bytes(int32_t n, int32_t m);
+int32_t qtqp_dense_large_blocks(void);
 #define QTQP_LARGE_HAS_P 1
 #define QTQP_LARGE_COLMAJOR 2
 int qtqp_dense_large_solve(int32_t n, int32_t m, int32_t z, int32_t flags,

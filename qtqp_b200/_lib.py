@@ -62,6 +62,7 @@ EXPORTS = (
     "qtqp_mlp_adam",
     "qtqp_mlp_decode",
     "qtqp_dense_large_workspace_bytes",
+    "qtqp_dense_large_blocks",
     "qtqp_dense_large_solve",
     "qtqp_tc_split_tf32",
     "qtqp_tc_gram_f32",
@@ -227,6 +228,8 @@ def load() -> ctypes.CDLL:
     lib.qtqp_mlp_decode.argtypes = [vp, vp, vp, i32, i32, i32, i32, f64, vp, vp, vp, vp]
     lib.qtqp_dense_large_workspace_bytes.restype = sz
     lib.qtqp_dense_large_workspace_bytes.argtypes = [i32, i32]
+    lib.qtqp_dense_large_blocks.restype = i32
+    lib.qtqp_dense_large_blocks.argtypes = []
     lib.qtqp_dense_large_solve.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp,
                                            vp, vp, sz, ctypes.POINTER(Options), vp]
     lib.qtqp_band_grid_default_parts.restype = i32

@@ -306,8 +306,16 @@ struct Ipm {
   }
 
   __device__ __forceinline__ double* vec(int id) const { return V + size_t(id) * np; }
-  // First index >= lo owned by this thread (k % NT == tid).
-  __device__ __forceinline__ int own(int lo) const { return lo + ((tid - lo) & (NT - 1)); }
+  // First index >= lo owned by this thread (k % NT == tid).  NT is a power of
+  // two except for the large grid (one CTA per SM of a B200: 148 x 256).
+  __device__ __forceinline__ int own(int lo) const {
+    if constexpr ((NT & (NT - 1)) == 0) {
+      return lo + ((tid - lo) & (NT - 1));
+    } else {
+      const int d = (tid - lo) % NT;
+      return lo + (d < 0 ? d + NT : d);
+    }
+  }
   __device__ __forceinline__ float* g32() const { return reinterpret_cast<float*>(G); }
 
   // Lanes cooperating on one dot product when K outputs share the block.

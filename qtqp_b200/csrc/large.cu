@@ -109,6 +109,8 @@ __global__ void __launch_bounds__(kGridBT, 1)
 
 using namespace qtqp;
 
+extern "C" int32_t qtqp_dense_large_blocks(void) { return kLargeBlocks; }
+
 extern "C" size_t qtqp_dense_large_workspace_bytes(int32_t n, int32_t m) {
   if (n < 1 || m < 1) return 0;
   return plan_large_layout(n, m).total;

@@ -27,8 +27,8 @@
 namespace qtqp {
 
 constexpr int kLB = 128;                          // panel / diagonal block size
-constexpr int kLargeBlocks = 128;                 // CTAs of the cooperative grid
-constexpr int kLargeNT = kLargeBlocks * kGridBT;  // 32768 threads
+constexpr int kLargeBlocks = 148;                 // CTAs of the cooperative grid: one per SM
+constexpr int kLargeNT = kLargeBlocks * kGridBT;  // 37888 threads
 constexpr int kTcStages = 3;
 constexpr uint32_t kTcTileBytes = kLB * 32 * 4;        // 128 rows x 32 FP32
 constexpr uint32_t kTcStageBytes = 4 * kTcTileBytes;   // A hi, B hi, A lo, B lo

@@ -52,7 +52,7 @@ def _runner(args):
     a, b, c, z, p = problems.large_dense(n=args.n, m=2 * args.n, z=args.n // 4)
     dl = large.DeviceLarge(batch.DenseProblem(a=a, b=b, c=c, z=z, p=p), opts, records=False)
     dl.upload()
-    return dl.launch, 128, lambda: dl.fetch()[0]
+    return dl.launch, int(_lib.load().qtqp_dense_large_blocks()), lambda: dl.fetch()[0]
   if args.workload == "sparse":
     a, b, c, z, p = problems.grid_flow(args.grid)
   elif args.workload == "sparse_random":

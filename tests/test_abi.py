@@ -43,6 +43,12 @@ def test_version_and_last_error(lib):
   assert isinstance(lib.qtqp_last_error(), bytes)
 
 
+def test_large_grid_is_one_block_per_b200_sm(lib):
+  assert lib.qtqp_dense_large_blocks() == 148
+  assert lib.qtqp_dense_large_workspace_bytes(4096, 8192) > 8 * 4096 * 8192
+  assert lib.qtqp_dense_large_workspace_bytes(0, 8) == 0
+
+
 def test_plan_orders_by_cost_and_sizes_workspace(lib):
   probs = [batch.DenseProblem(*_dense(problems.small_dense_instance(i))) for i in range(50)]
   hb = batch.HostBatch(probs, batch.SolveOptions())
