@@ -327,7 +327,10 @@ enum Phase : int {
   kPhBpCrStage, kPhBpCrSweep, kPhBpCrGemm, kPhBpCrGather,
   // Sub-phases of the supernodal factorisation and solves (subtrees / top levels).
   kPhSnSub, kPhSnTop, kPhSnFwdSub, kPhSnFwdTop, kPhSnBwdTop, kPhSnBwdSub,
-  kPhSnTopUpd, kPhSnTopDiag, kPhSnTopPanel, kNumPhases
+  kPhSnTopUpd, kPhSnTopDiag, kPhSnTopPanel,
+  // Sub-phases of the dense KKT solve: the column sums A^T (r_y / Ry) and the
+  // row products A x around the triangular solves.
+  kPhSolveCols, kPhSolveRows, kNumPhases
 };
 #ifdef QTQP_PHASE_TIMERS
 extern __device__ unsigned long long g_phase_cycles[kNumPhases];

@@ -1125,12 +1125,21 @@ struct Ipm {
     // (In grid mode a lane group per column streams A with many loads in
     // flight; a row pass with per-block column sums measured slower here,
     // where no row dot rides along.)
-    rowdot<1>(n, m,
-              [&](int k, int i, double* acc) {
-                acc[0] = fma(Ap[i * ld + k], iry[nn + i] * r[nn + i], acc[0]);
-              },
-              [&](int k, double* acc) { put_g(k, r[k] + acc[0]); });
-    sync();
+    {
+      QTQP_TIC();
+      if constexpr (FMT == kFmtLarge) {
+        large_products(*this, nullptr, r + n, iry + n, nullptr, [](int, double) {},
+                       [&](int k, double cs) { put_g(k, r[k] + cs); });
+      } else {
+        rowdot<1>(n, m,
+                  [&](int k, int i, double* acc) {
+                    acc[0] = fma(Ap[i * ld + k], iry[nn + i] * r[nn + i], acc[0]);
+                  },
+                  [&](int k, double* acc) { put_g(k, r[k] + acc[0]); });
+      }
+      sync();
+      QTQP_TOC(kPhSolveCols);
+    }
     if (fp64) {
       chol_solve<double>(G, tmp, vec(kW));
     } else {
@@ -1141,15 +1150,19 @@ struct Ipm {
       out[k] = accumulate ? out[k] + val : val;
     }
     // y = (A x - r_y) / Ry
-    rowdot<1, false, kRowS>(m, n,
-              [&](int k, int j, double* acc) {
-                const double xj = fp64 ? tmp[j] : double(t32[j]);
-                acc[0] = fma(Ap[k * ld + j], xj, acc[0]);
-              },
-              [&](int k, double* acc) {
-                const double val = iry[nn + k] * (acc[0] - r[nn + k]);
-                out[nn + k] = accumulate ? out[nn + k] + val : val;
-              });
+    {
+      QTQP_TIC();
+      rowdot<1, false, kRowS>(m, n,
+                [&](int k, int j, double* acc) {
+                  const double xj = fp64 ? tmp[j] : double(t32[j]);
+                  acc[0] = fma(Ap[k * ld + j], xj, acc[0]);
+                },
+                [&](int k, double* acc) {
+                  const double val = iry[nn + k] * (acc[0] - r[nn + k]);
+                  out[nn + k] = accumulate ? out[nn + k] + val : val;
+                });
+      QTQP_TOC(kPhSolveRows);
+    }
     QTQP_TOC(kPhSolve);
   }
 

@@ -136,23 +136,53 @@ __device__ void large_products(S& s, const double* vx, const double* vy, const d
       double acc[kPrCpl];
 #pragma unroll
       for (int t = 0; t < kPrCpl; ++t) acc[t] = 0.0;
-      for (int i = c0; i < c1; ++i) {
-        const bool arow = i < m;
-        const double* Mi = arow ? A + size_t(i) * lda : P + size_t(i - m) * ldp;
-        const double wi = arow ? (vs != nullptr ? vy[i] * vs[i] : vy[i]) : vp[i - m];
-        double a[kPrCpl];
-#pragma unroll
-        for (int t = 0; t < kPrCpl; ++t) a[t] = cb + 32 * t < n ? Mi[cb + 32 * t] : 0.0;
-        double d = 0.0;
-#pragma unroll
-        for (int t = 0; t < kPrCpl; ++t) acc[t] = fma(a[t], wi, acc[t]);
-        if (arow && vx != nullptr) {  // the row dot (the same branch for the whole warp)
+      auto row_of = [&](int i) {
+        return i < m ? A + size_t(i) * lda : P + size_t(i - m) * ldp;
+      };
+      auto weight_of = [&](int i) {
+        return i < m ? (vs != nullptr ? vy[i] * vs[i] : vy[i]) : vp[i - m];
+      };
+      // The row dot of row i from its loaded values (the same branch for the
+      // whole warp).
+      auto row_dot = [&](int i, const double (&a)[kPrCpl]) {
+        if (i < m && vx != nullptr) {
+          double d = 0.0;
 #pragma unroll
           for (int t = 0; t < kPrCpl; ++t) d = fma(a[t], xs[cb - t0 + 32 * t], d);
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
           if (lane == 0) rowpart[(i - c0) * NW + warp] += d;
         }
+      };
+      // Two rows per step, all of their loads issued before the first use
+      // (2 x kPrCpl loads in flight per lane); the column sums still add row
+      // i before row i + 1.
+      int i = c0;
+      for (; i + 1 < c1; i += 2) {
+        const double* M0 = row_of(i);
+        const double* M1 = row_of(i + 1);
+        double a0[kPrCpl], a1[kPrCpl];
+#pragma unroll
+        for (int t = 0; t < kPrCpl; ++t) {
+          const bool in = cb + 32 * t < n;
+          a0[t] = in ? M0[cb + 32 * t] : 0.0;
+          a1[t] = in ? M1[cb + 32 * t] : 0.0;
+        }
+        const double w0 = weight_of(i), w1 = weight_of(i + 1);
+#pragma unroll
+        for (int t = 0; t < kPrCpl; ++t) acc[t] = fma(a1[t], w1, fma(a0[t], w0, acc[t]));
+        row_dot(i, a0);
+        row_dot(i + 1, a1);
+      }
+      if (i < c1) {
+        const double* M0 = row_of(i);
+        double a0[kPrCpl];
+#pragma unroll
+        for (int t = 0; t < kPrCpl; ++t) a0[t] = cb + 32 * t < n ? M0[cb + 32 * t] : 0.0;
+        const double w0 = weight_of(i);
+#pragma unroll
+        for (int t = 0; t < kPrCpl; ++t) acc[t] = fma(a0[t], w0, acc[t]);
+        row_dot(i, a0);
       }
 #pragma unroll
       for (int t = 0; t < kPrCpl; ++t)

@@ -32,7 +32,8 @@ PHASES = ["load", "normalize", "gram", "chol", "solve", "residual", "tau", "step
           "other", "lg_diag", "lg_panel", "lg_trail", "lg_inv", "lg_fwd", "lg_bwd",
           "bp_interior", "bp_chain", "bp_fwd", "bp_chains", "bp_bwd", "cr_stage", "cr_sweep",
           "cr_gemm", "cr_gather", "sn_sub", "sn_top", "sn_fwd_sub", "sn_fwd_top",
-          "sn_bwd_top", "sn_bwd_sub", "sn_top_upd", "sn_top_diag", "sn_top_panel"]
+          "sn_bwd_top", "sn_bwd_sub", "sn_top_upd", "sn_top_diag", "sn_top_panel",
+          "solve_cols", "solve_rows"]
 
 
 def _runner(args):
