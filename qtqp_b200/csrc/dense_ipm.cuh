@@ -167,7 +167,8 @@ struct IrOutcome {
   (void)tid; (void)n; (void)m; (void)z; (void)N; (void)lda; (void)ldp; (void)ldg; \
   (void)A; (void)P; (void)G; (void)has_p
 
-// Independent partial sums per lane of a block's row dots (rowdot).
+// Independent partial sums per lane of a block's row dots (rowdot) outside
+// the per-block dense format, which sets its own by block size (rowdot).
 #ifndef QTQP_ROWDOT_UNROLL
 #define QTQP_ROWDOT_UNROLL 4
 #endif
@@ -347,8 +348,15 @@ struct Ipm {
       if (k < K) {
         // U independent partial sums per lane keep U loads (and U FMA
         // chains) in flight: grid mode streams A and P from HBM; a block's
-        // loads come from shared memory or L2.
-        constexpr int U = NT > 1024 ? 16 : QTQP_ROWDOT_UNROLL;
+        // loads come from shared memory or L2.  The per-block dense format
+        // keeps its loops short (one or two sums): its QPs are small, and
+        // several blocks per SM run different phases of the IPM, whose code
+        // then competes for the instruction cache (measured per block size:
+        // 2-14 % faster at n = 16..64 than four sums).
+        constexpr int U = NT > 1024                           ? 16
+                          : (FMT == kFmtDense && NT <= 128)   ? 1
+                          : FMT == kFmtDense                  ? 2
+                                                              : QTQP_ROWDOT_UNROLL;
         AccT part[U][NACC];
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -1001,11 +1009,17 @@ struct Ipm {
   }
 
   // In-place inverse of each 32x32 lower-triangular diagonal block of L, one
-  // warp per block, lane c computing column c in registers (top-down):
-  // X_cc = 1 / L_cc, X_rc = -(sum_{c<=k<r} L_rk X_kc) / L_rr for r > c, with
-  // L read from shared memory (the same entry in every lane: a broadcast).
+  // warp per block, lane c computing column c top-down:
+  // X_cc = 1 / L_cc, X_rc = -(sum_{c<=k<r} L_rk X_kc) / L_rr for r > c.
   // Both Cholesky variants already store 1 / L_jj on the diagonal, which is
-  // also the inverse's diagonal.
+  // also the inverse's diagonal.  Lane c keeps X_kc (k > c) in the block's
+  // unused upper triangle at (c, k), so with the diagonal U_ck = X_kc for
+  // every k >= c; L_rk is the same entry in every lane (a broadcast).  The
+  // loops stay rolled: the batch kernel runs many QPs per SM at different
+  // phases, and its per-iteration code has to stay small for the
+  // instruction cache.  The sums run in the same order (even k into a0, odd
+  // k into a1) as the fully unrolled register form did.  After the warp's
+  // columns are done, the upper triangle is copied into the lower one.
   template <typename T>
   QTQP_PHASE void invert_diag_blocks(T* g) {
     QTQP_LOCALS;
@@ -1016,28 +1030,33 @@ struct Ipm {
       const int kb = blk * 32, bs = min(32, n - kb);
       T* L = g + kb * ldg + kb;
       const int c = lane;
-      T x[32];
-#pragma unroll
-      for (int r = 0; r < 32; ++r) {
+      T* U = L + c * ldg;  // row c: U[k] = X_kc for k >= c
+#pragma unroll 1
+      for (int r = 1; r < bs; ++r) {
+        const T* Lr = L + r * ldg;
         T a0 = T(0), a1 = T(0);
+        // Eight entries per step (loads issued ahead of the two FMA chains).
+#pragma unroll 1
+        for (int k = 0; k < r; k += 8) {
+          T lv[8], uv[8];
 #pragma unroll
-        for (int k = 0; k < r; ++k) {
-          if (k >= c && r < bs) {  // rows past the block are never read
-            if (k & 1) {
-              a1 = fma(L[r * ldg + k], x[k], a1);
-            } else {
-              a0 = fma(L[r * ldg + k], x[k], a0);
-            }
+          for (int u = 0; u < 8; ++u) {
+            const bool in = k + u < r && k + u >= c;
+            lv[u] = in ? Lr[k + u] : T(0);
+            uv[u] = in ? U[k + u] : T(0);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; u += 2) {
+            if (k + u < r && k + u >= c) a0 = fma(lv[u], uv[u], a0);
+            if (k + u + 1 < r && k + u + 1 >= c) a1 = fma(lv[u + 1], uv[u + 1], a1);
           }
         }
-        const T idg = r < bs ? L[r * ldg + r] : T(0);
-        x[r] = r < c ? T(0) : (r == c ? idg : -(a0 + a1) * idg);
+        if (c < r) U[r] = -(a0 + a1) * Lr[r];
       }
       __syncwarp();
       if (c < bs) {
-#pragma unroll
-        for (int r = 0; r < 32; ++r)
-          if (r > c && r < bs) L[r * ldg + c] = x[r];
+#pragma unroll 1
+        for (int r = c + 1; r < bs; ++r) L[r * ldg + c] = U[r];
       }
       __syncwarp();
     }
@@ -1354,26 +1373,33 @@ struct Ipm {
               [&](int k, double* acc) { out[nn + k] = acc[0] - (-reg[nn + k]) * v[nn + k]; });
   }
 
-  // --------------------------------------------------------------------------
-  // DirectKktSolver.solve (direct.py:218-307).  `rhs_k(k)` produces the
-  // un-negated right-hand side element k (owner-wise); `sol` holds the warm
-  // start and receives the solution.  Entry: sol complete (barrier passed).
-  // --------------------------------------------------------------------------
+  // The KKT right-hand side of a solve into vec(kRHS): krhs[k] = rhs_k(k),
+  // negated on the dual block (k >= n), owner-wise (k % NT == tid).
   template <typename RhsF>
-  QTQP_PHASE IrOutcome ir_solve(RhsF rhs_k, double* sol, bool fp64) {
-    const qtqp_options& op = *o;
+  __device__ __forceinline__ void set_rhs(RhsF rhs_k) {
     double* krhs = vec(kRHS);
+    for (int k = tid; k < N; k += NT) {
+      const double r = rhs_k(k);
+      krhs[k] = k >= n ? -r : r;
+    }
+  }
+
+  // --------------------------------------------------------------------------
+  // DirectKktSolver.solve (direct.py:218-307).  The right-hand side is in
+  // vec(kRHS) (set_rhs, written owner-wise by this thread); `sol` holds the
+  // warm start and receives the solution.  Entry: sol complete (barrier
+  // passed).  One copy of this function serves every solve of an iteration,
+  // which keeps the per-iteration code small for the instruction cache.
+  // --------------------------------------------------------------------------
+  QTQP_PHASE IrOutcome ir_solve(double* sol, bool fp64) {
+    const qtqp_options& op = *o;
+    const double* krhs = vec(kRHS);
     double* res = vec(kRES);
     double dummy[1] = {0.0};
     IrOutcome out;
     {
       double mx[3] = {0.0, 0.0, 0.0};  // |rhs|, |res|, nan(sol)
-      for (int k = tid; k < N; k += NT) {
-        double r = rhs_k(k);
-        if (k >= n) r = -r;
-        krhs[k] = r;
-        mx[0] = nanmax(mx[0], fabs(r));
-      }
+      for (int k = tid; k < N; k += NT) mx[0] = nanmax(mx[0], fabs(krhs[k]));
       sync();
       QTQP_TIC();
       kkt_residual(sol, krhs, res, mx[1], mx[2]);
@@ -1428,12 +1454,15 @@ struct Ipm {
   // not converge is replaced by an FP64 factor (kept for the rest of the
   // solve) and the refinement is redone from the same warm start, so the
   // outcome is the one the plain FP64 path would produce.
-  template <typename RhsF, typename WarmF>
-  __device__ IrOutcome ir_solve_policy(RhsF rhs_k, WarmF warm_k, double* sol, bool& fp64,
+  // `warm` is the warm start (a vector that the solve leaves unchanged); the
+  // right-hand side is set once and kept in vec(kRHS) for the second try.
+  template <typename RhsF>
+  __device__ IrOutcome ir_solve_policy(RhsF rhs_k, const double* warm, double* sol, bool& fp64,
                                        int& n32, int& n64, int& err) {
-    for (int k = tid; k < N; k += NT) sol[k] = warm_k(k);
+    set_rhs(rhs_k);
+    for (int k = tid; k < N; k += NT) sol[k] = warm[k];
     sync();
-    IrOutcome r = ir_solve(rhs_k, sol, fp64);
+    IrOutcome r = ir_solve(sol, fp64);
     if (!fp64 && r.status != 1) {
       fp64 = true;
       ++n64;
@@ -1442,9 +1471,9 @@ struct Ipm {
         err = QTQP_ERR_NOT_SPD;
         return r;
       }
-      for (int k = tid; k < N; k += NT) sol[k] = warm_k(k);
+      for (int k = tid; k < N; k += NT) sol[k] = warm[k];
       sync();
-      r = ir_solve(rhs_k, sol, fp64);
+      r = ir_solve(sol, fp64);
     }
     return r;
   }
@@ -1837,7 +1866,7 @@ struct Ipm {
       }
       if (info != 0) return false;  // not an error of the problem: fall back
       int err = 0;
-      IrOutcome r = ir_solve_policy([&](int k) { return -q[k]; }, [&](int k) { return xy[k]; },
+      IrOutcome r = ir_solve_policy([&](int k) { return -q[k]; }, xy,
                                     xyc, fp64, n32, n64, err);
       nsolves += r.solves;
       if (err || r.nan) return false;
@@ -2041,7 +2070,7 @@ struct Ipm {
       }
       // kinv_q = K^{-1} q, warm-started (__init__.py:484).
       for (int k = tid; k < N; k += NT) kq0[k] = kq[k];
-      IrOutcome rq = ir_solve_policy([&](int k) { return q[k]; }, [&](int k) { return kq0[k]; },
+      IrOutcome rq = ir_solve_policy([&](int k) { return q[k]; }, kq0,
                                      kq, fp64, n32, n64, err);
       nsolves += rq.solves;
       if (err) break;
@@ -2099,7 +2128,7 @@ struct Ipm {
         if (k >= n + z) r += s[k];
         return r;
       };
-      IrOutcome rp = ir_solve_policy(rhs_pred, [&](int k) { return xy[k]; }, xyp, fp64, n32,
+      IrOutcome rp = ir_solve_policy(rhs_pred, xy, xyp, fp64, n32,
                                      n64, err);
       nsolves += rp.solves;
       if (err) break;
@@ -2162,7 +2191,7 @@ struct Ipm {
         return r;
       };
       sync();  // x_p, y_p complete before the corrector reads them
-      IrOutcome rc = ir_solve_policy(rhs_corr, [&](int k) { return xyp[k]; }, xyc, fp64, n32,
+      IrOutcome rc = ir_solve_policy(rhs_corr, xyp, xyc, fp64, n32,
                                      n64, err);
       nsolves += rc.solves;
       if (err) break;
