@@ -84,6 +84,8 @@ def _args():
   ap.add_argument("--no-cpu-baseline", action="store_true")
   ap.add_argument("--no-tune", action="store_true",
                   help="batch_small: use the library's default launch shapes")
+  ap.add_argument("--no-tune-batch-pass", action="store_true",
+                  help="batch_small: tune each launch group alone only (no whole-batch pass)")
   return ap.parse_args()
 
 
@@ -256,7 +258,8 @@ def run_ours(args) -> None:
   tuning, t_tune = None, 0.0
   if not args.no_tune:
     t0 = time.perf_counter()
-    tuning = autotune.tune_dense_batch(qps, batch.SolveOptions(precision="fp64"), device=dev)
+    tuning = autotune.tune_dense_batch(qps, batch.SolveOptions(precision="fp64"), device=dev,
+                                       batch_pass=not args.no_tune_batch_pass)
     t_tune = time.perf_counter() - t0
 
   def prepare(precision):
@@ -426,8 +429,12 @@ def run_ours(args) -> None:
                    "launch_groups": [list(g) for g in hb.groups],
                    "autotuned": None if tuning is None else {
                        "seconds": round(t_tune, 2),
+                       "columns": ["n_lo", "n_hi", "block_threads", "lean", "onchip",
+                                   "default_ms alone", "ms alone"],
                        "table": [[e["n_lo"], e["n_hi"], e["block_threads"], e["lean"],
-                                  e["onchip"], e["default_ms"], e["ms"]] for e in tuning]}},
+                                  e["onchip"], e["default_ms"], e["ms"]] for e in tuning],
+                       "batch_default_ms": tuning[0]["batch_default_ms"] if tuning else None,
+                       "batch_ms": tuning[0]["batch_ms"] if tuning else None}},
         "fp64_value": fp64_value, "chosen_over_fp64": value / fp64_value,
         "mixed_value": mixed_solved * args.steps / forms["mixed"]["time"],
         "mixed_statuses_identical_to_fp64": bool(np.array_equal(

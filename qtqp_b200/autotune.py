@@ -6,8 +6,17 @@ shape: threads per block, the register-capped ("lean") or unrestricted
 kernel, and whether A and P stay in shared memory or are read through L2.
 The default plan chooses by heuristics.  tune_dense_batch times every
 candidate shape on each launch group of a representative batch, on the
-device (CUDA events, each group launched alone), keeps the fastest, and
-returns a table of {n_lo, n_hi, block_threads, lean, onchip} entries that
+device (CUDA events), in two stages:
+
+1. each group launched alone, keeping its fastest shape;
+2. the whole batch, whose groups run concurrently on side streams: one pass
+   of coordinate descent over the groups (largest first) that changes a
+   group's shape only when the whole solve gets faster.  A group that is
+   fastest alone with large blocks (low latency per QP) can be faster inside
+   the batch with small ones (more QPs per SM), because the other groups
+   fill the GPU meanwhile.
+
+It returns a table of {n_lo, n_hi, block_threads, lean, onchip} entries that
 qtqp_dense_batch_plan_tuned applies to later plans.  Tables are cached per
 GPU model in a JSON file (save / load), which solve_batch picks up.
 """
@@ -54,13 +63,34 @@ def _time_group(torch, db, g, stream, reps) -> float:
   return best
 
 
+def _time_batch(torch, db, stream, reps, flush) -> float:
+  """Mean ms of `reps` whole-batch solves, each after a write of `flush` (a
+  buffer larger than L2), as a caller that solves one batch at a time sees
+  them."""
+  db.launch(stream)  # warm-up
+  total = 0.0
+  for _ in range(reps):
+    flush.fill_(1)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    db.launch(stream)
+    e1.record(stream)
+    e1.synchronize()
+    total += e0.elapsed_time(e1)
+  return total / reps
+
+
 def tune_dense_batch(problems, opts: _batch.SolveOptions | None = None, candidates=None,
-                     reps: int = 3, device=None) -> list[dict]:
+                     reps: int = 3, device=None, batch_pass: bool = True) -> list[dict]:
   """Times each candidate (block_threads, lean, onchip) on every launch group
   of the default plan of `problems` and returns the tuning table of the
-  fastest shapes (ms of the default and the chosen shape in each entry).  A
-  candidate that changes any instance's status against the default shape is
-  never chosen."""
+  chosen shapes.  Each entry carries ms and default_ms (the group launched
+  alone with the chosen and the default shape) and batch_ms and
+  batch_default_ms (the whole batch solve with the table and with the
+  default plan).  A candidate that changes any instance's status against the
+  default shape is never chosen.  batch_pass=False keeps the first stage
+  only."""
   torch = _lib.require_device()
   opts = opts or _batch.SolveOptions()
   dev = torch.device(device or "cuda")
@@ -69,15 +99,20 @@ def tune_dense_batch(problems, opts: _batch.SolveOptions | None = None, candidat
   db = _batch.DeviceBatch(hb, device=dev, records=False)
   db.upload(stream)
   groups = [(hb.group_n_range(g), hb.plan.groups[g]) for g in range(hb.plan.num_groups)]
-  table = []
+  alone = {}    # (group, candidate) -> ms alone (valid candidates only)
+  default = {}  # group -> ms alone with the default shape
+  chosen = {}   # group -> entry of the fastest shape alone (None: the default)
+  cands_of = {}
   for g, ((n_lo, n_hi), grp) in enumerate(groups):
     hb.replan(None)
     db.refresh_plan()
     t_default = _time_group(torch, db, g, stream, reps)
+    default[g] = t_default
     ids = hb.order[grp.begin:grp.begin + grp.count]
     status_ref = db.fetch()[0]["status"][ids].copy()
     best = (t_default, None)
     cands = candidates or (CANDIDATES + (SMALL_CANDIDATES if n_hi <= SMALL_N else []))
+    cands_of[g] = []
     for nt, lean, onchip in cands:
       entry = {"n_lo": n_lo, "n_hi": n_hi, "block_threads": nt, "lean": lean,
                "onchip": onchip}
@@ -90,12 +125,71 @@ def tune_dense_batch(problems, opts: _batch.SolveOptions | None = None, candidat
       status = db.fetch()[0]["status"][ids]
       if not np.array_equal(status, status_ref):
         continue
+      alone[(g, (nt, lean, onchip))] = t
+      cands_of[g].append(entry)
       if t < best[0]:
         best = (t, entry)
-    if best[1] is not None:
-      entry = dict(best[1])
-      entry.update({"ms": round(best[0], 4), "default_ms": round(t_default, 4)})
-      table.append(entry)
+    chosen[g] = best[1]
+
+  def table_of(sel):
+    return [sel[g] for g in sorted(sel) if sel[g] is not None]
+
+  # 256 MiB, larger than the 126 MB L2 of a B200 (the write evicts it).
+  flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+  hb.replan(None)
+  db.refresh_plan()
+  t_batch_default = _time_batch(torch, db, stream, reps, flush)
+  status_all = db.fetch()[0]["status"].copy()
+
+  def time_table(sel, r=reps):
+    hb.replan(table_of(sel) or None)
+    db.refresh_plan()
+    try:
+      t = _time_batch(torch, db, stream, r, flush)
+    except _lib.QtqpCudaError:
+      return None
+    if not np.array_equal(db.fetch()[0]["status"], status_all):
+      return None
+    return t
+
+  t_best = time_table(chosen)
+  if t_best is None or t_best > t_batch_default:
+    chosen = {g: None for g in chosen}
+    t_best = t_batch_default
+  if batch_pass:
+    first = dict(chosen)
+    # A change must beat the current table by 2 %, well above the spread of
+    # repeated means, so that the pass does not chase noise.
+    for g in sorted(default, key=lambda k: -default[k]):
+      for entry in cands_of[g]:
+        if chosen[g] is not None and entry == chosen[g]:
+          continue
+        trial = dict(chosen)
+        trial[g] = entry
+        t = time_table(trial)
+        if t is not None and t < 0.98 * t_best:
+          chosen, t_best = trial, t
+    if chosen != first:
+      # The first-stage table against the new one, longer runs, alternated.
+      t_first = t_new = 0.0
+      for _ in range(2):
+        t_first += time_table(first, 2 * reps) or float("inf")
+        t_new += time_table(chosen, 2 * reps) or float("inf")
+      if t_new >= t_first:
+        chosen, t_best = first, t_first / 2
+      else:
+        t_best = t_new / 2
+  table = []
+  for g in sorted(chosen):
+    e = chosen[g]
+    if e is None:
+      continue
+    key = (e["block_threads"], e["lean"], e["onchip"])
+    entry = dict(e)
+    entry.update({"ms": round(alone[(g, key)], 4), "default_ms": round(default[g], 4),
+                  "batch_ms": round(t_best, 4),
+                  "batch_default_ms": round(t_batch_default, 4)})
+    table.append(entry)
   hb.replan(None)
   return table
 

@@ -330,7 +330,10 @@ enum Phase : int {
   kPhSnTopUpd, kPhSnTopDiag, kPhSnTopPanel,
   // Sub-phases of the dense KKT solve: the column sums A^T (r_y / Ry) and the
   // row products A x around the triangular solves.
-  kPhSolveCols, kPhSolveRows, kNumPhases
+  kPhSolveCols, kPhSolveRows,
+  // Sub-phases of the per-block dense format: the inverse of the factor's
+  // 32 x 32 diagonal blocks and the triangular solves of a KKT solve.
+  kPhInv, kPhTri, kNumPhases
 };
 #ifdef QTQP_PHASE_TIMERS
 extern __device__ unsigned long long g_phase_cycles[kNumPhases];

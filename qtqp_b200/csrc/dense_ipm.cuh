@@ -708,7 +708,23 @@ struct Ipm {
       const int ci = bi8 * 8 + lc, cj = bj8 * 8 + lc;
       const bool ci_ok = ci < n, cj_ok = cj < n;
       double d[2] = {0.0, 0.0};
-      for (int r = 0; r < m; r += 4) {
+      int r = 0;
+      // Four slices per step with their loads issued first (A may come from
+      // L2 when it does not fit on chip); the products accumulate in the
+      // same order as one slice at a time.
+      for (; r + 16 <= m; r += 16) {
+        double a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int rr = r + 4 * u + lr;
+          const double* row = A + rr * lda;
+          a[u] = ci_ok ? row[ci] * iry[rr] : 0.0;
+          b[u] = cj_ok ? row[cj] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) dmma_8x8x4(d, a[u], b[u]);
+      }
+      for (; r < m; r += 4) {
         const int rr = r + lr;
         double a = 0.0, b = 0.0;
         if (rr < m) {
@@ -1008,59 +1024,69 @@ struct Ipm {
     return 0;
   }
 
-  // In-place inverse of each 32x32 lower-triangular diagonal block of L, one
-  // warp per block, lane c computing column c top-down:
-  // X_cc = 1 / L_cc, X_rc = -(sum_{c<=k<r} L_rk X_kc) / L_rr for r > c.
-  // Both Cholesky variants already store 1 / L_jj on the diagonal, which is
-  // also the inverse's diagonal.  Lane c keeps X_kc (k > c) in the block's
-  // unused upper triangle at (c, k), so with the diagonal U_ck = X_kc for
-  // every k >= c; L_rk is the same entry in every lane (a broadcast).  The
-  // loops stay rolled: the batch kernel runs many QPs per SM at different
-  // phases, and its per-iteration code has to stay small for the
-  // instruction cache.  The sums run in the same order (even k into a0, odd
-  // k into a1) as the fully unrolled register form did.  After the warp's
-  // columns are done, the upper triangle is copied into the lower one.
+  // In-place inverse of each 32x32 lower-triangular diagonal block of L,
+  // top-down: X_cc = 1 / L_cc, X_rc = -(sum_{c<=k<r} L_rk X_kc) / L_rr for
+  // r > c.  Both Cholesky variants already store 1 / L_jj on the diagonal,
+  // which is also the inverse's diagonal.  Column c of X keeps X_kc (k > c)
+  // in the block's unused upper triangle at (c, k), so with the diagonal
+  // U_ck = X_kc for every k >= c; L_rk is the same entry for every column (a
+  // broadcast).  A block gets a team of P warps (P = 1, 2 or 4, as many as
+  // the block's warps allow) and each column P neighbouring lanes of one
+  // warp, which split the row's dot product (strided over k, combined by
+  // xor shuffles), so the columns of a warp need no barrier but __syncwarp.
+  // The loops stay rolled: the batch kernel runs several QPs per SM at
+  // different phases of the IPM, and their code competes for the
+  // instruction cache.  After a barrier the columns are copied from the
+  // upper triangles into the lower ones.
   template <typename T>
   QTQP_PHASE void invert_diag_blocks(T* g) {
     QTQP_LOCALS;
+    QTQP_TIC();
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
     const int nblk = (n + 31) >> 5;
-    for (int blk = warp; blk < nblk; blk += NW) {
+    int lanes = 1;  // P, the lanes per column
+    while (lanes < 4 && 2 * lanes * nblk <= NW) lanes <<= 1;
+    const int teams = NW / lanes, team = warp / lanes;
+    const int c = (warp % lanes) * (32 / lanes) + lane / lanes, sub = lane % lanes;
+    for (int blk = team; blk < nblk; blk += teams) {
       const int kb = blk * 32, bs = min(32, n - kb);
       T* L = g + kb * ldg + kb;
-      const int c = lane;
       T* U = L + c * ldg;  // row c: U[k] = X_kc for k >= c
 #pragma unroll 1
       for (int r = 1; r < bs; ++r) {
         const T* Lr = L + r * ldg;
-        T a0 = T(0), a1 = T(0);
-        // Eight entries per step (loads issued ahead of the two FMA chains).
+        T acc = T(0);
+        // Four entries per lane and step, loads issued ahead of the FMAs.
 #pragma unroll 1
-        for (int k = 0; k < r; k += 8) {
-          T lv[8], uv[8];
+        for (int k0 = c + sub; k0 < r; k0 += 4 * lanes) {
+          T lv[4], uv[4];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const bool in = k + u < r && k + u >= c;
-            lv[u] = in ? Lr[k + u] : T(0);
-            uv[u] = in ? U[k + u] : T(0);
+          for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * lanes;
+            lv[u] = k < r ? Lr[k] : T(0);
+            uv[u] = k < r ? U[k] : T(0);
           }
 #pragma unroll
-          for (int u = 0; u < 8; u += 2) {
-            if (k + u < r && k + u >= c) a0 = fma(lv[u], uv[u], a0);
-            if (k + u + 1 < r && k + u + 1 >= c) a1 = fma(lv[u + 1], uv[u + 1], a1);
-          }
+          for (int u = 0; u < 4; ++u) acc = fma(lv[u], uv[u], acc);
         }
-        if (c < r) U[r] = -(a0 + a1) * Lr[r];
+        for (int o = 1; o < lanes; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (sub == 0 && c < r) U[r] = -acc * Lr[r];
+        __syncwarp();
       }
-      __syncwarp();
-      if (c < bs) {
+    }
+    // Every column reads row r of L up to r - 1, including the columns of
+    // the team's other warps, so the copy waits for all of them.
+    sync();
+    for (int blk = team; blk < nblk; blk += teams) {
+      const int kb = blk * 32, bs = min(32, n - kb);
+      T* L = g + kb * ldg + kb;
+      const T* U = L + c * ldg;
 #pragma unroll 1
-        for (int r = c + 1; r < bs; ++r) L[r * ldg + c] = U[r];
-      }
-      __syncwarp();
+      for (int r = c + 1 + sub; r < bs; r += lanes) L[r * ldg + c] = U[r];
     }
     sync();
+    QTQP_TOC(kPhInv);
   }
 
   // Solves L L^T v = v in place with the block-inverted factor: forward
@@ -1159,10 +1185,14 @@ struct Ipm {
       sync();
       QTQP_TOC(kPhSolveCols);
     }
-    if (fp64) {
-      chol_solve<double>(G, tmp, vec(kW));
-    } else {
-      chol_solve<float>(g32(), t32, t32 + n);
+    {
+      QTQP_TIC();
+      if (fp64) {
+        chol_solve<double>(G, tmp, vec(kW));
+      } else {
+        chol_solve<float>(g32(), t32, t32 + n);
+      }
+      QTQP_TOC(kPhTri);
     }
     for (int k = tid; k < n; k += NT) {
       const double val = fp64 ? tmp[k] : double(t32[k]);

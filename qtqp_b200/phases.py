@@ -33,7 +33,7 @@ PHASES = ["load", "normalize", "gram", "chol", "solve", "residual", "tau", "step
           "bp_interior", "bp_chain", "bp_fwd", "bp_chains", "bp_bwd", "cr_stage", "cr_sweep",
           "cr_gemm", "cr_gather", "sn_sub", "sn_top", "sn_fwd_sub", "sn_fwd_top",
           "sn_bwd_top", "sn_bwd_sub", "sn_top_upd", "sn_top_diag", "sn_top_panel",
-          "solve_cols", "solve_rows"]
+          "solve_cols", "solve_rows", "inv", "tri"]
 
 
 def _runner(args):

@@ -27,9 +27,12 @@ def test_tuned_plan_matches_default_plan(tmp_path):
   qps = _qps(600)
   table = autotune.tune_dense_batch(qps, reps=1)
   for e in table:
-    assert e["block_threads"] in (64, 128, 256) and e["lean"] in (0, 1)
+    assert e["block_threads"] in (32, 64, 128, 256) and e["lean"] in (0, 1)
     assert e["onchip"] in (0, 1) and e["n_lo"] <= e["n_hi"]
-    assert e["ms"] <= e["default_ms"]
+    # The whole batch (groups running concurrently) is not slower with the
+    # table than with the default plan, within the spread of repeated
+    # timings; a group alone may be.
+    assert e["batch_ms"] <= 1.05 * e["batch_default_ms"]
   default = qb.solve_batch(qps, tuning=None)
   tuned = qb.solve_batch(qps, tuning=table)
   for q, sd, st in zip(qps, default, tuned):
