@@ -6,10 +6,11 @@ shape: threads per block, the register-capped ("lean") or unrestricted
 kernel, and whether A and P stay in shared memory or are read through L2.
 The default plan chooses by heuristics.  tune_dense_batch times every
 candidate shape on each launch group of a representative batch, on the
-device (CUDA events), in two stages:
+device (CUDA events), in one or two stages:
 
 1. each group launched alone, keeping its fastest shape;
-2. the whole batch, whose groups run concurrently on side streams: one pass
+2. (optional) the whole batch, whose groups run concurrently on side
+   streams, timed as a caller sees it (L2 flushed before each solve): one pass
    of coordinate descent over the groups (largest first) that changes a
    group's shape only when the whole solve gets faster.  A group that is
    fastest alone with large blocks (low latency per QP) can be faster inside
@@ -82,15 +83,17 @@ def _time_batch(torch, db, stream, reps, flush) -> float:
 
 
 def tune_dense_batch(problems, opts: _batch.SolveOptions | None = None, candidates=None,
-                     reps: int = 3, device=None, batch_pass: bool = True) -> list[dict]:
+                     reps: int = 3, device=None, batch_pass: bool = False) -> list[dict]:
   """Times each candidate (block_threads, lean, onchip) on every launch group
   of the default plan of `problems` and returns the tuning table of the
   chosen shapes.  Each entry carries ms and default_ms (the group launched
   alone with the chosen and the default shape) and batch_ms and
   batch_default_ms (the whole batch solve with the table and with the
   default plan).  A candidate that changes any instance's status against the
-  default shape is never chosen.  batch_pass=False keeps the first stage
-  only."""
+  default shape is never chosen.  batch_pass=True adds the second stage (on
+  the 4096 small dense QPs it measured no gain over the first stage alone:
+  160.0k / 157.7k against 160.0k / 157.2k QPs/s in two bench runs each, for
+  12 s more tuning, so it is off by default)."""
   torch = _lib.require_device()
   opts = opts or _batch.SolveOptions()
   dev = torch.device(device or "cuda")

@@ -43,7 +43,12 @@ __device__ __forceinline__ void block_reduce(double (&sums)[NS > 0 ? NS : 1],
                                              double* red, int& phase) {
   static_assert(NS + NM <= kRedMax, "too many reduction slots");
   constexpr int NW = NT / 32;
-#pragma unroll
+  // The loops over shuffle distances and warps stay rolled (the values of
+  // one step unrolled): every reduction of the IPM is inlined at its call
+  // site, and fully unrolled they made up much of the per-iteration code
+  // that competes for the instruction cache.  The order of the operations
+  // is the same either way.
+#pragma unroll 1
   for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
     for (int k = 0; k < NS; ++k) sums[k] += __shfl_xor_sync(0xffffffffu, sums[k], off);
@@ -65,18 +70,17 @@ __device__ __forceinline__ void block_reduce(double (&sums)[NS > 0 ? NS : 1],
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      double acc = 0.0;
+    for (int k = 0; k < NS; ++k) sums[k] = 0.0;
 #pragma unroll
-      for (int w = 0; w < NW; ++w) acc += buf[w * kRedMax + k];
-      sums[k] = acc;
-    }
+    for (int k = 0; k < NM; ++k) maxs[k] = buf[NS + k];
+#pragma unroll 1
+    for (int w = 0; w < NW; ++w) {
 #pragma unroll
-    for (int k = 0; k < NM; ++k) {
-      double acc = buf[NS + k];
+      for (int k = 0; k < NS; ++k) sums[k] += buf[w * kRedMax + k];
+      if (w > 0) {
 #pragma unroll
-      for (int w = 1; w < NW; ++w) acc = nanmax(acc, buf[w * kRedMax + NS + k]);
-      maxs[k] = acc;
+        for (int k = 0; k < NM; ++k) maxs[k] = nanmax(maxs[k], buf[w * kRedMax + NS + k]);
+      }
     }
   }
 }

@@ -376,6 +376,7 @@ struct Ipm {
           acc[a] = t;
         }
       }
+#pragma unroll 1
       for (int off = 16; off >= per_warp; off >>= 1) {
 #pragma unroll
         for (int a = 0; a < NACC; ++a) {

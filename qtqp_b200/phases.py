@@ -4,6 +4,7 @@ Usage (on a machine with a B200):
 
   python -m qtqp_b200.build --phase-timers         # libqtqp_cuda_phase.so
   python -m qtqp_b200.phases batch [--count 4096]  # the 4096 small dense QPs
+  python -m qtqp_b200.phases batch --count 1024 --uniform-n 64  # one size
   python -m qtqp_b200.phases large [--n 4096]      # one dense QP, m = 2n
   python -m qtqp_b200.phases sparse [--grid 40]    # one grid-network flow QP
   python -m qtqp_b200.phases sparse_random [--n 6000]
@@ -42,8 +43,12 @@ def _runner(args):
   from . import batch, large, problems, sparse  # pylint: disable=g-import-not-at-top
   opts = batch.SolveOptions(precision=args.precision)
   if args.workload == "batch":
-    qps = [qb.QTQP(**dict(zip("abczp", problems.small_dense_instance(i))))
-           for i in range(args.count)]
+    if args.uniform_n:
+      qps = [qb.QTQP(**dict(zip("abczp", problems.small_dense_instance_n(args.uniform_n, i))))
+             for i in range(args.count)]
+    else:
+      qps = [qb.QTQP(**dict(zip("abczp", problems.small_dense_instance(i))))
+             for i in range(args.count)]
     hb = batch.HostBatch(qps, opts, pinned=True)
     db = batch.DeviceBatch(hb, records=False)
     db.upload()
@@ -72,6 +77,8 @@ def main(argv=None) -> None:
   ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
   ap.add_argument("workload", choices=["batch", "large", "sparse", "sparse_random", "mpc"])
   ap.add_argument("--count", type=int, default=4096)
+  ap.add_argument("--uniform-n", type=int, default=0,
+                  help="batch: every QP of this n (m = 2n) instead of n ~ U{8..64}")
   ap.add_argument("--n", type=int, default=None)
   ap.add_argument("--grid", type=int, default=40)
   ap.add_argument("--horizon", type=int, default=100)
@@ -105,9 +112,13 @@ def main(argv=None) -> None:
   print(f"{args.workload}: {e0.elapsed_time(e1):.1f} ms (profiling build), "
         f"iterations {int(np.sum(res['iterations']))}, "
         f"refinement solves {int(np.sum(res['ir_solves']))}")
-  for name, v in zip(PHASES, ms):
+  # A batch also reports thousands of SM cycles per QP and IPM iteration.
+  per_it = (cyc / blocks / max(float(np.mean(res["iterations"])), 1.0) / 1e3
+            if args.workload == "batch" else None)
+  for k, (name, v) in enumerate(zip(PHASES, ms)):
     if v > 0.005:
-      print(f"  {name:14s} {v:10.2f} ms")
+      extra = f"  {per_it[k]:8.1f} kcycles per QP-iteration" if per_it is not None else ""
+      print(f"  {name:14s} {v:10.2f} ms{extra}")
 
 
 if __name__ == "__main__":

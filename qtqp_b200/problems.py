@@ -70,6 +70,19 @@ def small_dense_instance(i: int, base: int = 1001):
   return sp.csc_matrix(a_d), b, c, z, sp.csc_matrix(p_d)
 
 
+def small_dense_instance_n(n: int, i: int, base: int = 7):
+  """Like small_dense_instance, with n fixed (m = 2n, z = n // 4): batches of
+  one size, for per-size timing of the batch kernel."""
+  rng = np.random.default_rng([base, n, i])
+  m, z = 2 * n, n // 4
+  a_d = rng.normal(size=(m, n))
+  l = rng.normal(size=(n, n // 2))
+  p_d = l @ l.T + 1e-3 * np.eye(n)
+  p_d = 0.5 * (p_d + p_d.T)
+  b, c = _feasible_pair(rng, a_d, p_d, z)
+  return sp.csc_matrix(a_d), b, c, z, sp.csc_matrix(p_d)
+
+
 def small_dense_size(i: int, base: int = 1001) -> tuple[int, int]:
   """(n, m) of small_dense_instance(i) without building it (the same first
   draw of the same generator)."""

@@ -61,3 +61,16 @@ def test_every_candidate_shape_solves_the_same():
     db.launch()
     got = db.fetch()[0]["status"]
     np.testing.assert_array_equal(got, ref)
+
+
+def test_batch_pass_keeps_statuses():
+  """The optional pass over the whole concurrent batch returns a table that
+  solves every instance with the default plan's status."""
+  qps = _qps(300)
+  table = autotune.tune_dense_batch(qps, reps=1, batch_pass=True)
+  for e in table:
+    assert e["block_threads"] in (32, 64, 128, 256)
+    assert e["batch_ms"] > 0.0 and e["batch_default_ms"] > 0.0
+  default = qb.solve_batch(qps, tuning=None)
+  tuned = qb.solve_batch(qps, tuning=table)
+  assert [s.status for s in default] == [s.status for s in tuned]
