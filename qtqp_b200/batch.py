@@ -584,9 +584,11 @@ QTQP_COPY_STREAM = 8  # the side stream after the 8 launch groups' ones: read-ba
 
 
 def _side_streams(torch, device, count: int):
-  """`count` reusable side streams of `device` (created once per device)."""
+  """`count` reusable side streams of `device` (created once per device).
+  Stream 0 (launch group 0, the costliest instances) has a high priority, as
+  the library's own side streams do."""
   key = str(device)
   have = _SIDE_STREAMS.setdefault(key, [])
   while len(have) < count:
-    have.append(torch.cuda.Stream(device=device))
+    have.append(torch.cuda.Stream(device=device, priority=-1 if not have else 0))
   return have[:count]
