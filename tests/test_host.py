@@ -376,3 +376,17 @@ def test_storage_routing_of_sparse_problems():
   assert q.storage_format(single=True) == "large"
   a, b, c, z, p = problems.mpc_feasible(30)
   assert qb.QTQP(a=a, b=b, c=c, z=z, p=p).storage_format(single=True) == "band_grid"
+
+
+def test_one_size_instances_are_dense_csc_and_solvable():
+  """problems.small_dense_instance_n (the per-size batches of the phase
+  reporter): m = 2n, z = n // 4, every entry of A and P stored in CSC order
+  (so a batch packs them in place), and the oracle solves them."""
+  for n in (8, 13):
+    a, b, c, z, p = problems.small_dense_instance_n(n, 0)
+    assert a.shape == (2 * n, n) and p.shape == (n, n) and z == n // 4
+    assert a.format == "csc" and a.nnz == 2 * n * n and p.nnz == n * n
+    again = problems.small_dense_instance_n(n, 0)
+    np.testing.assert_array_equal(again[0].toarray(), a.toarray())
+    r = orc.solve(a.toarray(), b, c, z, p.toarray())
+    assert r.status == "solved"
